@@ -1,0 +1,370 @@
+"""Benchmark: DG right-hand side + LSRK4 on the 3D Maxwell cavity workload.
+
+Workload (one GPU): [-1,1]^3 split into 20^3 cubes x 6 tetrahedra
+(K = 48000), interior vertices jittered +-0.05h (seed 1), order N = 4
+(Np = 35, Nfp = 15), Maxwell with eps = mu = 1, upwind flux, PEC walls;
+initial condition the (1,1,1) cavity mode plus 1e-3 uniform noise (seed 2).
+A "step" is one LSRK4 time step = 5 fused RHS+stage launches.
+
+  value  = DOF-updates/s with the state resident in HBM
+           (DOF-update = one nodal value of one field through one RK stage)
+  e2e    = the same metric through the public API with the state in pinned
+           host memory: every step copies the state in, runs the step and
+           copies the new state out (host<->device copies timed)
+
+The three buffers of a stage (q_in, q_out, res: 3 x 80.6 MB in FP64) exceed
+the 126 MB L2, so no flush is needed between iterations.
+
+``--impl reference`` times the CPU oracle (a restatement of the reference jit
+backend, which itself cannot be built in this image) on the host cores; each
+of its steps is a bounded sample: one RK stage over the whole mesh.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CAVITY_MODE = (1, 1, 1)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "bf16x3"])
+    p.add_argument("--n", type=int, default=20, help="cubes per axis")
+    p.add_argument("--order", type=int, default=4)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def build_problem(n, order, precision, device=None):
+    import hedge_b200 as hb
+    h = 2.0 / n
+    mesh = hb.make_box_tet_mesh(n=(n, n, n), jitter=0.05 * h, seed=1)
+    discr = hb.Discretization(mesh, order=order, precision=precision, device=device)
+    op = hb.MaxwellOperator(1.0, 1.0, flux_type=1)
+    return hb, mesh, discr, op
+
+
+def cavity_ic(discr):
+    """(1,1,1) mode of the cavity [-1,1]^3 (reference
+    examples/maxwell/analytic_solutions.py:240-300, dimensions (2,2,2),
+    coordinates shifted by +1), real part at t=0, plus noise."""
+    x, y, z = (discr.nodes + 1.0).T
+    f, g, h = [np.pi * m / 2.0 for m in CAVITY_MODE]
+    k2 = f * f + g * g
+    # zdep_add = 2 cos(hz), zdep_sub = 2i sin(hz), C = i/(f^2+g^2)
+    ex = -(1.0 / k2) * f * h * np.cos(f * x) * np.sin(g * y) * 2 * np.sin(h * z)
+    ey = -(1.0 / k2) * g * h * np.sin(f * x) * np.cos(g * y) * 2 * np.sin(h * z)
+    ez = np.sin(f * x) * np.sin(g * y) * 2 * np.cos(h * z)
+    w = np.stack([ex, ey, ez, np.zeros_like(x), np.zeros_like(x), np.zeros_like(x)])
+    rng = np.random.default_rng(2)
+    return w + 1e-3 * rng.uniform(-1, 1, w.shape)
+
+
+def algorithmic_bytes_per_dof_update(discr, state_bytes):
+    """read q, read res, write q, write res per DOF-update, plus per-element
+    geometry (d^2 metric + Nf (normal, Fscale)) and connectivity (Nf x
+    (u32 neighbour, u8 face, u8 perm)) spread over Np*F DOF-updates."""
+    d, nf = discr.dimensions, discr.Nfaces
+    g_el = 8 * (d * d + nf * (d + 1)) + nf * 6
+    return 4 * state_bytes + g_el / (discr.Np * 6)
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            parts = [p.strip() for p in l.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    import torch
+    import torch.distributed as dist
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def max_over_ranks(x, world):
+    import torch
+    import torch.distributed as dist
+    if world == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    import torch
+    import torch.distributed as dist
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def load_traffic(kernel_key):
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(kernel_key)
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_baseline(discr, op, w0, dt, threads=None):
+    """Oracle (CPU port of the jit backend) on a bounded sample: one LSRK
+    stage over the whole mesh, all host threads."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc_mod
+    ncores = os.cpu_count() or 1
+    used = orc_mod.set_threads(threads or ncores)
+    orc = orc_mod.OracleRHS(discr, op.op_template())
+    res = np.zeros_like(w0)
+    r = orc(w0)                     # warm-up
+    t0 = time.perf_counter()
+    r = orc(w0)
+    res = 0.0 * res + dt * r
+    y = w0 + 0.149 * res
+    el = time.perf_counter() - t0
+    dofs = discr.K * discr.Np * 6
+    return {"value": dofs / el, "unit": "DOF-updates/s", "cores": used,
+            "kind": "port",
+            "sample": "one LSRK stage (RHS + update) over the full K=%d mesh, "
+                      "%d OpenMP threads, C++ oracle -O3" % (discr.K, used)}, el
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    hb, mesh, discr, op = build_problem(args.n, args.order, "fp64")
+    w0 = cavity_ic(discr)
+    dt = op.estimate_timestep(discr)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc_mod
+    ncores = os.cpu_count() or 1
+    used = orc_mod.set_threads(ncores)
+    orc = orc_mod.OracleRHS(discr, op.op_template())
+    from hedge_b200.timestep import RK4A, RK4B
+    y, res = w0.copy(), np.zeros_like(w0)
+    for s in range(args.warmup):
+        r = orc(y)
+        res = RK4A[s % 5] * res + dt * r
+        y = y + RK4B[s % 5] * res
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        r = orc(y)
+        res = RK4A[s % 5] * res + dt * r
+        y = y + RK4B[s % 5] * res
+    el = time.perf_counter() - t0
+    dofs = discr.K * discr.Np * 6 * args.steps
+    v = dofs / el
+    line = {
+        "impl": "reference", "metric": "DG RHS DOF-updates/s (3D Maxwell N=4, LSRK4)",
+        "value": v, "unit": "DOF-updates/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "maxwell3d_cavity_K48000_N4", "K": discr.K,
+                   "order": args.order, "fields": 6, "step": "one LSRK stage per step"},
+        "cpu_baseline": {"value": v, "unit": "DOF-updates/s", "cores": used,
+                         "kind": "port",
+                         "sample": "one LSRK stage over the full mesh per step; C++ "
+                                   "oracle (restated jit loops), OpenMP"},
+        "e2e": {"value": v, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    hb, mesh, discr, op = build_problem(args.n, args.order, args.precision, device=dev)
+    w0 = cavity_ic(discr)
+    dt = op.estimate_timestep(discr)
+    rhs = op.bind(discr)
+    comp = rhs.compiled
+    stepper = hb.LSRK4TimeStepper()
+    y = discr.to_device(w0).reshape(6, -1)
+    # warm-up
+    t = 0.0
+    for _ in range(args.warmup):
+        y = stepper(y, t, dt, rhs)
+        t += dt
+    comp.check()
+    barrier(world)
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clk:
+        barrier(world)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            y = stepper(y, t, dt, rhs)
+            t += dt
+        ev1.record(stream)
+        barrier(world)
+    ms = ev0.elapsed_time(ev1)
+    comp.check()
+    ms_max = max_over_ranks(ms, world)
+    dofs_rank = discr.K * discr.Np * 6 * 5 * args.steps
+    value = dofs_rank * world / (ms_max * 1e-3)
+    launches = 5 * args.steps
+    launch_ms = ms / launches
+    state_bytes = 8 if args.precision != "fp32" else 4
+    bpd = algorithmic_bytes_per_dof_update(discr, state_bytes)
+    bytes_per_launch = bpd * discr.K * discr.Np * 6
+    achieved = bytes_per_launch / (launch_ms * 1e-3) / 1e9
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except (OSError, ValueError):
+        pass
+    peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    kernel_key = "rhs_stage_%s_maxwell3d_N%d" % (args.precision, args.order)
+    traffic = load_traffic(kernel_key)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                "algorithmic_bytes_per_dof_update": bpd,
+                "kernel": kernel_key}
+
+    # ---- end to end through the public API with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        host_in = torch.from_numpy(np.ascontiguousarray(w0)).pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        e2e_steps = max(1, min(args.steps, 10))
+        for _ in range(2):
+            yd = host_in.to(dev, non_blocking=True)
+            yd = stepper(yd, 0.0, dt, rhs)
+            host_out.copy_(yd, non_blocking=True)
+        barrier(world)
+        ev0.record(stream)
+        for _ in range(e2e_steps):
+            yd = host_in.to(dev, non_blocking=True)
+            yd = stepper(yd, 0.0, dt, rhs)
+            host_out.copy_(yd, non_blocking=True)
+        ev1.record(stream)
+        barrier(world)
+        e_ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+        nbytes = host_in.numel() * host_in.element_size()
+        e2e = {"value": discr.K * discr.Np * 6 * 5 * e2e_steps * world / (e_ms * 1e-3),
+               "unit": "DOF-updates/s", "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "steps": e2e_steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu, _ = cpu_baseline(discr, op, w0, dt)
+        except Exception as exc:   # the baseline must not sink the GPU line
+            cpu = {"value": None, "error": str(exc)}
+
+    if rank == 0:
+        line = {
+            "metric": "DG RHS DOF-updates/s (3D Maxwell N=4, LSRK4)",
+            "value": value, "unit": "DOF-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"fp64": "f64", "fp32": "f32", "bf16x3": "bf16x3+f32acc, f64 state"}[
+                args.precision],
+            "data": "synthetic",
+            "config": {"workload": "maxwell3d_cavity_K48000_N4", "K": discr.K,
+                       "order": args.order, "Np": discr.Np, "fields": 6,
+                       "precision": args.precision, "stepper": "LSRK4 (5 fused stages)",
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "working set 3 x %.1f MB > 126 MB L2, no flush" %
+                             (discr.K * discr.Np * 6 * state_bytes / 1e6)},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

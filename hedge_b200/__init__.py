@@ -1,0 +1,24 @@
+"""hedge_b200: a B200-native (sm_100a) backend for hedge's DG right-hand side.
+
+Host set-up (reference element, mesh, connectivity) is FP64 numpy; every
+right-hand-side evaluation and LSRK stage runs in hand-written CUDA kernels
+(libhedge_b200.so) behind a C ABI (include/hedge_b200.h).
+"""
+
+from .mesh import (Mesh, TAG_ALL, TAG_NONE, make_regular_rect_mesh,
+                   make_box_tet_mesh, check_bc_coverage)
+from .refelem import TriangleElement, TetrahedronElement, make_element
+from .models import (StrongAdvectionOperator, StrongWaveOperator,
+                     VariableVelocityStrongWaveOperator, MaxwellOperator,
+                     make_tdep_constant, TimeConstantGivenFunction)
+from .discretization import Discretization, CompiledOperator, BoundRHS
+from .timestep import LSRK4TimeStepper, RK4TimeStepper
+
+__all__ = [
+    "Mesh", "TAG_ALL", "TAG_NONE", "make_regular_rect_mesh", "make_box_tet_mesh",
+    "check_bc_coverage", "TriangleElement", "TetrahedronElement", "make_element",
+    "StrongAdvectionOperator", "StrongWaveOperator",
+    "VariableVelocityStrongWaveOperator", "MaxwellOperator", "make_tdep_constant",
+    "TimeConstantGivenFunction", "Discretization", "CompiledOperator", "BoundRHS",
+    "LSRK4TimeStepper", "RK4TimeStepper",
+]

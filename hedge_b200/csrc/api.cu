@@ -1,0 +1,308 @@
+// C-ABI entry points of libhedge_b200 (declared in include/hedge_b200.h).
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace hb {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+hb_status fail(hb_status st, const std::string& msg) {
+  set_error(msg);
+  return st;
+}
+
+hb_status cuda_fail(cudaError_t err, const char* what) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(err));
+  return HB_ERR_CUDA;
+}
+
+// Makes `dev` current for the scope of one C-ABI call and restores the
+// caller's device afterwards.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = false;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) return;
+    ok = prev == dev || cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    int cur;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+template <typename T>
+static hb_status upload(T** dst, const T* src, size_t n) {
+  HB_CUDA(cudaMalloc(reinterpret_cast<void**>(dst), sizeof(T) * (n ? n : 1)));
+  if (n) HB_CUDA(cudaMemcpy(*dst, src, sizeof(T) * n, cudaMemcpyHostToDevice));
+  return HB_OK;
+}
+
+static void free_discr(Discr* d) {
+  if (!d) return;
+  cudaFree(d->dmats_t); cudaFree(d->lift_t); cudaFree(d->geo);
+  cudaFree(d->dmats_t32); cudaFree(d->lift_t32); cudaFree(d->geo32);
+  cudaFree(d->fmask); cudaFree(d->shuffle);
+  delete d;
+}
+
+hb_status ensure_fp32(Discr* d) {
+  if (d->geo32) return HB_OK;
+  const double* host = reinterpret_cast<const double*>(d->host_blob.data());
+  const size_t nd = (size_t)d->dim * d->np * d->np;
+  const size_t nl = (size_t)d->nfaces * d->nfp * d->np;
+  const size_t ng = (size_t)d->K * d->G;
+  std::vector<float> tmp(nd + nl + ng);
+  for (size_t x = 0; x < nd + nl + ng; ++x) tmp[x] = (float)host[x];
+  hb_status st;
+  if ((st = upload(&d->dmats_t32, tmp.data(), nd))) return st;
+  if ((st = upload(&d->lift_t32, tmp.data() + nd, nl))) return st;
+  if ((st = upload(&d->geo32, tmp.data() + nd + nl, ng))) return st;
+  return HB_OK;
+}
+
+hb_status check_device_flag(Op* op, cudaStream_t s) {
+  int flag = 0;
+  HB_CUDA(cudaMemcpyAsync(&flag, op->err_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  HB_CUDA(cudaStreamSynchronize(s));
+  if (flag != DEV_OK) {
+    static const char* what[] = {"ok", "face neighbour out of range",
+                                 "invalid neighbour face / permutation code",
+                                 "boundary index out of range", "missing input vector"};
+    return fail(HB_ERR_DEVICE_FLAG,
+                std::string("device check failed: ") + (flag < 5 ? what[flag] : "unknown"));
+  }
+  return HB_OK;
+}
+
+hb_status launch_gather_map(Op* op, int64_t* int_idx, int64_t* ext_idx, cudaStream_t s);
+hb_status launch_lincomb(int64_t n, int dtype, double a, const void* x, double b,
+                         const void* y, void* out, cudaStream_t s);
+hb_status prepare_split(Op* op);
+hb_status launch_split(Op* op, int mode, double ra, double rb, double dt,
+                       const void* q_in, void* q_out, void* res, const double* coeff,
+                       const double* bdry, const double* source, cudaStream_t s);
+void free_split(Op* op);
+
+}  // namespace hb
+
+using namespace hb;
+
+extern "C" {
+
+const char* hb_last_error_string(void) { return g_last_error.c_str(); }
+
+hb_status hb_discr_create(const hb_discr_desc* desc, hb_discr** out) {
+  if (!desc || !out) return fail(HB_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  if (desc->dim != 2 && desc->dim != 3)
+    return fail(HB_ERR_UNSUPPORTED, "dim must be 2 or 3");
+  if (desc->nfaces != desc->dim + 1 || desc->np < 1 || desc->nfp < 1 ||
+      desc->num_elements < 1 || desc->nperm < 1 || desc->nperm > 6)
+    return fail(HB_ERR_INVALID_ARGUMENT, "inconsistent element sizes");
+  if (!desc->dmats || !desc->lift || !desc->geometry || !desc->fmask || !desc->shuffle)
+    return fail(HB_ERR_INVALID_ARGUMENT, "null operator or geometry pointer");
+  const int np = desc->np, nfp = desc->nfp, nf = desc->nfaces, dim = desc->dim;
+  for (int x = 0; x < nf * nfp; ++x)
+    if (desc->fmask[x] < 0 || desc->fmask[x] >= np)
+      return fail(HB_ERR_INVALID_ARGUMENT, "fmask entry out of range");
+  for (int x = 0; x < desc->nperm * nfp; ++x)
+    if (desc->shuffle[x] < 0 || desc->shuffle[x] >= nfp)
+      return fail(HB_ERR_INVALID_ARGUMENT, "shuffle entry out of range");
+  DeviceGuard g(desc->device);
+  if (!g.ok) return fail(HB_ERR_CUDA, "cannot select the CUDA device");
+  Discr* d = new (std::nothrow) Discr();
+  if (!d) return fail(HB_ERR_INVALID_ARGUMENT, "out of host memory");
+  d->device = desc->device;
+  d->dim = dim; d->order = desc->order; d->np = np; d->nfp = nfp; d->nfaces = nf;
+  d->nperm = desc->nperm; d->K = desc->num_elements;
+  d->G = dim * dim + nf * (dim + 1);
+  const size_t nd = (size_t)dim * np * np, nl = (size_t)nf * nfp * np;
+  const size_t ng = (size_t)d->K * d->G;
+  // transposed operators + geometry, kept on the host for other precisions
+  d->host_blob.resize(sizeof(double) * (nd + nl + ng));
+  double* h = reinterpret_cast<double*>(&d->host_blob[0]);
+  for (int r = 0; r < dim; ++r)
+    for (int i = 0; i < np; ++i)
+      for (int j = 0; j < np; ++j)
+        h[((size_t)r * np + j) * np + i] = desc->dmats[((size_t)r * np + i) * np + j];
+  for (int i = 0; i < np; ++i)
+    for (int k = 0; k < nf * nfp; ++k)
+      h[nd + (size_t)k * np + i] = desc->lift[(size_t)i * nf * nfp + k];
+  std::memcpy(h + nd + nl, desc->geometry, sizeof(double) * ng);
+  hb_status st;
+  if ((st = upload(&d->dmats_t, h, nd)) || (st = upload(&d->lift_t, h + nd, nl)) ||
+      (st = upload(&d->geo, h + nd + nl, ng)) ||
+      (st = upload(&d->fmask, desc->fmask, (size_t)nf * nfp)) ||
+      (st = upload(&d->shuffle, desc->shuffle, (size_t)desc->nperm * nfp))) {
+    free_discr(d);
+    return st;
+  }
+  *out = reinterpret_cast<hb_discr*>(d);
+  return HB_OK;
+}
+
+hb_status hb_discr_destroy(hb_discr* discr) {
+  if (!discr) return HB_OK;
+  Discr* d = reinterpret_cast<Discr*>(discr);
+  DeviceGuard g(d->device);
+  free_discr(d);
+  return HB_OK;
+}
+
+hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
+  if (!discr || !desc || !out) return fail(HB_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  Discr* d = reinterpret_cast<Discr*>(discr);
+  const int model = desc->model;
+  int F;
+  switch (model) {
+    case HB_MODEL_ADVECTION: F = 1; break;
+    case HB_MODEL_WAVE: case HB_MODEL_VARWAVE: F = d->dim + 1; break;
+    case HB_MODEL_MAXWELL:
+      if (d->dim != 3) return fail(HB_ERR_UNSUPPORTED, "Maxwell needs a 3D mesh");
+      F = 6; break;
+    default: return fail(HB_ERR_INVALID_ARGUMENT, "unknown model id");
+  }
+  if (desc->num_fields != F)
+    return fail(HB_ERR_INVALID_ARGUMENT, "num_fields does not match the model");
+  if (desc->precision < HB_PREC_FP64 || desc->precision > HB_PREC_BF16X3)
+    return fail(HB_ERR_INVALID_ARGUMENT, "unknown precision");
+  if (!desc->conn) return fail(HB_ERR_INVALID_ARGUMENT, "null connectivity");
+  if (model == HB_MODEL_MAXWELL && !(desc->eps > 0 && desc->mu > 0))
+    return fail(HB_ERR_INVALID_ARGUMENT, "Maxwell material must be positive");
+  // host validation of the face table (the kernels also flag bad entries)
+  const int64_t nfc = d->K * d->nfaces;
+  int64_t max_given = 0;
+  for (int64_t x = 0; x < nfc; ++x) {
+    const int nbr = desc->conn[2 * x], code = desc->conn[2 * x + 1];
+    if (nbr >= 0) {
+      if (nbr >= d->K || (code & 3) >= d->nfaces || (code >> 2) >= d->nperm || code < 0)
+        return fail(HB_ERR_INVALID_ARGUMENT, "connectivity entry out of range");
+    } else {
+      if (code < HB_BC_NONE || code > HB_BC_ABSORB)
+        return fail(HB_ERR_INVALID_ARGUMENT, "unknown boundary-condition kind");
+      if (code == HB_BC_GIVEN)
+        max_given = std::max<int64_t>(max_given, ((int64_t)(-1 - nbr) + 1) * d->nfp);
+    }
+  }
+  if (max_given > desc->num_given_bdry_nodes)
+    return fail(HB_ERR_INVALID_ARGUMENT, "given-BC face beyond num_given_bdry_nodes");
+  DeviceGuard g(d->device);
+  if (!g.ok) return fail(HB_ERR_CUDA, "cannot select the CUDA device");
+  Op* op = new (std::nothrow) Op();
+  if (!op) return fail(HB_ERR_INVALID_ARGUMENT, "out of host memory");
+  op->d = d;
+  op->model = model;
+  op->F = F;
+  op->precision = desc->precision;
+  op->n_given = desc->num_given_bdry_nodes;
+  ModelParams& mp = op->mp;
+  for (int k = 0; k < 3; ++k) mp.v[k] = desc->v[k];
+  mp.c = desc->c; mp.eps = desc->eps; mp.mu = desc->mu;
+  mp.alpha = desc->alpha; mp.bdry_alpha = desc->bdry_alpha;
+  mp.time_sign = desc->time_sign;
+  mp.flux_type = desc->flux_type; mp.bdry_flux_type = desc->bdry_flux_type;
+  hb_status st;
+  auto bail = [&](hb_status s) {
+    cudaFree(op->conn); cudaFree(op->err_flag);
+    free_split(op);
+    delete op;
+    return s;
+  };
+  if ((st = upload(&op->conn, reinterpret_cast<const int2*>(desc->conn), (size_t)nfc)))
+    return bail(st);
+  if (cudaMalloc(&op->err_flag, sizeof(int)) != cudaSuccess ||
+      cudaMemset(op->err_flag, 0, sizeof(int)) != cudaSuccess)
+    return bail(fail(HB_ERR_CUDA, "cannot allocate the device error flag"));
+  if (op->precision == HB_PREC_FP32 && (st = ensure_fp32(d))) return bail(st);
+  if (op->precision == HB_PREC_BF16X3)
+    st = prepare_split(op);
+  else
+    st = prepare_simt(op);
+  if (st) return bail(st);
+  *out = reinterpret_cast<hb_op*>(op);
+  return HB_OK;
+}
+
+hb_status hb_op_destroy(hb_op* handle) {
+  if (!handle) return HB_OK;
+  Op* op = reinterpret_cast<Op*>(handle);
+  DeviceGuard g(op->d->device);
+  cudaFree(op->conn);
+  cudaFree(op->err_flag);
+  free_split(op);
+  delete op;
+  return HB_OK;
+}
+
+static hb_status check_inputs(Op* op, const void* q_in, const void* q_out,
+                              const double* coeff) {
+  if (!q_in || !q_out) return fail(HB_ERR_INVALID_ARGUMENT, "null state pointer");
+  if (q_in == q_out) return fail(HB_ERR_INVALID_ARGUMENT, "output aliases the input state");
+  if (op->model == HB_MODEL_VARWAVE && !coeff)
+    return fail(HB_ERR_INVALID_ARGUMENT, "variable-velocity wave needs the c field");
+  return HB_OK;
+}
+
+static hb_status run(Op* op, int mode, double a, double b, double dt, const void* q_in,
+                     void* q_out, void* res, const double* coeff, const double* bdry,
+                     const double* source, void* stream) {
+  DeviceGuard g(op->d->device);
+  if (!g.ok) return fail(HB_ERR_CUDA, "cannot select the CUDA device");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (op->precision == HB_PREC_BF16X3)
+    return launch_split(op, mode, a, b, dt, q_in, q_out, res, coeff, bdry, source, s);
+  return launch_simt(op, mode, a, b, dt, q_in, q_out, res, coeff, bdry, source, s);
+}
+
+hb_status hb_rhs(hb_op* handle, const void* q, void* rhs, const double* coeff,
+                 const double* bdry, const double* source, void* stream) {
+  if (!handle) return fail(HB_ERR_INVALID_ARGUMENT, "null operator");
+  Op* op = reinterpret_cast<Op*>(handle);
+  hb_status st = check_inputs(op, q, rhs, coeff);
+  if (st) return st;
+  return run(op, 0, 0, 0, 0, q, rhs, nullptr, coeff, bdry, source, stream);
+}
+
+hb_status hb_lsrk_stage(hb_op* handle, double a, double b, double dt, const void* q_in,
+                        void* q_out, void* res, const double* coeff, const double* bdry,
+                        const double* source, void* stream) {
+  if (!handle) return fail(HB_ERR_INVALID_ARGUMENT, "null operator");
+  Op* op = reinterpret_cast<Op*>(handle);
+  hb_status st = check_inputs(op, q_in, q_out, coeff);
+  if (st) return st;
+  if (!res) return fail(HB_ERR_INVALID_ARGUMENT, "null residual pointer");
+  return run(op, 1, a, b, dt, q_in, q_out, res, coeff, bdry, source, stream);
+}
+
+hb_status hb_lincomb(int64_t n, int32_t dtype, double a, const void* x, double b,
+                     const void* y, void* out, void* stream) {
+  if (n < 0 || (dtype != 0 && dtype != 1))
+    return fail(HB_ERR_INVALID_ARGUMENT, "bad size or dtype");
+  if (n > 0 && (!x || !y || !out)) return fail(HB_ERR_INVALID_ARGUMENT, "null vector");
+  return launch_lincomb(n, dtype, a, x, b, y, out, reinterpret_cast<cudaStream_t>(stream));
+}
+
+hb_status hb_gather_map(hb_op* handle, int64_t* int_idx, int64_t* ext_idx, void* stream) {
+  if (!handle || !int_idx || !ext_idx) return fail(HB_ERR_INVALID_ARGUMENT, "null argument");
+  Op* op = reinterpret_cast<Op*>(handle);
+  DeviceGuard g(op->d->device);
+  return launch_gather_map(op, int_idx, ext_idx, reinterpret_cast<cudaStream_t>(stream));
+}
+
+hb_status hb_op_check(hb_op* handle, void* stream) {
+  if (!handle) return fail(HB_ERR_INVALID_ARGUMENT, "null operator");
+  Op* op = reinterpret_cast<Op*>(handle);
+  DeviceGuard g(op->d->device);
+  return check_device_flag(op, reinterpret_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

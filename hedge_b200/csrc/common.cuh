@@ -1,0 +1,83 @@
+// Shared declarations of the hedge_b200 CUDA library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+
+#include "../../include/hedge_b200.h"
+
+namespace hb {
+
+// Per-thread last-error text (hb_last_error_string).
+void set_error(const std::string& msg);
+hb_status fail(hb_status st, const std::string& msg);
+hb_status cuda_fail(cudaError_t err, const char* what);
+
+#define HB_CUDA(call)                                              \
+  do {                                                             \
+    cudaError_t err__ = (call);                                    \
+    if (err__ != cudaSuccess) return ::hb::cuda_fail(err__, #call); \
+  } while (0)
+
+// Model parameters passed by value to every kernel.
+struct ModelParams {
+  double v[3];
+  double c, eps, mu, alpha, bdry_alpha, time_sign;
+  int flux_type, bdry_flux_type;
+};
+
+// Device error-flag codes (first error wins).
+enum : int {
+  DEV_OK = 0,
+  DEV_BAD_NEIGHBOUR = 1,
+  DEV_BAD_CODE = 2,
+  DEV_BAD_BDRY_INDEX = 3,
+  DEV_MISSING_INPUT = 4
+};
+
+// Operator data uploaded once per discretization.
+struct Discr {
+  int device;
+  int dim, order, np, nfp, nfaces, nperm, G;
+  int64_t K;
+  // FP64 copies (device)
+  double* dmats_t = nullptr;   // [dim][np(j)][np(i)] transposed
+  double* lift_t = nullptr;    // [nfaces*nfp(k)][np(i)] transposed
+  double* geo = nullptr;       // [K][G]
+  // FP32 copies (device), made on first FP32 operator
+  float* dmats_t32 = nullptr;
+  float* lift_t32 = nullptr;
+  float* geo32 = nullptr;
+  int* fmask = nullptr;        // [nfaces][nfp]
+  int* shuffle = nullptr;      // [nperm][nfp]
+  // host copies kept for split-operator construction
+  std::string host_blob;
+};
+
+struct Op {
+  Discr* d;
+  int model, F, precision;
+  ModelParams mp;
+  int2* conn = nullptr;        // [K][nfaces] (nbr, code)
+  int64_t n_given;
+  int* err_flag = nullptr;     // device int
+  // launch configuration chosen at create time
+  int elems_per_block = 0;
+  int threads = 0;
+  size_t smem = 0;
+  int grid = 0;
+  // split-precision operator planes (BF16X3)
+  void* split_ops = nullptr;
+};
+
+hb_status check_device_flag(Op* op, cudaStream_t s);
+
+// kernel launchers (rhs_simt.cu)
+hb_status launch_simt(Op* op, int mode, double a, double b, double dt,
+                      const void* q_in, void* q_out, void* res,
+                      const double* coeff, const double* bdry,
+                      const double* source, cudaStream_t s);
+hb_status prepare_simt(Op* op);
+
+}  // namespace hb

@@ -1,0 +1,494 @@
+"""The B200 discretization backend: set-up on the host, RHS on the device.
+
+Mirrors the reference's discretization plug-in surface
+(hedge/discretization/__init__.py:217-1302): ``Discretization(mesh, order=)``,
+``.nodes``, ``.volume_zeros``, ``.interpolate_volume_function``,
+``.get_boundary``, ``.norm``, ``.integral``, ``.get_point_evaluator``,
+``.dt_*_factor`` and ``.compile(op_template)``.  Volume vectors are torch
+CUDA tensors in the reference layout ([K*Np], element-major; F fields are
+stacked as [F, K*Np]).  ``compile`` uploads the operator once and returns a
+callable that evaluates the right-hand side through the C ABI
+(libhedge_b200.so); there is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from functools import cached_property
+
+import numpy as np
+
+from . import _native
+from .facegroups import Boundary, build_compact_connectivity, build_interior_face_group
+from .mesh import Mesh, TAG_ALL, TAG_NONE, check_bc_coverage
+from .models import (BC_GIVEN, BC_NONE, MODEL_MAXWELL, MODEL_VARWAVE, MODEL_WAVE,
+                     MODEL_ADVECTION, OpTemplate)
+from .refelem import make_element
+
+PRECISIONS = {"plain": None, "fp64": _native.PREC_FP64, "fp32": _native.PREC_FP32,
+              "bf16x3": _native.PREC_BF16X3}
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class Discretization:
+    """Nodal DG discretization of a conformal simplicial mesh.
+
+    precision: "plain" (the state dtype is ``default_scalar_type``, FP64 or
+    FP32, and so is the arithmetic), "fp32", "fp64", or "bf16x3" (FP64 state,
+    differentiation and lift as split-BF16 tensor-core products with FP32
+    accumulation).
+    """
+
+    def __init__(self, mesh: Mesh, order=None, local_discretization=None,
+                 default_scalar_type=np.float64, precision="plain", debug=(),
+                 device=None, quad_min_degrees=None):
+        if not isinstance(mesh, Mesh):
+            raise TypeError("mesh must be of type hedge_b200.mesh.Mesh")
+        if (order is None) == (local_discretization is None):
+            raise ValueError("must supply exactly one of local_discretization and order")
+        if quad_min_degrees:
+            raise NotImplementedError("quadrature (over-integration) is not on this path")
+        self.mesh = mesh
+        self.ldis = local_discretization or make_element(mesh.dimensions, order)
+        self.dimensions = mesh.dimensions
+        self.order = self.ldis.order
+        self.debug = set(debug)
+        self.default_scalar_type = np.dtype(default_scalar_type).type
+        if precision not in PRECISIONS:
+            raise ValueError("unknown precision %r" % precision)
+        if precision == "plain":
+            precision = "fp64" if self.default_scalar_type == np.float64 else "fp32"
+        if self.default_scalar_type not in (np.float64, np.float32):
+            raise ValueError("default_scalar_type must be float64 or float32")
+        self.precision = precision
+        self._device = device
+        self._handle = None
+
+        ld = self.ldis
+        self.K = len(mesh.elements)
+        self.Np = ld.node_count()
+        self.Nfp = ld.face_node_count()
+        self.Nfaces = ld.face_count()
+        un = ld.unit_nodes
+        # nodes[el*Np + i] = A_el r_i + b_el  (wrap_base.cpp:82-90)
+        self.nodes = np.ascontiguousarray(
+            (np.einsum("kxr,nr->knx", mesh.map_a, un) + mesh.map_b[:, None, :])
+            .reshape(-1, self.dimensions))
+        self.fmask = ld.fmask
+        self.nbr, self.nbr_code = build_compact_connectivity(mesh, ld)
+        d, nf = self.dimensions, self.Nfaces
+        geo = np.empty((self.K, d * d + nf * (d + 1)))
+        geo[:, :d * d] = mesh.inv_map_a.reshape(self.K, d * d)
+        fs = mesh.face_jacobians / np.abs(mesh.jacobians)[:, None]
+        per_face = np.concatenate([mesh.face_normals, fs[..., None]], axis=-1)
+        geo[:, d * d:] = per_face.reshape(self.K, nf * (d + 1))
+        self.geometry = np.ascontiguousarray(geo)
+        self._boundaries = {}
+        if "node_permutation" in self.debug:
+            self.check_node_permutation()
+
+    # -- sizes / vectors ------------------------------------------------------
+    def __len__(self):
+        return self.K * self.Np
+
+    @property
+    def state_dtype(self):
+        torch = _torch()
+        return torch.float32 if self.precision == "fp32" else torch.float64
+
+    @property
+    def device(self):
+        torch = _torch()
+        if self._device is None:
+            self._device = torch.device("cuda", torch.cuda.current_device())
+        return torch.device(self._device)
+
+    def volume_zeros(self, shape=(), dtype=None, kind="gpu"):
+        torch = _torch()
+        dt = self.state_dtype if dtype is None else dtype
+        if kind == "numpy":
+            return np.zeros(tuple(shape) + (len(self),), dtype=self.default_scalar_type)
+        return torch.zeros(tuple(shape) + (len(self),), dtype=dt, device=self.device)
+
+    def volume_empty(self, shape=(), dtype=None):
+        torch = _torch()
+        dt = self.state_dtype if dtype is None else dtype
+        return torch.empty(tuple(shape) + (len(self),), dtype=dt, device=self.device)
+
+    def interpolate_volume_function(self, f, dtype=None, kind="gpu"):
+        """f(x) evaluated at all nodes; f takes an [N, d] array and returns
+        [N] (or [F, N])."""
+        vals = np.asarray(f(self.nodes), dtype=np.float64)
+        if kind == "numpy":
+            return vals
+        return self.to_device(vals, dtype)
+
+    def to_device(self, arr, dtype=None):
+        torch = _torch()
+        dt = self.state_dtype if dtype is None else dtype
+        if isinstance(arr, torch.Tensor):
+            return arr.to(device=self.device, dtype=dt).contiguous()
+        return torch.as_tensor(np.ascontiguousarray(arr)).to(
+            device=self.device, dtype=dt).contiguous()
+
+    # -- set-up data ------------------------------------------------------------
+    @cached_property
+    def interior_face_group(self):
+        """Reference-format interior face group (face pairs, index lists)."""
+        return build_interior_face_group(self.mesh, self.ldis)
+
+    def get_boundary(self, tag) -> Boundary:
+        try:
+            return self._boundaries[tag]
+        except KeyError:
+            b = self._boundaries[tag] = Boundary(self.mesh, self.ldis, self.nodes, tag)
+            return b
+
+    def is_boundary_tag_nonempty(self, tag):
+        return self.mesh.is_boundary_tag_nonempty(tag)
+
+    def len_boundary(self, tag):
+        return len(self.get_boundary(tag).vol_indices)
+
+    def interpolate_boundary_function(self, f, tag, kind="numpy"):
+        b = self.get_boundary(tag)
+        if b.is_empty():
+            return np.zeros(0)
+        return np.asarray(f(b.nodes), dtype=np.float64)
+
+    def boundary_normals(self, tag):
+        """[n_bdry_nodes, d] int-side normals of a boundary's nodes."""
+        b = self.get_boundary(tag)
+        if b.is_empty():
+            return np.zeros((0, self.dimensions))
+        n = self.mesh.face_normals[b.element_faces[:, 0], b.element_faces[:, 1]]
+        return np.repeat(n, self.Nfp, axis=0)
+
+    def check_node_permutation(self):
+        """The reference's "node_permutation" debug check
+        (discretization/__init__.py:667-678): matched face nodes coincide."""
+        fg = self.interior_face_group
+        il = fg.index_lists.astype(np.int64)
+        ii = (fg.int_el_base[:, None] + il[fg.int_ilist]).ravel()
+        ee = (fg.ext_el_base[:, None] + il[fg.ext_ilist]).ravel()
+        dist = self.nodes[ii] - self.nodes[ee]
+        lo, hi = self.mesh.points.min(0), self.mesh.points.max(0)
+        for ax, per in enumerate(self.mesh.periodicity):
+            if per is not None:
+                ext = hi[ax] - lo[ax]
+                dist[:, ax] = np.where(np.abs(np.abs(dist[:, ax]) - ext) < 1e-9, 0,
+                                       dist[:, ax])
+        err = np.abs(dist).max() if len(dist) else 0.0
+        if err >= 1e-13:
+            raise AssertionError("face node mismatch %g" % err)
+        return err
+
+    # -- time step factors (local.py:531-540, 1052-1056, 1378-1386) -----------
+    def dt_non_geometric_factor(self):
+        return self.ldis.dt_non_geometric_factor()
+
+    def dt_geometric_factor(self):
+        m = self.mesh
+        if self.dimensions == 2:
+            v = m.points[m.elements]
+            area = np.abs(2 * m.jacobians)
+            semi = (np.linalg.norm(v[:, 0] - v[:, 1], axis=1)
+                    + np.linalg.norm(v[:, 1] - v[:, 2], axis=1)
+                    + np.linalg.norm(v[:, 2] - v[:, 0], axis=1)) / 2
+            return float(np.min(area / semi))
+        res = np.abs(m.jacobians) / np.max(np.abs(m.face_jacobians), axis=1)
+        if self.order in (1, 2):
+            res = res / 2
+        return float(np.min(res))
+
+    # -- reductions -----------------------------------------------------------
+    @cached_property
+    def _mass_dev(self):
+        torch = _torch()
+        return (torch.as_tensor(self.ldis.mass_matrix, device=self.device),
+                torch.as_tensor(np.abs(self.mesh.jacobians), device=self.device))
+
+    def integral(self, u):
+        """Sum over elements of |J| 1^T M u (FP64)."""
+        torch = _torch()
+        M, J = self._mass_dev
+        u = self.to_device(u, torch.float64)
+        uu = u.reshape(*u.shape[:-1], self.K, self.Np)
+        return torch.einsum("i,...ki,k->...", M.sum(0), uu, J)
+
+    def norm(self, u, p=2):
+        """L2 norm sqrt(sum_k |J_k| u_k^T M u_k), summed over leading field
+        axes (FP64)."""
+        if p != 2:
+            raise NotImplementedError("only the L2 norm")
+        torch = _torch()
+        M, J = self._mass_dev
+        u = self.to_device(u, torch.float64)
+        uu = u.reshape(-1, self.K, self.Np)
+        return float(torch.sqrt(torch.einsum("fki,ij,fkj,k->", uu, M, uu, J)))
+
+    def get_point_evaluator(self, point, thresh=0.0):
+        """(discretization/__init__.py:1217-1249)"""
+        m = self.mesh
+        x = np.asarray(point, dtype=np.float64)
+        r = np.einsum("kij,kj->ki", m.inv_map_a, x[None, :] - m.map_b)
+        inside = np.all(r >= -1 - thresh, axis=1) & \
+            (r.sum(axis=1) <= -(self.dimensions - 2) + thresh)
+        hits = np.nonzero(inside)[0]
+        if len(hits) == 0:
+            raise RuntimeError("point %s not found" % (point,))
+        el = int(hits[0])
+        ld = self.ldis
+        phi = np.array([ld.basis(mid, r[el][None, :])[0] for mid in ld.mode_ids()])
+        coeff = np.linalg.solve(ld.vandermonde.T, phi)
+        return PointEvaluator(self, el, coeff)
+
+    # -- device handle ----------------------------------------------------------
+    def _native_handle(self):
+        if self._handle is None:
+            lib = _native.load()
+            ld = self.ldis
+            self._keep = dict(
+                dmats=np.ascontiguousarray(np.stack(ld.differentiation_matrices)),
+                lift=np.ascontiguousarray(ld.lifting_matrix),
+                geo=self.geometry,
+                fmask=np.ascontiguousarray(ld.fmask, dtype=np.int32),
+                shuffle=np.ascontiguousarray(ld.face_shuffle_table, dtype=np.int32))
+            k = self._keep
+            desc = _native.hb_discr_desc(
+                self.dimensions, self.order, self.Np, self.Nfp, self.Nfaces,
+                len(ld.face_shuffle_perms), self.K,
+                k["dmats"].ctypes.data, k["lift"].ctypes.data, k["geo"].ctypes.data,
+                k["fmask"].ctypes.data, k["shuffle"].ctypes.data,
+                int(self.device.index or 0))
+            h = C.c_void_p()
+            _native.check(lib.hb_discr_create(C.byref(desc), C.byref(h)))
+            self._handle = h
+        return self._handle
+
+    def close(self):
+        if self._handle is not None:
+            _native.load().hb_discr_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def compile(self, optemplate: OpTemplate, precision=None):
+        return CompiledOperator(self, optemplate, precision or self.precision)
+
+
+class PointEvaluator:
+    def __init__(self, discr, el, coeff):
+        self.discr, self.el, self.coeff = discr, el, coeff
+
+    def __call__(self, field):
+        torch = _torch()
+        s = slice(self.el * self.discr.Np, (self.el + 1) * self.discr.Np)
+        if isinstance(field, torch.Tensor):
+            c = torch.as_tensor(self.coeff, dtype=field.dtype, device=field.device)
+            return field[..., s] @ c
+        return np.asarray(field)[..., s] @ self.coeff
+
+
+class CompiledOperator:
+    """A model right-hand side compiled for the device.
+
+    ``op(w=..., t=..., bc_in=...)`` returns the RHS as a tensor [F, K*Np]
+    ([K*Np] for a single field), like the reference's compiled op template
+    (hedge/backends/jit/__init__.py:521-523).
+    """
+
+    def __init__(self, discr: Discretization, ot: OpTemplate, precision: str):
+        self.discr = discr
+        self.ot = ot
+        self.precision = precision
+        self.F = ot.n_fields
+        mesh = discr.mesh
+        model = ot.operator
+        if model is not None and hasattr(model, "bc_tags"):
+            check_bc_coverage(mesh, model.bc_tags())
+        nbr = discr.nbr.astype(np.int64).copy()
+        code = discr.nbr_code.astype(np.int64).copy()
+        bdry_faces = nbr < 0
+        # boundary faces without a BC of this operator contribute no flux
+        code[bdry_faces] = BC_NONE
+        self.given_tag = None
+        n_given = 0
+        for tag, kind in ot.bcs:
+            if tag is TAG_NONE:
+                continue
+            ef = mesh.boundary_faces(tag)
+            if len(ef) == 0:
+                continue
+            code[ef[:, 0], ef[:, 1]] = kind
+            if kind == BC_GIVEN:
+                nbr[ef[:, 0], ef[:, 1]] = -1 - np.arange(len(ef))
+                self.given_tag = tag
+                n_given = len(ef) * discr.Nfp
+        self.conn = np.ascontiguousarray(np.stack([nbr, code], axis=-1).astype(np.int32))
+        self.n_given = n_given
+        p = ot.params
+        v = np.zeros(3)
+        if "v" in p:
+            v[:len(p["v"])] = p["v"]
+        prec = PRECISIONS[precision] if precision != "plain" else (
+            _native.PREC_FP64 if discr.default_scalar_type == np.float64
+            else _native.PREC_FP32)
+        self.prec_code = prec
+        desc = _native.hb_op_desc(
+            ot.model, ot.n_fields, prec, ot.flux_type, p.get("bdry_flux_type", ot.flux_type),
+            (C.c_double * 3)(*v), p.get("c", 0.0), p.get("eps", 1.0), p.get("mu", 1.0),
+            p.get("alpha", 1.0), p.get("bdry_alpha", p.get("alpha", 1.0)),
+            p.get("time_sign", 1.0), self.conn.ctypes.data, n_given)
+        lib = _native.load()
+        h = C.c_void_p()
+        _native.check(lib.hb_op_create(discr._native_handle(), C.byref(desc), C.byref(h)))
+        self._handle = h
+        self._lib = lib
+        self._coeff = None
+        self._source = None
+        if ot.model == MODEL_VARWAVE:
+            self.set_coefficient(model.c if model is not None else 1.0)
+        src = p.get("source", 0) if ot.model == MODEL_WAVE else (
+            getattr(model, "source", 0) if ot.model == MODEL_VARWAVE else 0)
+        if not (np.isscalar(src) and src == 0):
+            self.set_source(src)
+
+    @property
+    def state_dtype(self):
+        torch = _torch()
+        return torch.float32 if self.prec_code == _native.PREC_FP32 else torch.float64
+
+    def set_coefficient(self, c):
+        """Variable-velocity wave speed: a number or a volume vector."""
+        torch = _torch()
+        d = self.discr
+        if np.isscalar(c):
+            t = torch.full((len(d),), float(c), dtype=torch.float64, device=d.device)
+        else:
+            t = d.to_device(c, torch.float64)
+        if t.shape != (len(d),):
+            raise ValueError("c must be a volume vector of length %d" % len(d))
+        self._coeff = t
+
+    def set_source(self, s):
+        torch = _torch()
+        d = self.discr
+        t = torch.full((len(d),), float(s), dtype=torch.float64, device=d.device) \
+            if np.isscalar(s) else d.to_device(s, torch.float64)
+        self._source = t
+
+    def __del__(self):
+        try:
+            if getattr(self, "_handle", None) is not None:
+                self._lib.hb_op_destroy(self._handle)
+                self._handle = None
+        except Exception:
+            pass
+
+    # -- argument marshalling ---------------------------------------------------
+    def as_state(self, w):
+        """[F, K*Np] contiguous device tensor of the state dtype (copies only
+        when the input is not already that)."""
+        torch = _torch()
+        d = self.discr
+        if isinstance(w, (list, tuple)) or (isinstance(w, np.ndarray) and w.dtype == object):
+            w = torch.stack([d.to_device(x, self.state_dtype) for x in w])
+        elif not isinstance(w, torch.Tensor):
+            w = torch.as_tensor(np.asarray(w))
+        w = w.to(device=d.device, dtype=self.state_dtype)
+        w = w.reshape(self.F, len(d))
+        return w.contiguous()
+
+    def _bdry_ptr(self, bc_in):
+        if self.n_given == 0:
+            return None, None
+        torch = _torch()
+        if bc_in is None:
+            raise ValueError("this operator needs boundary values (bc_in)")
+        t = self.discr.to_device(bc_in, torch.float64)
+        if t.numel() != self.n_given:
+            raise ValueError("bc_in must have %d entries" % self.n_given)
+        return t, t.data_ptr()
+
+    def _stream(self):
+        torch = _torch()
+        return torch.cuda.current_stream(self.discr.device).cuda_stream
+
+    # -- evaluation -------------------------------------------------------------
+    def rhs_into(self, q, out, bc_in=None):
+        """out <- RHS(q); q, out: [F, K*Np] device tensors of the state dtype."""
+        keep, bptr = self._bdry_ptr(bc_in)
+        _native.check(self._lib.hb_rhs(
+            self._handle, q.data_ptr(), out.data_ptr(),
+            self._coeff.data_ptr() if self._coeff is not None else None,
+            bptr, self._source.data_ptr() if self._source is not None else None,
+            self._stream()))
+        return out
+
+    def lsrk_stage(self, a, b, dt, q_in, q_out, res, bc_in=None):
+        keep, bptr = self._bdry_ptr(bc_in)
+        _native.check(self._lib.hb_lsrk_stage(
+            self._handle, float(a), float(b), float(dt), q_in.data_ptr(),
+            q_out.data_ptr(), res.data_ptr(),
+            self._coeff.data_ptr() if self._coeff is not None else None,
+            bptr, self._source.data_ptr() if self._source is not None else None,
+            self._stream()))
+
+    def check(self):
+        """Synchronise and raise if a kernel flagged bad input."""
+        _native.check(self._lib.hb_op_check(self._handle, self._stream()))
+
+    def gather_map(self):
+        """Device-expanded (int, ext) gather indices, [K*Nf*Nfp] each."""
+        torch = _torch()
+        d = self.discr
+        n = d.K * d.Nfaces * d.Nfp
+        ii = torch.empty(n, dtype=torch.int64, device=d.device)
+        ee = torch.empty(n, dtype=torch.int64, device=d.device)
+        _native.check(self._lib.hb_gather_map(self._handle, ii.data_ptr(),
+                                              ee.data_ptr(), self._stream()))
+        return ii, ee
+
+    def __call__(self, w=None, t=0.0, bc_in=None, u=None, **kwargs):
+        if w is None:
+            w = u
+        q = self.as_state(w)
+        out = self.discr.volume_empty((self.F,), self.state_dtype)
+        self.rhs_into(q, out, bc_in=bc_in)
+        return out[0] if self.F == 1 and self.ot.model == MODEL_ADVECTION else out
+
+    def bind_model(self, model):
+        return BoundRHS(self, model)
+
+
+class BoundRHS:
+    """``rhs(t, w)`` of a bound model (the reference's closure from
+    ``op.bind(discr)``)."""
+
+    def __init__(self, compiled: CompiledOperator, model):
+        self.compiled = compiled
+        self.model = model
+        self.discr = compiled.discr
+
+    def context(self, t):
+        if self.compiled.n_given:
+            m = self.model
+            return {"bc_in": m.inflow_u.boundary_interpolant(t, self.discr,
+                                                             self.compiled.given_tag)}
+        return {}
+
+    def __call__(self, t, w):
+        return self.compiled(w=w, t=t, **self.context(t))
+
+
+__all__ = ["Discretization", "CompiledOperator", "BoundRHS", "PointEvaluator",
+           "TAG_ALL", "TAG_NONE", "MODEL_ADVECTION", "MODEL_MAXWELL"]

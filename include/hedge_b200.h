@@ -1,0 +1,141 @@
+/* hedge_b200 -- B200 (sm_100a) DG right-hand-side backend, C ABI.
+ *
+ * Plain pointers and sizes only.  All state/field buffers are device memory
+ * owned by the caller (the reference writes into caller-allocated
+ * volume_zeros() arrays the same way, hedge/backends/jit/__init__.py:167-168);
+ * the library owns only the descriptor objects it creates (create/destroy
+ * pairs).  Every call returns an hb_status; no call aborts or traps.  Device
+ * kernels report bad input through a device error flag that the host turns
+ * into HB_ERR_DEVICE_FLAG.  Calls on distinct descriptors are re-entrant;
+ * each call is enqueued on the stream it is given (a cudaStream_t passed as
+ * void*; NULL = legacy default stream).
+ *
+ * Layouts.  A volume vector is [K * Np], element-major, node order of the
+ * reference element (hedge/discretization/__init__.py:405-417).  A state of
+ * F fields is F such vectors back to back: [F][K * Np].
+ */
+#ifndef HEDGE_B200_H
+#define HEDGE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  HB_OK = 0,
+  HB_ERR_INVALID_ARGUMENT = 1,
+  HB_ERR_UNSUPPORTED = 2,
+  HB_ERR_CUDA = 3,
+  HB_ERR_DEVICE_FLAG = 4
+} hb_status;
+
+enum {
+  HB_MODEL_ADVECTION = 1, /* hedge/models/advection.py:124-149 */
+  HB_MODEL_WAVE = 2,      /* hedge/models/wave.py:37-197 */
+  HB_MODEL_VARWAVE = 3,   /* hedge/models/wave.py:204-418 */
+  HB_MODEL_MAXWELL = 4    /* hedge/models/em.py:38-387 */
+};
+
+enum {
+  HB_PREC_FP64 = 0,   /* FP64 state, FP64 arithmetic */
+  HB_PREC_FP32 = 1,   /* FP32 state, FP32 arithmetic */
+  HB_PREC_BF16X3 = 2  /* FP64 state, split-BF16 tensor-core products, FP32 accumulation */
+};
+
+enum {
+  HB_BC_NONE = 0, HB_BC_GIVEN = 1, HB_BC_DIRICHLET = 2, HB_BC_NEUMANN = 3,
+  HB_BC_RADIATION = 4, HB_BC_PEC = 5, HB_BC_PMC = 6, HB_BC_ABSORB = 7
+};
+
+typedef struct hb_discr hb_discr;
+typedef struct hb_op hb_op;
+
+/* Reference element + mesh geometry of one discretization, host FP64.
+ * geometry: [K][G], G = dim*dim + nfaces*(dim+1); per element first
+ *   d(r_a)/d(x_b) at [a*dim + b], then per face f its outward unit normal
+ *   (dim values) and Fscale = face Jacobian / |element Jacobian|. */
+typedef struct {
+  int32_t dim, order, np, nfp, nfaces, nperm;
+  int64_t num_elements;
+  const double* dmats;     /* [dim][np][np] row-major: D_r = V_r V^-1 */
+  const double* lift;      /* [np][nfaces*nfp]: LIFT = M^-1 E */
+  const double* geometry;  /* [K][G] */
+  const int32_t* fmask;    /* [nfaces][nfp] local node of each face node */
+  const int32_t* shuffle;  /* [nperm][nfp] face-node shuffle per vertex perm */
+  int32_t device;          /* CUDA device ordinal */
+} hb_discr_desc;
+
+/* Replaces the device-side part of Discretization.__init__ /
+ * _calculate_local_matrices (hedge/discretization/__init__.py:217-262,
+ * 440-453): uploads operators and geometry once. */
+hb_status hb_discr_create(const hb_discr_desc* desc, hb_discr** out);
+hb_status hb_discr_destroy(hb_discr* discr);
+
+/* One compiled model operator.  conn: host [K][nfaces][2] int32,
+ * interior face: (neighbour element, nbr_face | perm_id << 2);
+ * boundary face: (-1 - b, bc kind), b = the face's number in the
+ * BC_GIVEN boundary vector (nodes b*nfp .. b*nfp+nfp-1). */
+typedef struct {
+  int32_t model, num_fields, precision;
+  int32_t flux_type, bdry_flux_type;
+  double v[3];             /* advection velocity */
+  double c;                /* constant wave speed */
+  double eps, mu;          /* Maxwell material */
+  double alpha, bdry_alpha;/* Maxwell numeric flux weight (1 = upwind) */
+  double time_sign;        /* variable-velocity wave */
+  const int32_t* conn;
+  int64_t num_given_bdry_nodes;
+} hb_op_desc;
+
+/* Replaces Discretization.compile -> jit Executor construction
+ * (hedge/discretization/__init__.py:1288-1302,
+ *  hedge/backends/jit/__init__.py:366-438). */
+hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out);
+hb_status hb_op_destroy(hb_op* op);
+
+/* rhs = RHS(q).  Replaces Executor.__call__ (hedge/backends/jit/__init__.py:
+ * 521-523): diff batch (jit/diff.py:137-175), chain rule vector expressions,
+ * flux gather interior + boundary (jit/flux.py:239-480), lift
+ * (jit/lift.py:110-141) and inverse mass (jit/__init__.py:501-519).
+ * q, rhs: [F][K*Np] in the operator's state dtype.  coeff: var-c wave
+ * speed [K*Np] FP64 (else NULL); bdry: BC_GIVEN values [n] FP64 (else NULL);
+ * source: var-c / constant-c wave source on u, [K*Np] FP64 (else NULL). */
+hb_status hb_rhs(hb_op* op, const void* q, void* rhs, const double* coeff,
+                 const double* bdry, const double* source, void* stream);
+
+/* Fused LSRK stage: res = a*res + dt*RHS(q_in); q_out = q_in + b*res.
+ * Replaces one pass of the LSRK4TimeStepper loop body
+ * (hedge/timestep/runge_kutta.py:123-128).  q_out must not alias q_in. */
+hb_status hb_lsrk_stage(hb_op* op, double a, double b, double dt,
+                        const void* q_in, void* q_out, void* res,
+                        const double* coeff, const double* bdry,
+                        const double* source, void* stream);
+
+/* out = a*x + b*y, n elements of dtype (0 = FP64, 1 = FP32).  Replaces
+ * NumpyLinearCombiner (hedge/vector_primitives.py:58-77). */
+hb_status hb_lincomb(int64_t n, int32_t dtype, double a, const void* x,
+                     double b, const void* y, void* out, void* stream);
+
+/* The face gather maps the kernels use, expanded on the device: for every
+ * element face node (e, f, i) in [K][nfaces][nfp] order, the int volume
+ * index and the ext volume index (interior) or -1 - boundary node
+ * (boundary).  Device int64 buffers of K*nfaces*nfp entries.  Replaces the
+ * face-pair index lists of hedge/discretization/data.py:199-248. */
+hb_status hb_gather_map(hb_op* op, int64_t* int_idx, int64_t* ext_idx,
+                        void* stream);
+
+/* Synchronises `stream` and returns HB_ERR_DEVICE_FLAG if a kernel of this
+ * operator flagged bad input (out-of-range neighbour or code, missing
+ * boundary vector); the flag stays set. */
+hb_status hb_op_check(hb_op* op, void* stream);
+
+/* Thread-local text of the last error. */
+const char* hb_last_error_string(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HEDGE_B200_H */
