@@ -10,7 +10,8 @@ from .mesh import (Mesh, TAG_ALL, TAG_NONE, make_regular_rect_mesh,
 from .refelem import TriangleElement, TetrahedronElement, make_element
 from .models import (StrongAdvectionOperator, StrongWaveOperator,
                      VariableVelocityStrongWaveOperator, MaxwellOperator,
-                     make_tdep_constant, TimeConstantGivenFunction)
+                     make_tdep_constant, TimeConstantGivenFunction,
+                     TimeDependentGivenFunction)
 from .discretization import Discretization, CompiledOperator, BoundRHS
 from .timestep import LSRK4TimeStepper, RK4TimeStepper
 
@@ -19,6 +20,6 @@ __all__ = [
     "check_bc_coverage", "TriangleElement", "TetrahedronElement", "make_element",
     "StrongAdvectionOperator", "StrongWaveOperator",
     "VariableVelocityStrongWaveOperator", "MaxwellOperator", "make_tdep_constant",
-    "TimeConstantGivenFunction", "Discretization", "CompiledOperator", "BoundRHS",
+    "TimeConstantGivenFunction", "TimeDependentGivenFunction", "Discretization", "CompiledOperator", "BoundRHS",
     "LSRK4TimeStepper", "RK4TimeStepper",
 ]

@@ -67,6 +67,7 @@ struct Op {
   int threads = 0;
   size_t smem = 0;
   int grid = 0;
+  int ops_in_smem = 1;
   // split-precision operator planes (BF16X3)
   void* split_ops = nullptr;
 };

@@ -45,6 +45,7 @@ struct SimtArgs {
   const double* source;
   double ra, rb, dt;
   int mode;  // 0: write rhs, 1: LSRK stage
+  int ops_in_smem;  // operators staged in shared memory (else read via L1)
   ModelParams mp;
   int* err;
 };
@@ -79,12 +80,12 @@ __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(
 
 __host__ __device__ inline SimtLayout simt_layout(int tsize, int dim, int np, int nfp,
                                                   int nf, int nperm, int G, int E,
-                                                  int F, int C) {
+                                                  int F, int C, int ops) {
   SimtLayout L;
   const int nfpt = nf * nfp;
   size_t o = 0;
-  L.oD = o;    o = align16(o + (size_t)tsize * dim * np * np);
-  L.oL = o;    o = align16(o + (size_t)tsize * nfpt * np);
+  L.oD = o;    o = align16(o + (size_t)tsize * dim * np * np * ops);
+  L.oL = o;    o = align16(o + (size_t)tsize * nfpt * np * ops);
   L.oq = o;    o = align16(o + (size_t)tsize * F * E * np);
   L.ofl = o;   o = align16(o + (size_t)tsize * F * E * nfpt);
   L.ogeo = o;  o = align16(o + (size_t)tsize * E * G);
@@ -105,9 +106,10 @@ __global__ void __launch_bounds__(256) rhs_simt_kernel(SimtArgs<T, S> a) {
 
   const int np = a.np, nfp = a.nfp, nf = a.nf, E = a.E, G = a.G;
   const int nfpt = nf * nfp;
-  const SimtLayout L = simt_layout((int)sizeof(T), DIM, np, nfp, nf, a.nperm, G, E, F, C);
-  T* sD = reinterpret_cast<T*>(smem_raw + L.oD);
-  T* sL = reinterpret_cast<T*>(smem_raw + L.oL);
+  const SimtLayout L = simt_layout((int)sizeof(T), DIM, np, nfp, nf, a.nperm, G, E, F, C,
+                                   a.ops_in_smem);
+  const T* sD = a.ops_in_smem ? reinterpret_cast<T*>(smem_raw + L.oD) : a.dmats_t;
+  const T* sL = a.ops_in_smem ? reinterpret_cast<T*>(smem_raw + L.oL) : a.lift_t;
   T* sq = reinterpret_cast<T*>(smem_raw + L.oq);
   T* sfl = reinterpret_cast<T*>(smem_raw + L.ofl);
   T* sgeo = reinterpret_cast<T*>(smem_raw + L.ogeo);
@@ -118,8 +120,12 @@ __global__ void __launch_bounds__(256) rhs_simt_kernel(SimtArgs<T, S> a) {
 
   const int tid = threadIdx.x;
   const int nthr = blockDim.x;
-  for (int x = tid; x < DIM * np * np; x += nthr) sD[x] = a.dmats_t[x];
-  for (int x = tid; x < nfpt * np; x += nthr) sL[x] = a.lift_t[x];
+  if (a.ops_in_smem) {
+    T* wD = reinterpret_cast<T*>(smem_raw + L.oD);
+    T* wL = reinterpret_cast<T*>(smem_raw + L.oL);
+    for (int x = tid; x < DIM * np * np; x += nthr) wD[x] = a.dmats_t[x];
+    for (int x = tid; x < nfpt * np; x += nthr) wL[x] = a.lift_t[x];
+  }
   for (int x = tid; x < nfpt; x += nthr) sfm[x] = a.fmask[x];
   for (int x = tid; x < a.nperm * nfp; x += nthr) ssh[x] = a.shuffle[x];
 
@@ -266,11 +272,11 @@ __global__ void __launch_bounds__(256) rhs_simt_kernel(SimtArgs<T, S> a) {
 
 // ---------------------------------------------------------------------------
 template <typename T>
-static size_t simt_smem(const Op* op, int E) {
+static size_t simt_smem(const Op* op, int E, int ops) {
   const Discr* d = op->d;
   const int C = op->model == HB_MODEL_VARWAVE ? 1 : 0;
   return simt_layout((int)sizeof(T), d->dim, d->np, d->nfp, d->nfaces, d->nperm,
-                     d->G, E, op->F, C).total;
+                     d->G, E, op->F, C, ops).total;
 }
 
 template <int MODEL, int DIM, typename T, typename S>
@@ -283,15 +289,18 @@ static hb_status launch_one(Op* op, int mode, double ra, double rb, double dt,
   if (configure) {
     int E = 256 / d->np;
     if (E < 1) E = 1;
-    size_t smem = simt_smem<T>(op, E);
     int dev;
     HB_CUDA(cudaGetDevice(&dev));
     int max_optin = 0;
     HB_CUDA(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    // operators in shared memory when they leave room for two CTAs per SM
+    int ops = simt_smem<T>(op, E, 1) * 2 <= (size_t)max_optin ? 1 : 0;
+    size_t smem = simt_smem<T>(op, E, ops);
     while (E > 1 && smem > (size_t)max_optin) {
       --E;
-      smem = simt_smem<T>(op, E);
+      smem = simt_smem<T>(op, E, ops);
     }
+    op->ops_in_smem = ops;
     if (smem > (size_t)max_optin)
       return fail(HB_ERR_UNSUPPORTED, "element too large for the shared-memory kernel");
     HB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -327,6 +336,7 @@ static hb_status launch_one(Op* op, int mode, double ra, double rb, double dt,
   a.rhs_out = static_cast<S*>(q_out);
   a.coeff = coeff; a.bdry = bdry; a.source = source;
   a.ra = ra; a.rb = rb; a.dt = dt; a.mode = mode;
+  a.ops_in_smem = op->ops_in_smem;
   a.mp = op->mp;
   a.err = op->err_flag;
   kern<<<op->grid, op->threads, op->smem, s>>>(a);

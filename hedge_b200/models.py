@@ -83,6 +83,20 @@ class TimeConstantGivenFunction:
         return discr.interpolate_boundary_function(self.f, tag)
 
 
+class TimeDependentGivenFunction:
+    """Boundary/volume data given as f(x, t) with x an [N, d] array
+    (hedge/data.py TimeDependentGivenFunction)."""
+
+    def __init__(self, f):
+        self.f = f
+
+    def boundary_interpolant(self, t, discr, tag):
+        return discr.interpolate_boundary_function(lambda x: self.f(x, t), tag)
+
+    def volume_interpolant(self, t, discr):
+        return discr.interpolate_volume_function(lambda x: self.f(x, t))
+
+
 def make_tdep_constant(value):
     return TimeConstantGivenFunction(lambda x, el=None: value)
 
@@ -246,4 +260,5 @@ def _to_numpy(x):
 __all__ = ["StrongAdvectionOperator", "StrongWaveOperator",
            "VariableVelocityStrongWaveOperator", "MaxwellOperator",
            "OpTemplate", "make_tdep_constant", "TimeConstantGivenFunction",
+           "TimeDependentGivenFunction",
            "check_bc_coverage"]

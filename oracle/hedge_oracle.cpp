@@ -38,7 +38,8 @@
 
 extern "C" {
 
-enum { OR_ADVECTION = 1, OR_WAVE = 2, OR_VARWAVE = 3, OR_MAXWELL = 4 };
+enum { OR_ADVECTION = 1, OR_WAVE = 2, OR_VARWAVE = 3, OR_MAXWELL = 4,
+       OR_NORMAL_DOT = 5 };  // test flux sum_k n_k (u_int,k - alpha u_ext,k)
 
 struct or_flux_params {
   int model;
@@ -172,6 +173,14 @@ static void model_flux(const or_flux_params& p, const double* ui,
       }
       break;
     }
+    case OR_NORMAL_DOT: {
+      // the known-answer tests' fluxes, e.g. f.int * n_x (one-sided) or
+      // (u.int - u.ext) * n_y (test/test_jit_discretization.py:164-236, 528-618)
+      double s = 0;
+      for (int k = 0; k < d; ++k) s += n[k] * (ui[k] - p.alpha * ue[k]);
+      f[0] = s;
+      break;
+    }
     case OR_MAXWELL: {
       const double* ei = ui; const double* hi = ui + 3;
       const double* ee = ue; const double* he = ue + 3;
@@ -211,6 +220,7 @@ static int n_flux_components(const or_flux_params& p) {
     case OR_WAVE: return p.dim + 1;
     case OR_VARWAVE: return p.dim + 1;
     case OR_MAXWELL: return 6;
+    case OR_NORMAL_DOT: return 1;
   }
   return 0;
 }

@@ -31,7 +31,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 
-OR_ADVECTION, OR_WAVE, OR_VARWAVE, OR_MAXWELL = 1, 2, 3, 4
+OR_ADVECTION, OR_WAVE, OR_VARWAVE, OR_MAXWELL, OR_NORMAL_DOT = 1, 2, 3, 4, 5
 BC_NONE, BC_GIVEN, BC_DIRICHLET, BC_NEUMANN, BC_RADIATION, BC_PEC, BC_PMC, BC_ABSORB = range(8)
 
 
