@@ -49,6 +49,7 @@ class hb_op_desc(C.Structure):
 EXPORTED = [
     "hb_discr_create", "hb_discr_destroy", "hb_op_create", "hb_op_destroy",
     "hb_rhs", "hb_lsrk_stage", "hb_lincomb", "hb_gather_map", "hb_op_check",
+    "hb_op_launch_info",
     "hb_last_error_string",
 ]
 
@@ -78,6 +79,7 @@ def load(path=LIB_PATH):
             "hb_lincomb": [i64, i32, d, vp, d, vp, vp, vp],
             "hb_gather_map": [vp, vp, vp, vp],
             "hb_op_check": [vp, vp],
+            "hb_op_launch_info": [vp, vp, i32],
         }
         for name, args in sig.items():
             fn = getattr(lib, name)

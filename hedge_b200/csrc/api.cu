@@ -75,9 +75,10 @@ hb_status check_device_flag(Op* op, cudaStream_t s) {
   if (flag != DEV_OK) {
     static const char* what[] = {"ok", "face neighbour out of range",
                                  "invalid neighbour face / permutation code",
-                                 "boundary index out of range", "missing input vector"};
+                                 "boundary index out of range", "missing input vector",
+                                 "tensor-core MMA did not complete in time"};
     return fail(HB_ERR_DEVICE_FLAG,
-                std::string("device check failed: ") + (flag < 5 ? what[flag] : "unknown"));
+                std::string("device check failed: ") + (flag < 6 ? what[flag] : "unknown"));
   }
   return HB_OK;
 }
@@ -296,6 +297,15 @@ hb_status hb_gather_map(hb_op* handle, int64_t* int_idx, int64_t* ext_idx, void*
   Op* op = reinterpret_cast<Op*>(handle);
   DeviceGuard g(op->d->device);
   return launch_gather_map(op, int_idx, ext_idx, reinterpret_cast<cudaStream_t>(stream));
+}
+
+hb_status hb_op_launch_info(hb_op* handle, int64_t* info, int32_t n) {
+  if (!handle || !info || n < 1) return fail(HB_ERR_INVALID_ARGUMENT, "null argument");
+  Op* op = reinterpret_cast<Op*>(handle);
+  const int64_t v[6] = {op->grid, op->threads, (int64_t)op->smem, op->elems_per_block,
+                        op->ops_in_smem, op->blocks_per_sm};
+  for (int k = 0; k < n && k < 6; ++k) info[k] = v[k];
+  return HB_OK;
 }
 
 hb_status hb_op_check(hb_op* handle, void* stream) {

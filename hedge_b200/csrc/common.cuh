@@ -33,7 +33,8 @@ enum : int {
   DEV_BAD_NEIGHBOUR = 1,
   DEV_BAD_CODE = 2,
   DEV_BAD_BDRY_INDEX = 3,
-  DEV_MISSING_INPUT = 4
+  DEV_MISSING_INPUT = 4,
+  DEV_MMA_TIMEOUT = 5
 };
 
 // Operator data uploaded once per discretization.
@@ -68,6 +69,7 @@ struct Op {
   size_t smem = 0;
   int grid = 0;
   int ops_in_smem = 1;
+  int blocks_per_sm = 0;
   // split-precision operator planes (BF16X3)
   void* split_ops = nullptr;
 };

@@ -313,6 +313,7 @@ static hb_status launch_one(Op* op, int mode, double ra, double rb, double dt,
     HB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int64_t nbatch = (d->K + E - 1) / E;
     op->elems_per_block = E;
+    op->blocks_per_sm = per_sm;
     op->threads = threads;
     op->smem = smem;
     op->grid = (int)std::min<int64_t>(nbatch, (int64_t)sms * per_sm);

@@ -1,0 +1,736 @@
+// Split-precision (BF16x3) fused DG right-hand side + LSRK stage on the
+// sm_100a tensor cores (tcgen05.mma kind::f16, FP32 accumulation in TMEM).
+//
+// The two contractions of the DG operator run as GEMMs whose M dimension is
+// the batch's (element, field) pairs -- one TMEM lane per pair, EPW = 32/F
+// elements per 32-lane quadrant, EB = 4*EPW elements per batch:
+//
+//   diff:  C[(e,f)][(r,i)] = sum_j q[(e,f)][j] * D_r[i][j]
+//          A = state (K-major, j contiguous), B = [D_r]^T stacked over r,
+//          M = 128, N = dim*Np (padded to 16), K = Np (padded to 16)
+//   lift:  L[(e,f)][i] = sum_p flux[(e,f)][p] * LIFT[i][p]
+//          A = face fluxes, B = LIFT^T, M = 128, N = Np, K = Nf*Nfp
+//
+// Each operand x is split into BF16 planes hi = bf16(x), lo = bf16(x - hi);
+// a product is hi*hi + hi*lo + lo*hi, accumulated in FP32 ("BF16x3").  The
+// operator planes are built once on the host in the tensor core's canonical
+// K-major layout and stay resident in shared memory; the state and flux
+// planes are written per batch.  Two accuracy measures keep smooth fields
+// accurate: the state is split after subtracting its value at the
+// element's first node (D_r annihilates constants, so only the
+// within-element variation goes through BF16), and face jumps of the
+// models whose numerical flux is linear in the jump are formed in FP64.
+//
+// One lane holds every derivative d_r q_f(x_i) of its (e, f): the chain
+// rule needs only the element's metric, and the model's volume terms
+// (curl, div, grad) gather the element's other fields with warp shuffles.
+// Element shapes are compile-time (template on the order) so that all
+// batch index arithmetic folds to constants.  The RK stage update (res, q)
+// stays in FP64.  Restated reference loops: jit/diff.py:137-175,
+// jit/flux.py:311-353 and 429-472, jit/lift.py:110-141,
+// jit/__init__.py:501-519, timestep/runge_kutta.py:123-128.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "models.cuh"
+#include "tc.cuh"
+
+namespace hb {
+
+hb_status ensure_fp32(Discr* d);
+
+constexpr int SPLIT_THREADS = 256;
+// register rounds: state values and face points a thread keeps in flight
+constexpr int ROUND = 9;
+constexpr int FROUND = 4;
+// bounded wait for the tensor core: 2 s, far above any batch's MMA time
+constexpr uint64_t MBAR_MAX_NS = 2000000000ull;
+
+__host__ __device__ constexpr int ru16(int x) { return (x + 15) / 16 * 16; }
+__host__ __device__ constexpr int ru32(int x) { return (x + 31) / 32 * 32; }
+__host__ __device__ constexpr uint32_t al128(uint32_t x) { return (x + 127u) & ~127u; }
+
+// Compile-time shape of one (model, dim, order) instance.
+template <int MODEL, int DIM, int ORDER>
+struct Shape {
+  static constexpr int F = Traits<MODEL, DIM>::F;
+  static constexpr int C = Traits<MODEL, DIM>::COEFF;
+  static constexpr int NA = F + C;
+  static constexpr int NP = DIM == 2 ? (ORDER + 1) * (ORDER + 2) / 2
+                                     : (ORDER + 1) * (ORDER + 2) * (ORDER + 3) / 6;
+  static constexpr int NFP = DIM == 2 ? ORDER + 1 : (ORDER + 1) * (ORDER + 2) / 2;
+  static constexpr int NF = DIM + 1;
+  static constexpr int NFPT = NF * NFP;
+  static constexpr int G = DIM * DIM + NF * (DIM + 1);
+  static constexpr int EPW = 32 / F;
+  static constexpr int EB = 4 * EPW;
+  static constexpr int KD = ru16(NP), KL = ru16(NFPT);
+  static constexpr int ND = ru16(DIM * NP), NL = ru16(NP);
+  static constexpr int LIFT_COL = ru32(ND);
+  static constexpr int NVAL = F * EB * NP;
+  static constexpr int NV = (NVAL + SPLIT_THREADS - 1) / SPLIT_THREADS;
+  static constexpr int NFACE = EB * NFPT;
+  static constexpr int NFV = (NFACE + SPLIT_THREADS - 1) / SPLIT_THREADS;
+  static constexpr int NPH = ((NP + 1) / 2 + 3) & ~3;  // node split of the epilogue
+  // shared-memory carve-up
+  static constexpr uint32_t oDh = 0;
+  static constexpr uint32_t oDl = al128(oDh + ND * KD * 2);
+  static constexpr uint32_t oLh = al128(oDl + ND * KD * 2);
+  static constexpr uint32_t oLl = al128(oLh + NL * KL * 2);
+  static constexpr uint32_t oAqh = al128(oLl + NL * KL * 2);
+  static constexpr uint32_t oAql = al128(oAqh + 128 * KD * 2);
+  static constexpr uint32_t oAfh = al128(oAql + 128 * KD * 2);
+  static constexpr uint32_t oAfl = al128(oAfh + 128 * KL * 2);
+  static constexpr uint32_t osq = al128(oAfl + 128 * KL * 2);
+  static constexpr uint32_t osc = al128(osq + F * EB * NP * 4);
+  static constexpr uint32_t ogeo = al128(osc + C * EB * NP * 4);
+  static constexpr uint32_t oconn = al128(ogeo + EB * G * 4);
+  static constexpr uint32_t ofm = al128(oconn + EB * NF * 8);
+  static constexpr uint32_t osh = al128(ofm + NFPT * 4);
+  static constexpr uint32_t obar = al128(osh + 6 * NFP * 4);
+  static constexpr uint32_t total = al128(obar + 32);
+  static constexpr int TMEM_NEED = LIFT_COL + NL + 4;
+  static constexpr uint32_t TMEM_COLS = TMEM_NEED <= 32 ? 32 : TMEM_NEED <= 64 ? 64
+                                        : TMEM_NEED <= 128 ? 128 : TMEM_NEED <= 256 ? 256 : 512;
+  static constexpr bool FITS = ND <= 256 && NL <= 256 && TMEM_NEED <= 512;
+};
+
+struct SplitArgs {
+  int64_t K, nbatch, n_given;
+  int nperm;
+  const uint8_t* ops;   // [D_hi | D_lo | L_hi | L_lo] canonical images
+  const float* geo32;
+  const int2* conn;
+  const int* fmask;
+  const int* shuffle;
+  const double* q_in;
+  double* q_out;
+  double* res;
+  const double* coeff;
+  const double* bdry;
+  const double* source;
+  double ra, rb, dt;
+  int mode;
+  ModelParams mp;
+  int* err;
+};
+
+// byte offset of element (row, k) in a K-major no-swizzle operand image with
+// K padded to kp: 8x8 core matrices (8 rows x 16 bytes), K chunks 128 B
+// apart, 8-row groups kp*16 B apart
+__host__ __device__ constexpr uint32_t kmajor_off(int row, int k, int kp) {
+  return (uint32_t)((row >> 3) * (kp * 16) + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ void store_split_f64(uint8_t* hi, uint8_t* lo, uint32_t off,
+                                                double v) {
+  const float vf = (float)v;
+  const __nv_bfloat16 h = __float2bfloat16_rn(vf);
+  const __nv_bfloat16 l = __float2bfloat16_rn((float)(v - (double)__bfloat162float(h)));
+  *reinterpret_cast<__nv_bfloat16*>(hi + off) = h;
+  *reinterpret_cast<__nv_bfloat16*>(lo + off) = l;
+}
+
+__device__ __forceinline__ void store_split_f32(uint8_t* hi, uint8_t* lo, uint32_t off,
+                                                float v) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(v);
+  const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+  *reinterpret_cast<__nv_bfloat16*>(hi + off) = h;
+  *reinterpret_cast<__nv_bfloat16*>(lo + off) = l;
+}
+
+// models whose numerical flux depends on the state only through the jump
+// q- - q+ (so f(q-, q+) == f(q- - q+, 0))
+template <int MODEL>
+struct JumpLinear { static constexpr bool value = MODEL != HB_MODEL_VARWAVE; };
+
+// The volume term of this lane's own field at one node, from the physical
+// gradients g[x] that every lane of the element's F lanes (base..base+F-1)
+// holds for its own field; the other fields' gradients come over warp
+// shuffles, only the ones the model needs (warp-collective: every lane of
+// the warp calls this).
+template <int MODEL, int DIM>
+__device__ __forceinline__ float volume_own(const ModelParams& mp, const float (&g)[DIM],
+                                            int base, int fown, float cnode) {
+  constexpr unsigned FULL = 0xffffffffu;
+  if constexpr (MODEL == HB_MODEL_ADVECTION) {
+    float s = 0.f;
+#pragma unroll
+    for (int x = 0; x < DIM; ++x) s += (float)mp.v[x] * g[x];
+    return -s;
+  } else if constexpr (MODEL == HB_MODEL_WAVE || MODEL == HB_MODEL_VARWAVE) {
+    // u lane: c div v = c sum_x d_x v_x; v_x lane: c d_x u
+    const float c = (MODEL == HB_MODEL_WAVE) ? (float)mp.c : (float)mp.time_sign * cnode;
+    float offer = g[0];
+#pragma unroll
+    for (int x = 1; x < DIM; ++x) offer = (fown == 1 + x) ? g[x] : offer;
+    float div = 0.f;
+#pragma unroll
+    for (int x = 0; x < DIM; ++x) div += __shfl_sync(FULL, offer, base + 1 + x);
+    float gu = 0.f;
+#pragma unroll
+    for (int x = 0; x < DIM; ++x) {
+      const float v = __shfl_sync(FULL, g[x], base);
+      gu = (fown == 1 + x) ? v : gu;
+    }
+    return c * (fown == 0 ? div : gu);
+  } else {
+    // Maxwell: E_c lane: (curl H)_c; H_c lane: -(curl E)_c, with
+    // curl(A)_c = d_{c+1} A_{c+2} - d_{c+2} A_{c+1}
+    const int c = fown % 3;
+    const int other = fown < 3 ? 3 : 0;
+    const int c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+    float a0[3], a1[3];
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      a0[x] = __shfl_sync(FULL, g[x], base + other + c2);
+      a1[x] = __shfl_sync(FULL, g[x], base + other + c1);
+    }
+    float t0 = a0[0], t1 = a1[0];
+#pragma unroll
+    for (int x = 1; x < 3; ++x) {
+      t0 = (x == c1) ? a0[x] : t0;
+      t1 = (x == c2) ? a1[x] : t1;
+    }
+    const float curl = t0 - t1;
+    return fown < 3 ? curl : -curl;
+  }
+}
+
+template <int MODEL, int DIM, int ORDER>
+__global__ void __launch_bounds__(SPLIT_THREADS, 2) rhs_split_kernel(SplitArgs a) {
+  using S = Shape<MODEL, DIM, ORDER>;
+  constexpr int F = S::F, C = S::C, NA = S::NA, NP = S::NP, NFP = S::NFP, NF = S::NF;
+  constexpr int NFPT = S::NFPT, G = S::G, EPW = S::EPW, EB = S::EB;
+  constexpr int KD = S::KD, KL = S::KL;
+  extern __shared__ __align__(128) uint8_t smem[];
+  uint8_t* Aqh = smem + S::oAqh;
+  uint8_t* Aql = smem + S::oAql;
+  uint8_t* Afh = smem + S::oAfh;
+  uint8_t* Afl = smem + S::oAfl;
+  float* sq = reinterpret_cast<float*>(smem + S::osq);    // state, then the staged rhs
+  float* sc = reinterpret_cast<float*>(smem + S::osc);
+  float* sgeo = reinterpret_cast<float*>(smem + S::ogeo);
+  int2* sconn = reinterpret_cast<int2*>(smem + S::oconn);
+  int* sfm = reinterpret_cast<int*>(smem + S::ofm);
+  int* ssh = reinterpret_cast<int*>(smem + S::osh);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + S::obar);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + S::obar + 16);
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+
+  // ---- one-time set-up: resident operators, zeroed operand planes ----
+  {
+    constexpr uint32_t dD = S::ND * KD * 2, dL = S::NL * KL * 2;
+    constexpr uint32_t nchunk = (2 * dD + 2 * dL) / 16;
+    const uint4* src = reinterpret_cast<const uint4*>(a.ops);
+    for (uint32_t x = tid; x < nchunk; x += SPLIT_THREADS) {
+      const uint32_t b = x * 16;
+      uint32_t o;
+      if (b < dD) o = S::oDh + b;
+      else if (b < 2 * dD) o = S::oDl + (b - dD);
+      else if (b < 2 * dD + dL) o = S::oLh + (b - 2 * dD);
+      else o = S::oLl + (b - 2 * dD - dL);
+      *reinterpret_cast<uint4*>(smem + o) = src[x];
+    }
+    const uint4 z = make_uint4(0, 0, 0, 0);
+    for (uint32_t o = S::oAqh + tid * 16; o < S::osq; o += SPLIT_THREADS * 16)
+      *reinterpret_cast<uint4*>(smem + o) = z;
+    for (int x = tid; x < NFPT; x += SPLIT_THREADS) sfm[x] = a.fmask[x];
+    for (int x = tid; x < a.nperm * NFP; x += SPLIT_THREADS) ssh[x] = a.shuffle[x];
+    if (tid == 0) {
+      tc::mbar_init(&mbar[0], 1);
+      tc::mbar_init(&mbar[1], 1);
+    }
+    if (warp == 0) tc::tmem_alloc(tmem_slot, S::TMEM_COLS);
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+  }
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t tmem_diff = tmem;
+  const uint32_t tmem_lift = tmem + S::LIFT_COL;
+  constexpr uint32_t ID_DIFF = tc::idesc_bf16(128, S::ND);
+  constexpr uint32_t ID_LIFT = tc::idesc_bf16(128, S::NL);
+  const int64_t Knp = a.K * NP;
+
+  // epilogue geometry of this thread's TMEM lane
+  const int quad = warp & 3, half = warp >> 2;
+  const int lf = lane / F;                 // element within the quadrant
+  const int fown = lane - lf * F;          // own field
+  const bool lane_used = lf < EPW;
+  const int e_lane = quad * EPW + lf;
+  const uint32_t lane_addr = (uint32_t)(quad * 32) << 16;
+
+  uint32_t it = 0;
+  for (int64_t batch = blockIdx.x; batch < a.nbatch; batch += gridDim.x, ++it) {
+    const int64_t el0 = batch * EB;
+    const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
+
+    // ---- A: state -> FP32 copy + BF16 planes of q - q(node 0); geometry ----
+    // every load of a thread is issued before any is used
+    {
+#pragma unroll 1
+      for (int u0 = 0; u0 < S::NV; u0 += ROUND) {
+      double v[ROUND];
+#pragma unroll
+      for (int u = 0; u < ROUND; ++u) {
+        const int x = tid + (u0 + u) * SPLIT_THREADS;
+        const int f = x / (EB * NP), r = x % (EB * NP), e = r / NP;
+        if (u0 + u < S::NV && x < S::NVAL && e < ne) v[u] = a.q_in[f * Knp + el0 * NP + r];
+      }
+#pragma unroll
+      for (int u = 0; u < ROUND; ++u) {
+        const int x = tid + (u0 + u) * SPLIT_THREADS;
+        const int f = x / (EB * NP), r = x % (EB * NP), e = r / NP, j = r % NP;
+        if (u0 + u < S::NV && x < S::NVAL && e < ne) {
+          sq[f * EB * NP + r] = (float)v[u];
+          // the element's first node was just fetched: an L1 hit
+          const double v0 = __ldg(a.q_in + f * Knp + (el0 + e) * NP);
+          const int row = (e / EPW) * 32 + (e % EPW) * F + f;
+          store_split_f64(Aqh, Aql, kmajor_off(row, j, KD), v[u] - v0);
+        }
+      }
+      }
+    }
+    for (int x = tid; x < ne * G; x += SPLIT_THREADS) sgeo[x] = a.geo32[el0 * G + x];
+    for (int x = tid; x < ne * NF; x += SPLIT_THREADS) sconn[x] = a.conn[el0 * NF + x];
+    if constexpr (C != 0) {
+      for (int x = tid; x < ne * NP; x += SPLIT_THREADS) sc[x] = (float)a.coeff[el0 * NP + x];
+    }
+    tc::fence_proxy_async();
+    __syncthreads();
+
+    // ---- B: diff MMAs (one thread) ----
+    if (tid == 0) {
+      tc::fence_after_sync();
+      const uint32_t aq_h = tc::smem_u32(Aqh), aq_l = tc::smem_u32(Aql);
+      const uint32_t d_h = tc::smem_u32(smem + S::oDh), d_l = tc::smem_u32(smem + S::oDl);
+#pragma unroll
+      for (int kk = 0; kk < KD / 16; ++kk) {
+        const uint32_t off = kk * 256;
+        const uint64_t ah = tc::smem_desc(aq_h + off, 128, KD * 16);
+        const uint64_t al = tc::smem_desc(aq_l + off, 128, KD * 16);
+        const uint64_t bh = tc::smem_desc(d_h + off, 128, KD * 16);
+        const uint64_t bl = tc::smem_desc(d_l + off, 128, KD * 16);
+        tc::mma_bf16(tmem_diff, ah, bh, ID_DIFF, kk > 0 ? 1u : 0u);
+        tc::mma_bf16(tmem_diff, ah, bl, ID_DIFF, 1u);
+        tc::mma_bf16(tmem_diff, al, bh, ID_DIFF, 1u);
+      }
+      tc::mma_commit(&mbar[0]);
+    }
+
+    // ---- C: face fluxes (FP32) -> lift operand planes ----
+    {
+      // pass 1: every gather of the thread's face points (ext state, and
+      // the int state in FP64 for the jump)
+#pragma unroll 1
+      for (int u0 = 0; u0 < S::NFV; u0 += FROUND) {
+      float uPs[FROUND][NA];
+      bool okp[FROUND];
+#pragma unroll
+      for (int u = 0; u < FROUND; ++u) {
+        const int x = u0 + u < S::NFV ? tid + (u0 + u) * SPLIT_THREADS : S::NFACE;
+        const int e = x / NFPT, p = x % NFPT, face = p / NFP, k = p % NFP;
+        okp[u] = false;
+        if (x < S::NFACE && e < ne) {
+          const int2 cn = sconn[e * NF + face];
+          if (cn.x >= 0) {
+            const int nface = cn.y & 3, perm = cn.y >> 2;
+            if (nface < NF && perm < a.nperm && cn.x < a.K) {
+              const int nn = sfm[nface * NFP + ssh[perm * NFP + k]];
+              const int64_t gi = (int64_t)cn.x * NP + nn;
+              const int64_t li = (el0 + e) * NP + sfm[p];
+              if constexpr (JumpLinear<MODEL>::value) {
+#pragma unroll
+                for (int f = 0; f < F; ++f)
+                  uPs[u][f] = (float)(__ldg(a.q_in + f * Knp + li) -
+                                      __ldg(a.q_in + f * Knp + gi));
+              } else {
+                if constexpr (C != 0) uPs[u][0] = (float)__ldg(a.coeff + gi);
+#pragma unroll
+                for (int f = 0; f < F; ++f) uPs[u][C + f] = (float)__ldg(a.q_in + f * Knp + gi);
+              }
+              okp[u] = true;
+            } else {
+              atomicCAS(a.err, 0, DEV_BAD_CODE);
+            }
+          }
+        }
+      }
+      // pass 2: fluxes
+#pragma unroll
+      for (int u = 0; u < FROUND; ++u) {
+        const int x = u0 + u < S::NFV ? tid + (u0 + u) * SPLIT_THREADS : S::NFACE;
+        const int e = x / NFPT, p = x % NFPT, face = p / NFP, k = p % NFP;
+        if (x < S::NFACE && e < ne) {
+          const int lnode = sfm[p];
+          float uM[NA], uP[NA], n[DIM], fl[F];
+          if constexpr (C != 0) uM[0] = sc[e * NP + lnode];
+#pragma unroll
+          for (int f = 0; f < F; ++f) uM[C + f] = sq[f * EB * NP + e * NP + lnode];
+          const float* gf = sgeo + e * G + DIM * DIM + face * (DIM + 1);
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) n[d] = gf[d];
+          const float fscale = gf[DIM];
+          const int2 cn = sconn[e * NF + face];
+          bool have = true, bdry = false;
+          if (cn.x >= 0) {
+            have = okp[u];
+            if constexpr (JumpLinear<MODEL>::value) {
+#pragma unroll
+              for (int q = 0; q < NA; ++q) { uM[q] = uPs[u][q]; uP[q] = 0.f; }
+            } else {
+#pragma unroll
+              for (int q = 0; q < NA; ++q) uP[q] = uPs[u][q];
+            }
+          } else {
+            bdry = true;
+            float given = 0.f;
+            if (cn.y == HB_BC_GIVEN) {
+              const int64_t bi = (int64_t)(-1 - cn.x) * NFP + k;
+              if (a.bdry == nullptr || bi >= a.n_given) {
+                atomicCAS(a.err, 0, a.bdry == nullptr ? DEV_MISSING_INPUT : DEV_BAD_BDRY_INDEX);
+                have = false;
+              } else {
+                given = (float)__ldg(a.bdry + bi);
+              }
+            }
+            if (have) have = model_bc<MODEL, DIM, float>(a.mp, cn.y, uM, n, given, uP);
+          }
+          if (have) model_flux<MODEL, DIM, float>(a.mp, bdry, uM, uP, n, fl);
+          const int rowb = (e / EPW) * 32 + (e % EPW) * F;
+#pragma unroll
+          for (int f = 0; f < F; ++f)
+            store_split_f32(Afh, Afl, kmajor_off(rowb + f, p, KL), have ? fscale * fl[f] : 0.f);
+        }
+      }
+      }
+    }
+    tc::fence_proxy_async();
+    __syncthreads();
+
+    // ---- D: lift MMAs (one thread) ----
+    if (tid == 0) {
+      tc::fence_after_sync();
+      const uint32_t af_h = tc::smem_u32(Afh), af_l = tc::smem_u32(Afl);
+      const uint32_t l_h = tc::smem_u32(smem + S::oLh), l_l = tc::smem_u32(smem + S::oLl);
+#pragma unroll
+      for (int kk = 0; kk < KL / 16; ++kk) {
+        const uint32_t off = kk * 256;
+        const uint64_t ah = tc::smem_desc(af_h + off, 128, KL * 16);
+        const uint64_t al = tc::smem_desc(af_l + off, 128, KL * 16);
+        const uint64_t bh = tc::smem_desc(l_h + off, 128, KL * 16);
+        const uint64_t bl = tc::smem_desc(l_l + off, 128, KL * 16);
+        tc::mma_bf16(tmem_lift, ah, bh, ID_LIFT, kk > 0 ? 1u : 0u);
+        tc::mma_bf16(tmem_lift, ah, bl, ID_LIFT, 1u);
+        tc::mma_bf16(tmem_lift, al, bh, ID_LIFT, 1u);
+      }
+      tc::mma_commit(&mbar[1]);
+    }
+
+    // ---- E: TMEM -> chain rule, volume terms, + lift -> staged rhs ----
+    // one thread waits on the tensor core; the others sleep in the barrier
+    int late = 0;
+    if (tid == 0) {
+      const bool w0 = tc::mbar_wait(&mbar[0], it & 1u, MBAR_MAX_NS);
+      const bool w1 = tc::mbar_wait(&mbar[1], it & 1u, MBAR_MAX_NS);
+      late = !(w0 && w1);
+    }
+    if (__syncthreads_or(late)) {
+      // the MMAs did not complete in time: flag, give them one more bounded
+      // wait, then leave (TMEM is released below)
+      if (tid == 0) {
+        atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+        tc::mbar_wait(&mbar[0], it & 1u, MBAR_MAX_NS);
+        tc::mbar_wait(&mbar[1], it & 1u, MBAR_MAX_NS);
+      }
+      __syncthreads();
+      break;
+    }
+    tc::fence_after_sync();
+    {
+      const bool valid = lane_used && e_lane < ne;
+      const int e = valid ? e_lane : 0;
+      const float* ge = sgeo + e * G;
+      float gm[DIM][DIM];
+#pragma unroll
+      for (int r = 0; r < DIM; ++r)
+#pragma unroll
+        for (int x = 0; x < DIM; ++x) gm[r][x] = ge[r * DIM + x];
+      const int base = lf * F;
+      constexpr int I_END0 = S::NPH < NP ? S::NPH : NP;
+      const int i_lo = half ? S::NPH : 0;
+      const int i_hi = half ? NP : I_END0;
+#pragma unroll 1
+      for (int i0 = i_lo; i0 < i_hi; i0 += 4) {
+        float dv[DIM][4], lv[4];
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) tc::tmem_ld4(tmem_diff + lane_addr + r * NP + i0, dv[r]);
+        tc::tmem_ld4(tmem_lift + lane_addr + i0, lv);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const int i = i0 + c;
+          float g[DIM];
+#pragma unroll
+          for (int x = 0; x < DIM; ++x) {
+            float s = 0.f;
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) s += gm[r][x] * dv[r][c];
+            g[x] = s;
+          }
+          const float cnode = C ? sc[e * NP + i] : 0.f;
+          const float mine = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
+          if (valid && i < i_hi) {
+            const float src = a.source ? (float)a.source[(el0 + e) * NP + i] : 0.f;
+            sq[fown * EB * NP + e * NP + i] =
+                model_finish<MODEL, DIM, float>(a.mp, fown, mine, lv[c], src);
+          }
+        }
+      }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+
+    // ---- F: FP64 stage update (coalesced, loads batched) ----
+    {
+      constexpr int H = ROUND;
+#pragma unroll 1
+      for (int u0 = 0; u0 < S::NV; u0 += H) {
+        double rv[H], qv[H];
+        if (a.mode != 0) {
+#pragma unroll
+          for (int u = 0; u < H; ++u) {
+            const int x = tid + (u0 + u) * SPLIT_THREADS;
+            const int f = x / (EB * NP), r = x % (EB * NP), e = r / NP;
+            if (u0 + u < S::NV && x < S::NVAL && e < ne) {
+              const int64_t idx = f * Knp + el0 * NP + r;
+              rv[u] = a.res[idx];
+              qv[u] = a.q_in[idx];
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < H; ++u) {
+          const int x = tid + (u0 + u) * SPLIT_THREADS;
+          const int f = x / (EB * NP), r = x % (EB * NP), e = r / NP;
+          if (u0 + u < S::NV && x < S::NVAL && e < ne) {
+            const int64_t idx = f * Knp + el0 * NP + r;
+            const double rr = (double)sq[f * EB * NP + r];
+            if (a.mode == 0) {
+              a.q_out[idx] = rr;
+            } else {
+              const double nr = a.ra * rv[u] + a.dt * rr;
+              a.res[idx] = nr;
+              a.q_out[idx] = qv[u] + a.rb * nr;
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- tear-down ----
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, S::TMEM_COLS);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+struct SplitOps {
+  uint8_t* dev = nullptr;
+  int order = 0;
+};
+
+static uint16_t host_bf16(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return 0x7fc0;  // NaN
+  const uint32_t lsb = (u >> 16) & 1u;
+  u += 0x7fffu + lsb;
+  return (uint16_t)(u >> 16);
+}
+static float host_bf16_to_float(uint16_t h) {
+  uint32_t u = (uint32_t)h << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+// hi/lo planes of a (rows x cols) FP64 matrix in the canonical K-major image
+static void build_planes(const std::vector<double>& m, int rows, int cols, int rp, int kp,
+                         uint8_t* hi, uint8_t* lo) {
+  std::memset(hi, 0, (size_t)rp * kp * 2);
+  std::memset(lo, 0, (size_t)rp * kp * 2);
+  for (int r = 0; r < rows; ++r)
+    for (int k = 0; k < cols; ++k) {
+      const double v = m[(size_t)r * cols + k];
+      const uint16_t h = host_bf16((float)v);
+      const uint16_t l = host_bf16((float)(v - (double)host_bf16_to_float(h)));
+      const uint32_t off = kmajor_off(r, k, kp);
+      std::memcpy(hi + off, &h, 2);
+      std::memcpy(lo + off, &l, 2);
+    }
+}
+
+template <int MODEL, int DIM, int ORDER>
+static hb_status configure_split(Op* op) {
+  using S = Shape<MODEL, DIM, ORDER>;
+  Discr* d = op->d;
+  if constexpr (!S::FITS) {
+    return fail(HB_ERR_UNSUPPORTED, "BF16x3 kernel: element beyond one MMA (N <= 256)");
+  } else {
+    if (d->np != S::NP || d->nfp != S::NFP)
+      return fail(HB_ERR_INVALID_ARGUMENT, "element sizes do not match the order");
+    auto kern = rhs_split_kernel<MODEL, DIM, ORDER>;
+    int dev;
+    HB_CUDA(cudaGetDevice(&dev));
+    int max_optin = 0, sms = 0, smem_sm = 0;
+    HB_CUDA(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    HB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    HB_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    if (S::total > (uint32_t)max_optin)
+      return fail(HB_ERR_UNSUPPORTED, "BF16x3 kernel: element too large for shared memory");
+    // TMEM: at most 512 columns per SM are shared by the resident CTAs; pad
+    // the shared-memory request so that no more CTAs fit than TMEM allows.
+    const int max_ctas = 512 / (int)S::TMEM_COLS;
+    size_t smem = S::total;
+    if ((size_t)smem_sm / (smem + 1024) > (size_t)max_ctas)
+      smem = (size_t)smem_sm / max_ctas - 1024 + 16;
+    if (smem > (size_t)max_optin) smem = max_optin;
+    HB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    HB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // resident CTAs per SM from the kernel's own resource use (the runtime's
+    // occupancy query under-reports this kernel)
+    cudaFuncAttributes fa;
+    HB_CUDA(cudaFuncGetAttributes(&fa, kern));
+    int regs_sm = 0, thr_sm = 0;
+    HB_CUDA(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
+    HB_CUDA(cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev));
+    const int by_smem = (int)(smem_sm / (smem + 1024));
+    const int regs_cta = ((fa.numRegs * 32 + 255) / 256 * 256) * (SPLIT_THREADS / 32);
+    const int by_regs = regs_sm / std::max(regs_cta, 1);
+    const int per_sm = std::min(std::min(by_smem, by_regs), thr_sm / SPLIT_THREADS);
+    if (per_sm < 1) return fail(HB_ERR_UNSUPPORTED, "BF16x3 kernel does not fit on an SM");
+    if (per_sm > max_ctas) return fail(HB_ERR_UNSUPPORTED, "TMEM oversubscribed");
+    const int64_t nbatch = (d->K + S::EB - 1) / S::EB;
+    op->threads = SPLIT_THREADS;
+    op->blocks_per_sm = per_sm;
+    op->smem = smem;
+    op->grid = (int)std::min<int64_t>(nbatch, (int64_t)sms * per_sm);
+    op->elems_per_block = S::EB;
+    // operator images from the FP64 operators (host copies, transposed blob)
+    const int np = S::NP, nfpt = S::NFPT;
+    const double* h = reinterpret_cast<const double*>(d->host_blob.data());
+    const size_t ndm = (size_t)DIM * np * np;
+    std::vector<double> Dt((size_t)DIM * np * np);   // rows (r, i), cols j
+    for (int r = 0; r < DIM; ++r)
+      for (int j = 0; j < np; ++j)
+        for (int i = 0; i < np; ++i)
+          Dt[((size_t)r * np + i) * np + j] = h[((size_t)r * np + j) * np + i];
+    std::vector<double> Lt((size_t)np * nfpt);        // rows i, cols p
+    for (int k = 0; k < nfpt; ++k)
+      for (int i = 0; i < np; ++i) Lt[(size_t)i * nfpt + k] = h[ndm + (size_t)k * np + i];
+    const size_t bD = (size_t)S::ND * S::KD * 2, bL = (size_t)S::NL * S::KL * 2;
+    std::vector<uint8_t> img(2 * bD + 2 * bL);
+    build_planes(Dt, DIM * np, np, S::ND, S::KD, img.data(), img.data() + bD);
+    build_planes(Lt, np, nfpt, S::NL, S::KL, img.data() + 2 * bD, img.data() + 2 * bD + bL);
+    SplitOps* so = static_cast<SplitOps*>(op->split_ops);
+    if (cudaMalloc(&so->dev, img.size()) != cudaSuccess ||
+        cudaMemcpy(so->dev, img.data(), img.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(HB_ERR_CUDA, "cannot upload the split operator planes");
+    return HB_OK;
+  }
+}
+
+template <int MODEL, int DIM, int ORDER>
+static hb_status launch_split_t(Op* op, int mode, double ra, double rb, double dt,
+                                const void* q_in, void* q_out, void* res,
+                                const double* coeff, const double* bdry,
+                                const double* source, cudaStream_t s) {
+  using S = Shape<MODEL, DIM, ORDER>;
+  if constexpr (!S::FITS) {
+    return fail(HB_ERR_UNSUPPORTED, "BF16x3 kernel: element beyond one MMA");
+  } else {
+    Discr* d = op->d;
+    SplitOps* so = static_cast<SplitOps*>(op->split_ops);
+    SplitArgs a;
+    a.K = d->K;
+    a.nbatch = (d->K + S::EB - 1) / S::EB;
+    a.n_given = op->n_given;
+    a.nperm = d->nperm;
+    a.ops = so->dev;
+    a.geo32 = d->geo32;
+    a.conn = op->conn; a.fmask = d->fmask; a.shuffle = d->shuffle;
+    a.q_in = static_cast<const double*>(q_in);
+    a.q_out = static_cast<double*>(q_out);
+    a.res = static_cast<double*>(res);
+    a.coeff = coeff; a.bdry = bdry; a.source = source;
+    a.ra = ra; a.rb = rb; a.dt = dt; a.mode = mode;
+    a.mp = op->mp;
+    a.err = op->err_flag;
+    rhs_split_kernel<MODEL, DIM, ORDER><<<op->grid, op->threads, op->smem, s>>>(a);
+    HB_CUDA(cudaGetLastError());
+    return HB_OK;
+  }
+}
+
+// (model, dim, order) instances built into the library
+#define HB_SPLIT_INSTANCES(X)                                                          \
+  X(HB_MODEL_ADVECTION, 2, 3) X(HB_MODEL_ADVECTION, 2, 4) X(HB_MODEL_ADVECTION, 2, 5)  \
+  X(HB_MODEL_ADVECTION, 2, 6) X(HB_MODEL_ADVECTION, 3, 3) X(HB_MODEL_ADVECTION, 3, 4)  \
+  X(HB_MODEL_WAVE, 2, 3) X(HB_MODEL_WAVE, 2, 4) X(HB_MODEL_WAVE, 2, 5)                 \
+  X(HB_MODEL_WAVE, 2, 6) X(HB_MODEL_WAVE, 3, 3) X(HB_MODEL_WAVE, 3, 4)                 \
+  X(HB_MODEL_WAVE, 3, 5)                                                               \
+  X(HB_MODEL_VARWAVE, 2, 3) X(HB_MODEL_VARWAVE, 2, 4) X(HB_MODEL_VARWAVE, 2, 5)        \
+  X(HB_MODEL_VARWAVE, 2, 6) X(HB_MODEL_VARWAVE, 3, 3) X(HB_MODEL_VARWAVE, 3, 4)        \
+  X(HB_MODEL_MAXWELL, 3, 3) X(HB_MODEL_MAXWELL, 3, 4) X(HB_MODEL_MAXWELL, 3, 5)
+
+hb_status prepare_split(Op* op) {
+  Discr* d = op->d;
+  hb_status st = ensure_fp32(d);
+  if (st) return st;
+  op->split_ops = new SplitOps();
+  static_cast<SplitOps*>(op->split_ops)->order = d->order;
+  const int dim = d->dim, order = d->order;
+#define HB_CASE(M, D, O) \
+  if (op->model == M && dim == D && order == O) return configure_split<M, D, O>(op);
+  HB_SPLIT_INSTANCES(HB_CASE)
+#undef HB_CASE
+  return fail(HB_ERR_UNSUPPORTED,
+              "BF16x3 path: this (model, dimension, order) is not built (see "
+              "HB_SPLIT_INSTANCES)");
+}
+
+hb_status launch_split(Op* op, int mode, double ra, double rb, double dt,
+                       const void* q_in, void* q_out, void* res, const double* coeff,
+                       const double* bdry, const double* source, cudaStream_t s) {
+  const int dim = op->d->dim, order = op->d->order;
+#define HB_CASE(M, D, O)                                                              \
+  if (op->model == M && dim == D && order == O)                                       \
+    return launch_split_t<M, D, O>(op, mode, ra, rb, dt, q_in, q_out, res, coeff,    \
+                                   bdry, source, s);
+  HB_SPLIT_INSTANCES(HB_CASE)
+#undef HB_CASE
+  return fail(HB_ERR_UNSUPPORTED, "model/dimension/order combination not built");
+}
+
+void free_split(Op* op) {
+  SplitOps* so = static_cast<SplitOps*>(op->split_ops);
+  if (!so) return;
+  cudaFree(so->dev);
+  delete so;
+  op->split_ops = nullptr;
+}
+
+}  // namespace hb

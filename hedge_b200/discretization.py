@@ -447,6 +447,13 @@ class CompiledOperator:
         """Synchronise and raise if a kernel flagged bad input."""
         _native.check(self._lib.hb_op_check(self._handle, self._stream()))
 
+    def launch_info(self):
+        """{grid, threads, smem, elems_per_batch, ops_in_smem, blocks_per_sm}."""
+        info = (C.c_int64 * 6)()
+        _native.check(self._lib.hb_op_launch_info(self._handle, info, 6))
+        return dict(zip(["grid", "threads", "smem", "elems_per_batch", "ops_in_smem",
+                         "blocks_per_sm"], list(info)))
+
     def gather_map(self):
         """Device-expanded (int, ext) gather indices, [K*Nf*Nfp] each."""
         torch = _torch()

@@ -131,6 +131,11 @@ hb_status hb_gather_map(hb_op* op, int64_t* int_idx, int64_t* ext_idx,
  * boundary vector); the flag stays set. */
 hb_status hb_op_check(hb_op* op, void* stream);
 
+/* Launch configuration chosen at hb_op_create, for diagnostics: up to n of
+ * {grid, threads per CTA, dynamic shared bytes, elements per batch,
+ *  operators in shared memory (0/1), CTAs per SM}. */
+hb_status hb_op_launch_info(hb_op* op, int64_t* info, int32_t n);
+
 /* Thread-local text of the last error. */
 const char* hb_last_error_string(void);
 
