@@ -43,7 +43,7 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "bf16x3"])
+    p.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "bf16x3", "fp16x3"])
     p.add_argument("--n", type=int, default=20, help="cubes per axis")
     p.add_argument("--order", type=int, default=4)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -340,8 +340,8 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": {"fp64": "f64", "fp32": "f32", "bf16x3": "bf16x3+f32acc, f64 state"}[
-                args.precision],
+            "dtype": {"fp64": "f64", "fp32": "f32", "bf16x3": "bf16x3+f32acc, f64 state",
+                      "fp16x3": "fp16x3(scaled)+f32acc, f64 state"}[args.precision],
             "data": "synthetic",
             "config": {"workload": "maxwell3d_cavity_K48000_N4", "K": discr.K,
                        "order": args.order, "Np": discr.Np, "fields": 6,

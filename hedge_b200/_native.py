@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libhedge_b200.so")
 
 HB_OK, HB_ERR_INVALID_ARGUMENT, HB_ERR_UNSUPPORTED, HB_ERR_CUDA, HB_ERR_DEVICE_FLAG = range(5)
-PREC_FP64, PREC_FP32, PREC_BF16X3 = 0, 1, 2
+PREC_FP64, PREC_FP32, PREC_BF16X3, PREC_FP16X3 = 0, 1, 2, 3
 
 
 class HedgeB200Error(RuntimeError):
@@ -33,7 +33,7 @@ class hb_discr_desc(C.Structure):
                 ("num_elements", C.c_int64),
                 ("dmats", C.c_void_p), ("lift", C.c_void_p), ("geometry", C.c_void_p),
                 ("fmask", C.c_void_p), ("shuffle", C.c_void_p),
-                ("device", C.c_int32)]
+                ("device", C.c_int32), ("unit_nodes", C.c_void_p)]
 
 
 class hb_op_desc(C.Structure):

@@ -108,7 +108,8 @@ hb_status hb_discr_create(const hb_discr_desc* desc, hb_discr** out) {
   if (desc->nfaces != desc->dim + 1 || desc->np < 1 || desc->nfp < 1 ||
       desc->num_elements < 1 || desc->nperm < 1 || desc->nperm > 6)
     return fail(HB_ERR_INVALID_ARGUMENT, "inconsistent element sizes");
-  if (!desc->dmats || !desc->lift || !desc->geometry || !desc->fmask || !desc->shuffle)
+  if (!desc->dmats || !desc->lift || !desc->geometry || !desc->fmask || !desc->shuffle ||
+      !desc->unit_nodes)
     return fail(HB_ERR_INVALID_ARGUMENT, "null operator or geometry pointer");
   const int np = desc->np, nfp = desc->nfp, nf = desc->nfaces, dim = desc->dim;
   for (int x = 0; x < nf * nfp; ++x)
@@ -138,6 +139,7 @@ hb_status hb_discr_create(const hb_discr_desc* desc, hb_discr** out) {
     for (int k = 0; k < nf * nfp; ++k)
       h[nd + (size_t)k * np + i] = desc->lift[(size_t)i * nf * nfp + k];
   std::memcpy(h + nd + nl, desc->geometry, sizeof(double) * ng);
+  d->unit_nodes.assign(desc->unit_nodes, desc->unit_nodes + (size_t)np * dim);
   hb_status st;
   if ((st = upload(&d->dmats_t, h, nd)) || (st = upload(&d->lift_t, h + nd, nl)) ||
       (st = upload(&d->geo, h + nd + nl, ng)) ||
@@ -174,7 +176,7 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
   }
   if (desc->num_fields != F)
     return fail(HB_ERR_INVALID_ARGUMENT, "num_fields does not match the model");
-  if (desc->precision < HB_PREC_FP64 || desc->precision > HB_PREC_BF16X3)
+  if (desc->precision < HB_PREC_FP64 || desc->precision > HB_PREC_FP16X3)
     return fail(HB_ERR_INVALID_ARGUMENT, "unknown precision");
   if (!desc->conn) return fail(HB_ERR_INVALID_ARGUMENT, "null connectivity");
   if (model == HB_MODEL_MAXWELL && !(desc->eps > 0 && desc->mu > 0))
@@ -224,7 +226,7 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
       cudaMemset(op->err_flag, 0, sizeof(int)) != cudaSuccess)
     return bail(fail(HB_ERR_CUDA, "cannot allocate the device error flag"));
   if (op->precision == HB_PREC_FP32 && (st = ensure_fp32(d))) return bail(st);
-  if (op->precision == HB_PREC_BF16X3)
+  if (op->precision == HB_PREC_BF16X3 || op->precision == HB_PREC_FP16X3)
     st = prepare_split(op);
   else
     st = prepare_simt(op);
@@ -259,7 +261,7 @@ static hb_status run(Op* op, int mode, double a, double b, double dt, const void
   DeviceGuard g(op->d->device);
   if (!g.ok) return fail(HB_ERR_CUDA, "cannot select the CUDA device");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  if (op->precision == HB_PREC_BF16X3)
+  if (op->precision == HB_PREC_BF16X3 || op->precision == HB_PREC_FP16X3)
     return launch_split(op, mode, a, b, dt, q_in, q_out, res, coeff, bdry, source, s);
   return launch_simt(op, mode, a, b, dt, q_in, q_out, res, coeff, bdry, source, s);
 }

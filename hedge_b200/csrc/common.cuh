@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "../../include/hedge_b200.h"
 
@@ -54,6 +55,7 @@ struct Discr {
   int* shuffle = nullptr;      // [nperm][nfp]
   // host copies kept for split-operator construction
   std::string host_blob;
+  std::vector<double> unit_nodes;   // [np][dim]
 };
 
 struct Op {

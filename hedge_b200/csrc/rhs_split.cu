@@ -30,8 +30,10 @@
 // jit/flux.py:311-353 and 429-472, jit/lift.py:110-141,
 // jit/__init__.py:501-519, timestep/runge_kutta.py:123-128.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -45,7 +47,7 @@ hb_status ensure_fp32(Discr* d);
 
 constexpr int SPLIT_THREADS = 256;
 // register rounds: state values and face points a thread keeps in flight
-constexpr int ROUND = 9;
+constexpr int ROUND = 4;
 constexpr int FROUND = 4;
 // bounded wait for the tensor core: 2 s, far above any batch's MMA time
 constexpr uint64_t MBAR_MAX_NS = 2000000000ull;
@@ -53,6 +55,7 @@ constexpr uint64_t MBAR_MAX_NS = 2000000000ull;
 __host__ __device__ constexpr int ru16(int x) { return (x + 15) / 16 * 16; }
 __host__ __device__ constexpr int ru32(int x) { return (x + 31) / 32 * 32; }
 __host__ __device__ constexpr uint32_t al128(uint32_t x) { return (x + 127u) & ~127u; }
+__host__ __device__ constexpr uint32_t al16(uint32_t x) { return (x + 15u) & ~15u; }
 
 // Compile-time shape of one (model, dim, order) instance.
 template <int MODEL, int DIM, int ORDER>
@@ -76,7 +79,8 @@ struct Shape {
   static constexpr int NFACE = EB * NFPT;
   static constexpr int NFV = (NFACE + SPLIT_THREADS - 1) / SPLIT_THREADS;
   static constexpr int NPH = ((NP + 1) / 2 + 3) & ~3;  // node split of the epilogue
-  // shared-memory carve-up
+
+  // shared-memory carve-up (operand planes 128-byte aligned, the rest 16)
   static constexpr uint32_t oDh = 0;
   static constexpr uint32_t oDl = al128(oDh + ND * KD * 2);
   static constexpr uint32_t oLh = al128(oDl + ND * KD * 2);
@@ -85,14 +89,24 @@ struct Shape {
   static constexpr uint32_t oAql = al128(oAqh + 128 * KD * 2);
   static constexpr uint32_t oAfh = al128(oAql + 128 * KD * 2);
   static constexpr uint32_t oAfl = al128(oAfh + 128 * KL * 2);
-  static constexpr uint32_t osq = al128(oAfl + 128 * KL * 2);
-  static constexpr uint32_t osc = al128(osq + F * EB * NP * 4);
-  static constexpr uint32_t ogeo = al128(osc + C * EB * NP * 4);
-  static constexpr uint32_t oconn = al128(ogeo + EB * G * 4);
-  static constexpr uint32_t ofm = al128(oconn + EB * NF * 8);
-  static constexpr uint32_t osh = al128(ofm + NFPT * 4);
-  static constexpr uint32_t obar = al128(osh + 6 * NFP * 4);
-  static constexpr uint32_t total = al128(obar + 32);
+  static constexpr uint32_t osq = al128(oAfl + 128 * KL * 2);        // FP32 remainders / rhs
+  static constexpr uint32_t osv = al16(osq + F * EB * NP * 4);       // FP64 vertex values
+  static constexpr uint32_t olam = al16(osv + F * EB * (DIM + 1) * 8);  // FP64 weights
+  static constexpr uint32_t osc = al16(olam + NP * DIM * 8);
+  static constexpr uint32_t ogeo = al16(osc + C * EB * NP * 4);
+  static constexpr uint32_t onbr = al16(ogeo + EB * G * 4);          // int32 neighbours
+  static constexpr uint32_t ocode = al16(onbr + EB * NF * 4);        // uint8 face codes
+  static constexpr uint32_t ofm = al16(ocode + EB * NF);             // uint8 fmask
+  static constexpr uint32_t osh = al16(ofm + NFPT);                  // uint8 shuffles
+  static constexpr uint32_t overt = al16(osh + 6 * NFP);             // uint8 vertex nodes
+  static constexpr uint32_t ors = al16(overt + 4);                   // row maxima
+  static constexpr uint32_t obar = al16(ors + 4 * EPW * F * 4);
+  static constexpr uint32_t total = al16(obar + 24);
+  static constexpr uint32_t LIN_BYTES = 8 + NP * DIM * 8;  // vertex nodes + weights (image)
+  // the operand-plane region doubles as an FP64 staging area in phases A and F
+  static constexpr uint32_t STAGE_BYTES = osq - oAqh;
+  static constexpr int CH = (int)(STAGE_BYTES / 16u);   // (res, q) pairs per F chunk
+  static_assert(F * EB * NP * 8 <= (int)STAGE_BYTES, "state staging does not fit");
   static constexpr int TMEM_NEED = LIFT_COL + NL + 4;
   static constexpr uint32_t TMEM_COLS = TMEM_NEED <= 32 ? 32 : TMEM_NEED <= 64 ? 64
                                         : TMEM_NEED <= 128 ? 128 : TMEM_NEED <= 256 ? 256 : 512;
@@ -114,6 +128,7 @@ struct SplitArgs {
   const double* bdry;
   const double* source;
   double ra, rb, dt;
+  float op_scale_d, op_scale_l;   // operator plane scales (powers of two)
   int mode;
   ModelParams mp;
   int* err;
@@ -126,21 +141,41 @@ __host__ __device__ constexpr uint32_t kmajor_off(int row, int k, int kp) {
   return (uint32_t)((row >> 3) * (kp * 16) + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
 }
 
-__device__ __forceinline__ void store_split_f64(uint8_t* hi, uint8_t* lo, uint32_t off,
-                                                double v) {
-  const float vf = (float)v;
-  const __nv_bfloat16 h = __float2bfloat16_rn(vf);
-  const __nv_bfloat16 l = __float2bfloat16_rn((float)(v - (double)__bfloat162float(h)));
-  *reinterpret_cast<__nv_bfloat16*>(hi + off) = h;
-  *reinterpret_cast<__nv_bfloat16*>(lo + off) = l;
+// Plane types: BF16 split (PT_BF16, unscaled) or FP16 split of a row scaled
+// by a power of two that maps the row's largest magnitude into [2^13, 2^14)
+// (PT_FP16: 11 significant bits per plane, so hi*hi + hi*lo + lo*hi is ~8x
+// more accurate than the BF16 split at the same tensor-core cost).
+enum { PT_BF16 = 0, PT_FP16 = 1 };
+
+template <int PT>
+__device__ __forceinline__ void store_split(uint8_t* hi, uint8_t* lo, uint32_t off, float v) {
+  if constexpr (PT == PT_BF16) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+    *reinterpret_cast<__nv_bfloat16*>(hi + off) = h;
+    *reinterpret_cast<__nv_bfloat16*>(lo + off) = l;
+  } else {
+    const __half h = __float2half_rn(v);
+    const __half l = __float2half_rn(v - __half2float(h));
+    *reinterpret_cast<__half*>(hi + off) = h;
+    *reinterpret_cast<__half*>(lo + off) = l;
+  }
 }
 
-__device__ __forceinline__ void store_split_f32(uint8_t* hi, uint8_t* lo, uint32_t off,
-                                                float v) {
-  const __nv_bfloat16 h = __float2bfloat16_rn(v);
-  const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
-  *reinterpret_cast<__nv_bfloat16*>(hi + off) = h;
-  *reinterpret_cast<__nv_bfloat16*>(lo + off) = l;
+// power-of-two row scale from the bit pattern of the row's largest |value|
+__device__ __forceinline__ float row_scale(uint32_t maxbits) {
+  int e = (int)((maxbits >> 23) & 0xffu) - 13;   // max / 2^(e-127) in [2^13, 2^14)
+  e = e < 1 ? 1 : (e > 254 ? 254 : e);
+  return maxbits == 0 ? 1.0f : __uint_as_float((uint32_t)e << 23);
+}
+
+// Ampere-style asynchronous 8-byte global -> shared copy (no registers held)
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(tc::smem_u32(sdst)), "l"(gsrc)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
 // models whose numerical flux depends on the state only through the jump
@@ -201,23 +236,31 @@ __device__ __forceinline__ float volume_own(const ModelParams& mp, const float (
   }
 }
 
-template <int MODEL, int DIM, int ORDER>
+template <int MODEL, int DIM, int ORDER, int PT>
 __global__ void __launch_bounds__(SPLIT_THREADS, 2) rhs_split_kernel(SplitArgs a) {
   using S = Shape<MODEL, DIM, ORDER>;
   constexpr int F = S::F, C = S::C, NA = S::NA, NP = S::NP, NFP = S::NFP, NF = S::NF;
   constexpr int NFPT = S::NFPT, G = S::G, EPW = S::EPW, EB = S::EB;
-  constexpr int KD = S::KD, KL = S::KL;
+  constexpr int KD = S::KD, KL = S::KL, NV1 = DIM + 1;
   extern __shared__ __align__(128) uint8_t smem[];
   uint8_t* Aqh = smem + S::oAqh;
   uint8_t* Aql = smem + S::oAql;
   uint8_t* Afh = smem + S::oAfh;
   uint8_t* Afl = smem + S::oAfl;
-  float* sq = reinterpret_cast<float*>(smem + S::osq);    // state, then the staged rhs
+  // The batch's state is held as the FP64 values at each (field, element)'s
+  // vertex nodes (sv) plus FP32 remainders after their linear interpolant
+  // (sq); sq is later reused for the staged rhs.
+  float* sq = reinterpret_cast<float*>(smem + S::osq);
+  double* sv = reinterpret_cast<double*>(smem + S::osv);
+  const double* slam = reinterpret_cast<const double*>(smem + S::olam);  // [NP][DIM]
   float* sc = reinterpret_cast<float*>(smem + S::osc);
   float* sgeo = reinterpret_cast<float*>(smem + S::ogeo);
-  int2* sconn = reinterpret_cast<int2*>(smem + S::oconn);
-  int* sfm = reinterpret_cast<int*>(smem + S::ofm);
-  int* ssh = reinterpret_cast<int*>(smem + S::osh);
+  int* snbr = reinterpret_cast<int*>(smem + S::onbr);
+  uint8_t* scode = smem + S::ocode;
+  uint8_t* sfm = smem + S::ofm;
+  uint8_t* ssh = smem + S::osh;
+  const uint8_t* svert = smem + S::overt;                  // vertex nodes B, C(, D)
+  uint32_t* rsq = reinterpret_cast<uint32_t*>(smem + S::ors);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + S::obar);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + S::obar + 16);
 
@@ -241,8 +284,16 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2) rhs_split_kernel(SplitArgs a
     const uint4 z = make_uint4(0, 0, 0, 0);
     for (uint32_t o = S::oAqh + tid * 16; o < S::osq; o += SPLIT_THREADS * 16)
       *reinterpret_cast<uint4*>(smem + o) = z;
-    for (int x = tid; x < NFPT; x += SPLIT_THREADS) sfm[x] = a.fmask[x];
-    for (int x = tid; x < a.nperm * NFP; x += SPLIT_THREADS) ssh[x] = a.shuffle[x];
+    {
+      // image tail: 4 vertex-node bytes, 4 pad, then the FP64 weights
+      const uint8_t* lsrc = a.ops + 2 * dD + 2 * dL;
+      if (tid < 4) smem[S::overt + tid] = lsrc[tid];
+      double* lam = reinterpret_cast<double*>(smem + S::olam);
+      const double* lsrcd = reinterpret_cast<const double*>(lsrc + 8);
+      for (int x = tid; x < NP * DIM; x += SPLIT_THREADS) lam[x] = lsrcd[x];
+    }
+    for (int x = tid; x < NFPT; x += SPLIT_THREADS) sfm[x] = (uint8_t)a.fmask[x];
+    for (int x = tid; x < a.nperm * NFP; x += SPLIT_THREADS) ssh[x] = (uint8_t)a.shuffle[x];
     if (tid == 0) {
       tc::mbar_init(&mbar[0], 1);
       tc::mbar_init(&mbar[1], 1);
@@ -256,9 +307,18 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2) rhs_split_kernel(SplitArgs a
   const uint32_t tmem = *tmem_slot;
   const uint32_t tmem_diff = tmem;
   const uint32_t tmem_lift = tmem + S::LIFT_COL;
-  constexpr uint32_t ID_DIFF = tc::idesc_bf16(128, S::ND);
-  constexpr uint32_t ID_LIFT = tc::idesc_bf16(128, S::NL);
+  constexpr uint32_t ID_DIFF = tc::idesc_16bit(128, S::ND, PT == PT_BF16);
+  constexpr uint32_t ID_LIFT = tc::idesc_16bit(128, S::NL, true);
   const int64_t Knp = a.K * NP;
+
+  // FP64 linear interpolant of (field f, batch element e) at node j
+  auto lin_at = [&](int f, int e, int j) -> double {
+    const double* v = sv + (f * EB + e) * NV1;
+    double s = v[0];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) s += slam[j * DIM + d] * (v[1 + d] - v[0]);
+    return s;
+  };
 
   // epilogue geometry of this thread's TMEM lane
   const int quad = warp & 3, half = warp >> 2;
@@ -273,36 +333,63 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2) rhs_split_kernel(SplitArgs a
     const int64_t el0 = batch * EB;
     const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
 
-    // ---- A: state -> FP32 copy + BF16 planes of q - q(node 0); geometry ----
-    // every load of a thread is issued before any is used
+    // ---- A: vertex values (FP64), remainders (FP32), split planes ----
     {
-#pragma unroll 1
-      for (int u0 = 0; u0 < S::NV; u0 += ROUND) {
-      double v[ROUND];
-#pragma unroll
-      for (int u = 0; u < ROUND; ++u) {
-        const int x = tid + (u0 + u) * SPLIT_THREADS;
+      // the batch's state lands in the staging area by asynchronous copies
+      // (every copy of the batch in flight at once)
+      double* stg = reinterpret_cast<double*>(smem + S::oAqh);   // [F][EB][NP]
+#pragma unroll 4
+      for (int x = tid; x < S::NVAL; x += SPLIT_THREADS) {
         const int f = x / (EB * NP), r = x % (EB * NP), e = r / NP;
-        if (u0 + u < S::NV && x < S::NVAL && e < ne) v[u] = a.q_in[f * Knp + el0 * NP + r];
+        if (e < ne) cp_async8(stg + x, a.q_in + f * Knp + el0 * NP + r);
       }
-#pragma unroll
-      for (int u = 0; u < ROUND; ++u) {
-        const int x = tid + (u0 + u) * SPLIT_THREADS;
+      for (int x = tid; x < F * EB * NV1; x += SPLIT_THREADS) {
+        const int fe = x / NV1, vv = x % NV1, f = fe / EB, e = fe % EB;
+        const int node = vv == 0 ? 0 : svert[vv - 1];
+        if (e < ne) sv[x] = a.q_in[f * Knp + (el0 + e) * NP + node];
+      }
+      for (int x = tid; x < 4 * EPW * F; x += SPLIT_THREADS) rsq[x] = 0u;
+      for (int x = tid; x < ne * G; x += SPLIT_THREADS) sgeo[x] = a.geo32[el0 * G + x];
+      for (int x = tid; x < ne * NF; x += SPLIT_THREADS) {
+        const int2 cn = a.conn[el0 * NF + x];
+        snbr[x] = cn.x;
+        scode[x] = (uint8_t)cn.y;
+      }
+      if constexpr (C != 0) {
+        for (int x = tid; x < ne * NP; x += SPLIT_THREADS) sc[x] = (float)a.coeff[el0 * NP + x];
+      }
+      cp_async_wait_all();
+      __syncthreads();
+      // remainders after the element's linear interpolant through its vertex
+      // nodes (D_r maps that interpolant to the constants added back in the
+      // epilogue): only the remainder goes through the split
+#pragma unroll 4
+      for (int x = tid; x < S::NVAL; x += SPLIT_THREADS) {
         const int f = x / (EB * NP), r = x % (EB * NP), e = r / NP, j = r % NP;
-        if (u0 + u < S::NV && x < S::NVAL && e < ne) {
-          sq[f * EB * NP + r] = (float)v[u];
-          // the element's first node was just fetched: an L1 hit
-          const double v0 = __ldg(a.q_in + f * Knp + (el0 + e) * NP);
-          const int row = (e / EPW) * 32 + (e % EPW) * F + f;
-          store_split_f64(Aqh, Aql, kmajor_off(row, j, KD), v[u] - v0);
+        if (e < ne) {
+          const float rem = (float)(stg[x] - lin_at(f, e, j));
+          sq[x] = rem;
+          if constexpr (PT == PT_FP16) {
+            const int row = (e / EPW) * 32 + (e % EPW) * F + f;
+            atomicMax(&rsq[(row >> 5) * (EPW * F) + (row & 31)], __float_as_uint(fabsf(rem)));
+          }
         }
       }
+      __syncthreads();
+      // split pass over the whole plane (zeros in K padding and dead rows,
+      // which the staging overwrote)
+#pragma unroll 4
+      for (int x = tid; x < 128 * KD; x += SPLIT_THREADS) {
+        const int row = x / KD, j = x % KD;
+        const int q = row & 31, e = (row >> 5) * EPW + q / F, f = q % F;
+        float val = 0.f;
+        if (j < NP && q < EPW * F && e < ne) {
+          float inv = 1.0f;
+          if constexpr (PT == PT_FP16) inv = 1.0f / row_scale(rsq[(row >> 5) * (EPW * F) + q]);
+          val = sq[f * EB * NP + e * NP + j] * inv;
+        }
+        store_split<PT>(Aqh, Aql, kmajor_off(row, j, KD), val);
       }
-    }
-    for (int x = tid; x < ne * G; x += SPLIT_THREADS) sgeo[x] = a.geo32[el0 * G + x];
-    for (int x = tid; x < ne * NF; x += SPLIT_THREADS) sconn[x] = a.conn[el0 * NF + x];
-    if constexpr (C != 0) {
-      for (int x = tid; x < ne * NP; x += SPLIT_THREADS) sc[x] = (float)a.coeff[el0 * NP + x];
     }
     tc::fence_proxy_async();
     __syncthreads();
@@ -326,36 +413,47 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2) rhs_split_kernel(SplitArgs a
       tc::mma_commit(&mbar[0]);
     }
 
-    // ---- C: face fluxes (FP32) -> lift operand planes ----
-    {
-      // pass 1: every gather of the thread's face points (ext state, and
-      // the int state in FP64 for the jump)
+    // ---- C: face fluxes (FP32 on jumps formed in FP64) -> BF16 lift planes ----
 #pragma unroll 1
-      for (int u0 = 0; u0 < S::NFV; u0 += FROUND) {
+    for (int u0 = 0; u0 < S::NFV; u0 += FROUND) {
       float uPs[FROUND][NA];
       bool okp[FROUND];
+      // pass 1: ext-side values (global gathers for neighbours outside the batch)
 #pragma unroll
       for (int u = 0; u < FROUND; ++u) {
         const int x = u0 + u < S::NFV ? tid + (u0 + u) * SPLIT_THREADS : S::NFACE;
         const int e = x / NFPT, p = x % NFPT, face = p / NFP, k = p % NFP;
         okp[u] = false;
         if (x < S::NFACE && e < ne) {
-          const int2 cn = sconn[e * NF + face];
-          if (cn.x >= 0) {
-            const int nface = cn.y & 3, perm = cn.y >> 2;
-            if (nface < NF && perm < a.nperm && cn.x < a.K) {
+          const int nb = snbr[e * NF + face];
+          if (nb >= 0) {
+            const int code = scode[e * NF + face];
+            const int nface = code & 3, perm = code >> 2;
+            if (nface < NF && perm < a.nperm && nb < a.K) {
               const int nn = sfm[nface * NFP + ssh[perm * NFP + k]];
-              const int64_t gi = (int64_t)cn.x * NP + nn;
-              const int64_t li = (el0 + e) * NP + sfm[p];
+              const int64_t gi = (int64_t)nb * NP + nn;
+              const int lnode = sfm[p];
+              const int lb = (int)(nb - el0);   // neighbour inside this batch?
+              const bool inb = lb >= 0 && lb < ne;
               if constexpr (JumpLinear<MODEL>::value) {
+                // jump = (lin- - q+) in FP64 + remainder- in FP32
+#pragma unroll
+                for (int f = 0; f < F; ++f) {
+                  const double lm = lin_at(f, e, lnode);
+                  const float rm = sq[f * EB * NP + e * NP + lnode];
+                  if (inb)
+                    uPs[u][f] = (float)(lm - lin_at(f, lb, nn)) +
+                                (rm - sq[f * EB * NP + lb * NP + nn]);
+                  else
+                    uPs[u][f] = (float)(lm - __ldg(a.q_in + f * Knp + gi)) + rm;
+                }
+              } else {
+                if constexpr (C != 0)
+                  uPs[u][0] = inb ? sc[lb * NP + nn] : (float)__ldg(a.coeff + gi);
 #pragma unroll
                 for (int f = 0; f < F; ++f)
-                  uPs[u][f] = (float)(__ldg(a.q_in + f * Knp + li) -
-                                      __ldg(a.q_in + f * Knp + gi));
-              } else {
-                if constexpr (C != 0) uPs[u][0] = (float)__ldg(a.coeff + gi);
-#pragma unroll
-                for (int f = 0; f < F; ++f) uPs[u][C + f] = (float)__ldg(a.q_in + f * Knp + gi);
+                  uPs[u][C + f] = inb ? (float)lin_at(f, lb, nn) + sq[f * EB * NP + lb * NP + nn]
+                                      : (float)__ldg(a.q_in + f * Knp + gi);
               }
               okp[u] = true;
             } else {
@@ -364,7 +462,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2) rhs_split_kernel(SplitArgs a
           }
         }
       }
-      // pass 2: fluxes
+      // pass 2: fluxes, split straight into the BF16 lift planes
 #pragma unroll
       for (int u = 0; u < FROUND; ++u) {
         const int x = u0 + u < S::NFV ? tid + (u0 + u) * SPLIT_THREADS : S::NFACE;
@@ -372,45 +470,55 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2) rhs_split_kernel(SplitArgs a
         if (x < S::NFACE && e < ne) {
           const int lnode = sfm[p];
           float uM[NA], uP[NA], n[DIM], fl[F];
-          if constexpr (C != 0) uM[0] = sc[e * NP + lnode];
-#pragma unroll
-          for (int f = 0; f < F; ++f) uM[C + f] = sq[f * EB * NP + e * NP + lnode];
           const float* gf = sgeo + e * G + DIM * DIM + face * (DIM + 1);
 #pragma unroll
           for (int d = 0; d < DIM; ++d) n[d] = gf[d];
           const float fscale = gf[DIM];
-          const int2 cn = sconn[e * NF + face];
+          const int nb = snbr[e * NF + face];
           bool have = true, bdry = false;
-          if (cn.x >= 0) {
+          if (nb >= 0 && JumpLinear<MODEL>::value) {
             have = okp[u];
-            if constexpr (JumpLinear<MODEL>::value) {
 #pragma unroll
-              for (int q = 0; q < NA; ++q) { uM[q] = uPs[u][q]; uP[q] = 0.f; }
-            } else {
+            for (int q = 0; q < NA; ++q) { uM[q] = uPs[u][q]; uP[q] = 0.f; }
+          } else {
+            if constexpr (C != 0) uM[0] = sc[e * NP + lnode];
+#pragma unroll
+            for (int f = 0; f < F; ++f)
+              uM[C + f] = (float)lin_at(f, e, lnode) + sq[f * EB * NP + e * NP + lnode];
+            if (nb >= 0) {
+              have = okp[u];
 #pragma unroll
               for (int q = 0; q < NA; ++q) uP[q] = uPs[u][q];
-            }
-          } else {
-            bdry = true;
-            float given = 0.f;
-            if (cn.y == HB_BC_GIVEN) {
-              const int64_t bi = (int64_t)(-1 - cn.x) * NFP + k;
-              if (a.bdry == nullptr || bi >= a.n_given) {
-                atomicCAS(a.err, 0, a.bdry == nullptr ? DEV_MISSING_INPUT : DEV_BAD_BDRY_INDEX);
-                have = false;
-              } else {
-                given = (float)__ldg(a.bdry + bi);
+            } else {
+              bdry = true;
+              const int kind = scode[e * NF + face];
+              float given = 0.f;
+              if (kind == HB_BC_GIVEN) {
+                const int64_t bi = (int64_t)(-1 - nb) * NFP + k;
+                if (a.bdry == nullptr || bi >= a.n_given) {
+                  atomicCAS(a.err, 0, a.bdry == nullptr ? DEV_MISSING_INPUT : DEV_BAD_BDRY_INDEX);
+                  have = false;
+                } else {
+                  given = (float)__ldg(a.bdry + bi);
+                }
               }
+              if (have) have = model_bc<MODEL, DIM, float>(a.mp, kind, uM, n, given, uP);
             }
-            if (have) have = model_bc<MODEL, DIM, float>(a.mp, cn.y, uM, n, given, uP);
           }
           if (have) model_flux<MODEL, DIM, float>(a.mp, bdry, uM, uP, n, fl);
           const int rowb = (e / EPW) * 32 + (e % EPW) * F;
 #pragma unroll
           for (int f = 0; f < F; ++f)
-            store_split_f32(Afh, Afl, kmajor_off(rowb + f, p, KL), have ? fscale * fl[f] : 0.f);
+            store_split<PT_BF16>(Afh, Afl, kmajor_off(rowb + f, p, KL),
+                                 have ? fscale * fl[f] : 0.f);
         }
       }
+    }
+    // K padding of the lift planes (the staging area overwrote it)
+    if constexpr (KL > NFPT) {
+      for (int x = tid; x < 128 * (KL - NFPT); x += SPLIT_THREADS) {
+        const int row = x / (KL - NFPT), p = NFPT + x % (KL - NFPT);
+        store_split<PT_BF16>(Afh, Afl, kmajor_off(row, p, KL), 0.f);
       }
     }
     tc::fence_proxy_async();
@@ -465,6 +573,15 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2) rhs_split_kernel(SplitArgs a
 #pragma unroll
         for (int x = 0; x < DIM; ++x) gm[r][x] = ge[r * DIM + x];
       const int base = lf * F;
+      // reference derivatives of the removed linear interpolant: (q_v - q_A)/2
+      float lin[DIM];
+      {
+        const double* vv = sv + (fown * EB + e) * NV1;
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) lin[r] = (float)(0.5 * (vv[1 + r] - vv[0]));
+      }
+      float sdiff = a.op_scale_d;
+      if constexpr (PT == PT_FP16) sdiff *= row_scale(rsq[quad * (EPW * F) + (lane_used ? lane : 0)]);
       constexpr int I_END0 = S::NPH < NP ? S::NPH : NP;
       const int i_lo = half ? S::NPH : 0;
       const int i_hi = half ? NP : I_END0;
@@ -483,7 +600,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2) rhs_split_kernel(SplitArgs a
           for (int x = 0; x < DIM; ++x) {
             float s = 0.f;
 #pragma unroll
-            for (int r = 0; r < DIM; ++r) s += gm[r][x] * dv[r][c];
+            for (int r = 0; r < DIM; ++r) s += gm[r][x] * (dv[r][c] * sdiff + lin[r]);
             g[x] = s;
           }
           const float cnode = C ? sc[e * NP + i] : 0.f;
@@ -499,43 +616,44 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2) rhs_split_kernel(SplitArgs a
     tc::fence_before_sync();
     __syncthreads();
 
-    // ---- F: FP64 stage update (coalesced, loads batched) ----
+    // ---- F: FP64 stage update; residual and state staged by async copies,
+    // CH values at a time ----
     {
-      constexpr int H = ROUND;
+      double* stg = reinterpret_cast<double*>(smem + S::oAqh);  // [2][CH]
+      constexpr int FNP = EB * NP;
 #pragma unroll 1
-      for (int u0 = 0; u0 < S::NV; u0 += H) {
-        double rv[H], qv[H];
+      for (int x0 = 0; x0 < S::NVAL; x0 += S::CH) {
+        const int nx = S::NVAL - x0 < S::CH ? S::NVAL - x0 : S::CH;
         if (a.mode != 0) {
-#pragma unroll
-          for (int u = 0; u < H; ++u) {
-            const int x = tid + (u0 + u) * SPLIT_THREADS;
-            const int f = x / (EB * NP), r = x % (EB * NP), e = r / NP;
-            if (u0 + u < S::NV && x < S::NVAL && e < ne) {
+          for (int x = tid; x < nx; x += SPLIT_THREADS) {
+            const int g = x0 + x, f = g / FNP, r = g % FNP, e = r / NP;
+            if (e < ne) {
               const int64_t idx = f * Knp + el0 * NP + r;
-              rv[u] = a.res[idx];
-              qv[u] = a.q_in[idx];
+              cp_async8(stg + x, a.res + idx);
+              cp_async8(stg + S::CH + x, a.q_in + idx);
             }
           }
+          cp_async_wait_all();
+          __syncthreads();
         }
-#pragma unroll
-        for (int u = 0; u < H; ++u) {
-          const int x = tid + (u0 + u) * SPLIT_THREADS;
-          const int f = x / (EB * NP), r = x % (EB * NP), e = r / NP;
-          if (u0 + u < S::NV && x < S::NVAL && e < ne) {
+#pragma unroll 4
+        for (int x = tid; x < nx; x += SPLIT_THREADS) {
+          const int g = x0 + x, f = g / FNP, r = g % FNP, e = r / NP;
+          if (e < ne) {
             const int64_t idx = f * Knp + el0 * NP + r;
-            const double rr = (double)sq[f * EB * NP + r];
+            const double rr = (double)sq[g];
             if (a.mode == 0) {
               a.q_out[idx] = rr;
             } else {
-              const double nr = a.ra * rv[u] + a.dt * rr;
+              const double nr = a.ra * stg[x] + a.dt * rr;
               a.res[idx] = nr;
-              a.q_out[idx] = qv[u] + a.rb * nr;
+              a.q_out[idx] = stg[S::CH + x] + a.rb * nr;
             }
           }
         }
+        __syncthreads();
       }
     }
-    __syncthreads();
   }
 
   // ---- tear-down ----
@@ -550,6 +668,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2) rhs_split_kernel(SplitArgs a
 struct SplitOps {
   uint8_t* dev = nullptr;
   int order = 0;
+  float scale_d = 1.f, scale_l = 1.f;
 };
 
 static uint16_t host_bf16(float f) {
@@ -567,23 +686,80 @@ static float host_bf16_to_float(uint16_t h) {
   return f;
 }
 
-// hi/lo planes of a (rows x cols) FP64 matrix in the canonical K-major image
+static uint16_t host_fp16(float f) {
+  // round-to-nearest-even FP32 -> FP16 for normal-range values (the operator
+  // planes are scaled into [2^-14, 2^14))
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  const uint32_t sign = (u >> 16) & 0x8000u;
+  const int exp = (int)((u >> 23) & 0xff) - 127 + 15;
+  uint32_t mant = u & 0x7fffffu;
+  if (exp <= 0) {  // subnormal / zero in FP16
+    if (exp < -10) return (uint16_t)sign;
+    mant |= 0x800000u;
+    const int shift = 14 - exp;
+    uint32_t half = mant >> shift;
+    const uint32_t rem = mant & ((1u << shift) - 1), mid = 1u << (shift - 1);
+    if (rem > mid || (rem == mid && (half & 1u))) ++half;
+    return (uint16_t)(sign | half);
+  }
+  uint32_t half = ((uint32_t)exp << 10) | (mant >> 13);
+  const uint32_t rem = mant & 0x1fffu;
+  if (rem > 0x1000u || (rem == 0x1000u && (half & 1u))) ++half;
+  return (uint16_t)(sign | half);
+}
+static float host_fp16_to_float(uint16_t h) {
+  const uint32_t sign = (uint32_t)(h & 0x8000u) << 16;
+  const int exp = (h >> 10) & 0x1f;
+  const uint32_t mant = h & 0x3ffu;
+  float f;
+  if (exp == 0) {
+    f = std::ldexp((float)mant, -24);
+  } else {
+    f = std::ldexp((float)(mant | 0x400u), exp - 25);
+  }
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  u |= sign;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+// hi/lo planes of a (rows x cols) FP64 matrix (scaled by 1/scale) in the
+// canonical K-major image, BF16 or FP16
 static void build_planes(const std::vector<double>& m, int rows, int cols, int rp, int kp,
-                         uint8_t* hi, uint8_t* lo) {
+                         int pt, double scale, uint8_t* hi, uint8_t* lo) {
   std::memset(hi, 0, (size_t)rp * kp * 2);
   std::memset(lo, 0, (size_t)rp * kp * 2);
   for (int r = 0; r < rows; ++r)
     for (int k = 0; k < cols; ++k) {
-      const double v = m[(size_t)r * cols + k];
-      const uint16_t h = host_bf16((float)v);
-      const uint16_t l = host_bf16((float)(v - (double)host_bf16_to_float(h)));
+      const double v = m[(size_t)r * cols + k] / scale;
+      uint16_t h, l;
+      if (pt == PT_BF16) {
+        h = host_bf16((float)v);
+        l = host_bf16((float)(v - (double)host_bf16_to_float(h)));
+      } else {
+        h = host_fp16((float)v);
+        l = host_fp16((float)(v - (double)host_fp16_to_float(h)));
+      }
       const uint32_t off = kmajor_off(r, k, kp);
       std::memcpy(hi + off, &h, 2);
       std::memcpy(lo + off, &l, 2);
     }
 }
 
-template <int MODEL, int DIM, int ORDER>
+// power of two that maps max|m| into [2^13, 2^14) (FP16 planes), else 1
+static double plane_scale(const std::vector<double>& m, int pt) {
+  if (pt == PT_BF16) return 1.0;
+  double mx = 0;
+  for (double v : m) mx = std::max(mx, std::fabs(v));
+  if (mx == 0) return 1.0;
+  int e;
+  std::frexp(mx, &e);          // mx in [2^(e-1), 2^e)
+  return std::ldexp(1.0, e - 14);
+}
+
+template <int MODEL, int DIM, int ORDER, int PT>
 static hb_status configure_split(Op* op) {
   using S = Shape<MODEL, DIM, ORDER>;
   Discr* d = op->d;
@@ -592,7 +768,7 @@ static hb_status configure_split(Op* op) {
   } else {
     if (d->np != S::NP || d->nfp != S::NFP)
       return fail(HB_ERR_INVALID_ARGUMENT, "element sizes do not match the order");
-    auto kern = rhs_split_kernel<MODEL, DIM, ORDER>;
+    auto kern = rhs_split_kernel<MODEL, DIM, ORDER, PT>;
     int dev;
     HB_CUDA(cudaGetDevice(&dev));
     int max_optin = 0, sms = 0, smem_sm = 0;
@@ -642,10 +818,40 @@ static hb_status configure_split(Op* op) {
     for (int k = 0; k < nfpt; ++k)
       for (int i = 0; i < np; ++i) Lt[(size_t)i * nfpt + k] = h[ndm + (size_t)k * np + i];
     const size_t bD = (size_t)S::ND * S::KD * 2, bL = (size_t)S::NL * S::KL * 2;
-    std::vector<uint8_t> img(2 * bD + 2 * bL);
-    build_planes(Dt, DIM * np, np, S::ND, S::KD, img.data(), img.data() + bD);
-    build_planes(Lt, np, nfpt, S::NL, S::KL, img.data() + 2 * bD, img.data() + 2 * bD + bL);
+    std::vector<uint8_t> img(2 * bD + 2 * bL + S::LIN_BYTES);
+    {
+      // vertex nodes B, C(, D) of the reference element and the FP64 linear
+      // barycentric weights (1 + r_d)/2 of every node
+      uint8_t vert[4] = {0, 0, 0, 0};
+      for (int dd = 0; dd < DIM; ++dd) {
+        int best = -1;
+        for (int j = 0; j < np; ++j) {
+          bool hit = true;
+          for (int c = 0; c < DIM; ++c) {
+            const double want = (c == dd) ? 1.0 : -1.0;
+            if (std::fabs(d->unit_nodes[(size_t)j * DIM + c] - want) > 1e-12) hit = false;
+          }
+          if (hit) best = j;
+        }
+        if (best < 0) return fail(HB_ERR_INVALID_ARGUMENT, "reference element lacks vertex nodes");
+        vert[dd] = (uint8_t)best;
+      }
+      for (int c = 0; c < DIM; ++c)
+        if (std::fabs(d->unit_nodes[c] + 1.0) > 1e-12)
+          return fail(HB_ERR_INVALID_ARGUMENT, "node 0 is not the first vertex");
+      std::memcpy(img.data() + 2 * bD + 2 * bL, vert, 4);
+      double* lam = reinterpret_cast<double*>(img.data() + 2 * bD + 2 * bL + 8);
+      for (int j = 0; j < np; ++j)
+        for (int dd = 0; dd < DIM; ++dd)
+          lam[j * DIM + dd] = 0.5 * (1.0 + d->unit_nodes[(size_t)j * DIM + dd]);
+    }
+    const double sd = plane_scale(Dt, PT), sl = 1.0;   // the lift is always BF16
+    build_planes(Dt, DIM * np, np, S::ND, S::KD, PT, sd, img.data(), img.data() + bD);
+    build_planes(Lt, np, nfpt, S::NL, S::KL, PT_BF16, sl, img.data() + 2 * bD,
+                 img.data() + 2 * bD + bL);
     SplitOps* so = static_cast<SplitOps*>(op->split_ops);
+    so->scale_d = (float)sd;
+    so->scale_l = (float)sl;
     if (cudaMalloc(&so->dev, img.size()) != cudaSuccess ||
         cudaMemcpy(so->dev, img.data(), img.size(), cudaMemcpyHostToDevice) != cudaSuccess)
       return fail(HB_ERR_CUDA, "cannot upload the split operator planes");
@@ -653,7 +859,7 @@ static hb_status configure_split(Op* op) {
   }
 }
 
-template <int MODEL, int DIM, int ORDER>
+template <int MODEL, int DIM, int ORDER, int PT>
 static hb_status launch_split_t(Op* op, int mode, double ra, double rb, double dt,
                                 const void* q_in, void* q_out, void* res,
                                 const double* coeff, const double* bdry,
@@ -677,9 +883,11 @@ static hb_status launch_split_t(Op* op, int mode, double ra, double rb, double d
     a.res = static_cast<double*>(res);
     a.coeff = coeff; a.bdry = bdry; a.source = source;
     a.ra = ra; a.rb = rb; a.dt = dt; a.mode = mode;
+    a.op_scale_d = so->scale_d;
+    a.op_scale_l = so->scale_l;
     a.mp = op->mp;
     a.err = op->err_flag;
-    rhs_split_kernel<MODEL, DIM, ORDER><<<op->grid, op->threads, op->smem, s>>>(a);
+    rhs_split_kernel<MODEL, DIM, ORDER, PT><<<op->grid, op->threads, op->smem, s>>>(a);
     HB_CUDA(cudaGetLastError());
     return HB_OK;
   }
@@ -703,8 +911,11 @@ hb_status prepare_split(Op* op) {
   op->split_ops = new SplitOps();
   static_cast<SplitOps*>(op->split_ops)->order = d->order;
   const int dim = d->dim, order = d->order;
-#define HB_CASE(M, D, O) \
-  if (op->model == M && dim == D && order == O) return configure_split<M, D, O>(op);
+  const int pt = op->precision == HB_PREC_FP16X3 ? PT_FP16 : PT_BF16;
+#define HB_CASE(M, D, O)                                                       \
+  if (op->model == M && dim == D && order == O)                                \
+    return pt == PT_FP16 ? configure_split<M, D, O, PT_FP16>(op)               \
+                         : configure_split<M, D, O, PT_BF16>(op);
   HB_SPLIT_INSTANCES(HB_CASE)
 #undef HB_CASE
   return fail(HB_ERR_UNSUPPORTED,
@@ -716,10 +927,14 @@ hb_status launch_split(Op* op, int mode, double ra, double rb, double dt,
                        const void* q_in, void* q_out, void* res, const double* coeff,
                        const double* bdry, const double* source, cudaStream_t s) {
   const int dim = op->d->dim, order = op->d->order;
+  const int pt = op->precision == HB_PREC_FP16X3 ? PT_FP16 : PT_BF16;
 #define HB_CASE(M, D, O)                                                              \
   if (op->model == M && dim == D && order == O)                                       \
-    return launch_split_t<M, D, O>(op, mode, ra, rb, dt, q_in, q_out, res, coeff,    \
-                                   bdry, source, s);
+    return pt == PT_FP16                                                              \
+               ? launch_split_t<M, D, O, PT_FP16>(op, mode, ra, rb, dt, q_in, q_out,  \
+                                                  res, coeff, bdry, source, s)        \
+               : launch_split_t<M, D, O, PT_BF16>(op, mode, ra, rb, dt, q_in, q_out,  \
+                                                  res, coeff, bdry, source, s);
   HB_SPLIT_INSTANCES(HB_CASE)
 #undef HB_CASE
   return fail(HB_ERR_UNSUPPORTED, "model/dimension/order combination not built");

@@ -24,13 +24,14 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
   return d;                // base offset 0, layout type 0 (no swizzle)
 }
 
-// Instruction descriptor: BF16 x BF16 -> FP32, both operands K-major.
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
-  return (1u << 4)                      // D format F32
-         | (1u << 7)                    // A format BF16
-         | (1u << 10)                   // B format BF16
-         | ((uint32_t)(N >> 3) << 17)   // N / 8
-         | ((uint32_t)(M >> 4) << 24);  // M / 16
+// Instruction descriptor of kind::f16: A and B both BF16 (bf16 = true) or
+// both FP16, FP32 accumulation, both operands K-major.
+__host__ __device__ constexpr uint32_t idesc_16bit(int M, int N, bool bf16) {
+  return (1u << 4)                            // D format F32
+         | ((bf16 ? 1u : 0u) << 7)            // A format (0 F16, 1 BF16)
+         | ((bf16 ? 1u : 0u) << 10)           // B format, same as A
+         | ((uint32_t)(N >> 3) << 17)         // N / 8
+         | ((uint32_t)(M >> 4) << 24);        // M / 16
 }
 
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,

@@ -1,5 +1,6 @@
-"""BF16x3 split-precision tensor-core path (tcgen05) against the FP64 oracle:
-relative L2 error of one RHS and of LSRK4 steps."""
+"""Split-precision tensor-core paths (tcgen05) against the FP64 oracle:
+relative L2 error of one RHS and of LSRK4 steps.  "bf16x3" splits into BF16
+planes; "fp16x3" into FP16 planes of power-of-two-scaled rows."""
 import numpy as np
 import pytest
 
@@ -9,14 +10,20 @@ from test_gpu_parity import _fields, rect, box
 
 pytestmark = pytest.mark.gpu
 
-# Tolerance of one BF16x3 RHS against the FP64 oracle (relative L2).
-SPLIT_TOL = 1e-4
+# Tolerance of one split-precision RHS against the FP64 oracle (relative L2)
+# on rough fields (smooth modes + 10% uniform noise: large face jumps, where
+# the BF16 lift contraction dominates the error of both variants)
+TOL = {"bf16x3": 1e-5, "fp16x3": 1e-5}
+# ... and on the benchmark's smooth cavity field, where the differentiation
+# dominates and the scaled FP16 split meets 1e-6
+TOL_SMOOTH = {"bf16x3": 1e-5, "fp16x3": 1e-6}
+PRECS = ["bf16x3", "fp16x3"]
 
 
-def _split_err(discr, op, seed=0, bc_in=None, c_field=None):
+def _split_err(discr, op, seed=0, bc_in=None, c_field=None, precision="bf16x3"):
     from oracle import OracleRHS
     ot = op.op_template()
-    comp = discr.compile(ot, precision="bf16x3")
+    comp = discr.compile(ot, precision=precision)
     if c_field is not None:
         comp.set_coefficient(c_field)
     q = _fields(discr, ot.n_fields, seed)
@@ -26,42 +33,62 @@ def _split_err(discr, op, seed=0, bc_in=None, c_field=None):
     return rel_l2(got.cpu().numpy().reshape(ref.shape), ref)
 
 
-@pytest.mark.parametrize("n,order", [(2, 4), (3, 4), (2, 3)])
-def test_split_maxwell(cuda_device, n, order):
+@pytest.mark.parametrize("precision", PRECS)
+@pytest.mark.parametrize("n,order", [(2, 4), (3, 4), (2, 3), (2, 5)])
+def test_split_maxwell(cuda_device, n, order, precision):
     d = hb.Discretization(box(n, 0.05, 5), order=order)
-    err = _split_err(d, hb.MaxwellOperator(1.0, 1.0, flux_type=1))
-    print("bf16x3 maxwell n=%d N=%d rel-L2 %.3e" % (n, order, err))
-    assert err <= SPLIT_TOL
+    err = _split_err(d, hb.MaxwellOperator(1.0, 1.0, flux_type=1), precision=precision)
+    print("%s maxwell n=%d N=%d rel-L2 %.3e" % (precision, n, order, err))
+    assert err <= TOL[precision]
 
 
-def test_split_advection_2d(cuda_device):
+@pytest.mark.parametrize("precision", PRECS)
+def test_split_advection_2d(cuda_device, precision):
     d = hb.Discretization(rect(9, True, 0.02, 0), order=4)
-    err = _split_err(d, hb.StrongAdvectionOperator(np.array([1.0, 0.5]), flux_type="upwind"))
-    print("bf16x3 advection rel-L2 %.3e" % err)
-    assert err <= SPLIT_TOL
+    err = _split_err(d, hb.StrongAdvectionOperator(np.array([1.0, 0.5]), flux_type="upwind"),
+                     precision=precision)
+    print("%s advection rel-L2 %.3e" % (precision, err))
+    assert err <= TOL[precision]
 
 
-def test_split_wave_3d(cuda_device):
+@pytest.mark.parametrize("precision", PRECS)
+def test_split_wave_3d(cuda_device, precision):
     d = hb.Discretization(box(2, 0.05, 3), order=4)
-    err = _split_err(d, hb.StrongWaveOperator(1.0, 3, flux_type="upwind"))
-    print("bf16x3 wave3d rel-L2 %.3e" % err)
-    assert err <= SPLIT_TOL
+    err = _split_err(d, hb.StrongWaveOperator(1.0, 3, flux_type="upwind"), precision=precision)
+    print("%s wave3d rel-L2 %.3e" % (precision, err))
+    assert err <= TOL[precision]
 
 
-def test_split_varwave_2d(cuda_device):
+@pytest.mark.parametrize("precision", PRECS)
+def test_split_varwave_2d(cuda_device, precision):
     d = hb.Discretization(rect(8, False, 0.02, 4), order=5)
     c = np.repeat(np.random.default_rng(4).uniform(0.8, 1.2, d.K), d.Np)
     op = hb.VariableVelocityStrongWaveOperator(c, 2, flux_type="upwind")
-    err = _split_err(d, op, c_field=c)
-    print("bf16x3 varwave2d rel-L2 %.3e" % err)
-    assert err <= SPLIT_TOL
+    err = _split_err(d, op, c_field=c, precision=precision)
+    print("%s varwave2d rel-L2 %.3e" % (precision, err))
+    assert err <= TOL[precision]
 
 
-def test_split_lsrk_steps(cuda_device):
-    """Fused BF16x3 RHS + FP64 stage update over 5 steps vs the FP64 oracle."""
+@pytest.mark.parametrize("precision", PRECS)
+def test_split_cavity_rhs(cuda_device, precision):
+    """The benchmark's field (cavity mode + 1e-3 noise) on a 6^3 box."""
+    import bench
+    from oracle import OracleRHS
+    _, _, d, op = bench.build_problem(6, 4, precision)
+    w = bench.cavity_ic(d)
+    ref = OracleRHS(d, op.op_template())(w)
+    got = op.bind(d)(0.0, w).cpu().numpy()
+    err = rel_l2(got, ref)
+    print("%s cavity rhs rel-L2 %.3e" % (precision, err))
+    assert err <= TOL_SMOOTH[precision]
+
+
+@pytest.mark.parametrize("precision", PRECS)
+def test_split_lsrk_steps(cuda_device, precision):
+    """Fused split RHS + FP64 stage update over 5 steps vs the FP64 oracle."""
     import torch
     from oracle import OracleRHS
-    d = hb.Discretization(box(2, 0.05, 1), order=4, precision="bf16x3")
+    d = hb.Discretization(box(2, 0.05, 1), order=4, precision=precision)
     op = hb.MaxwellOperator(1.0, 1.0, flux_type=1)
     rhs = op.bind(d)
     x = d.nodes
@@ -77,5 +104,5 @@ def test_split_lsrk_steps(cuda_device):
         yo, res = orc.lsrk4_step(yo, s * dt, dt, res)
     rhs.compiled.check()
     err = rel_l2(y.cpu().numpy().reshape(yo.shape), yo)
-    print("bf16x3 5 LSRK4 steps rel-L2 %.3e" % err)
-    assert err <= SPLIT_TOL
+    print("%s 5 LSRK4 steps rel-L2 %.3e" % (precision, err))
+    assert err <= 2e-4
