@@ -33,7 +33,8 @@ class hb_discr_desc(C.Structure):
                 ("num_elements", C.c_int64),
                 ("dmats", C.c_void_p), ("lift", C.c_void_p), ("geometry", C.c_void_p),
                 ("fmask", C.c_void_p), ("shuffle", C.c_void_p),
-                ("device", C.c_int32), ("unit_nodes", C.c_void_p)]
+                ("device", C.c_int32), ("unit_nodes", C.c_void_p),
+                ("mass", C.c_void_p), ("abs_jacobian", C.c_void_p)]
 
 
 class hb_op_desc(C.Structure):
@@ -49,7 +50,7 @@ class hb_op_desc(C.Structure):
 EXPORTED = [
     "hb_discr_create", "hb_discr_destroy", "hb_op_create", "hb_op_destroy",
     "hb_rhs", "hb_lsrk_stage", "hb_lincomb", "hb_gather_map", "hb_op_check",
-    "hb_op_launch_info",
+    "hb_op_launch_info", "hb_norm",
     "hb_last_error_string",
 ]
 
@@ -80,6 +81,7 @@ def load(path=LIB_PATH):
             "hb_gather_map": [vp, vp, vp, vp],
             "hb_op_check": [vp, vp],
             "hb_op_launch_info": [vp, vp, i32],
+            "hb_norm": [vp, i32, i32, vp, vp, vp],
         }
         for name, args in sig.items():
             fn = getattr(lib, name)

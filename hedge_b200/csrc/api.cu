@@ -50,6 +50,7 @@ static void free_discr(Discr* d) {
   cudaFree(d->dmats_t); cudaFree(d->lift_t); cudaFree(d->geo);
   cudaFree(d->dmats_t32); cudaFree(d->lift_t32); cudaFree(d->geo32);
   cudaFree(d->fmask); cudaFree(d->shuffle);
+  cudaFree(d->mass); cudaFree(d->absjac); cudaFree(d->norm_partials);
   delete d;
 }
 
@@ -109,7 +110,7 @@ hb_status hb_discr_create(const hb_discr_desc* desc, hb_discr** out) {
       desc->num_elements < 1 || desc->nperm < 1 || desc->nperm > 6)
     return fail(HB_ERR_INVALID_ARGUMENT, "inconsistent element sizes");
   if (!desc->dmats || !desc->lift || !desc->geometry || !desc->fmask || !desc->shuffle ||
-      !desc->unit_nodes)
+      !desc->unit_nodes || !desc->mass || !desc->abs_jacobian)
     return fail(HB_ERR_INVALID_ARGUMENT, "null operator or geometry pointer");
   const int np = desc->np, nfp = desc->nfp, nf = desc->nfaces, dim = desc->dim;
   for (int x = 0; x < nf * nfp; ++x)
@@ -144,9 +145,19 @@ hb_status hb_discr_create(const hb_discr_desc* desc, hb_discr** out) {
   if ((st = upload(&d->dmats_t, h, nd)) || (st = upload(&d->lift_t, h + nd, nl)) ||
       (st = upload(&d->geo, h + nd + nl, ng)) ||
       (st = upload(&d->fmask, desc->fmask, (size_t)nf * nfp)) ||
-      (st = upload(&d->shuffle, desc->shuffle, (size_t)desc->nperm * nfp))) {
+      (st = upload(&d->shuffle, desc->shuffle, (size_t)desc->nperm * nfp)) ||
+      (st = upload(&d->mass, desc->mass, (size_t)np * np)) ||
+      (st = upload(&d->absjac, desc->abs_jacobian, (size_t)d->K))) {
     free_discr(d);
     return st;
+  }
+  {
+    const int epb = norm_elems_per_block(np);
+    d->norm_blocks = (int)((d->K + epb - 1) / epb);
+    if (cudaMalloc(&d->norm_partials, sizeof(double) * d->norm_blocks) != cudaSuccess) {
+      free_discr(d);
+      return fail(HB_ERR_CUDA, "cannot allocate the norm partial sums");
+    }
   }
   *out = reinterpret_cast<hb_discr*>(d);
   return HB_OK;
@@ -308,6 +319,18 @@ hb_status hb_op_launch_info(hb_op* handle, int64_t* info, int32_t n) {
                         op->ops_in_smem, op->blocks_per_sm};
   for (int k = 0; k < n && k < 6; ++k) info[k] = v[k];
   return HB_OK;
+}
+
+hb_status hb_norm(hb_discr* discr, int32_t nfields, int32_t dtype, const void* u,
+                  double* out, void* stream) {
+  if (!discr || !u || !out) return fail(HB_ERR_INVALID_ARGUMENT, "null argument");
+  if (nfields < 1 || (dtype != 0 && dtype != 1))
+    return fail(HB_ERR_INVALID_ARGUMENT, "bad field count or dtype");
+  Discr* d = reinterpret_cast<Discr*>(discr);
+  DeviceGuard g(d->device);
+  if (!g.ok) return fail(HB_ERR_CUDA, "cannot select the CUDA device");
+  return launch_norm(d->K, d->np, nfields, dtype, d->mass, d->absjac, u, d->norm_partials,
+                     d->norm_blocks, out, reinterpret_cast<cudaStream_t>(stream));
 }
 
 hb_status hb_op_check(hb_op* handle, void* stream) {

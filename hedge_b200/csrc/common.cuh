@@ -51,6 +51,10 @@ struct Discr {
   float* dmats_t32 = nullptr;
   float* lift_t32 = nullptr;
   float* geo32 = nullptr;
+  double* mass = nullptr;      // [np][np] reference mass matrix
+  double* absjac = nullptr;    // [K]
+  double* norm_partials = nullptr;  // one FP64 partial sum per norm block
+  int norm_blocks = 0;
   int* fmask = nullptr;        // [nfaces][nfp]
   int* shuffle = nullptr;      // [nperm][nfp]
   // host copies kept for split-operator construction
@@ -77,6 +81,13 @@ struct Op {
 };
 
 hb_status check_device_flag(Op* op, cudaStream_t s);
+
+// energy norm (norm.cu)
+constexpr int NORM_THREADS = 256;
+int norm_elems_per_block(int np);
+hb_status launch_norm(int64_t K, int np, int nfields, int dtype, const double* mass,
+                      const double* absjac, const void* u, double* partials, int nblocks,
+                      double* out, cudaStream_t s);
 
 // kernel launchers (rhs_simt.cu)
 hb_status launch_simt(Op* op, int mode, double a, double b, double dt,

@@ -222,15 +222,22 @@ class Discretization:
         return torch.einsum("i,...ki,k->...", M.sum(0), uu, J)
 
     def norm(self, u, p=2):
-        """L2 norm sqrt(sum_k |J_k| u_k^T M u_k), summed over leading field
-        axes (FP64)."""
+        """L2 (energy) norm sqrt(sum_k |J_k| u_k^T M u_k), summed over leading
+        field axes; FP64 accumulation on the device (hb_norm)."""
         if p != 2:
             raise NotImplementedError("only the L2 norm")
         torch = _torch()
-        M, J = self._mass_dev
-        u = self.to_device(u, torch.float64)
-        uu = u.reshape(-1, self.K, self.Np)
-        return float(torch.sqrt(torch.einsum("fki,ij,fkj,k->", uu, M, uu, J)))
+        uu = u if isinstance(u, torch.Tensor) and u.is_cuda else self.to_device(u)
+        if uu.dtype not in (torch.float64, torch.float32):
+            uu = uu.double()
+        uu = uu.reshape(-1, len(self)).contiguous()
+        out = torch.empty(1, dtype=torch.float64, device=self.device)
+        lib = _native.load()
+        _native.check(lib.hb_norm(self._native_handle(), uu.shape[0],
+                                  0 if uu.dtype == torch.float64 else 1, uu.data_ptr(),
+                                  out.data_ptr(),
+                                  torch.cuda.current_stream(self.device).cuda_stream))
+        return float(out.item())
 
     def get_point_evaluator(self, point, thresh=0.0):
         """(discretization/__init__.py:1217-1249)"""
@@ -259,14 +266,17 @@ class Discretization:
                 geo=self.geometry,
                 fmask=np.ascontiguousarray(ld.fmask, dtype=np.int32),
                 shuffle=np.ascontiguousarray(ld.face_shuffle_table, dtype=np.int32),
-                unit_nodes=np.ascontiguousarray(ld.unit_nodes, dtype=np.float64))
+                unit_nodes=np.ascontiguousarray(ld.unit_nodes, dtype=np.float64),
+                mass=np.ascontiguousarray(ld.mass_matrix, dtype=np.float64),
+                absjac=np.ascontiguousarray(np.abs(self.mesh.jacobians), dtype=np.float64))
             k = self._keep
             desc = _native.hb_discr_desc(
                 self.dimensions, self.order, self.Np, self.Nfp, self.Nfaces,
                 len(ld.face_shuffle_perms), self.K,
                 k["dmats"].ctypes.data, k["lift"].ctypes.data, k["geo"].ctypes.data,
                 k["fmask"].ctypes.data, k["shuffle"].ctypes.data,
-                int(self.device.index or 0), k["unit_nodes"].ctypes.data)
+                int(self.device.index or 0), k["unit_nodes"].ctypes.data,
+                k["mass"].ctypes.data, k["absjac"].ctypes.data)
             h = C.c_void_p()
             _native.check(lib.hb_discr_create(C.byref(desc), C.byref(h)))
             self._handle = h

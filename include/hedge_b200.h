@@ -68,6 +68,8 @@ typedef struct {
   const int32_t* shuffle;  /* [nperm][nfp] face-node shuffle per vertex perm */
   int32_t device;          /* CUDA device ordinal */
   const double* unit_nodes;/* [np][dim] reference-element nodes (r, s, t) */
+  const double* mass;      /* [np][np] reference mass matrix (V V^T)^-1 */
+  const double* abs_jacobian; /* [K] |det A| of each element's map */
 } hb_discr_desc;
 
 /* Replaces the device-side part of Discretization.__init__ /
@@ -128,6 +130,14 @@ hb_status hb_lincomb(int64_t n, int32_t dtype, double a, const void* x,
  * face-pair index lists of hedge/discretization/data.py:199-248. */
 hb_status hb_gather_map(hb_op* op, int64_t* int_idx, int64_t* ext_idx,
                         void* stream);
+
+/* out[0] = sqrt(sum_f sum_k |J_k| u_fk^T M u_fk): the L2 (energy) norm of
+ * nfields volume vectors u [nfields][K*Np] of dtype (0 = FP64, 1 = FP32),
+ * accumulated in FP64 with a fixed-order (deterministic) reduction.  out is
+ * one device double.  Replaces Discretization.norm
+ * (hedge/discretization/__init__.py:1126-1139). */
+hb_status hb_norm(hb_discr* discr, int32_t nfields, int32_t dtype, const void* u,
+                  double* out, void* stream);
 
 /* Synchronises `stream` and returns HB_ERR_DEVICE_FLAG if a kernel of this
  * operator flagged bad input (out-of-range neighbour or code, missing

@@ -221,3 +221,22 @@ def test_invalid_connectivity_rejected(cuda_device):
     st = _native.load().hb_op_create(d._native_handle(), C.byref(desc), C.byref(h))
     assert st == _native.HB_ERR_INVALID_ARGUMENT
     assert b"out of range" in _native.load().hb_last_error_string()
+
+
+def test_energy_norm_matches_oracle(cuda_device):
+    """hb_norm (FP64, deterministic) vs sqrt(sum |J| u^T M u) in numpy."""
+    for m, order in ((rect(9, True, 0.02, 0), 4), (box(3, 0.05, 1), 4)):
+        d = hb.Discretization(m, order=order)
+        u = _fields(d, 3, 5)
+        M = d.ldis.mass_matrix
+        J = np.abs(m.jacobians)
+        uu = u.reshape(3, d.K, d.Np)
+        ref = np.sqrt(np.einsum("fki,ij,fkj,k->", uu, M, uu, J))
+        got = d.norm(u)
+        assert abs(got - ref) <= 1e-13 * ref
+        assert d.norm(u) == got   # bitwise reproducible
+        d32 = hb.Discretization(m, order=order, default_scalar_type=np.float32)
+        u32 = u.astype(np.float32)
+        uu32 = u32.astype(np.float64).reshape(3, d.K, d.Np)
+        ref32 = np.sqrt(np.einsum("fki,ij,fkj,k->", uu32, M, uu32, J))
+        assert abs(d32.norm(u32) - ref32) <= 1e-12 * ref32
