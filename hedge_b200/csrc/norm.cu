@@ -6,6 +6,9 @@
 // forms u_i (M u)_i |J| in FP64 and the block reduces them in a fixed tree
 // order into partials[b].  Pass 2: one block reduces the partials in a fixed
 // order and writes sqrt(sum).  The result is bitwise reproducible.
+#include <cstdio>
+#include <mutex>
+
 #include "common.cuh"
 
 namespace hb {
@@ -80,3 +83,81 @@ hb_status launch_norm(int64_t K, int np, int nfields, int dtype, const double* m
 }
 
 }  // namespace hb
+
+// ---------------------------------------------------------------------------
+// Allocation-free energy norm (hb_norm_noalloc).  Same two kernels as hb_norm;
+// the per-block partial sums live in a fixed device array of this file instead
+// of a buffer owned by an hb_discr.  Some callers cannot allocate device
+// memory while they run: code that holds no hb_discr (it brings its own mass
+// matrix and Jacobians) and must not grow the footprint of a time loop that
+// has reserved the device's memory for its fields, or that must not let an
+// allocation synchronise the device between two time steps.  They call this
+// entry point instead.
+//
+// The array keeps whatever the last call on the device left in it.  Nothing
+// in it has to start at zero: the partial pass of a call writes every slot
+// [0, blocks) that the final pass of the same call reads.  Two calls whose
+// kernels overlap on one device (other streams, other host threads) share the
+// array and race; callers serialise them.
+// ---------------------------------------------------------------------------
+namespace hb {
+
+static __device__ __align__(256) double norm_noalloc_partials[HB_NORM_NOALLOC_MAX_BLOCKS];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[kMaxDevices] = {};
+
+// Address of the array on the current device, looked up once per device.
+// The lookup may load this library's device code on that device, which is why
+// the first call on a device belongs before any stream capture.
+hb_status noalloc_scratch(double** ptr) {
+  int dev = -1;
+  HB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices)
+    return fail(HB_ERR_UNSUPPORTED, "norm_noalloc: device index beyond 63");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, norm_noalloc_partials);
+    if (e != cudaSuccess || !p)
+      return cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidSymbol,
+                       "norm_noalloc: cudaGetSymbolAddress of the scratch array");
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *ptr = g_noalloc_ptr[dev];
+  return HB_OK;
+}
+}  // namespace
+
+}  // namespace hb
+
+extern "C" hb_status hb_norm_noalloc(int64_t num_elements, int32_t np, int32_t nfields,
+                                     int32_t dtype, const double* mass,
+                                     const double* abs_jacobian, const void* u, double* out,
+                                     void* stream) {
+  using namespace hb;
+  if (!mass || !abs_jacobian || !u || !out)
+    return fail(HB_ERR_INVALID_ARGUMENT, "norm_noalloc: null argument");
+  if (num_elements < 1 || nfields < 1 || (dtype != 0 && dtype != 1))
+    return fail(HB_ERR_INVALID_ARGUMENT,
+                "norm_noalloc: need num_elements >= 1, nfields >= 1, dtype 0 or 1");
+  if (np < 1 || np > NORM_THREADS)
+    return fail(HB_ERR_UNSUPPORTED, "norm_noalloc: element node count must be 1..256");
+  const int epb = norm_elems_per_block(np);
+  const int64_t max_elements = (int64_t)HB_NORM_NOALLOC_MAX_BLOCKS * epb;
+  if (num_elements > max_elements) {
+    char msg[160];
+    snprintf(msg, sizeof msg,
+             "norm_noalloc: %lld elements exceed the scratch limit of %lld for %d nodes "
+             "per element (8192 blocks of %d elements); use hb_norm",
+             (long long)num_elements, (long long)max_elements, (int)np, epb);
+    return fail(HB_ERR_INVALID_ARGUMENT, msg);
+  }
+  double* partials = nullptr;
+  const hb_status st = noalloc_scratch(&partials);
+  if (st != HB_OK) return st;
+  return launch_norm(num_elements, np, nfields, dtype, mass, abs_jacobian, u, partials,
+                     HB_NORM_NOALLOC_MAX_BLOCKS, out, reinterpret_cast<cudaStream_t>(stream));
+}

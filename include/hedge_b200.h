@@ -139,6 +139,31 @@ hb_status hb_gather_map(hb_op* op, int64_t* int_idx, int64_t* ext_idx,
 hb_status hb_norm(hb_discr* discr, int32_t nfields, int32_t dtype, const void* u,
                   double* out, void* stream);
 
+/* Allocation-free variant of hb_norm.  This entry point has no counterpart in
+ * the reference.  It is for callers that may not allocate device memory while
+ * they run: code that holds no hb_discr and brings its own device copies of
+ * the element mass matrix `mass` [np][np] (FP64) and |J_k| `abs_jacobian`
+ * [num_elements] (FP64), inside a time loop that has reserved the device's
+ * memory for its fields or must not let an allocation synchronise the device
+ * between steps.  Same result and reduction order as hb_norm on the current
+ * CUDA device; u and out as for hb_norm, all pointers on the current device.
+ *
+ * The partial sums go to a fixed device array inside the library of
+ * HB_NORM_NOALLOC_MAX_BLOCKS doubles (64 KiB), so the call allocates nothing.
+ * Limit: num_elements <= HB_NORM_NOALLOC_MAX_BLOCKS * max(1, 256 / np)
+ * (e.g. 57344 tetrahedra at order 4, np = 35); larger meshes are rejected
+ * with HB_ERR_INVALID_ARGUMENT and must use hb_norm.
+ * The first call on a device looks up the array's device address (which may
+ * load the library's device code) and should come before any stream capture.
+ * The array keeps the last call's contents; nothing in it has to start at
+ * zero, since each call writes every partial it reads.  Calls whose kernels
+ * overlap on one device (several streams or host threads) share the array and
+ * race: serialise them. */
+#define HB_NORM_NOALLOC_MAX_BLOCKS 8192
+hb_status hb_norm_noalloc(int64_t num_elements, int32_t np, int32_t nfields,
+                          int32_t dtype, const double* mass, const double* abs_jacobian,
+                          const void* u, double* out, void* stream);
+
 /* Synchronises `stream` and returns HB_ERR_DEVICE_FLAG if a kernel of this
  * operator flagged bad input (out-of-range neighbour or code, missing
  * boundary vector); the flag stays set. */

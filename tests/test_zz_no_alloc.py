@@ -1,0 +1,59 @@
+"""hb_norm_noalloc through the C ABI against hb_norm on the same inputs.
+
+Two calls in a row (a larger mesh, then a smaller one, so the second call
+reads a scratch array the first one left full), each within 1e-13 of hb_norm,
+plus the size limit rejected before any launch."""
+import numpy as np
+import pytest
+
+import hedge_b200 as hb
+from hedge_b200 import _native
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-13
+
+
+def _case(n, order, nfields, seed):
+    import torch
+    d = hb.Discretization(hb.make_box_tet_mesh(n=(n, n, n), jitter=0.05, seed=1),
+                          order=order)
+    rng = np.random.default_rng(seed)
+    u = torch.as_tensor(rng.standard_normal((nfields, len(d))), device=d.device)
+    mass = torch.as_tensor(np.ascontiguousarray(d.ldis.mass_matrix), device=d.device)
+    absjac = torch.as_tensor(np.abs(d.mesh.jacobians), device=d.device)
+    return d, u, mass, absjac
+
+
+def _noalloc(d, u, mass, absjac):
+    import torch
+    out = torch.full((1,), -1.0, dtype=torch.float64, device=d.device)
+    lib = _native.load()
+    _native.check(lib.hb_norm_noalloc(
+        d.K, d.Np, u.shape[0], 0, mass.data_ptr(), absjac.data_ptr(), u.data_ptr(),
+        out.data_ptr(), torch.cuda.current_stream(d.device).cuda_stream))
+    return float(out.item())
+
+
+def test_noalloc_norm_matches_hb_norm_twice(cuda_device):
+    big = _case(6, 4, 6, 3)       # K = 1296, 186 partial blocks
+    small = _case(2, 3, 3, 4)     # K = 48, 4 partial blocks
+    for d, u, mass, absjac in (big, small):
+        want = d.norm(u)
+        got = _noalloc(d, u, mass, absjac)
+        assert abs(got - want) <= TOL * want, (got, want)
+    d, u, mass, absjac = big
+    assert abs(_noalloc(d, u, mass, absjac) - d.norm(u)) <= TOL * d.norm(u)
+
+
+def test_noalloc_norm_rejects_oversized_mesh(cuda_device):
+    import torch
+    d, u, mass, absjac = _case(2, 4, 1, 5)
+    lib = _native.load()
+    epb = max(1, 256 // d.Np)
+    too_many = 8192 * epb + 1
+    out = torch.zeros(1, dtype=torch.float64, device=d.device)
+    st = lib.hb_norm_noalloc(too_many, d.Np, 1, 0, mass.data_ptr(), absjac.data_ptr(),
+                             u.data_ptr(), out.data_ptr(), None)
+    assert st == _native.HB_ERR_INVALID_ARGUMENT
+    assert b"scratch limit" in lib.hb_last_error_string()
