@@ -1,5 +1,5 @@
-// Split-precision (BF16x3) fused DG right-hand side + LSRK stage on the
-// sm_100a tensor cores (tcgen05.mma kind::f16, FP32 accumulation in TMEM).
+// Split-precision (BF16x3 / FP16x3) fused DG right-hand side + LSRK stage on
+// the sm_100a tensor cores (tcgen05.mma kind::f16, FP32 accumulation in TMEM).
 //
 // The two contractions of the DG operator run as GEMMs whose M dimension is
 // the batch's (element, field) pairs -- one TMEM lane per pair, EPW = 32/F
@@ -11,22 +11,29 @@
 //   lift:  L[(e,f)][i] = sum_p flux[(e,f)][p] * LIFT[i][p]
 //          A = face fluxes, B = LIFT^T, M = 128, N = Np, K = Nf*Nfp
 //
-// Each operand x is split into BF16 planes hi = bf16(x), lo = bf16(x - hi);
-// a product is hi*hi + hi*lo + lo*hi, accumulated in FP32 ("BF16x3").  The
-// operator planes are built once on the host in the tensor core's canonical
-// K-major layout and stay resident in shared memory; the state and flux
-// planes are written per batch.  Two accuracy measures keep smooth fields
-// accurate: the state is split after subtracting its value at the
-// element's first node (D_r annihilates constants, so only the
-// within-element variation goes through BF16), and face jumps of the
-// models whose numerical flux is linear in the jump are formed in FP64.
+// Each operand x is split into 16-bit planes hi = h(x), lo = h(x - hi); a
+// product is hi*hi + hi*lo + lo*hi, accumulated in FP32.  The operator planes
+// are built once on the host in the tensor core's canonical K-major layout
+// and stay resident in shared memory; the state and flux planes are written
+// per batch.  The state is split after subtracting its element-wise linear
+// interpolant through the vertex nodes (D_r maps it to constants that the
+// epilogue adds back exactly), so only the within-element variation goes
+// through 16 bits; face jumps are formed in FP64.
 //
-// One lane holds every derivative d_r q_f(x_i) of its (e, f): the chain
-// rule needs only the element's metric, and the model's volume terms
-// (curl, div, grad) gather the element's other fields with warp shuffles.
-// Element shapes are compile-time (template on the order) so that all
-// batch index arithmetic folds to constants.  The RK stage update (res, q)
-// stays in FP64.  Restated reference loops: jit/diff.py:137-175,
+// One CTA per SM runs a persistent loop over batches with warp roles:
+//   * a producer warp streams each batch's FP64 state, geometry and face
+//     table into one of two stage buffers (cp.async, completion counted on
+//     an mbarrier) while the previous batch is computed, and the batch's
+//     residual into a residual buffer once the previous update is done;
+//   * 12 consumer warps split the state, issue the diff MMA (one thread),
+//     evaluate the face fluxes into the lift planes, issue the lift MMA, read
+//     the accumulators back (chain rule, volume terms, + lift: one lane holds
+//     every derivative of its (e, f); the model's curl/div/grad gather the
+//     element's other fields with warp shuffles) and apply the FP64 stage
+//     update from shared memory with coalesced stores.
+// All waits are bounded (2 s); a timeout sets the device error flag and the
+// CTA leaves after releasing its TMEM.  Element shapes are compile-time
+// (template on the order).  Restated reference loops: jit/diff.py:137-175,
 // jit/flux.py:311-353 and 429-472, jit/lift.py:110-141,
 // jit/__init__.py:501-519, timestep/runge_kutta.py:123-128.
 #include <cuda_bf16.h>
@@ -45,12 +52,26 @@ namespace hb {
 
 hb_status ensure_fp32(Discr* d);
 
-constexpr int SPLIT_THREADS = 256;
-// register rounds: state values and face points a thread keeps in flight
-constexpr int ROUND = 4;
-constexpr int FROUND = 4;
-// bounded wait for the tensor core: 2 s, far above any batch's MMA time
+// consumer warps (the phases of a batch) plus one producer warp that streams
+// the next batch's state and the current batch's residual into shared memory
+// (a multiple of 4: warp w reads TMEM lane quadrant w % 4).  Registers are
+// split over the SM's 4 sub-partitions (16K each) by warp: 13 warps put at
+// most 4 warps on one, which leaves 128 registers per thread.
+#ifndef HB_SPLIT_NCW
+#define HB_SPLIT_NCW 12
+#endif
+constexpr int NCW = HB_SPLIT_NCW;
+static_assert(NCW % 4 == 0, "consumer warps must cover the TMEM quadrants evenly");
+constexpr int CONSUMERS = NCW * 32;
+constexpr int SPLIT_THREADS = CONSUMERS + 32;
+// face points a consumer thread keeps in flight (fewer for many fields)
+template <int NA, int NFV>
+struct FaceRound { static constexpr int value = NFV < (NA > 4 ? 3 : 4) ? NFV : (NA > 4 ? 3 : 4); };
+// bounded waits (tensor core, producer/consumer hand-offs): 2 s, far above any
+// batch's time
 constexpr uint64_t MBAR_MAX_NS = 2000000000ull;
+// dynamic shared memory one CTA may use on sm_100
+constexpr uint32_t SMEM_LIMIT = 232448;
 
 __host__ __device__ constexpr int ru16(int x) { return (x + 15) / 16 * 16; }
 __host__ __device__ constexpr int ru32(int x) { return (x + 31) / 32 * 32; }
@@ -74,43 +95,58 @@ struct Shape {
   static constexpr int KD = ru16(NP), KL = ru16(NFPT);
   static constexpr int ND = ru16(DIM * NP), NL = ru16(NP);
   static constexpr int LIFT_COL = ru32(ND);
-  static constexpr int NVAL = F * EB * NP;
-  static constexpr int NV = (NVAL + SPLIT_THREADS - 1) / SPLIT_THREADS;
+  static constexpr int FNP = EB * NP;              // values of one field in a batch
+  static constexpr int NVAL = F * FNP;
   static constexpr int NFACE = EB * NFPT;
-  static constexpr int NFV = (NFACE + SPLIT_THREADS - 1) / SPLIT_THREADS;
-  static constexpr int NPH = ((NP + 1) / 2 + 3) & ~3;  // node split of the epilogue
+  static constexpr int NFV = (NFACE + CONSUMERS - 1) / CONSUMERS;
+  // epilogue: the NCW/4 warps of a TMEM quadrant split the nodes, NPQ each (even)
+  static constexpr int NPQ = (((NP + NCW / 4 - 1) / (NCW / 4)) + 1) & ~1;
+  // split pass: (quadrant, 8-column chunk) items, IPW per consumer warp
+  static constexpr int NITEM = 4 * (KD / 8);
+  static constexpr int IPW = (NITEM + NCW - 1) / NCW;
 
-  // shared-memory carve-up (operand planes 128-byte aligned, the rest 16)
+  static constexpr uint32_t bD = ND * KD * 2, bL = NL * KL * 2;
+  static constexpr uint32_t bAq = 128 * KD * 2, bAf = 128 * KL * 2;
+  static constexpr uint32_t bState = NVAL * 8;
+  // one stage buffer: state [F][EB][NP] FP64, geometry [EB][G] FP32,
+  // face table [EB][NF] int2, coefficient [EB][NP] FP64
+  static constexpr uint32_t sGeo = bState;
+  static constexpr uint32_t sConn = al16(sGeo + EB * G * 4);
+  static constexpr uint32_t sCoef = al16(sConn + EB * NF * 8);
+  static constexpr uint32_t bStage = al128(sCoef + (C ? FNP * 8 : 0));
+
   static constexpr uint32_t oDh = 0;
-  static constexpr uint32_t oDl = al128(oDh + ND * KD * 2);
-  static constexpr uint32_t oLh = al128(oDl + ND * KD * 2);
-  static constexpr uint32_t oLl = al128(oLh + NL * KL * 2);
-  static constexpr uint32_t oAqh = al128(oLl + NL * KL * 2);
-  static constexpr uint32_t oAql = al128(oAqh + 128 * KD * 2);
-  static constexpr uint32_t oAfh = al128(oAql + 128 * KD * 2);
-  static constexpr uint32_t oAfl = al128(oAfh + 128 * KL * 2);
-  static constexpr uint32_t osq = al128(oAfl + 128 * KL * 2);        // FP32 remainders / rhs
-  static constexpr uint32_t osv = al16(osq + F * EB * NP * 4);       // FP64 vertex values
-  static constexpr uint32_t olam = al16(osv + F * EB * (DIM + 1) * 8);  // FP64 weights
-  static constexpr uint32_t osc = al16(olam + NP * DIM * 8);
-  static constexpr uint32_t ogeo = al16(osc + C * EB * NP * 4);
-  static constexpr uint32_t onbr = al16(ogeo + EB * G * 4);          // int32 neighbours
-  static constexpr uint32_t ocode = al16(onbr + EB * NF * 4);        // uint8 face codes
-  static constexpr uint32_t ofm = al16(ocode + EB * NF);             // uint8 fmask
-  static constexpr uint32_t osh = al16(ofm + NFPT);                  // uint8 shuffles
-  static constexpr uint32_t overt = al16(osh + 6 * NFP);             // uint8 vertex nodes
-  static constexpr uint32_t ors = al16(overt + 4);                   // row maxima
-  static constexpr uint32_t obar = al16(ors + 4 * EPW * F * 4);
-  static constexpr uint32_t total = al16(obar + 24);
+  static constexpr uint32_t oDl = al128(oDh + bD);
+  static constexpr uint32_t oLh = al128(oDl + bD);
+  static constexpr uint32_t oLl = al128(oLh + bL);
+  static constexpr uint32_t oAqh = al128(oLl + bL);
+  static constexpr uint32_t oAql = al128(oAqh + bAq);
+  static constexpr uint32_t oAfh = al128(oAql + bAq);
+  static constexpr uint32_t oAfl = al128(oAfh + bAf);
+  static constexpr uint32_t osq = oAqh;   // FP32 rhs staging reuses the state planes
+  static constexpr uint32_t ostg = al128(oAfl + bAf);
+  static constexpr uint32_t SMALL = 1024 + NP * DIM * 8 + NFPT + 6 * NFP + 4 + 128 * 4 + 80;
+  // double-buffered stages and a residual buffer when they fit, else fewer
+  static constexpr bool fits(int nstg, bool res) {
+    return ostg + nstg * bStage + (res ? bState : 0) + SMALL <= SMEM_LIMIT;
+  }
+  static constexpr int NSTG = fits(2, false) ? 2 : 1;
+  static constexpr bool RES = fits(NSTG, true);
+  static constexpr uint32_t ores = ostg + NSTG * bStage;
+  static constexpr uint32_t olam = al16(ores + (RES ? bState : 0));   // FP64 weights
+  static constexpr uint32_t ofm = al16(olam + NP * DIM * 8);           // uint8 fmask
+  static constexpr uint32_t osh = al16(ofm + NFPT);                    // uint8 shuffles
+  static constexpr uint32_t overt = al16(osh + 6 * NFP);               // uint8 vertex nodes
+  static constexpr uint32_t ors = al16(overt + 4);                     // row maxima
+  static constexpr uint32_t obar = al16(ors + 128 * 4);                // 8 mbarriers + TMEM slot
+  static constexpr uint32_t total = al16(obar + 80);
   static constexpr uint32_t LIN_BYTES = 8 + NP * DIM * 8;  // vertex nodes + weights (image)
-  // the operand-plane region doubles as an FP64 staging area in phases A and F
-  static constexpr uint32_t STAGE_BYTES = osq - oAqh;
-  static constexpr int CH = (int)(STAGE_BYTES / 16u);   // (res, q) pairs per F chunk
-  static_assert(F * EB * NP * 8 <= (int)STAGE_BYTES, "state staging does not fit");
+  static_assert(F * FNP * 4 <= (int)(2 * bAq), "rhs staging does not fit the state planes");
   static constexpr int TMEM_NEED = LIFT_COL + NL + 4;
   static constexpr uint32_t TMEM_COLS = TMEM_NEED <= 32 ? 32 : TMEM_NEED <= 64 ? 64
                                         : TMEM_NEED <= 128 ? 128 : TMEM_NEED <= 256 ? 256 : 512;
-  static constexpr bool FITS = ND <= 256 && NL <= 256 && TMEM_NEED <= 512;
+  static constexpr bool FITS = ND <= 256 && NL <= 256 && TMEM_NEED <= 512 &&
+                               total <= SMEM_LIMIT;
 };
 
 struct SplitArgs {
@@ -174,9 +210,6 @@ __device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(tc::smem_u32(sdst)), "l"(gsrc)
                : "memory");
 }
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-}
 
 // models whose numerical flux depends on the state only through the jump
 // q- - q+ (so f(q-, q+) == f(q- - q+, 0))
@@ -236,40 +269,66 @@ __device__ __forceinline__ float volume_own(const ModelParams& mp, const float (
   }
 }
 
+// consumer-only barrier (named barrier 1; the producer warp never joins it)
+__device__ __forceinline__ void cbar() {
+  asm volatile("bar.sync 1, %0;" ::"n"(CONSUMERS) : "memory");
+}
+__device__ __forceinline__ int cbar_or(int v) {
+  int r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.s32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.s32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"(v), "n"(CONSUMERS)
+      : "memory");
+  return r;
+}
+__device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(tc::smem_u32(sdst)), "l"(gsrc)
+               : "memory");
+}
+// the mbarrier counts one arrival once all earlier cp.async of this thread landed
+__device__ __forceinline__ void cp_async_arrive(uint64_t* mbar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(tc::smem_u32(mbar))
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_drain() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// mbarriers: 0 diff MMA, 1 lift MMA, 2..3 stage full, 4 residual full,
+// 5..6 stage free, 7 residual free
+enum { MB_DIFF = 0, MB_LIFT = 1, MB_FULL = 2, MB_RES_FULL = 4, MB_FREE = 5, MB_RES_FREE = 7 };
+
 template <int MODEL, int DIM, int ORDER, int PT>
-__global__ void __launch_bounds__(SPLIT_THREADS, 2) rhs_split_kernel(SplitArgs a) {
+__global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a) {
   using S = Shape<MODEL, DIM, ORDER>;
   constexpr int F = S::F, C = S::C, NA = S::NA, NP = S::NP, NFP = S::NFP, NF = S::NF;
-  constexpr int NFPT = S::NFPT, G = S::G, EPW = S::EPW, EB = S::EB;
-  constexpr int KD = S::KD, KL = S::KL, NV1 = DIM + 1;
+  constexpr int NFPT = S::NFPT, G = S::G, EPW = S::EPW, EB = S::EB, FNP = S::FNP;
+  constexpr int KD = S::KD, KL = S::KL, NSTG = S::NSTG;
   extern __shared__ __align__(128) uint8_t smem[];
   uint8_t* Aqh = smem + S::oAqh;
   uint8_t* Aql = smem + S::oAql;
   uint8_t* Afh = smem + S::oAfh;
   uint8_t* Afl = smem + S::oAfl;
-  // The batch's state is held as the FP64 values at each (field, element)'s
-  // vertex nodes (sv) plus FP32 remainders after their linear interpolant
-  // (sq); sq is later reused for the staged rhs.
-  float* sq = reinterpret_cast<float*>(smem + S::osq);
-  double* sv = reinterpret_cast<double*>(smem + S::osv);
+  float* sq = reinterpret_cast<float*>(smem + S::osq);      // staged rhs [F][EB][NP]
+  double* rbuf = reinterpret_cast<double*>(smem + S::ores);  // residual [F][EB][NP]
   const double* slam = reinterpret_cast<const double*>(smem + S::olam);  // [NP][DIM]
-  float* sc = reinterpret_cast<float*>(smem + S::osc);
-  float* sgeo = reinterpret_cast<float*>(smem + S::ogeo);
-  int* snbr = reinterpret_cast<int*>(smem + S::onbr);
-  uint8_t* scode = smem + S::ocode;
   uint8_t* sfm = smem + S::ofm;
   uint8_t* ssh = smem + S::osh;
   const uint8_t* svert = smem + S::overt;                  // vertex nodes B, C(, D)
   uint32_t* rsq = reinterpret_cast<uint32_t*>(smem + S::ors);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + S::obar);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + S::obar + 16);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + S::obar + 64);
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
 
-  // ---- one-time set-up: resident operators, zeroed operand planes ----
+  // ---- one-time set-up: resident operators, zeroed lift planes ----
   {
-    constexpr uint32_t dD = S::ND * KD * 2, dL = S::NL * KL * 2;
+    constexpr uint32_t dD = S::bD, dL = S::bL;
     constexpr uint32_t nchunk = (2 * dD + 2 * dL) / 16;
     const uint4* src = reinterpret_cast<const uint4*>(a.ops);
     for (uint32_t x = tid; x < nchunk; x += SPLIT_THREADS) {
@@ -281,8 +340,9 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2) rhs_split_kernel(SplitArgs a
       else o = S::oLl + (b - 2 * dD - dL);
       *reinterpret_cast<uint4*>(smem + o) = src[x];
     }
+    // the lift planes' K padding and unused rows are never written again
     const uint4 z = make_uint4(0, 0, 0, 0);
-    for (uint32_t o = S::oAqh + tid * 16; o < S::osq; o += SPLIT_THREADS * 16)
+    for (uint32_t o = S::oAfh + tid * 16; o < S::ostg; o += SPLIT_THREADS * 16)
       *reinterpret_cast<uint4*>(smem + o) = z;
     {
       // image tail: 4 vertex-node bytes, 4 pad, then the FP64 weights
@@ -294,9 +354,16 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2) rhs_split_kernel(SplitArgs a
     }
     for (int x = tid; x < NFPT; x += SPLIT_THREADS) sfm[x] = (uint8_t)a.fmask[x];
     for (int x = tid; x < a.nperm * NFP; x += SPLIT_THREADS) ssh[x] = (uint8_t)a.shuffle[x];
+    for (int x = tid; x < 128; x += SPLIT_THREADS) rsq[x] = 0u;
     if (tid == 0) {
-      tc::mbar_init(&mbar[0], 1);
-      tc::mbar_init(&mbar[1], 1);
+      tc::mbar_init(&mbar[MB_DIFF], 1);
+      tc::mbar_init(&mbar[MB_LIFT], 1);
+      tc::mbar_init(&mbar[MB_FULL], 32);
+      tc::mbar_init(&mbar[MB_FULL + 1], 32);
+      tc::mbar_init(&mbar[MB_RES_FULL], 32);
+      tc::mbar_init(&mbar[MB_FREE], 1);
+      tc::mbar_init(&mbar[MB_FREE + 1], 1);
+      tc::mbar_init(&mbar[MB_RES_FREE], 1);
     }
     if (warp == 0) tc::tmem_alloc(tmem_slot, S::TMEM_COLS);
     tc::fence_proxy_async();
@@ -305,353 +372,399 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 2) rhs_split_kernel(SplitArgs a
     tc::fence_after_sync();
   }
   const uint32_t tmem = *tmem_slot;
-  const uint32_t tmem_diff = tmem;
-  const uint32_t tmem_lift = tmem + S::LIFT_COL;
-  constexpr uint32_t ID_DIFF = tc::idesc_16bit(128, S::ND, PT == PT_BF16);
-  constexpr uint32_t ID_LIFT = tc::idesc_16bit(128, S::NL, true);
   const int64_t Knp = a.K * NP;
+  const bool stage_res = a.mode != 0 && S::RES;
 
-  // FP64 linear interpolant of (field f, batch element e) at node j
-  auto lin_at = [&](int f, int e, int j) -> double {
-    const double* v = sv + (f * EB + e) * NV1;
-    double s = v[0];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) s += slam[j * DIM + d] * (v[1 + d] - v[0]);
-    return s;
-  };
-
-  // epilogue geometry of this thread's TMEM lane
-  const int quad = warp & 3, half = warp >> 2;
-  const int lf = lane / F;                 // element within the quadrant
-  const int fown = lane - lf * F;          // own field
-  const bool lane_used = lf < EPW;
-  const int e_lane = quad * EPW + lf;
-  const uint32_t lane_addr = (uint32_t)(quad * 32) << 16;
-
-  uint32_t it = 0;
-  for (int64_t batch = blockIdx.x; batch < a.nbatch; batch += gridDim.x, ++it) {
-    const int64_t el0 = batch * EB;
-    const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
-
-    // ---- A: vertex values (FP64), remainders (FP32), split planes ----
-    {
-      // the batch's state lands in the staging area by asynchronous copies
-      // (every copy of the batch in flight at once)
-      double* stg = reinterpret_cast<double*>(smem + S::oAqh);   // [F][EB][NP]
-#pragma unroll 4
-      for (int x = tid; x < S::NVAL; x += SPLIT_THREADS) {
-        const int f = x / (EB * NP), r = x % (EB * NP), e = r / NP;
-        if (e < ne) cp_async8(stg + x, a.q_in + f * Knp + el0 * NP + r);
+  if (warp == NCW) {
+    // ================= producer warp =================
+    constexpr unsigned FULL = 0xffffffffu;
+    uint32_t it = 0;
+    for (int64_t batch = blockIdx.x; batch < a.nbatch; batch += gridDim.x, ++it) {
+      const int b = NSTG == 2 ? (int)(it & 1u) : 0;
+      const int64_t el0 = batch * EB;
+      const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
+      if (it >= (uint32_t)NSTG) {
+        int ok = 0;
+        if (lane == 0) ok = tc::mbar_wait(&mbar[MB_FREE + b], ((it / NSTG) - 1) & 1u, MBAR_MAX_NS);
+        if (!__shfl_sync(FULL, ok, 0)) {
+          if (lane == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+          break;
+        }
       }
-      for (int x = tid; x < F * EB * NV1; x += SPLIT_THREADS) {
-        const int fe = x / NV1, vv = x % NV1, f = fe / EB, e = fe % EB;
-        const int node = vv == 0 ? 0 : svert[vv - 1];
-        if (e < ne) sv[x] = a.q_in[f * Knp + (el0 + e) * NP + node];
+      uint8_t* stg = smem + S::ostg + b * S::bStage;
+      double* st = reinterpret_cast<double*>(stg);
+      for (int x = lane; x < S::NVAL; x += 32) {
+        const int f = x / FNP, r = x - f * FNP;
+        if (r < ne * NP) cp_async8(st + x, a.q_in + f * Knp + el0 * NP + r);
       }
-      for (int x = tid; x < 4 * EPW * F; x += SPLIT_THREADS) rsq[x] = 0u;
-      for (int x = tid; x < ne * G; x += SPLIT_THREADS) sgeo[x] = a.geo32[el0 * G + x];
-      for (int x = tid; x < ne * NF; x += SPLIT_THREADS) {
-        const int2 cn = a.conn[el0 * NF + x];
-        snbr[x] = cn.x;
-        scode[x] = (uint8_t)cn.y;
-      }
+      float* geo = reinterpret_cast<float*>(stg + S::sGeo);
+      for (int x = lane; x < ne * G; x += 32) cp_async4(geo + x, a.geo32 + el0 * G + x);
+      int2* cn = reinterpret_cast<int2*>(stg + S::sConn);
+      for (int x = lane; x < ne * NF; x += 32) cp_async8(cn + x, a.conn + el0 * NF + x);
       if constexpr (C != 0) {
-        for (int x = tid; x < ne * NP; x += SPLIT_THREADS) sc[x] = (float)a.coeff[el0 * NP + x];
+        double* cf = reinterpret_cast<double*>(stg + S::sCoef);
+        for (int x = lane; x < ne * NP; x += 32) cp_async8(cf + x, a.coeff + el0 * NP + x);
       }
-      cp_async_wait_all();
-      __syncthreads();
-      // remainders after the element's linear interpolant through its vertex
-      // nodes (D_r maps that interpolant to the constants added back in the
-      // epilogue): only the remainder goes through the split
-#pragma unroll 4
-      for (int x = tid; x < S::NVAL; x += SPLIT_THREADS) {
-        const int f = x / (EB * NP), r = x % (EB * NP), e = r / NP, j = r % NP;
-        if (e < ne) {
-          const float rem = (float)(stg[x] - lin_at(f, e, j));
-          sq[x] = rem;
-          if constexpr (PT == PT_FP16) {
-            const int row = (e / EPW) * 32 + (e % EPW) * F + f;
-            atomicMax(&rsq[(row >> 5) * (EPW * F) + (row & 31)], __float_as_uint(fabsf(rem)));
+      cp_async_arrive(&mbar[MB_FULL + b]);
+      if (stage_res) {
+        if (it >= 1) {
+          int ok = 0;
+          if (lane == 0) ok = tc::mbar_wait(&mbar[MB_RES_FREE], (it - 1) & 1u, MBAR_MAX_NS);
+          if (!__shfl_sync(FULL, ok, 0)) {
+            if (lane == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+            break;
+          }
+        }
+        for (int x = lane; x < S::NVAL; x += 32) {
+          const int f = x / FNP, r = x - f * FNP;
+          if (r < ne * NP) cp_async8(rbuf + x, a.res + f * Knp + el0 * NP + r);
+        }
+        cp_async_arrive(&mbar[MB_RES_FULL]);
+      }
+    }
+    cp_async_drain();
+  } else {
+    // ================= consumer warps =================
+    const uint32_t tmem_diff = tmem;
+    const uint32_t tmem_lift = tmem + S::LIFT_COL;
+    constexpr uint32_t ID_DIFF = tc::idesc_16bit(128, S::ND, PT == PT_BF16);
+    constexpr uint32_t ID_LIFT = tc::idesc_16bit(128, S::NL, true);
+    // TMEM lane of this thread (epilogue) = state-plane row (split pass)
+    const int quad = warp & 3, part = warp >> 2;
+    const int lf = lane / F;                 // element within the quadrant
+    const int fown = lane - lf * F;          // own field
+    const bool lane_used = lf < EPW;
+    const int e_lane = quad * EPW + lf;
+    const uint32_t lane_addr = (uint32_t)(quad * 32) << 16;
+    const int row = quad * 32 + lane;
+
+    uint32_t it = 0;
+    for (int64_t batch = blockIdx.x; batch < a.nbatch; batch += gridDim.x, ++it) {
+      const int b = NSTG == 2 ? (int)(it & 1u) : 0;
+      const int64_t el0 = batch * EB;
+      const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
+      const uint8_t* stg = smem + S::ostg + b * S::bStage;
+      const double* st = reinterpret_cast<const double*>(stg);   // [F][EB][NP]
+      const float* sgeo = reinterpret_cast<const float*>(stg + S::sGeo);
+      const int2* sconn = reinterpret_cast<const int2*>(stg + S::sConn);
+      const double* scoef = reinterpret_cast<const double*>(stg + S::sCoef);
+      const bool valid = lane_used && e_lane < ne;
+      const int e_own = valid ? e_lane : 0;
+
+      if (cbar_or(!tc::mbar_wait(&mbar[MB_FULL + b], (it / NSTG) & 1u, MBAR_MAX_NS))) {
+        if (tid == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+        break;
+      }
+
+      // ---- A: remainders after the element's FP64 linear interpolant, split
+      // into the state planes (one row per lane, 8 columns per item) ----
+      {
+        double v0 = 0.0, dv[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) dv[d] = 0.0;
+        if (valid) {
+          const double* q = st + fown * FNP + e_own * NP;
+          v0 = q[0];
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) dv[d] = q[svert[d]] - v0;
+        }
+        float rem[S::IPW][8];
+        uint32_t rmax = 0u;
+#pragma unroll
+        for (int k = 0; k < S::IPW; ++k) {
+          const int item = warp + k * NCW;
+          const int chunk = item >> 2;
+#pragma unroll
+          for (int c = 0; c < 8; ++c) {
+            const int j = chunk * 8 + c;
+            float v = 0.f;
+            if (item < S::NITEM && valid && j < NP) {
+              double lin = v0;
+#pragma unroll
+              for (int d = 0; d < DIM; ++d) lin += slam[j * DIM + d] * dv[d];
+              v = (float)(st[fown * FNP + e_own * NP + j] - lin);
+            }
+            rem[k][c] = v;
+            rmax = max(rmax, __float_as_uint(fabsf(v)));
+          }
+        }
+        float inv = 1.0f;
+        if constexpr (PT == PT_FP16) {
+          atomicMax(&rsq[row], rmax);
+          cbar();
+          inv = 1.0f / row_scale(rsq[row]);
+        }
+#pragma unroll
+        for (int k = 0; k < S::IPW; ++k) {
+          const int item = warp + k * NCW;
+          if (item < S::NITEM) {
+            const int chunk = item >> 2;
+            uint32_t hw[4], lw[4];
+#pragma unroll
+            for (int c = 0; c < 8; c += 2) {
+              const float x0 = rem[k][c] * inv, x1 = rem[k][c + 1] * inv;
+              if constexpr (PT == PT_BF16) {
+                const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+                const float2 hf = __bfloat1622float2(h);
+                const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+                hw[c / 2] = *reinterpret_cast<const uint32_t*>(&h);
+                lw[c / 2] = *reinterpret_cast<const uint32_t*>(&l);
+              } else {
+                const __half2 h = __floats2half2_rn(x0, x1);
+                const float2 hf = __half22float2(h);
+                const __half2 l = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+                hw[c / 2] = *reinterpret_cast<const uint32_t*>(&h);
+                lw[c / 2] = *reinterpret_cast<const uint32_t*>(&l);
+              }
+            }
+            const uint32_t off = kmajor_off(row, chunk * 8, KD);
+            *reinterpret_cast<uint4*>(Aqh + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+            *reinterpret_cast<uint4*>(Aql + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
           }
         }
       }
-      __syncthreads();
-      // split pass over the whole plane (zeros in K padding and dead rows,
-      // which the staging overwrote)
-#pragma unroll 4
-      for (int x = tid; x < 128 * KD; x += SPLIT_THREADS) {
-        const int row = x / KD, j = x % KD;
-        const int q = row & 31, e = (row >> 5) * EPW + q / F, f = q % F;
-        float val = 0.f;
-        if (j < NP && q < EPW * F && e < ne) {
-          float inv = 1.0f;
-          if constexpr (PT == PT_FP16) inv = 1.0f / row_scale(rsq[(row >> 5) * (EPW * F) + q]);
-          val = sq[f * EB * NP + e * NP + j] * inv;
+      tc::fence_proxy_async();
+      cbar();
+
+      // ---- B: diff MMAs (one thread) ----
+      if (tid == 0) {
+        tc::fence_after_sync();
+        const uint32_t aq_h = tc::smem_u32(Aqh), aq_l = tc::smem_u32(Aql);
+        const uint32_t d_h = tc::smem_u32(smem + S::oDh), d_l = tc::smem_u32(smem + S::oDl);
+#pragma unroll
+        for (int kk = 0; kk < KD / 16; ++kk) {
+          const uint32_t off = kk * 256;
+          const uint64_t ah = tc::smem_desc(aq_h + off, 128, KD * 16);
+          const uint64_t al = tc::smem_desc(aq_l + off, 128, KD * 16);
+          const uint64_t bh = tc::smem_desc(d_h + off, 128, KD * 16);
+          const uint64_t bl = tc::smem_desc(d_l + off, 128, KD * 16);
+          tc::mma_bf16(tmem_diff, ah, bh, ID_DIFF, kk > 0 ? 1u : 0u);
+          tc::mma_bf16(tmem_diff, ah, bl, ID_DIFF, 1u);
+          tc::mma_bf16(tmem_diff, al, bh, ID_DIFF, 1u);
         }
-        store_split<PT>(Aqh, Aql, kmajor_off(row, j, KD), val);
+        tc::mma_commit(&mbar[MB_DIFF]);
       }
-    }
-    tc::fence_proxy_async();
-    __syncthreads();
 
-    // ---- B: diff MMAs (one thread) ----
-    if (tid == 0) {
-      tc::fence_after_sync();
-      const uint32_t aq_h = tc::smem_u32(Aqh), aq_l = tc::smem_u32(Aql);
-      const uint32_t d_h = tc::smem_u32(smem + S::oDh), d_l = tc::smem_u32(smem + S::oDl);
-#pragma unroll
-      for (int kk = 0; kk < KD / 16; ++kk) {
-        const uint32_t off = kk * 256;
-        const uint64_t ah = tc::smem_desc(aq_h + off, 128, KD * 16);
-        const uint64_t al = tc::smem_desc(aq_l + off, 128, KD * 16);
-        const uint64_t bh = tc::smem_desc(d_h + off, 128, KD * 16);
-        const uint64_t bl = tc::smem_desc(d_l + off, 128, KD * 16);
-        tc::mma_bf16(tmem_diff, ah, bh, ID_DIFF, kk > 0 ? 1u : 0u);
-        tc::mma_bf16(tmem_diff, ah, bl, ID_DIFF, 1u);
-        tc::mma_bf16(tmem_diff, al, bh, ID_DIFF, 1u);
-      }
-      tc::mma_commit(&mbar[0]);
-    }
-
-    // ---- C: face fluxes (FP32 on jumps formed in FP64) -> BF16 lift planes ----
+      // ---- C: face fluxes (FP32 on jumps formed in FP64) -> BF16 lift planes ----
+      constexpr int FROUND = FaceRound<NA, S::NFV>::value;
 #pragma unroll 1
-    for (int u0 = 0; u0 < S::NFV; u0 += FROUND) {
-      float uPs[FROUND][NA];
-      bool okp[FROUND];
-      // pass 1: ext-side values (global gathers for neighbours outside the batch)
+      for (int u0 = 0; u0 < S::NFV; u0 += FROUND) {
+        float uPs[FROUND][NA];
+        bool okp[FROUND];
+        // pass 1: ext-side values (global gathers for neighbours outside the batch)
 #pragma unroll
-      for (int u = 0; u < FROUND; ++u) {
-        const int x = u0 + u < S::NFV ? tid + (u0 + u) * SPLIT_THREADS : S::NFACE;
-        const int e = x / NFPT, p = x % NFPT, face = p / NFP, k = p % NFP;
-        okp[u] = false;
-        if (x < S::NFACE && e < ne) {
-          const int nb = snbr[e * NF + face];
-          if (nb >= 0) {
-            const int code = scode[e * NF + face];
-            const int nface = code & 3, perm = code >> 2;
-            if (nface < NF && perm < a.nperm && nb < a.K) {
-              const int nn = sfm[nface * NFP + ssh[perm * NFP + k]];
-              const int64_t gi = (int64_t)nb * NP + nn;
-              const int lnode = sfm[p];
-              const int lb = (int)(nb - el0);   // neighbour inside this batch?
-              const bool inb = lb >= 0 && lb < ne;
-              if constexpr (JumpLinear<MODEL>::value) {
-                // jump = (lin- - q+) in FP64 + remainder- in FP32
+        for (int u = 0; u < FROUND; ++u) {
+          const int x = u0 + u < S::NFV ? tid + (u0 + u) * CONSUMERS : S::NFACE;
+          const int e = x / NFPT, p = x % NFPT, face = p / NFP, k = p % NFP;
+          okp[u] = false;
+          if (x < S::NFACE && e < ne) {
+            const int2 cn = sconn[e * NF + face];
+            const int nb = cn.x;
+            if (nb >= 0) {
+              const int code = cn.y;
+              const int nface = code & 3, perm = code >> 2;
+              if (nface < NF && perm < a.nperm && nb < a.K) {
+                const int nn = sfm[nface * NFP + ssh[perm * NFP + k]];
+                const int64_t gi = (int64_t)nb * NP + nn;
+                const int lnode = sfm[p];
+                const int lb = (int)(nb - el0);   // neighbour inside this batch?
+                const bool inb = lb >= 0 && lb < ne;
+                if constexpr (JumpLinear<MODEL>::value) {
 #pragma unroll
-                for (int f = 0; f < F; ++f) {
-                  const double lm = lin_at(f, e, lnode);
-                  const float rm = sq[f * EB * NP + e * NP + lnode];
-                  if (inb)
-                    uPs[u][f] = (float)(lm - lin_at(f, lb, nn)) +
-                                (rm - sq[f * EB * NP + lb * NP + nn]);
-                  else
-                    uPs[u][f] = (float)(lm - __ldg(a.q_in + f * Knp + gi)) + rm;
+                  for (int f = 0; f < F; ++f) {
+                    const double qm = st[f * FNP + e * NP + lnode];
+                    const double qp = inb ? st[f * FNP + lb * NP + nn]
+                                          : __ldg(a.q_in + f * Knp + gi);
+                    uPs[u][f] = (float)(qm - qp);
+                  }
+                } else {
+                  if constexpr (C != 0)
+                    uPs[u][0] = inb ? (float)scoef[lb * NP + nn] : (float)__ldg(a.coeff + gi);
+#pragma unroll
+                  for (int f = 0; f < F; ++f)
+                    uPs[u][C + f] = inb ? (float)st[f * FNP + lb * NP + nn]
+                                        : (float)__ldg(a.q_in + f * Knp + gi);
                 }
+                okp[u] = true;
               } else {
-                if constexpr (C != 0)
-                  uPs[u][0] = inb ? sc[lb * NP + nn] : (float)__ldg(a.coeff + gi);
-#pragma unroll
-                for (int f = 0; f < F; ++f)
-                  uPs[u][C + f] = inb ? (float)lin_at(f, lb, nn) + sq[f * EB * NP + lb * NP + nn]
-                                      : (float)__ldg(a.q_in + f * Knp + gi);
+                atomicCAS(a.err, 0, DEV_BAD_CODE);
               }
-              okp[u] = true;
-            } else {
-              atomicCAS(a.err, 0, DEV_BAD_CODE);
             }
           }
         }
-      }
-      // pass 2: fluxes, split straight into the BF16 lift planes
+        // pass 2: fluxes, split straight into the BF16 lift planes
 #pragma unroll
-      for (int u = 0; u < FROUND; ++u) {
-        const int x = u0 + u < S::NFV ? tid + (u0 + u) * SPLIT_THREADS : S::NFACE;
-        const int e = x / NFPT, p = x % NFPT, face = p / NFP, k = p % NFP;
-        if (x < S::NFACE && e < ne) {
-          const int lnode = sfm[p];
-          float uM[NA], uP[NA], n[DIM], fl[F];
-          const float* gf = sgeo + e * G + DIM * DIM + face * (DIM + 1);
+        for (int u = 0; u < FROUND; ++u) {
+          const int x = u0 + u < S::NFV ? tid + (u0 + u) * CONSUMERS : S::NFACE;
+          const int e = x / NFPT, p = x % NFPT, face = p / NFP, k = p % NFP;
+          if (x < S::NFACE && e < ne) {
+            const int lnode = sfm[p];
+            float uM[NA], uP[NA], n[DIM], fl[F];
+            const float* gf = sgeo + e * G + DIM * DIM + face * (DIM + 1);
 #pragma unroll
-          for (int d = 0; d < DIM; ++d) n[d] = gf[d];
-          const float fscale = gf[DIM];
-          const int nb = snbr[e * NF + face];
-          bool have = true, bdry = false;
-          if (nb >= 0 && JumpLinear<MODEL>::value) {
-            have = okp[u];
-#pragma unroll
-            for (int q = 0; q < NA; ++q) { uM[q] = uPs[u][q]; uP[q] = 0.f; }
-          } else {
-            if constexpr (C != 0) uM[0] = sc[e * NP + lnode];
-#pragma unroll
-            for (int f = 0; f < F; ++f)
-              uM[C + f] = (float)lin_at(f, e, lnode) + sq[f * EB * NP + e * NP + lnode];
-            if (nb >= 0) {
+            for (int d = 0; d < DIM; ++d) n[d] = gf[d];
+            const float fscale = gf[DIM];
+            const int2 cn = sconn[e * NF + face];
+            const int nb = cn.x;
+            bool have = true, bdry = false;
+            if (nb >= 0 && JumpLinear<MODEL>::value) {
               have = okp[u];
 #pragma unroll
-              for (int q = 0; q < NA; ++q) uP[q] = uPs[u][q];
+              for (int q = 0; q < NA; ++q) { uM[q] = uPs[u][q]; uP[q] = 0.f; }
             } else {
-              bdry = true;
-              const int kind = scode[e * NF + face];
-              float given = 0.f;
-              if (kind == HB_BC_GIVEN) {
-                const int64_t bi = (int64_t)(-1 - nb) * NFP + k;
-                if (a.bdry == nullptr || bi >= a.n_given) {
-                  atomicCAS(a.err, 0, a.bdry == nullptr ? DEV_MISSING_INPUT : DEV_BAD_BDRY_INDEX);
-                  have = false;
-                } else {
-                  given = (float)__ldg(a.bdry + bi);
+              if constexpr (C != 0) uM[0] = (float)scoef[e * NP + lnode];
+#pragma unroll
+              for (int f = 0; f < F; ++f) uM[C + f] = (float)st[f * FNP + e * NP + lnode];
+              if (nb >= 0) {
+                have = okp[u];
+#pragma unroll
+                for (int q = 0; q < NA; ++q) uP[q] = uPs[u][q];
+              } else {
+                bdry = true;
+                const int kind = cn.y;
+                float given = 0.f;
+                if (kind == HB_BC_GIVEN) {
+                  const int64_t bi = (int64_t)(-1 - nb) * NFP + k;
+                  if (a.bdry == nullptr || bi >= a.n_given) {
+                    atomicCAS(a.err, 0, a.bdry == nullptr ? DEV_MISSING_INPUT : DEV_BAD_BDRY_INDEX);
+                    have = false;
+                  } else {
+                    given = (float)__ldg(a.bdry + bi);
+                  }
                 }
+                if (have) have = model_bc<MODEL, DIM, float>(a.mp, kind, uM, n, given, uP);
               }
-              if (have) have = model_bc<MODEL, DIM, float>(a.mp, kind, uM, n, given, uP);
             }
-          }
-          if (have) model_flux<MODEL, DIM, float>(a.mp, bdry, uM, uP, n, fl);
-          const int rowb = (e / EPW) * 32 + (e % EPW) * F;
+            if (have) model_flux<MODEL, DIM, float>(a.mp, bdry, uM, uP, n, fl);
+            const int rowb = (e / EPW) * 32 + (e % EPW) * F;
 #pragma unroll
-          for (int f = 0; f < F; ++f)
-            store_split<PT_BF16>(Afh, Afl, kmajor_off(rowb + f, p, KL),
-                                 have ? fscale * fl[f] : 0.f);
+            for (int f = 0; f < F; ++f)
+              store_split<PT_BF16>(Afh, Afl, kmajor_off(rowb + f, p, KL),
+                                   have ? fscale * fl[f] : 0.f);
+          }
         }
       }
-    }
-    // K padding of the lift planes (the staging area overwrote it)
-    if constexpr (KL > NFPT) {
-      for (int x = tid; x < 128 * (KL - NFPT); x += SPLIT_THREADS) {
-        const int row = x / (KL - NFPT), p = NFPT + x % (KL - NFPT);
-        store_split<PT_BF16>(Afh, Afl, kmajor_off(row, p, KL), 0.f);
-      }
-    }
-    tc::fence_proxy_async();
-    __syncthreads();
+      tc::fence_proxy_async();
+      cbar();
 
-    // ---- D: lift MMAs (one thread) ----
-    if (tid == 0) {
-      tc::fence_after_sync();
-      const uint32_t af_h = tc::smem_u32(Afh), af_l = tc::smem_u32(Afl);
-      const uint32_t l_h = tc::smem_u32(smem + S::oLh), l_l = tc::smem_u32(smem + S::oLl);
-#pragma unroll
-      for (int kk = 0; kk < KL / 16; ++kk) {
-        const uint32_t off = kk * 256;
-        const uint64_t ah = tc::smem_desc(af_h + off, 128, KL * 16);
-        const uint64_t al = tc::smem_desc(af_l + off, 128, KL * 16);
-        const uint64_t bh = tc::smem_desc(l_h + off, 128, KL * 16);
-        const uint64_t bl = tc::smem_desc(l_l + off, 128, KL * 16);
-        tc::mma_bf16(tmem_lift, ah, bh, ID_LIFT, kk > 0 ? 1u : 0u);
-        tc::mma_bf16(tmem_lift, ah, bl, ID_LIFT, 1u);
-        tc::mma_bf16(tmem_lift, al, bh, ID_LIFT, 1u);
-      }
-      tc::mma_commit(&mbar[1]);
-    }
-
-    // ---- E: TMEM -> chain rule, volume terms, + lift -> staged rhs ----
-    // one thread waits on the tensor core; the others sleep in the barrier
-    int late = 0;
-    if (tid == 0) {
-      const bool w0 = tc::mbar_wait(&mbar[0], it & 1u, MBAR_MAX_NS);
-      const bool w1 = tc::mbar_wait(&mbar[1], it & 1u, MBAR_MAX_NS);
-      late = !(w0 && w1);
-    }
-    if (__syncthreads_or(late)) {
-      // the MMAs did not complete in time: flag, give them one more bounded
-      // wait, then leave (TMEM is released below)
+      // ---- D: lift MMAs (one thread) ----
       if (tid == 0) {
-        atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
-        tc::mbar_wait(&mbar[0], it & 1u, MBAR_MAX_NS);
-        tc::mbar_wait(&mbar[1], it & 1u, MBAR_MAX_NS);
-      }
-      __syncthreads();
-      break;
-    }
-    tc::fence_after_sync();
-    {
-      const bool valid = lane_used && e_lane < ne;
-      const int e = valid ? e_lane : 0;
-      const float* ge = sgeo + e * G;
-      float gm[DIM][DIM];
+        tc::fence_after_sync();
+        const uint32_t af_h = tc::smem_u32(Afh), af_l = tc::smem_u32(Afl);
+        const uint32_t l_h = tc::smem_u32(smem + S::oLh), l_l = tc::smem_u32(smem + S::oLl);
 #pragma unroll
-      for (int r = 0; r < DIM; ++r)
-#pragma unroll
-        for (int x = 0; x < DIM; ++x) gm[r][x] = ge[r * DIM + x];
-      const int base = lf * F;
-      // reference derivatives of the removed linear interpolant: (q_v - q_A)/2
-      float lin[DIM];
-      {
-        const double* vv = sv + (fown * EB + e) * NV1;
-#pragma unroll
-        for (int r = 0; r < DIM; ++r) lin[r] = (float)(0.5 * (vv[1 + r] - vv[0]));
-      }
-      float sdiff = a.op_scale_d;
-      if constexpr (PT == PT_FP16) sdiff *= row_scale(rsq[quad * (EPW * F) + (lane_used ? lane : 0)]);
-      constexpr int I_END0 = S::NPH < NP ? S::NPH : NP;
-      const int i_lo = half ? S::NPH : 0;
-      const int i_hi = half ? NP : I_END0;
-#pragma unroll 1
-      for (int i0 = i_lo; i0 < i_hi; i0 += 4) {
-        float dv[DIM][4], lv[4];
-#pragma unroll
-        for (int r = 0; r < DIM; ++r) tc::tmem_ld4(tmem_diff + lane_addr + r * NP + i0, dv[r]);
-        tc::tmem_ld4(tmem_lift + lane_addr + i0, lv);
-        tc::tmem_wait_ld();
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const int i = i0 + c;
-          float g[DIM];
-#pragma unroll
-          for (int x = 0; x < DIM; ++x) {
-            float s = 0.f;
-#pragma unroll
-            for (int r = 0; r < DIM; ++r) s += gm[r][x] * (dv[r][c] * sdiff + lin[r]);
-            g[x] = s;
-          }
-          const float cnode = C ? sc[e * NP + i] : 0.f;
-          const float mine = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
-          if (valid && i < i_hi) {
-            const float src = a.source ? (float)a.source[(el0 + e) * NP + i] : 0.f;
-            sq[fown * EB * NP + e * NP + i] =
-                model_finish<MODEL, DIM, float>(a.mp, fown, mine, lv[c], src);
-          }
+        for (int kk = 0; kk < KL / 16; ++kk) {
+          const uint32_t off = kk * 256;
+          const uint64_t ah = tc::smem_desc(af_h + off, 128, KL * 16);
+          const uint64_t al = tc::smem_desc(af_l + off, 128, KL * 16);
+          const uint64_t bh = tc::smem_desc(l_h + off, 128, KL * 16);
+          const uint64_t bl = tc::smem_desc(l_l + off, 128, KL * 16);
+          tc::mma_bf16(tmem_lift, ah, bh, ID_LIFT, kk > 0 ? 1u : 0u);
+          tc::mma_bf16(tmem_lift, ah, bl, ID_LIFT, 1u);
+          tc::mma_bf16(tmem_lift, al, bh, ID_LIFT, 1u);
         }
+        tc::mma_commit(&mbar[MB_LIFT]);
       }
-    }
-    tc::fence_before_sync();
-    __syncthreads();
 
-    // ---- F: FP64 stage update; residual and state staged by async copies,
-    // CH values at a time ----
-    {
-      double* stg = reinterpret_cast<double*>(smem + S::oAqh);  // [2][CH]
-      constexpr int FNP = EB * NP;
+      // ---- E: TMEM -> chain rule, volume terms, + lift -> staged rhs ----
+      // one thread waits on the tensor core; the others sleep in the barrier
+      int late = 0;
+      if (tid == 0) {
+        const bool w0 = tc::mbar_wait(&mbar[MB_DIFF], it & 1u, MBAR_MAX_NS);
+        const bool w1 = tc::mbar_wait(&mbar[MB_LIFT], it & 1u, MBAR_MAX_NS);
+        late = !(w0 && w1);
+      }
+      if (cbar_or(late)) {
+        // the MMAs did not complete in time: flag, give them one more bounded
+        // wait, then leave (TMEM is released below)
+        if (tid == 0) {
+          atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+          tc::mbar_wait(&mbar[MB_DIFF], it & 1u, MBAR_MAX_NS);
+          tc::mbar_wait(&mbar[MB_LIFT], it & 1u, MBAR_MAX_NS);
+        }
+        cbar();
+        break;
+      }
+      tc::fence_after_sync();
+      {
+        const float* ge = sgeo + e_own * G;
+        float gm[DIM][DIM];
+#pragma unroll
+        for (int r = 0; r < DIM; ++r)
+#pragma unroll
+          for (int x = 0; x < DIM; ++x) gm[r][x] = ge[r * DIM + x];
+        const int base = lf * F;
+        // reference derivatives of the removed linear interpolant: (q_v - q_A)/2
+        float lin[DIM];
+        {
+          const double* q = st + fown * FNP + e_own * NP;
+#pragma unroll
+          for (int r = 0; r < DIM; ++r) lin[r] = (float)(0.5 * (q[svert[r]] - q[0]));
+        }
+        float sdiff = a.op_scale_d;
+        if constexpr (PT == PT_FP16) sdiff *= row_scale(rsq[row]);
+        const int i_lo = part * S::NPQ;
+        const int i_hi = (part + 1) * S::NPQ < NP ? (part + 1) * S::NPQ : NP;
 #pragma unroll 1
-      for (int x0 = 0; x0 < S::NVAL; x0 += S::CH) {
-        const int nx = S::NVAL - x0 < S::CH ? S::NVAL - x0 : S::CH;
-        if (a.mode != 0) {
-          for (int x = tid; x < nx; x += SPLIT_THREADS) {
-            const int g = x0 + x, f = g / FNP, r = g % FNP, e = r / NP;
-            if (e < ne) {
-              const int64_t idx = f * Knp + el0 * NP + r;
-              cp_async8(stg + x, a.res + idx);
-              cp_async8(stg + S::CH + x, a.q_in + idx);
+        for (int i0 = i_lo; i0 < i_hi; i0 += 2) {
+          float dv[DIM][2], lv[2];
+#pragma unroll
+          for (int r = 0; r < DIM; ++r) tc::tmem_ld2(tmem_diff + lane_addr + r * NP + i0, dv[r]);
+          tc::tmem_ld2(tmem_lift + lane_addr + i0, lv);
+          tc::tmem_wait_ld();
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            const int i = i0 + c;
+            float g[DIM];
+#pragma unroll
+            for (int x = 0; x < DIM; ++x) {
+              float s = 0.f;
+#pragma unroll
+              for (int r = 0; r < DIM; ++r) s += gm[r][x] * (dv[r][c] * sdiff + lin[r]);
+              g[x] = s;
+            }
+            const float cnode = C ? (float)scoef[e_own * NP + (i < NP ? i : 0)] : 0.f;
+            const float mine = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
+            if (valid && i < i_hi) {
+              const float src = a.source ? (float)a.source[(el0 + e_own) * NP + i] : 0.f;
+              sq[fown * FNP + e_own * NP + i] =
+                  model_finish<MODEL, DIM, float>(a.mp, fown, mine, lv[c], src);
             }
           }
-          cp_async_wait_all();
-          __syncthreads();
         }
+      }
+      tc::fence_before_sync();
+      if (stage_res) {
+        if (cbar_or(!tc::mbar_wait(&mbar[MB_RES_FULL], it & 1u, MBAR_MAX_NS))) {
+          if (tid == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+          break;
+        }
+      } else {
+        cbar();
+      }
+
+      // ---- F: FP64 stage update (state and residual already in shared memory) ----
+      if (tid < 128) rsq[tid] = 0u;
 #pragma unroll 4
-        for (int x = tid; x < nx; x += SPLIT_THREADS) {
-          const int g = x0 + x, f = g / FNP, r = g % FNP, e = r / NP;
-          if (e < ne) {
-            const int64_t idx = f * Knp + el0 * NP + r;
-            const double rr = (double)sq[g];
-            if (a.mode == 0) {
-              a.q_out[idx] = rr;
-            } else {
-              const double nr = a.ra * stg[x] + a.dt * rr;
-              a.res[idx] = nr;
-              a.q_out[idx] = stg[S::CH + x] + a.rb * nr;
-            }
+      for (int x = tid; x < S::NVAL; x += CONSUMERS) {
+        const int f = x / FNP, r = x - f * FNP;
+        if (r < ne * NP) {
+          const int64_t idx = f * Knp + el0 * NP + r;
+          const double rr = (double)sq[x];
+          if (a.mode == 0) {
+            a.q_out[idx] = rr;
+          } else {
+            const double r0 = S::RES ? rbuf[x] : a.res[idx];
+            const double nr = a.ra * r0 + a.dt * rr;
+            a.res[idx] = nr;
+            a.q_out[idx] = st[x] + a.rb * nr;
           }
         }
-        __syncthreads();
+      }
+      cbar();
+      if (tid == 0) {
+        tc::mbar_arrive(&mbar[MB_FREE + b]);
+        if (stage_res) tc::mbar_arrive(&mbar[MB_RES_FREE]);
       }
     }
   }
@@ -794,8 +907,11 @@ static hb_status configure_split(Op* op) {
     HB_CUDA(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
     HB_CUDA(cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev));
     const int by_smem = (int)(smem_sm / (smem + 1024));
-    const int regs_cta = ((fa.numRegs * 32 + 255) / 256 * 256) * (SPLIT_THREADS / 32);
-    const int by_regs = regs_sm / std::max(regs_cta, 1);
+    // registers: each of the 4 sub-partitions holds a quarter of the file and
+    // receives every 4th warp
+    const int regs_warp = (fa.numRegs * 32 + 255) / 256 * 256;
+    const int warps_part = (SPLIT_THREADS / 32 + 3) / 4;
+    const int by_regs = (regs_sm / 4) / std::max(regs_warp * warps_part, 1);
     const int per_sm = std::min(std::min(by_smem, by_regs), thr_sm / SPLIT_THREADS);
     if (per_sm < 1) return fail(HB_ERR_UNSUPPORTED, "BF16x3 kernel does not fit on an SM");
     if (per_sm > max_ctas) return fail(HB_ERR_UNSUPPORTED, "TMEM oversubscribed");
