@@ -1,5 +1,6 @@
 // C-ABI entry points of libhedge_b200 (declared in include/hedge_b200.h).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <new>
 #include <string>
@@ -221,6 +222,8 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
   ModelParams& mp = op->mp;
   for (int k = 0; k < 3; ++k) mp.v[k] = desc->v[k];
   mp.c = desc->c; mp.eps = desc->eps; mp.mu = desc->mu;
+  mp.Z = (desc->eps > 0 && desc->mu > 0) ? std::sqrt(desc->mu / desc->eps) : 1.0;
+  mp.Y = 1.0 / mp.Z;
   mp.alpha = desc->alpha; mp.bdry_alpha = desc->bdry_alpha;
   mp.time_sign = desc->time_sign;
   mp.flux_type = desc->flux_type; mp.bdry_flux_type = desc->bdry_flux_type;

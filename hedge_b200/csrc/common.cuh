@@ -25,6 +25,7 @@ hb_status cuda_fail(cudaError_t err, const char* what);
 struct ModelParams {
   double v[3];
   double c, eps, mu, alpha, bdry_alpha, time_sign;
+  double Z, Y;   // Maxwell impedance sqrt(mu/eps) and admittance 1/Z
   int flux_type, bdry_flux_type;
 };
 

@@ -130,7 +130,7 @@ __device__ __forceinline__ bool model_bc(const ModelParams& mp, int kind,
 #pragma unroll
       for (int k = 0; k < 3; ++k) { uP[k] = e[k]; uP[3 + k] = -h[k]; }
     } else if (kind == HB_BC_ABSORB) {
-      const T Z = T(sqrt(mp.mu / mp.eps)), Y = T(1) / Z;
+      const T Z = T(mp.Z), Y = T(mp.Y);
       T ne[3], nh[3], nne[3], nnh[3];
       cross3(&n[0], e, ne);
       cross3(&n[0], h, nh);
@@ -224,14 +224,14 @@ __device__ __forceinline__ void model_flux(const ModelParams& mp, bool bdry,
 #pragma unroll
       for (int k = 0; k < 3; ++k) f[3 + k] = T(0.5) * t[k];
     } else {
-      const T Z = T(sqrt(mp.mu / mp.eps)), Y = T(1) / Z;
+      const T Z = T(mp.Z), Y = T(mp.Y);
       T nde[3], ndh[3], a[3];
       cross3(&n[0], de, nde);
       cross3(&n[0], dh, ndh);
 #pragma unroll
       for (int k = 0; k < 3; ++k) a[k] = Z * dh[k] - alpha * nde[k];
       cross3(&n[0], a, t);
-      const T fe = T(-1) / (Z + Z), fh = T(1) / (Y + Y);
+      const T fe = T(-0.5) * Y, fh = T(0.5) * Z;   // -1/(2Z), 1/(2Y)
 #pragma unroll
       for (int k = 0; k < 3; ++k) f[k] = fe * t[k];
 #pragma unroll

@@ -52,21 +52,19 @@ namespace hb {
 
 hb_status ensure_fp32(Discr* d);
 
-// consumer warps (the phases of a batch) plus one producer warp that streams
-// the next batch's state and the current batch's residual into shared memory
-// (a multiple of 4: warp w reads TMEM lane quadrant w % 4).  Registers are
-// split over the SM's 4 sub-partitions (16K each) by warp: 13 warps put at
-// most 4 warps on one, which leaves 128 registers per thread.
+// Consumer warps (the phases of a batch; a multiple of 4: warp w reads TMEM
+// lane quadrant w % 4), one I/O warp that streams the next batch's state and
+// the current batch's residual into shared memory and the results out, and
+// one warp that issues the tensor-core MMAs.  Registers are split over the
+// SM's 4 sub-partitions (16K each) by warp: 14 warps put at most 4 warps on
+// one, which leaves 128 registers per thread.
 #ifndef HB_SPLIT_NCW
 #define HB_SPLIT_NCW 12
 #endif
 constexpr int NCW = HB_SPLIT_NCW;
 static_assert(NCW % 4 == 0, "consumer warps must cover the TMEM quadrants evenly");
 constexpr int CONSUMERS = NCW * 32;
-constexpr int SPLIT_THREADS = CONSUMERS + 32;
-// face points a consumer thread keeps in flight (fewer for many fields)
-template <int NA, int NFV>
-struct FaceRound { static constexpr int value = NFV < (NA > 4 ? 3 : 4) ? NFV : (NA > 4 ? 3 : 4); };
+constexpr int SPLIT_THREADS = CONSUMERS + 64;
 // bounded waits (tensor core, producer/consumer hand-offs): 2 s, far above any
 // batch's time
 constexpr uint64_t MBAR_MAX_NS = 2000000000ull;
@@ -99,8 +97,9 @@ struct Shape {
   static constexpr int NVAL = F * FNP;
   static constexpr int NFACE = EB * NFPT;
   static constexpr int NFV = (NFACE + CONSUMERS - 1) / CONSUMERS;
-  // epilogue: the NCW/4 warps of a TMEM quadrant split the nodes, NPQ each (even)
-  static constexpr int NPQ = (((NP + NCW / 4 - 1) / (NCW / 4)) + 1) & ~1;
+  // epilogue: the NCW/4 warps of a TMEM quadrant split the nodes, NPQ each
+  // (a multiple of 4: TMEM is read 4 columns at a time)
+  static constexpr int NPQ = (((NP + NCW / 4 - 1) / (NCW / 4)) + 3) & ~3;
   // split pass: (quadrant, 8-column chunk) items, IPW per consumer warp
   static constexpr int NITEM = 4 * (KD / 8);
   static constexpr int IPW = (NITEM + NCW - 1) / NCW;
@@ -123,9 +122,8 @@ struct Shape {
   static constexpr uint32_t oAql = al128(oAqh + bAq);
   static constexpr uint32_t oAfh = al128(oAql + bAq);
   static constexpr uint32_t oAfl = al128(oAfh + bAf);
-  static constexpr uint32_t osq = oAqh;   // FP32 rhs staging reuses the state planes
   static constexpr uint32_t ostg = al128(oAfl + bAf);
-  static constexpr uint32_t SMALL = 1024 + NP * DIM * 8 + NFPT + 6 * NFP + 4 + 128 * 4 + 80;
+  static constexpr uint32_t SMALL = 1024 + NP * DIM * 8 + NFPT + 6 * NFP + 4 + 512 * 4 + 96;
   // double-buffered stages and a residual buffer when they fit, else fewer
   static constexpr bool fits(int nstg, bool res) {
     return ostg + nstg * bStage + (res ? bState : 0) + SMALL <= SMEM_LIMIT;
@@ -137,11 +135,11 @@ struct Shape {
   static constexpr uint32_t ofm = al16(olam + NP * DIM * 8);           // uint8 fmask
   static constexpr uint32_t osh = al16(ofm + NFPT);                    // uint8 shuffles
   static constexpr uint32_t overt = al16(osh + 6 * NFP);               // uint8 vertex nodes
-  static constexpr uint32_t ors = al16(overt + 4);                     // row maxima
-  static constexpr uint32_t obar = al16(ors + 128 * 4);                // 8 mbarriers + TMEM slot
-  static constexpr uint32_t total = al16(obar + 80);
+  // row maxima (FP16 planes): state rows [2][128] then flux rows [2][128]
+  static constexpr uint32_t ors = al16(overt + 4);
+  static constexpr uint32_t obar = al16(ors + 512 * 4);                // mbarriers + TMEM slot
+  static constexpr uint32_t total = al16(obar + 96);
   static constexpr uint32_t LIN_BYTES = 8 + NP * DIM * 8;  // vertex nodes + weights (image)
-  static_assert(F * FNP * 4 <= (int)(2 * bAq), "rhs staging does not fit the state planes");
   static constexpr int TMEM_NEED = LIFT_COL + NL + 4;
   static constexpr uint32_t TMEM_COLS = TMEM_NEED <= 32 ? 32 : TMEM_NEED <= 64 ? 64
                                         : TMEM_NEED <= 128 ? 128 : TMEM_NEED <= 256 ? 256 : 512;
@@ -269,7 +267,7 @@ __device__ __forceinline__ float volume_own(const ModelParams& mp, const float (
   }
 }
 
-// consumer-only barrier (named barrier 1; the producer warp never joins it)
+// consumer-only barriers (named barrier 1; the I/O and MMA warps never join)
 __device__ __forceinline__ void cbar() {
   asm volatile("bar.sync 1, %0;" ::"n"(CONSUMERS) : "memory");
 }
@@ -297,10 +295,81 @@ __device__ __forceinline__ void cp_async_arrive(uint64_t* mbar) {
 __device__ __forceinline__ void cp_async_drain() {
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
+// bulk (untiled, no multicast) copies: 16-byte aligned addresses and sizes
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;"
+               ::"r"(tc::smem_u32(mbar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* sdst, const void* gsrc, uint32_t bytes,
+                                          uint64_t* mbar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(tc::smem_u32(sdst)), "l"(gsrc), "r"(bytes), "r"(tc::smem_u32(mbar))
+      : "memory");
+}
+__device__ __forceinline__ void bulk_store(void* gdst, const void* ssrc, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+               ::"l"(gdst), "r"(tc::smem_u32(ssrc)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+__device__ __forceinline__ bool aligned16(const void* p, uint32_t bytes) {
+  return ((reinterpret_cast<uintptr_t>(p) | bytes) & 15u) == 0;
+}
 
-// mbarriers: 0 diff MMA, 1 lift MMA, 2..3 stage full, 4 residual full,
-// 5..6 stage free, 7 residual free
-enum { MB_DIFF = 0, MB_LIFT = 1, MB_FULL = 2, MB_RES_FULL = 4, MB_FREE = 5, MB_RES_FREE = 7 };
+// One contiguous range global -> shared: a bulk copy (counted as transaction
+// bytes on `mbar`, announced beforehand) when aligned, else 8- or 4-byte
+// cp.async by the warp's lanes (counted by their arrivals).
+template <typename T>
+__device__ __forceinline__ void stage_in(T* sdst, const T* gsrc, int n, int lane,
+                                         uint64_t* mbar) {
+  const uint32_t bytes = (uint32_t)n * sizeof(T);
+  if (n <= 0) return;
+  if (aligned16(gsrc, bytes)) {
+    if (lane == 0) bulk_load(sdst, gsrc, bytes, mbar);
+    return;
+  }
+  for (int x = lane; x < n; x += 32) {
+    if constexpr (sizeof(T) == 8) cp_async8(sdst + x, gsrc + x);
+    else cp_async4(sdst + x, gsrc + x);
+  }
+}
+template <typename T>
+__device__ __forceinline__ uint32_t bulk_bytes(const T* gsrc, int n) {
+  const uint32_t bytes = (uint32_t)n * sizeof(T);
+  return (n > 0 && aligned16(gsrc, bytes)) ? bytes : 0u;
+}
+// One contiguous range shared -> global (bulk store when aligned, else lanes).
+__device__ __forceinline__ void stage_out(double* gdst, const double* ssrc, int n, int lane) {
+  const uint32_t bytes = (uint32_t)n * 8u;
+  if (n <= 0) return;
+  if (aligned16(gdst, bytes)) {
+    if (lane == 0) bulk_store(gdst, ssrc, bytes);
+  } else {
+    for (int x = lane; x < n; x += 32) gdst[x] = ssrc[x];
+  }
+}
+
+// mbarriers
+enum {
+  MB_DIFF = 0,      // diff MMAs done (tcgen05.commit)
+  MB_LIFT = 1,      // lift MMAs done
+  MB_FULL = 2,      // 2..3: stage buffer loaded
+  MB_RES_FULL = 4,  // residual buffer loaded
+  MB_AREADY = 5,    // every consumer warp wrote its state-plane rows
+  MB_FREADY = 6,    // every consumer warp wrote its flux-plane entries
+  MB_DONE = 7,      // 7..8: every consumer warp left its results in that stage buffer
+  MB_COUNT = 9
+};
 
 template <int MODEL, int DIM, int ORDER, int PT>
 __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a) {
@@ -308,20 +377,21 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
   constexpr int F = S::F, C = S::C, NA = S::NA, NP = S::NP, NFP = S::NFP, NF = S::NF;
   constexpr int NFPT = S::NFPT, G = S::G, EPW = S::EPW, EB = S::EB, FNP = S::FNP;
   constexpr int KD = S::KD, KL = S::KL, NSTG = S::NSTG;
+  constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(128) uint8_t smem[];
   uint8_t* Aqh = smem + S::oAqh;
   uint8_t* Aql = smem + S::oAql;
   uint8_t* Afh = smem + S::oAfh;
   uint8_t* Afl = smem + S::oAfl;
-  float* sq = reinterpret_cast<float*>(smem + S::osq);      // staged rhs [F][EB][NP]
   double* rbuf = reinterpret_cast<double*>(smem + S::ores);  // residual [F][EB][NP]
   const double* slam = reinterpret_cast<const double*>(smem + S::olam);  // [NP][DIM]
   uint8_t* sfm = smem + S::ofm;
   uint8_t* ssh = smem + S::osh;
   const uint8_t* svert = smem + S::overt;                  // vertex nodes B, C(, D)
-  uint32_t* rsq = reinterpret_cast<uint32_t*>(smem + S::ors);
+  uint32_t* rsq = reinterpret_cast<uint32_t*>(smem + S::ors);        // [2][128] state rows
+  uint32_t* rsf = reinterpret_cast<uint32_t*>(smem + S::ors) + 256;  // [2][128] flux rows
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + S::obar);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + S::obar + 64);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + S::obar + 8 * MB_COUNT);
 
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
@@ -354,16 +424,17 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
     }
     for (int x = tid; x < NFPT; x += SPLIT_THREADS) sfm[x] = (uint8_t)a.fmask[x];
     for (int x = tid; x < a.nperm * NFP; x += SPLIT_THREADS) ssh[x] = (uint8_t)a.shuffle[x];
-    for (int x = tid; x < 128; x += SPLIT_THREADS) rsq[x] = 0u;
+    for (int x = tid; x < 512; x += SPLIT_THREADS) rsq[x] = 0u;
     if (tid == 0) {
       tc::mbar_init(&mbar[MB_DIFF], 1);
       tc::mbar_init(&mbar[MB_LIFT], 1);
       tc::mbar_init(&mbar[MB_FULL], 32);
       tc::mbar_init(&mbar[MB_FULL + 1], 32);
       tc::mbar_init(&mbar[MB_RES_FULL], 32);
-      tc::mbar_init(&mbar[MB_FREE], 1);
-      tc::mbar_init(&mbar[MB_FREE + 1], 1);
-      tc::mbar_init(&mbar[MB_RES_FREE], 1);
+      tc::mbar_init(&mbar[MB_AREADY], NCW);
+      tc::mbar_init(&mbar[MB_FREADY], NCW);
+      tc::mbar_init(&mbar[MB_DONE], NCW);
+      tc::mbar_init(&mbar[MB_DONE + 1], NCW);
     }
     if (warp == 0) tc::tmem_alloc(tmem_slot, S::TMEM_COLS);
     tc::fence_proxy_async();
@@ -372,63 +443,159 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
     tc::fence_after_sync();
   }
   const uint32_t tmem = *tmem_slot;
+  const uint32_t tmem_diff = tmem;
+  const uint32_t tmem_lift = tmem + S::LIFT_COL;
   const int64_t Knp = a.K * NP;
   const bool stage_res = a.mode != 0 && S::RES;
+  const int64_t nb_cta = a.nbatch > (int64_t)blockIdx.x
+                             ? (a.nbatch - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  // bounded wait by lane 0, result shared with (and ordered for) the warp
+  auto warp_wait = [&](uint64_t* mb, uint32_t parity) -> bool {
+    int ok = 0;
+    if (lane == 0) ok = tc::mbar_wait(mb, parity, MBAR_MAX_NS);
+    ok = __shfl_sync(FULL, ok, 0);
+    __syncwarp();
+    return ok != 0;
+  };
 
-  if (warp == NCW) {
-    // ================= producer warp =================
-    constexpr unsigned FULL = 0xffffffffu;
-    uint32_t it = 0;
-    for (int64_t batch = blockIdx.x; batch < a.nbatch; batch += gridDim.x, ++it) {
-      const int b = NSTG == 2 ? (int)(it & 1u) : 0;
-      const int64_t el0 = batch * EB;
-      const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
-      if (it >= (uint32_t)NSTG) {
-        int ok = 0;
-        if (lane == 0) ok = tc::mbar_wait(&mbar[MB_FREE + b], ((it / NSTG) - 1) & 1u, MBAR_MAX_NS);
-        if (!__shfl_sync(FULL, ok, 0)) {
-          if (lane == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
-          break;
+  if (warp == NCW + 1) {
+    // ================= MMA-issue warp =================
+    constexpr uint32_t ID_DIFF = tc::idesc_16bit(128, S::ND, PT == PT_BF16);
+    constexpr uint32_t ID_LIFT = tc::idesc_16bit(128, S::NL, PT == PT_BF16);
+    int64_t diff_issued = -1, lift_issued = -1;
+    for (int64_t i = 0; i < nb_cta; ++i) {
+      const uint32_t par = (uint32_t)(i & 1);
+      // diff MMAs once every consumer warp wrote its state-plane rows
+      if (!warp_wait(&mbar[MB_AREADY], par)) break;
+      if (lane == 0) {
+        tc::fence_after_sync();
+        const uint32_t aq_h = tc::smem_u32(Aqh), aq_l = tc::smem_u32(Aql);
+        const uint32_t d_h = tc::smem_u32(smem + S::oDh), d_l = tc::smem_u32(smem + S::oDl);
+#pragma unroll
+        for (int kk = 0; kk < KD / 16; ++kk) {
+          const uint32_t off = kk * 256;
+          const uint64_t ah = tc::smem_desc(aq_h + off, 128, KD * 16);
+          const uint64_t al = tc::smem_desc(aq_l + off, 128, KD * 16);
+          const uint64_t bh = tc::smem_desc(d_h + off, 128, KD * 16);
+          const uint64_t bl = tc::smem_desc(d_l + off, 128, KD * 16);
+          tc::mma_bf16(tmem_diff, ah, bh, ID_DIFF, kk > 0 ? 1u : 0u);
+          tc::mma_bf16(tmem_diff, ah, bl, ID_DIFF, 1u);
+          tc::mma_bf16(tmem_diff, al, bh, ID_DIFF, 1u);
         }
+        tc::mma_commit(&mbar[MB_DIFF]);
       }
+      diff_issued = i;
+      // lift MMAs once every consumer warp wrote its flux-plane entries
+      if (!warp_wait(&mbar[MB_FREADY], par)) break;
+      if (lane == 0) {
+        tc::fence_after_sync();
+        const uint32_t af_h = tc::smem_u32(Afh), af_l = tc::smem_u32(Afl);
+        const uint32_t l_h = tc::smem_u32(smem + S::oLh), l_l = tc::smem_u32(smem + S::oLl);
+#pragma unroll
+        for (int kk = 0; kk < KL / 16; ++kk) {
+          const uint32_t off = kk * 256;
+          const uint64_t ah = tc::smem_desc(af_h + off, 128, KL * 16);
+          const uint64_t al = tc::smem_desc(af_l + off, 128, KL * 16);
+          const uint64_t bh = tc::smem_desc(l_h + off, 128, KL * 16);
+          const uint64_t bl = tc::smem_desc(l_l + off, 128, KL * 16);
+          tc::mma_bf16(tmem_lift, ah, bh, ID_LIFT, kk > 0 ? 1u : 0u);
+          tc::mma_bf16(tmem_lift, ah, bl, ID_LIFT, 1u);
+          tc::mma_bf16(tmem_lift, al, bh, ID_LIFT, 1u);
+        }
+        tc::mma_commit(&mbar[MB_LIFT]);
+      }
+      lift_issued = i;
+    }
+    if (lane == 0 && lift_issued + 1 < nb_cta) {
+      // left early: let the MMAs already issued finish before TMEM is released
+      atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+      if (diff_issued >= 0)
+        tc::mbar_wait(&mbar[MB_DIFF], (uint32_t)(diff_issued & 1), MBAR_MAX_NS);
+      if (lift_issued >= 0)
+        tc::mbar_wait(&mbar[MB_LIFT], (uint32_t)(lift_issued & 1), MBAR_MAX_NS);
+    }
+    __syncwarp();
+  } else if (warp == NCW) {
+    // ====== I/O warp: stage buffers in (bulk copies), results out ======
+    auto batch_el0 = [&](int64_t i) { return ((int64_t)blockIdx.x + i * gridDim.x) * EB; };
+    auto batch_ne = [&](int64_t el0) { return (int)((a.K - el0) < EB ? (a.K - el0) : EB); };
+    auto load_stage = [&](int64_t i) {
+      const int b = NSTG == 2 ? (int)(i & 1) : 0;
+      const int64_t el0 = batch_el0(i);
+      const int ne = batch_ne(el0);
       uint8_t* stg = smem + S::ostg + b * S::bStage;
+      uint64_t* mb = &mbar[MB_FULL + b];
+      if (lane == 0) {
+        uint32_t want = 0;
+        for (int f = 0; f < F; ++f) want += bulk_bytes(a.q_in + f * Knp + el0 * NP, ne * NP);
+        want += bulk_bytes(a.geo32 + el0 * G, ne * G);
+        want += bulk_bytes(a.conn + el0 * NF, ne * NF);
+        if constexpr (C != 0) want += bulk_bytes(a.coeff + el0 * NP, ne * NP);
+        if (want) mbar_expect_tx(mb, want);
+      }
+      __syncwarp();
       double* st = reinterpret_cast<double*>(stg);
-      for (int x = lane; x < S::NVAL; x += 32) {
-        const int f = x / FNP, r = x - f * FNP;
-        if (r < ne * NP) cp_async8(st + x, a.q_in + f * Knp + el0 * NP + r);
+      for (int f = 0; f < F; ++f)
+        stage_in(st + f * FNP, a.q_in + f * Knp + el0 * NP, ne * NP, lane, mb);
+      stage_in(reinterpret_cast<float*>(stg + S::sGeo), a.geo32 + el0 * G, ne * G, lane, mb);
+      stage_in(reinterpret_cast<int2*>(stg + S::sConn), a.conn + el0 * NF, ne * NF, lane, mb);
+      if constexpr (C != 0)
+        stage_in(reinterpret_cast<double*>(stg + S::sCoef), a.coeff + el0 * NP, ne * NP, lane, mb);
+      cp_async_arrive(mb);
+    };
+    auto load_res = [&](int64_t i) {
+      const int64_t el0 = batch_el0(i);
+      const int ne = batch_ne(el0);
+      uint64_t* mb = &mbar[MB_RES_FULL];
+      if (lane == 0) {
+        uint32_t want = 0;
+        for (int f = 0; f < F; ++f) want += bulk_bytes(a.res + f * Knp + el0 * NP, ne * NP);
+        if (want) mbar_expect_tx(mb, want);
       }
-      float* geo = reinterpret_cast<float*>(stg + S::sGeo);
-      for (int x = lane; x < ne * G; x += 32) cp_async4(geo + x, a.geo32 + el0 * G + x);
-      int2* cn = reinterpret_cast<int2*>(stg + S::sConn);
-      for (int x = lane; x < ne * NF; x += 32) cp_async8(cn + x, a.conn + el0 * NF + x);
-      if constexpr (C != 0) {
-        double* cf = reinterpret_cast<double*>(stg + S::sCoef);
-        for (int x = lane; x < ne * NP; x += 32) cp_async8(cf + x, a.coeff + el0 * NP + x);
+      __syncwarp();
+      for (int f = 0; f < F; ++f)
+        stage_in(rbuf + f * FNP, a.res + f * Knp + el0 * NP, ne * NP, lane, mb);
+      cp_async_arrive(mb);
+    };
+    bool ok = true;
+    if (nb_cta > 0) {
+      load_stage(0);
+      if (stage_res) load_res(0);
+    }
+    for (int64_t i = 0; i < nb_cta; ++i) {
+      const int b = NSTG == 2 ? (int)(i & 1) : 0;
+      if (NSTG == 2 && i + 1 < nb_cta) load_stage(i + 1);   // its buffer was stored out
+      // results: the stage buffer holds q_out (or the rhs), the residual buffer res
+      if (!warp_wait(&mbar[MB_DONE + b], (uint32_t)((i / NSTG) & 1))) {
+        ok = false;
+        break;
       }
-      cp_async_arrive(&mbar[MB_FULL + b]);
-      if (stage_res) {
-        if (it >= 1) {
-          int ok = 0;
-          if (lane == 0) ok = tc::mbar_wait(&mbar[MB_RES_FREE], (it - 1) & 1u, MBAR_MAX_NS);
-          if (!__shfl_sync(FULL, ok, 0)) {
-            if (lane == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
-            break;
-          }
+      {
+        const int64_t el0 = batch_el0(i);
+        const int ne = batch_ne(el0);
+        const double* st = reinterpret_cast<const double*>(smem + S::ostg + b * S::bStage);
+        for (int f = 0; f < F; ++f)
+          stage_out(a.q_out + f * Knp + el0 * NP, st + f * FNP, ne * NP, lane);
+        if (stage_res)
+          for (int f = 0; f < F; ++f)
+            stage_out(a.res + f * Knp + el0 * NP, rbuf + f * FNP, ne * NP, lane);
+        if (lane == 0) {
+          bulk_commit();
+          bulk_wait_read();     // the buffers may be refilled now
         }
-        for (int x = lane; x < S::NVAL; x += 32) {
-          const int f = x / FNP, r = x - f * FNP;
-          if (r < ne * NP) cp_async8(rbuf + x, a.res + f * Knp + el0 * NP + r);
-        }
-        cp_async_arrive(&mbar[MB_RES_FULL]);
+        __syncwarp();
       }
+      if (NSTG == 1 && i + 1 < nb_cta) load_stage(i + 1);
+      if (stage_res && i + 1 < nb_cta) load_res(i + 1);
+    }
+    if (lane == 0) {
+      if (!ok) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+      bulk_wait_all();
     }
     cp_async_drain();
+    __syncwarp();
   } else {
     // ================= consumer warps =================
-    const uint32_t tmem_diff = tmem;
-    const uint32_t tmem_lift = tmem + S::LIFT_COL;
-    constexpr uint32_t ID_DIFF = tc::idesc_16bit(128, S::ND, PT == PT_BF16);
-    constexpr uint32_t ID_LIFT = tc::idesc_16bit(128, S::NL, true);
     // TMEM lane of this thread (epilogue) = state-plane row (split pass)
     const int quad = warp & 3, part = warp >> 2;
     const int lf = lane / F;                 // element within the quadrant
@@ -437,37 +604,52 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
     const int e_lane = quad * EPW + lf;
     const uint32_t lane_addr = (uint32_t)(quad * 32) << 16;
     const int row = quad * 32 + lane;
-
+    auto warp_arrive = [&](uint64_t* mb) {
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(mb);
+    };
+    // A warp whose bounded wait gave up sets `bad` and does no more work.  With
+    // FP16 planes the consumers meet at one barrier per batch (row maxima of
+    // the state): there every warp learns of it and all leave together, so no
+    // warp is left waiting at a barrier.
+    int bad = 0;
     uint32_t it = 0;
     for (int64_t batch = blockIdx.x; batch < a.nbatch; batch += gridDim.x, ++it) {
       const int b = NSTG == 2 ? (int)(it & 1u) : 0;
+      const uint32_t par = it & 1u;
       const int64_t el0 = batch * EB;
       const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
+      double* st = reinterpret_cast<double*>(smem + S::ostg + b * S::bStage);  // [F][EB][NP]
       const uint8_t* stg = smem + S::ostg + b * S::bStage;
-      const double* st = reinterpret_cast<const double*>(stg);   // [F][EB][NP]
       const float* sgeo = reinterpret_cast<const float*>(stg + S::sGeo);
       const int2* sconn = reinterpret_cast<const int2*>(stg + S::sConn);
       const double* scoef = reinterpret_cast<const double*>(stg + S::sCoef);
       const bool valid = lane_used && e_lane < ne;
       const int e_own = valid ? e_lane : 0;
+      uint32_t* rmx = rsq + par * 128;     // this batch's state row maxima
+      uint32_t* fmx = rsf + par * 128;     // this batch's flux row maxima
 
-      if (cbar_or(!tc::mbar_wait(&mbar[MB_FULL + b], (it / NSTG) & 1u, MBAR_MAX_NS))) {
-        if (tid == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
-        break;
+      if (!bad && !warp_wait(&mbar[MB_FULL + b], (it / NSTG) & 1u)) {
+        if (lane == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+        bad = 1;
       }
+      if (PT == PT_BF16 && bad) break;
 
       // ---- A: remainders after the element's FP64 linear interpolant, split
       // into the state planes (one row per lane, 8 columns per item) ----
+      float lin[DIM];   // reference derivatives of the removed interpolant
       {
         double v0 = 0.0, dv[DIM];
 #pragma unroll
         for (int d = 0; d < DIM; ++d) dv[d] = 0.0;
-        if (valid) {
+        if (valid && !bad) {
           const double* q = st + fown * FNP + e_own * NP;
           v0 = q[0];
 #pragma unroll
           for (int d = 0; d < DIM; ++d) dv[d] = q[svert[d]] - v0;
         }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) lin[d] = (float)(0.5 * dv[d]);
         float rem[S::IPW][8];
         uint32_t rmax = 0u;
 #pragma unroll
@@ -478,11 +660,11 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
           for (int c = 0; c < 8; ++c) {
             const int j = chunk * 8 + c;
             float v = 0.f;
-            if (item < S::NITEM && valid && j < NP) {
-              double lin = v0;
+            if (item < S::NITEM && valid && !bad && j < NP) {
+              double l = v0;
 #pragma unroll
-              for (int d = 0; d < DIM; ++d) lin += slam[j * DIM + d] * dv[d];
-              v = (float)(st[fown * FNP + e_own * NP + j] - lin);
+              for (int d = 0; d < DIM; ++d) l += slam[j * DIM + d] * dv[d];
+              v = (float)(st[fown * FNP + e_own * NP + j] - l);
             }
             rem[k][c] = v;
             rmax = max(rmax, __float_as_uint(fabsf(v)));
@@ -490,9 +672,14 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
         }
         float inv = 1.0f;
         if constexpr (PT == PT_FP16) {
-          atomicMax(&rsq[row], rmax);
-          cbar();
-          inv = 1.0f / row_scale(rsq[row]);
+          atomicMax(&rmx[row], rmax);
+          if (cbar_or(bad)) break;
+          // every warp is past the previous epilogue: clear the next maxima
+          if (tid < 128) {
+            rsq[(par ^ 1u) * 128 + tid] = 0u;
+            rsf[(par ^ 1u) * 128 + tid] = 0u;
+          }
+          inv = 1.0f / row_scale(rmx[row]);
         }
 #pragma unroll
         for (int k = 0; k < S::IPW; ++k) {
@@ -523,167 +710,160 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
           }
         }
       }
+      // the diff MMA (issued by the MMA warp) reads the planes
       tc::fence_proxy_async();
-      cbar();
+      tc::fence_before_sync();
+      warp_arrive(&mbar[MB_AREADY]);
 
-      // ---- B: diff MMAs (one thread) ----
-      if (tid == 0) {
-        tc::fence_after_sync();
-        const uint32_t aq_h = tc::smem_u32(Aqh), aq_l = tc::smem_u32(Aql);
-        const uint32_t d_h = tc::smem_u32(smem + S::oDh), d_l = tc::smem_u32(smem + S::oDl);
+      // ---- C: face fluxes (FP32 on jumps formed in FP64) -> lift planes;
+      // all of a thread's face points in one round ----
+      constexpr int FR = S::NFV;
+      static_assert(FR * NA <= 32, "face points in flight exceed the register budget");
+      float uPs[FR][NA];
+      bool okp[FR];
+      // pass 1: ext-side values (global gathers for neighbours outside the batch)
 #pragma unroll
-        for (int kk = 0; kk < KD / 16; ++kk) {
-          const uint32_t off = kk * 256;
-          const uint64_t ah = tc::smem_desc(aq_h + off, 128, KD * 16);
-          const uint64_t al = tc::smem_desc(aq_l + off, 128, KD * 16);
-          const uint64_t bh = tc::smem_desc(d_h + off, 128, KD * 16);
-          const uint64_t bl = tc::smem_desc(d_l + off, 128, KD * 16);
-          tc::mma_bf16(tmem_diff, ah, bh, ID_DIFF, kk > 0 ? 1u : 0u);
-          tc::mma_bf16(tmem_diff, ah, bl, ID_DIFF, 1u);
-          tc::mma_bf16(tmem_diff, al, bh, ID_DIFF, 1u);
-        }
-        tc::mma_commit(&mbar[MB_DIFF]);
-      }
-
-      // ---- C: face fluxes (FP32 on jumps formed in FP64) -> BF16 lift planes ----
-      constexpr int FROUND = FaceRound<NA, S::NFV>::value;
-#pragma unroll 1
-      for (int u0 = 0; u0 < S::NFV; u0 += FROUND) {
-        float uPs[FROUND][NA];
-        bool okp[FROUND];
-        // pass 1: ext-side values (global gathers for neighbours outside the batch)
+      for (int u = 0; u < FR; ++u) {
+        const int x = tid + u * CONSUMERS;
+        const int e = x / NFPT, p = x % NFPT, face = p / NFP, k = p % NFP;
+        okp[u] = false;
+        if (x < S::NFACE && e < ne) {
+          const int2 cn = sconn[e * NF + face];
+          const int nb = cn.x;
+          if (nb >= 0) {
+            const int code = cn.y;
+            const int nface = code & 3, perm = code >> 2;
+            if (nface < NF && perm < a.nperm && nb < a.K) {
+              const int nn = sfm[nface * NFP + ssh[perm * NFP + k]];
+              const int64_t gi = (int64_t)nb * NP + nn;
+              const int lnode = sfm[p];
+              const int lb = (int)(nb - el0);   // neighbour inside this batch?
+              const bool inb = lb >= 0 && lb < ne;
+              if constexpr (JumpLinear<MODEL>::value) {
 #pragma unroll
-        for (int u = 0; u < FROUND; ++u) {
-          const int x = u0 + u < S::NFV ? tid + (u0 + u) * CONSUMERS : S::NFACE;
-          const int e = x / NFPT, p = x % NFPT, face = p / NFP, k = p % NFP;
-          okp[u] = false;
-          if (x < S::NFACE && e < ne) {
-            const int2 cn = sconn[e * NF + face];
-            const int nb = cn.x;
-            if (nb >= 0) {
-              const int code = cn.y;
-              const int nface = code & 3, perm = code >> 2;
-              if (nface < NF && perm < a.nperm && nb < a.K) {
-                const int nn = sfm[nface * NFP + ssh[perm * NFP + k]];
-                const int64_t gi = (int64_t)nb * NP + nn;
-                const int lnode = sfm[p];
-                const int lb = (int)(nb - el0);   // neighbour inside this batch?
-                const bool inb = lb >= 0 && lb < ne;
-                if constexpr (JumpLinear<MODEL>::value) {
-#pragma unroll
-                  for (int f = 0; f < F; ++f) {
-                    const double qm = st[f * FNP + e * NP + lnode];
-                    const double qp = inb ? st[f * FNP + lb * NP + nn]
-                                          : __ldg(a.q_in + f * Knp + gi);
-                    uPs[u][f] = (float)(qm - qp);
-                  }
-                } else {
-                  if constexpr (C != 0)
-                    uPs[u][0] = inb ? (float)scoef[lb * NP + nn] : (float)__ldg(a.coeff + gi);
-#pragma unroll
-                  for (int f = 0; f < F; ++f)
-                    uPs[u][C + f] = inb ? (float)st[f * FNP + lb * NP + nn]
-                                        : (float)__ldg(a.q_in + f * Knp + gi);
+                for (int f = 0; f < F; ++f) {
+                  const double qm = st[f * FNP + e * NP + lnode];
+                  const double qp = inb ? st[f * FNP + lb * NP + nn]
+                                        : __ldg(a.q_in + f * Knp + gi);
+                  uPs[u][f] = (float)(qm - qp);
                 }
-                okp[u] = true;
               } else {
-                atomicCAS(a.err, 0, DEV_BAD_CODE);
+                if constexpr (C != 0)
+                  uPs[u][0] = inb ? (float)scoef[lb * NP + nn] : (float)__ldg(a.coeff + gi);
+#pragma unroll
+                for (int f = 0; f < F; ++f)
+                  uPs[u][C + f] = inb ? (float)st[f * FNP + lb * NP + nn]
+                                      : (float)__ldg(a.q_in + f * Knp + gi);
               }
+              okp[u] = true;
+            } else {
+              atomicCAS(a.err, 0, DEV_BAD_CODE);
             }
           }
         }
-        // pass 2: fluxes, split straight into the BF16 lift planes
+      }
+      // pass 2: fluxes times Fscale -> uPs[u][0..F)
 #pragma unroll
-        for (int u = 0; u < FROUND; ++u) {
-          const int x = u0 + u < S::NFV ? tid + (u0 + u) * CONSUMERS : S::NFACE;
-          const int e = x / NFPT, p = x % NFPT, face = p / NFP, k = p % NFP;
-          if (x < S::NFACE && e < ne) {
-            const int lnode = sfm[p];
-            float uM[NA], uP[NA], n[DIM], fl[F];
-            const float* gf = sgeo + e * G + DIM * DIM + face * (DIM + 1);
+      for (int u = 0; u < FR; ++u) {
+        const int x = tid + u * CONSUMERS;
+        const int e = x / NFPT, p = x % NFPT, face = p / NFP, k = p % NFP;
+        float fl[F];
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) n[d] = gf[d];
-            const float fscale = gf[DIM];
-            const int2 cn = sconn[e * NF + face];
-            const int nb = cn.x;
-            bool have = true, bdry = false;
-            if (nb >= 0 && JumpLinear<MODEL>::value) {
+        for (int f = 0; f < F; ++f) fl[f] = 0.f;
+        if (x < S::NFACE && e < ne) {
+          const int lnode = sfm[p];
+          float uM[NA], uP[NA], n[DIM];
+          const float* gf = sgeo + e * G + DIM * DIM + face * (DIM + 1);
+#pragma unroll
+          for (int d = 0; d < DIM; ++d) n[d] = gf[d];
+          const float fscale = gf[DIM];
+          const int2 cn = sconn[e * NF + face];
+          const int nb = cn.x;
+          bool have = true, bdry = false;
+          if (nb >= 0 && JumpLinear<MODEL>::value) {
+            have = okp[u];
+#pragma unroll
+            for (int q = 0; q < NA; ++q) { uM[q] = uPs[u][q]; uP[q] = 0.f; }
+          } else {
+            if constexpr (C != 0) uM[0] = (float)scoef[e * NP + lnode];
+#pragma unroll
+            for (int f = 0; f < F; ++f) uM[C + f] = (float)st[f * FNP + e * NP + lnode];
+            if (nb >= 0) {
               have = okp[u];
 #pragma unroll
-              for (int q = 0; q < NA; ++q) { uM[q] = uPs[u][q]; uP[q] = 0.f; }
+              for (int q = 0; q < NA; ++q) uP[q] = uPs[u][q];
             } else {
-              if constexpr (C != 0) uM[0] = (float)scoef[e * NP + lnode];
-#pragma unroll
-              for (int f = 0; f < F; ++f) uM[C + f] = (float)st[f * FNP + e * NP + lnode];
-              if (nb >= 0) {
-                have = okp[u];
-#pragma unroll
-                for (int q = 0; q < NA; ++q) uP[q] = uPs[u][q];
-              } else {
-                bdry = true;
-                const int kind = cn.y;
-                float given = 0.f;
-                if (kind == HB_BC_GIVEN) {
-                  const int64_t bi = (int64_t)(-1 - nb) * NFP + k;
-                  if (a.bdry == nullptr || bi >= a.n_given) {
-                    atomicCAS(a.err, 0, a.bdry == nullptr ? DEV_MISSING_INPUT : DEV_BAD_BDRY_INDEX);
-                    have = false;
-                  } else {
-                    given = (float)__ldg(a.bdry + bi);
-                  }
+              bdry = true;
+              const int kind = cn.y;
+              float given = 0.f;
+              if (kind == HB_BC_GIVEN) {
+                const int64_t bi = (int64_t)(-1 - nb) * NFP + k;
+                if (a.bdry == nullptr || bi >= a.n_given) {
+                  atomicCAS(a.err, 0, a.bdry == nullptr ? DEV_MISSING_INPUT : DEV_BAD_BDRY_INDEX);
+                  have = false;
+                } else {
+                  given = (float)__ldg(a.bdry + bi);
                 }
-                if (have) have = model_bc<MODEL, DIM, float>(a.mp, kind, uM, n, given, uP);
               }
+              if (have) have = model_bc<MODEL, DIM, float>(a.mp, kind, uM, n, given, uP);
             }
-            if (have) model_flux<MODEL, DIM, float>(a.mp, bdry, uM, uP, n, fl);
-            const int rowb = (e / EPW) * 32 + (e % EPW) * F;
+          }
+          if (have) {
+            model_flux<MODEL, DIM, float>(a.mp, bdry, uM, uP, n, fl);
 #pragma unroll
-            for (int f = 0; f < F; ++f)
-              store_split<PT_BF16>(Afh, Afl, kmajor_off(rowb + f, p, KL),
-                                   have ? fscale * fl[f] : 0.f);
+            for (int f = 0; f < F; ++f) fl[f] *= fscale;
+          }
+        }
+#pragma unroll
+        for (int f = 0; f < F; ++f) uPs[u][f] = fl[f];
+      }
+      if constexpr (PT == PT_FP16) {
+        // row maxima of the flux rows (e, f): the lanes of one element combine
+        // theirs, then one of them updates shared memory
+#pragma unroll
+        for (int u = 0; u < FR; ++u) {
+          const int x = tid + u * CONSUMERS;
+          const int e = x < S::NFACE ? x / NFPT : -1;
+          const unsigned grp = __match_any_sync(FULL, e);
+          const bool leader = (__ffs(grp) - 1) == lane;
+#pragma unroll
+          for (int f = 0; f < F; ++f) {
+            const unsigned m = __reduce_max_sync(grp, __float_as_uint(fabsf(uPs[u][f])));
+            if (leader && e >= 0 && e < ne)
+              atomicMax(&fmx[(e / EPW) * 32 + (e % EPW) * F + f], m);
+          }
+        }
+        cbar();   // no bounded wait lies between the state barrier and this one
+      }
+      // pass 3: split into the lift planes (FP16: each row scaled by a power
+      // of two from its maximum, like the state rows)
+#pragma unroll
+      for (int u = 0; u < FR; ++u) {
+        const int x = tid + u * CONSUMERS;
+        const int e = x / NFPT, p = x % NFPT;
+        if (x < S::NFACE && e < ne) {
+          const int rowb = (e / EPW) * 32 + (e % EPW) * F;
+#pragma unroll
+          for (int f = 0; f < F; ++f) {
+            float v = uPs[u][f];
+            if constexpr (PT == PT_FP16) v *= 1.0f / row_scale(fmx[rowb + f]);
+            store_split<PT>(Afh, Afl, kmajor_off(rowb + f, p, KL), v);
           }
         }
       }
       tc::fence_proxy_async();
-      cbar();
+      warp_arrive(&mbar[MB_FREADY]);
 
-      // ---- D: lift MMAs (one thread) ----
-      if (tid == 0) {
-        tc::fence_after_sync();
-        const uint32_t af_h = tc::smem_u32(Afh), af_l = tc::smem_u32(Afl);
-        const uint32_t l_h = tc::smem_u32(smem + S::oLh), l_l = tc::smem_u32(smem + S::oLl);
-#pragma unroll
-        for (int kk = 0; kk < KL / 16; ++kk) {
-          const uint32_t off = kk * 256;
-          const uint64_t ah = tc::smem_desc(af_h + off, 128, KL * 16);
-          const uint64_t al = tc::smem_desc(af_l + off, 128, KL * 16);
-          const uint64_t bh = tc::smem_desc(l_h + off, 128, KL * 16);
-          const uint64_t bl = tc::smem_desc(l_l + off, 128, KL * 16);
-          tc::mma_bf16(tmem_lift, ah, bh, ID_LIFT, kk > 0 ? 1u : 0u);
-          tc::mma_bf16(tmem_lift, ah, bl, ID_LIFT, 1u);
-          tc::mma_bf16(tmem_lift, al, bh, ID_LIFT, 1u);
-        }
-        tc::mma_commit(&mbar[MB_LIFT]);
-      }
-
-      // ---- E: TMEM -> chain rule, volume terms, + lift -> staged rhs ----
-      // one thread waits on the tensor core; the others sleep in the barrier
-      int late = 0;
-      if (tid == 0) {
-        const bool w0 = tc::mbar_wait(&mbar[MB_DIFF], it & 1u, MBAR_MAX_NS);
-        const bool w1 = tc::mbar_wait(&mbar[MB_LIFT], it & 1u, MBAR_MAX_NS);
-        late = !(w0 && w1);
-      }
-      if (cbar_or(late)) {
-        // the MMAs did not complete in time: flag, give them one more bounded
-        // wait, then leave (TMEM is released below)
-        if (tid == 0) {
-          atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
-          tc::mbar_wait(&mbar[MB_DIFF], it & 1u, MBAR_MAX_NS);
-          tc::mbar_wait(&mbar[MB_LIFT], it & 1u, MBAR_MAX_NS);
-        }
-        cbar();
-        break;
+      // ---- E: TMEM -> chain rule, volume terms, + lift -> FP64 stage update
+      // in place (the I/O warp stores the buffers out) ----
+      const bool w0 = warp_wait(&mbar[MB_DIFF], par);
+      const bool w1 = w0 && warp_wait(&mbar[MB_LIFT], par);
+      const bool wr = !stage_res || (w1 && warp_wait(&mbar[MB_RES_FULL], par));
+      if (!(w0 && w1 && wr)) {
+        if (lane == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+        bad = 1;
+        if (PT == PT_BF16) break;
+        continue;   // leaves at the next batch's barrier (or the loop's end)
       }
       tc::fence_after_sync();
       {
@@ -694,26 +874,25 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
 #pragma unroll
           for (int x = 0; x < DIM; ++x) gm[r][x] = ge[r * DIM + x];
         const int base = lf * F;
-        // reference derivatives of the removed linear interpolant: (q_v - q_A)/2
-        float lin[DIM];
-        {
-          const double* q = st + fown * FNP + e_own * NP;
-#pragma unroll
-          for (int r = 0; r < DIM; ++r) lin[r] = (float)(0.5 * (q[svert[r]] - q[0]));
+        float sdiff = a.op_scale_d, slift = a.op_scale_l;
+        if constexpr (PT == PT_FP16) {
+          sdiff *= row_scale(rmx[row]);
+          slift *= row_scale(fmx[row]);
         }
-        float sdiff = a.op_scale_d;
-        if constexpr (PT == PT_FP16) sdiff *= row_scale(rsq[row]);
+        double* qo = st + fown * FNP + e_own * NP;
+        double* ro = rbuf + fown * FNP + e_own * NP;
+        const int64_t gidx = fown * Knp + (el0 + e_own) * NP;
         const int i_lo = part * S::NPQ;
         const int i_hi = (part + 1) * S::NPQ < NP ? (part + 1) * S::NPQ : NP;
 #pragma unroll 1
-        for (int i0 = i_lo; i0 < i_hi; i0 += 2) {
-          float dv[DIM][2], lv[2];
+        for (int i0 = i_lo; i0 < i_hi; i0 += 4) {
+          float dv[DIM][4], lv[4];
 #pragma unroll
-          for (int r = 0; r < DIM; ++r) tc::tmem_ld2(tmem_diff + lane_addr + r * NP + i0, dv[r]);
-          tc::tmem_ld2(tmem_lift + lane_addr + i0, lv);
+          for (int r = 0; r < DIM; ++r) tc::tmem_ld4(tmem_diff + lane_addr + r * NP + i0, dv[r]);
+          tc::tmem_ld4(tmem_lift + lane_addr + i0, lv);
           tc::tmem_wait_ld();
 #pragma unroll
-          for (int c = 0; c < 2; ++c) {
+          for (int c = 0; c < 4; ++c) {
             const int i = i0 + c;
             float g[DIM];
 #pragma unroll
@@ -727,45 +906,24 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
             const float mine = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
             if (valid && i < i_hi) {
               const float src = a.source ? (float)a.source[(el0 + e_own) * NP + i] : 0.f;
-              sq[fown * FNP + e_own * NP + i] =
-                  model_finish<MODEL, DIM, float>(a.mp, fown, mine, lv[c], src);
+              const double rr =
+                  (double)model_finish<MODEL, DIM, float>(a.mp, fown, mine, lv[c] * slift, src);
+              if (a.mode == 0) {
+                qo[i] = rr;
+              } else {
+                const double r0 = S::RES ? ro[i] : a.res[gidx + i];
+                const double nr = a.ra * r0 + a.dt * rr;
+                if constexpr (S::RES) ro[i] = nr;
+                else a.res[gidx + i] = nr;
+                qo[i] = qo[i] + a.rb * nr;
+              }
             }
           }
         }
       }
       tc::fence_before_sync();
-      if (stage_res) {
-        if (cbar_or(!tc::mbar_wait(&mbar[MB_RES_FULL], it & 1u, MBAR_MAX_NS))) {
-          if (tid == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
-          break;
-        }
-      } else {
-        cbar();
-      }
-
-      // ---- F: FP64 stage update (state and residual already in shared memory) ----
-      if (tid < 128) rsq[tid] = 0u;
-#pragma unroll 4
-      for (int x = tid; x < S::NVAL; x += CONSUMERS) {
-        const int f = x / FNP, r = x - f * FNP;
-        if (r < ne * NP) {
-          const int64_t idx = f * Knp + el0 * NP + r;
-          const double rr = (double)sq[x];
-          if (a.mode == 0) {
-            a.q_out[idx] = rr;
-          } else {
-            const double r0 = S::RES ? rbuf[x] : a.res[idx];
-            const double nr = a.ra * r0 + a.dt * rr;
-            a.res[idx] = nr;
-            a.q_out[idx] = st[x] + a.rb * nr;
-          }
-        }
-      }
-      cbar();
-      if (tid == 0) {
-        tc::mbar_arrive(&mbar[MB_FREE + b]);
-        if (stage_res) tc::mbar_arrive(&mbar[MB_RES_FREE]);
-      }
+      tc::fence_proxy_async();
+      warp_arrive(&mbar[MB_DONE + b]);
     }
   }
 
@@ -961,9 +1119,9 @@ static hb_status configure_split(Op* op) {
         for (int dd = 0; dd < DIM; ++dd)
           lam[j * DIM + dd] = 0.5 * (1.0 + d->unit_nodes[(size_t)j * DIM + dd]);
     }
-    const double sd = plane_scale(Dt, PT), sl = 1.0;   // the lift is always BF16
+    const double sd = plane_scale(Dt, PT), sl = plane_scale(Lt, PT);
     build_planes(Dt, DIM * np, np, S::ND, S::KD, PT, sd, img.data(), img.data() + bD);
-    build_planes(Lt, np, nfpt, S::NL, S::KL, PT_BF16, sl, img.data() + 2 * bD,
+    build_planes(Lt, np, nfpt, S::NL, S::KL, PT, sl, img.data() + 2 * bD,
                  img.data() + 2 * bD + bL);
     SplitOps* so = static_cast<SplitOps*>(op->split_ops);
     so->scale_d = (float)sd;
