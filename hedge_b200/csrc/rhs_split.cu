@@ -199,8 +199,14 @@ __device__ __forceinline__ void store_split(uint8_t* hi, uint8_t* lo, uint32_t o
 // power-of-two row scale from the bit pattern of the row's largest |value|
 __device__ __forceinline__ float row_scale(uint32_t maxbits) {
   int e = (int)((maxbits >> 23) & 0xffu) - 13;   // max / 2^(e-127) in [2^13, 2^14)
-  e = e < 1 ? 1 : (e > 254 ? 254 : e);
+  e = e < 1 ? 1 : (e > 253 ? 253 : e);
   return maxbits == 0 ? 1.0f : __uint_as_float((uint32_t)e << 23);
+}
+// its exact reciprocal (also a power of two)
+__device__ __forceinline__ float row_scale_inv(uint32_t maxbits) {
+  int e = (int)((maxbits >> 23) & 0xffu) - 13;
+  e = e < 1 ? 1 : (e > 253 ? 253 : e);
+  return maxbits == 0 ? 1.0f : __uint_as_float((uint32_t)(254 - e) << 23);
 }
 
 // Ampere-style asynchronous 8-byte global -> shared copy (no registers held)
@@ -675,11 +681,8 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
           atomicMax(&rmx[row], rmax);
           if (cbar_or(bad)) break;
           // every warp is past the previous epilogue: clear the next maxima
-          if (tid < 128) {
-            rsq[(par ^ 1u) * 128 + tid] = 0u;
-            rsf[(par ^ 1u) * 128 + tid] = 0u;
-          }
-          inv = 1.0f / row_scale(rmx[row]);
+          if (tid < 128) rsq[(par ^ 1u) * 128 + tid] = 0u;
+          inv = row_scale_inv(rmx[row]);
         }
 #pragma unroll
         for (int k = 0; k < S::IPW; ++k) {
@@ -715,139 +718,146 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
       tc::fence_before_sync();
       warp_arrive(&mbar[MB_AREADY]);
 
-      // ---- C: face fluxes (FP32 on jumps formed in FP64) -> lift planes;
-      // all of a thread's face points in one round ----
-      constexpr int FR = S::NFV;
-      static_assert(FR * NA <= 32, "face points in flight exceed the register budget");
-      float uPs[FR][NA];
-      bool okp[FR];
-      // pass 1: ext-side values (global gathers for neighbours outside the batch)
-#pragma unroll
-      for (int u = 0; u < FR; ++u) {
-        const int x = tid + u * CONSUMERS;
-        const int e = x / NFPT, p = x % NFPT, face = p / NFP, k = p % NFP;
-        okp[u] = false;
-        if (x < S::NFACE && e < ne) {
-          const int2 cn = sconn[e * NF + face];
-          const int nb = cn.x;
-          if (nb >= 0) {
-            const int code = cn.y;
-            const int nface = code & 3, perm = code >> 2;
-            if (nface < NF && perm < a.nperm && nb < a.K) {
-              const int nn = sfm[nface * NFP + ssh[perm * NFP + k]];
-              const int64_t gi = (int64_t)nb * NP + nn;
-              const int lnode = sfm[p];
-              const int lb = (int)(nb - el0);   // neighbour inside this batch?
-              const bool inb = lb >= 0 && lb < ne;
-              if constexpr (JumpLinear<MODEL>::value) {
-#pragma unroll
-                for (int f = 0; f < F; ++f) {
-                  const double qm = st[f * FNP + e * NP + lnode];
-                  const double qp = inb ? st[f * FNP + lb * NP + nn]
-                                        : __ldg(a.q_in + f * Knp + gi);
-                  uPs[u][f] = (float)(qm - qp);
-                }
-              } else {
-                if constexpr (C != 0)
-                  uPs[u][0] = inb ? (float)scoef[lb * NP + nn] : (float)__ldg(a.coeff + gi);
-#pragma unroll
-                for (int f = 0; f < F; ++f)
-                  uPs[u][C + f] = inb ? (float)st[f * FNP + lb * NP + nn]
-                                      : (float)__ldg(a.q_in + f * Knp + gi);
-              }
-              okp[u] = true;
-            } else {
-              atomicCAS(a.err, 0, DEV_BAD_CODE);
-            }
-          }
-        }
-      }
-      // pass 2: fluxes times Fscale -> uPs[u][0..F)
-#pragma unroll
-      for (int u = 0; u < FR; ++u) {
-        const int x = tid + u * CONSUMERS;
-        const int e = x / NFPT, p = x % NFPT, face = p / NFP, k = p % NFP;
-        float fl[F];
-#pragma unroll
-        for (int f = 0; f < F; ++f) fl[f] = 0.f;
-        if (x < S::NFACE && e < ne) {
-          const int lnode = sfm[p];
-          float uM[NA], uP[NA], n[DIM];
-          const float* gf = sgeo + e * G + DIM * DIM + face * (DIM + 1);
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) n[d] = gf[d];
-          const float fscale = gf[DIM];
-          const int2 cn = sconn[e * NF + face];
-          const int nb = cn.x;
-          bool have = true, bdry = false;
-          if (nb >= 0 && JumpLinear<MODEL>::value) {
-            have = okp[u];
-#pragma unroll
-            for (int q = 0; q < NA; ++q) { uM[q] = uPs[u][q]; uP[q] = 0.f; }
-          } else {
-            if constexpr (C != 0) uM[0] = (float)scoef[e * NP + lnode];
-#pragma unroll
-            for (int f = 0; f < F; ++f) uM[C + f] = (float)st[f * FNP + e * NP + lnode];
-            if (nb >= 0) {
-              have = okp[u];
-#pragma unroll
-              for (int q = 0; q < NA; ++q) uP[q] = uPs[u][q];
-            } else {
-              bdry = true;
-              const int kind = cn.y;
-              float given = 0.f;
-              if (kind == HB_BC_GIVEN) {
-                const int64_t bi = (int64_t)(-1 - nb) * NFP + k;
-                if (a.bdry == nullptr || bi >= a.n_given) {
-                  atomicCAS(a.err, 0, a.bdry == nullptr ? DEV_MISSING_INPUT : DEV_BAD_BDRY_INDEX);
-                  have = false;
-                } else {
-                  given = (float)__ldg(a.bdry + bi);
-                }
-              }
-              if (have) have = model_bc<MODEL, DIM, float>(a.mp, kind, uM, n, given, uP);
-            }
-          }
-          if (have) {
-            model_flux<MODEL, DIM, float>(a.mp, bdry, uM, uP, n, fl);
-#pragma unroll
-            for (int f = 0; f < F; ++f) fl[f] *= fscale;
-          }
-        }
-#pragma unroll
-        for (int f = 0; f < F; ++f) uPs[u][f] = fl[f];
-      }
-      if constexpr (PT == PT_FP16) {
-        // row maxima of the flux rows (e, f): the lanes of one element combine
-        // theirs, then one of them updates shared memory
+      // ---- C: face fluxes (FP32 on jumps formed in FP64) -> lift planes.
+      // Warp w takes the elements w, w + NCW, ... of the batch and lane l
+      // their face points l, l + 32, ..., so each flux row (e, f) lies in one
+      // warp (its FP16 scale is a warp reduction) ----
+      constexpr int SPE = (NFPT + 31) / 32;                  // point slots per element
+      constexpr int NEPW = (EB + NCW - 1) / NCW;             // elements per warp
+      static_assert(SPE * NA <= 32, "face points in flight exceed the register budget");
+      constexpr int ER0 = 32 / (SPE * NA);
+      constexpr int ER = ER0 < NEPW ? ER0 : NEPW;            // elements per round
+      constexpr int FR = ER * SPE;
+#pragma unroll 1
+      for (int j0 = 0; j0 < NEPW; j0 += ER) {
+        float uPs[FR][NA];
+        bool okp[FR];
+        // pass 1: ext-side values (global gathers for neighbours outside the batch)
 #pragma unroll
         for (int u = 0; u < FR; ++u) {
-          const int x = tid + u * CONSUMERS;
-          const int e = x < S::NFACE ? x / NFPT : -1;
-          const unsigned grp = __match_any_sync(FULL, e);
-          const bool leader = (__ffs(grp) - 1) == lane;
+          const int j = j0 + u / SPE;
+          const int e = warp + j * NCW, p = lane + (u % SPE) * 32;
+          const int face = p / NFP, k = p % NFP;
+          okp[u] = false;
+          if (j < NEPW && e < ne && p < NFPT) {
+            const int2 cn = sconn[e * NF + face];
+            const int nb = cn.x;
+            if (nb >= 0) {
+              const int code = cn.y;
+              const int nface = code & 3, perm = code >> 2;
+              if (nface < NF && perm < a.nperm && nb < a.K) {
+                const int nn = sfm[nface * NFP + ssh[perm * NFP + k]];
+                const int64_t gi = (int64_t)nb * NP + nn;
+                const int lnode = sfm[p];
+                const int lb = (int)(nb - el0);   // neighbour inside this batch?
+                const bool inb = lb >= 0 && lb < ne;
+                if constexpr (JumpLinear<MODEL>::value) {
 #pragma unroll
-          for (int f = 0; f < F; ++f) {
-            const unsigned m = __reduce_max_sync(grp, __float_as_uint(fabsf(uPs[u][f])));
-            if (leader && e >= 0 && e < ne)
-              atomicMax(&fmx[(e / EPW) * 32 + (e % EPW) * F + f], m);
+                  for (int f = 0; f < F; ++f) {
+                    const double qm = st[f * FNP + e * NP + lnode];
+                    const double qp = inb ? st[f * FNP + lb * NP + nn]
+                                          : __ldg(a.q_in + f * Knp + gi);
+                    uPs[u][f] = (float)(qm - qp);
+                  }
+                } else {
+                  if constexpr (C != 0)
+                    uPs[u][0] = inb ? (float)scoef[lb * NP + nn] : (float)__ldg(a.coeff + gi);
+#pragma unroll
+                  for (int f = 0; f < F; ++f)
+                    uPs[u][C + f] = inb ? (float)st[f * FNP + lb * NP + nn]
+                                        : (float)__ldg(a.q_in + f * Knp + gi);
+                }
+                okp[u] = true;
+              } else {
+                atomicCAS(a.err, 0, DEV_BAD_CODE);
+              }
+            }
           }
         }
-        cbar();   // no bounded wait lies between the state barrier and this one
-      }
-      // pass 3: split into the lift planes (FP16: each row scaled by a power
-      // of two from its maximum, like the state rows)
+        // pass 2: fluxes times Fscale -> uPs[u][0..F)
 #pragma unroll
-      for (int u = 0; u < FR; ++u) {
-        const int x = tid + u * CONSUMERS;
-        const int e = x / NFPT, p = x % NFPT;
-        if (x < S::NFACE && e < ne) {
-          const int rowb = (e / EPW) * 32 + (e % EPW) * F;
+        for (int u = 0; u < FR; ++u) {
+          const int j = j0 + u / SPE;
+          const int e = warp + j * NCW, p = lane + (u % SPE) * 32;
+          const int face = p / NFP, k = p % NFP;
+          float fl[F];
 #pragma unroll
-          for (int f = 0; f < F; ++f) {
-            float v = uPs[u][f];
-            if constexpr (PT == PT_FP16) v *= 1.0f / row_scale(fmx[rowb + f]);
-            store_split<PT>(Afh, Afl, kmajor_off(rowb + f, p, KL), v);
+          for (int f = 0; f < F; ++f) fl[f] = 0.f;
+          if (j < NEPW && e < ne && p < NFPT) {
+            const int lnode = sfm[p];
+            float uM[NA], uP[NA], n[DIM];
+            const float* gf = sgeo + e * G + DIM * DIM + face * (DIM + 1);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) n[d] = gf[d];
+            const float fscale = gf[DIM];
+            const int2 cn = sconn[e * NF + face];
+            const int nb = cn.x;
+            bool have = true, bdry = false;
+            if (nb >= 0 && JumpLinear<MODEL>::value) {
+              have = okp[u];
+#pragma unroll
+              for (int q = 0; q < NA; ++q) { uM[q] = uPs[u][q]; uP[q] = 0.f; }
+            } else {
+              if constexpr (C != 0) uM[0] = (float)scoef[e * NP + lnode];
+#pragma unroll
+              for (int f = 0; f < F; ++f) uM[C + f] = (float)st[f * FNP + e * NP + lnode];
+              if (nb >= 0) {
+                have = okp[u];
+#pragma unroll
+                for (int q = 0; q < NA; ++q) uP[q] = uPs[u][q];
+              } else {
+                bdry = true;
+                const int kind = cn.y;
+                float given = 0.f;
+                if (kind == HB_BC_GIVEN) {
+                  const int64_t bi = (int64_t)(-1 - nb) * NFP + k;
+                  if (a.bdry == nullptr || bi >= a.n_given) {
+                    atomicCAS(a.err, 0, a.bdry == nullptr ? DEV_MISSING_INPUT : DEV_BAD_BDRY_INDEX);
+                    have = false;
+                  } else {
+                    given = (float)__ldg(a.bdry + bi);
+                  }
+                }
+                if (have) have = model_bc<MODEL, DIM, float>(a.mp, kind, uM, n, given, uP);
+              }
+            }
+            if (have) {
+              model_flux<MODEL, DIM, float>(a.mp, bdry, uM, uP, n, fl);
+#pragma unroll
+              for (int f = 0; f < F; ++f) fl[f] *= fscale;
+            }
+          }
+#pragma unroll
+          for (int f = 0; f < F; ++f) uPs[u][f] = fl[f];
+        }
+        // pass 3: split into the lift planes; FP16 rows are scaled by a power
+        // of two from the row's largest |flux| (a warp reduction), which the
+        // epilogue undoes
+#pragma unroll
+        for (int jj = 0; jj < ER; ++jj) {
+          const int j = j0 + jj;
+          const int e = warp + j * NCW;
+          if (j < NEPW && e < ne) {      // warp-uniform
+            const int rowb = (e / EPW) * 32 + (e % EPW) * F;
+#pragma unroll
+            for (int f = 0; f < F; ++f) {
+              float inv = 1.0f;
+              if constexpr (PT == PT_FP16) {
+                uint32_t m = 0u;
+#pragma unroll
+                for (int sl = 0; sl < SPE; ++sl)
+                  m = max(m, __float_as_uint(fabsf(uPs[jj * SPE + sl][f])));
+                m = __reduce_max_sync(FULL, m);
+                if (lane == 0) fmx[rowb + f] = m;
+                inv = row_scale_inv(m);
+              }
+#pragma unroll
+              for (int sl = 0; sl < SPE; ++sl) {
+                const int p = lane + sl * 32;
+                if (p < NFPT)
+                  store_split<PT>(Afh, Afl, kmajor_off(rowb + f, p, KL), uPs[jj * SPE + sl][f] * inv);
+              }
+            }
           }
         }
       }
@@ -856,7 +866,9 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
 
       // ---- E: TMEM -> chain rule, volume terms, + lift -> FP64 stage update
       // in place (the I/O warp stores the buffers out) ----
-      const bool w0 = warp_wait(&mbar[MB_DIFF], par);
+      // (FREADY also orders the flux row maxima the other warps wrote)
+      const bool wf = PT == PT_BF16 || warp_wait(&mbar[MB_FREADY], par);
+      const bool w0 = wf && warp_wait(&mbar[MB_DIFF], par);
       const bool w1 = w0 && warp_wait(&mbar[MB_LIFT], par);
       const bool wr = !stage_res || (w1 && warp_wait(&mbar[MB_RES_FULL], par));
       if (!(w0 && w1 && wr)) {
@@ -877,23 +889,34 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
         float sdiff = a.op_scale_d, slift = a.op_scale_l;
         if constexpr (PT == PT_FP16) {
           sdiff *= row_scale(rmx[row]);
-          slift *= row_scale(fmx[row]);
+          slift *= row_scale(fmx[row]);   // written in C by the row's owner warp
         }
         double* qo = st + fown * FNP + e_own * NP;
         double* ro = rbuf + fown * FNP + e_own * NP;
         const int64_t gidx = fown * Knp + (el0 + e_own) * NP;
         const int i_lo = part * S::NPQ;
         const int i_hi = (part + 1) * S::NPQ < NP ? (part + 1) * S::NPQ : NP;
+        // TMEM columns are read CHK at a time (one wait per chunk)
+        constexpr int CHK = S::NPQ < 8 ? S::NPQ : 8;
 #pragma unroll 1
-        for (int i0 = i_lo; i0 < i_hi; i0 += 4) {
-          float dv[DIM][4], lv[4];
+        for (int c0 = i_lo; c0 < i_hi; c0 += CHK) {
+          float dv[DIM][CHK], lv[CHK];
 #pragma unroll
-          for (int r = 0; r < DIM; ++r) tc::tmem_ld4(tmem_diff + lane_addr + r * NP + i0, dv[r]);
-          tc::tmem_ld4(tmem_lift + lane_addr + i0, lv);
+          for (int g = 0; g < CHK / 4; ++g) {
+            if (c0 + 4 * g < i_hi) {   // warp-uniform
+#pragma unroll
+              for (int r = 0; r < DIM; ++r)
+                tc::tmem_ld4(tmem_diff + lane_addr + r * NP + c0 + 4 * g,
+                             *reinterpret_cast<float(*)[4]>(&dv[r][4 * g]));
+              tc::tmem_ld4(tmem_lift + lane_addr + c0 + 4 * g,
+                           *reinterpret_cast<float(*)[4]>(&lv[4 * g]));
+            }
+          }
           tc::tmem_wait_ld();
 #pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            const int i = i0 + c;
+          for (int c = 0; c < CHK; ++c) {
+            const int i = c0 + c;
+            if (i >= i_hi) break;        // warp-uniform
             float g[DIM];
 #pragma unroll
             for (int x = 0; x < DIM; ++x) {
@@ -902,9 +925,9 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
               for (int r = 0; r < DIM; ++r) s += gm[r][x] * (dv[r][c] * sdiff + lin[r]);
               g[x] = s;
             }
-            const float cnode = C ? (float)scoef[e_own * NP + (i < NP ? i : 0)] : 0.f;
+            const float cnode = C ? (float)scoef[e_own * NP + i] : 0.f;
             const float mine = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
-            if (valid && i < i_hi) {
+            if (valid) {
               const float src = a.source ? (float)a.source[(el0 + e_own) * NP + i] : 0.f;
               const double rr =
                   (double)model_finish<MODEL, DIM, float>(a.mp, fown, mine, lv[c] * slift, src);
