@@ -50,7 +50,8 @@ class hb_op_desc(C.Structure):
 EXPORTED = [
     "hb_discr_create", "hb_discr_destroy", "hb_op_create", "hb_op_destroy",
     "hb_rhs", "hb_lsrk_stage", "hb_lincomb", "hb_gather_map", "hb_op_check",
-    "hb_op_launch_info", "hb_norm", "hb_norm_noalloc",
+    "hb_op_launch_info", "hb_norm", "hb_norm_noalloc", "hb_rhs_adjoint_work_size",
+    "hb_rhs_adjoint",
     "hb_last_error_string",
 ]
 
@@ -83,6 +84,8 @@ def load(path=LIB_PATH):
             "hb_op_launch_info": [vp, vp, i32],
             "hb_norm": [vp, i32, i32, vp, vp, vp],
             "hb_norm_noalloc": [i64, i32, i32, i32, vp, vp, vp, vp, vp],
+            "hb_rhs_adjoint_work_size": [vp, vp],
+            "hb_rhs_adjoint": [vp, vp, vp, vp, vp, vp, vp, vp],
         }
         for name, args in sig.items():
             fn = getattr(lib, name)

@@ -336,6 +336,29 @@ hb_status hb_norm(hb_discr* discr, int32_t nfields, int32_t dtype, const void* u
                      d->norm_blocks, out, reinterpret_cast<cudaStream_t>(stream));
 }
 
+hb_status hb_rhs_adjoint_work_size(hb_op* handle, int64_t* bytes) {
+  if (!handle || !bytes) return fail(HB_ERR_INVALID_ARGUMENT, "null argument");
+  *bytes = adjoint_work_bytes(reinterpret_cast<Op*>(handle));
+  return HB_OK;
+}
+
+hb_status hb_rhs_adjoint(hb_op* handle, const double* q, const double* lam, double* q_bar,
+                         double* c_bar, const double* coeff, void* work, void* stream) {
+  if (!handle) return fail(HB_ERR_INVALID_ARGUMENT, "null operator");
+  Op* op = reinterpret_cast<Op*>(handle);
+  if (!lam || !q_bar || !work) return fail(HB_ERR_INVALID_ARGUMENT, "null argument");
+  if (lam == q_bar) return fail(HB_ERR_INVALID_ARGUMENT, "q_bar aliases lam");
+  if (op->model == HB_MODEL_VARWAVE && !coeff)
+    return fail(HB_ERR_INVALID_ARGUMENT, "variable-velocity wave needs the c field");
+  if (c_bar && op->model != HB_MODEL_VARWAVE)
+    return fail(HB_ERR_INVALID_ARGUMENT, "c_bar: only the variable-velocity wave has a c field");
+  if (c_bar && !q) return fail(HB_ERR_INVALID_ARGUMENT, "c_bar needs the state q");
+  DeviceGuard g(op->d->device);
+  if (!g.ok) return fail(HB_ERR_CUDA, "cannot select the CUDA device");
+  return launch_adjoint(op, q, lam, q_bar, c_bar, coeff, static_cast<double*>(work),
+                        reinterpret_cast<cudaStream_t>(stream));
+}
+
 hb_status hb_op_check(hb_op* handle, void* stream) {
   if (!handle) return fail(HB_ERR_INVALID_ARGUMENT, "null operator");
   Op* op = reinterpret_cast<Op*>(handle);

@@ -90,6 +90,11 @@ hb_status launch_norm(int64_t K, int np, int nfields, int dtype, const double* m
                       const double* absjac, const void* u, double* partials, int nblocks,
                       double* out, cudaStream_t s);
 
+// adjoint of the RHS (adjoint.cu)
+int64_t adjoint_work_bytes(const Op* op);
+hb_status launch_adjoint(Op* op, const double* q, const double* lam, double* q_bar,
+                         double* c_bar, const double* coeff, double* work, cudaStream_t s);
+
 // kernel launchers (rhs_simt.cu)
 hb_status launch_simt(Op* op, int mode, double a, double b, double dt,
                       const void* q_in, void* q_out, void* res,

@@ -436,24 +436,60 @@ class CompiledOperator:
         return torch.cuda.current_stream(self.discr.device).cuda_stream
 
     # -- evaluation -------------------------------------------------------------
-    def rhs_into(self, q, out, bc_in=None):
+    def _field_ptrs(self, coeff, source):
+        """Device pointers of the c field and the source: the per-call
+        tensors when given (FP64 [K*Np] on the device), else the operator's."""
+        c = self._coeff if coeff is None else coeff
+        s = self._source if source is None else source
+        for t in (coeff, source):
+            if t is not None:
+                if t.dtype != _torch().float64 or not t.is_contiguous() or \
+                        t.numel() != len(self.discr) or t.device != self.discr.device:
+                    raise ValueError("c / source: contiguous FP64 [K*Np] on the device")
+        return (c.data_ptr() if c is not None else None,
+                s.data_ptr() if s is not None else None)
+
+    def rhs_into(self, q, out, bc_in=None, coeff=None, source=None):
         """out <- RHS(q); q, out: [F, K*Np] device tensors of the state dtype."""
         keep, bptr = self._bdry_ptr(bc_in)
-        _native.check(self._lib.hb_rhs(
-            self._handle, q.data_ptr(), out.data_ptr(),
-            self._coeff.data_ptr() if self._coeff is not None else None,
-            bptr, self._source.data_ptr() if self._source is not None else None,
-            self._stream()))
+        cptr, sptr = self._field_ptrs(coeff, source)
+        _native.check(self._lib.hb_rhs(self._handle, q.data_ptr(), out.data_ptr(), cptr,
+                                       bptr, sptr, self._stream()))
         return out
 
-    def lsrk_stage(self, a, b, dt, q_in, q_out, res, bc_in=None):
+    def lsrk_stage(self, a, b, dt, q_in, q_out, res, bc_in=None, coeff=None, source=None):
         keep, bptr = self._bdry_ptr(bc_in)
+        cptr, sptr = self._field_ptrs(coeff, source)
         _native.check(self._lib.hb_lsrk_stage(
             self._handle, float(a), float(b), float(dt), q_in.data_ptr(),
-            q_out.data_ptr(), res.data_ptr(),
-            self._coeff.data_ptr() if self._coeff is not None else None,
-            bptr, self._source.data_ptr() if self._source is not None else None,
-            self._stream()))
+            q_out.data_ptr(), res.data_ptr(), cptr, bptr, sptr, self._stream()))
+
+    def adjoint(self, lam, q=None, coeff=None, want_c=False):
+        """Adjoint of the RHS (hb_rhs_adjoint), FP64: returns
+        (q_bar, c_bar) = ((dR/dq)^T lam, (dR/dc)^T lam at the state q).
+        lam, q: [F, K*Np]; c_bar ([K*Np], per node of the c field) only for
+        the variable-velocity wave with ``want_c`` (else None)."""
+        torch = _torch()
+        d = self.discr
+        lam = lam.to(device=d.device, dtype=torch.float64).reshape(self.F, len(d)).contiguous()
+        if q is not None:
+            q = q.to(device=d.device, dtype=torch.float64).reshape(self.F, len(d)).contiguous()
+        if want_c and (self.ot.model != MODEL_VARWAVE or q is None):
+            raise ValueError("c gradient: variable-velocity wave, with the state q")
+        q_bar = torch.empty_like(lam)
+        c_bar = torch.empty(len(d), dtype=torch.float64, device=d.device) if want_c else None
+        nbytes = C.c_int64()
+        _native.check(self._lib.hb_rhs_adjoint_work_size(self._handle, C.byref(nbytes)))
+        work = getattr(self, "_adj_work", None)
+        if work is None or work.numel() * 8 < nbytes.value:
+            work = torch.empty((nbytes.value + 7) // 8, dtype=torch.float64, device=d.device)
+            self._adj_work = work
+        c = self._coeff if coeff is None else coeff
+        _native.check(self._lib.hb_rhs_adjoint(
+            self._handle, q.data_ptr() if q is not None else None, lam.data_ptr(),
+            q_bar.data_ptr(), c_bar.data_ptr() if c_bar is not None else None,
+            c.data_ptr() if c is not None else None, work.data_ptr(), self._stream()))
+        return q_bar, c_bar
 
     def check(self):
         """Synchronise and raise if a kernel flagged bad input."""

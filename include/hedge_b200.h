@@ -164,6 +164,23 @@ hb_status hb_norm_noalloc(int64_t num_elements, int32_t np, int32_t nfields,
                           int32_t dtype, const double* mass, const double* abs_jacobian,
                           const void* u, double* out, void* stream);
 
+/* Adjoint of the right-hand side, FP64.  For R(q; c) as evaluated by hb_rhs
+ * with this operator, and a cotangent lam [F][K*Np] of R:
+ *   q_bar = (dR/dq)^T lam                        [F][K*Np], overwritten
+ *   c_bar = (dR/dc)^T lam at the state q         [K*Np] per node of the c field,
+ *           overwritten; variable-velocity wave only, else pass NULL.
+ * R is linear in q (given boundary data and sources are constants), so q_bar
+ * does not depend on q, which may be NULL when c_bar is NULL.  coeff is the c
+ * field the forward used (variable-velocity wave).  work: device scratch of
+ * hb_rhs_adjoint_work_size() bytes, owned by the caller.  The transposed
+ * lift, differentiation and the scatter-add back through the face-pair map
+ * (written as a gather over the matched neighbour face points) adjoin
+ * jit/diff.py:137-175, jit/flux.py:239-480 (ext_native_write_map) and
+ * jit/lift.py:110-141; the reference has no adjoint of its own. */
+hb_status hb_rhs_adjoint_work_size(hb_op* op, int64_t* bytes);
+hb_status hb_rhs_adjoint(hb_op* op, const double* q, const double* lam, double* q_bar,
+                         double* c_bar, const double* coeff, void* work, void* stream);
+
 /* Synchronises `stream` and returns HB_ERR_DEVICE_FLAG if a kernel of this
  * operator flagged bad input (out-of-range neighbour or code, missing
  * boundary vector); the flag stays set. */
