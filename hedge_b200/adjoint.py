@@ -240,7 +240,11 @@ def make_wave_inversion_problem(n=61, order=5, jitter=0.1, mesh_seed=3, c_seed=4
                               dtype=torch.float64, device=discr.device)
     # the var-c wave subtracts its source from du/dt
     source = (src_vec, lambda t: -ricker(t, f0))
-    dt = op.estimate_timestep(discr)
+    # The variable-velocity upwind flux (hedge/models/wave.py:246-273) carries
+    # twice the jump penalty of the constant-c one, which puts its spectrum
+    # outside the LSRK4 region at the reference's CFL estimate (the solution
+    # grows without bound there); half of the estimate is stable.
+    dt = 0.5 * op.estimate_timestep(discr)
     return {"discr": discr, "op": op, "comp": comp, "receivers": receivers,
             "source": source, "c_k": torch.as_tensor(c_k, device=discr.device),
             "dt": dt}
@@ -249,3 +253,87 @@ def make_wave_inversion_problem(n=61, order=5, jitter=0.1, mesh_seed=3, c_seed=4
 def trace_loss(traces):
     """Squared L2 of the receiver traces over all steps."""
     return (traces * traces).sum()
+
+
+def check_gradients(P, nsteps=400, every=20, ndirs=32, h=1e-6, seed=5, q0=None):
+    """Gradient of the trace loss in (q0, c_k) by the adjoint, against central
+    finite differences on ``ndirs`` random joint directions.  Returns a dict
+    with the loss, the worst and median relative disagreement and timings
+    (forward, forward + backward) in seconds."""
+    import time
+    torch = _torch()
+    d = P["discr"]
+    rng = np.random.default_rng(seed)
+    if q0 is None:
+        q0 = torch.zeros((3, len(d)), dtype=torch.float64, device=d.device)
+    q0 = q0.clone().requires_grad_(True)
+    ck = P["c_k"].clone().requires_grad_(True)
+
+    def loss(q, c):
+        tr = ReceiverTraces.apply(q, c.repeat_interleave(d.Np), P["comp"], P["receivers"],
+                                  P["dt"], nsteps, P["source"], every)
+        return trace_loss(tr)
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with torch.no_grad():
+        L0 = float(loss(q0.detach(), ck.detach()))
+    torch.cuda.synchronize()
+    t_fwd = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    L = loss(q0, ck)
+    L.backward()
+    torch.cuda.synchronize()
+    t_fb = time.perf_counter() - t0
+    gq, gc = q0.grad.detach(), ck.grad.detach()
+    errs = {"q0": [], "c": []}
+    with torch.no_grad():
+        for k in range(ndirs):
+            # half of the directions move the initial field, half the c_k
+            if k % 2 == 0:
+                dq = torch.as_tensor(rng.standard_normal(q0.shape), device=d.device)
+                dc = torch.zeros_like(ck)
+            else:
+                dq = torch.zeros_like(q0)
+                dc = torch.as_tensor(rng.standard_normal(ck.shape), device=d.device)
+            lp = float(loss(q0 + h * dq, ck + h * dc))
+            lm = float(loss(q0 - h * dq, ck - h * dc))
+            fd = (lp - lm) / (2 * h)
+            an = float((gq * dq).sum() + (gc * dc).sum())
+            errs["q0" if k % 2 == 0 else "c"].append(abs(fd - an) / max(abs(an), 1e-300))
+    allerr = errs["q0"] + errs["c"]
+    return {"loss": L0, "fd_rel_err_max": max(allerr), "fd_rel_err_median": float(np.median(allerr)),
+            "fd_rel_err_max_q0": max(errs["q0"]), "fd_rel_err_max_c": max(errs["c"]),
+            "directions": ndirs, "h": h, "t_forward_s": t_fwd, "t_forward_backward_s": t_fb,
+            "grad_c_norm": float(gc.norm()), "grad_q0_norm": float(gq.norm())}
+
+
+def main(argv=None):
+    """Adjoint workload: K = 7200 triangles, order 5, var-c wave, 400 LSRK4
+    steps, checkpoints every 20, 32 central-difference directions (h = 1e-6).
+    Prints one JSON line."""
+    import argparse
+    import json
+    p = argparse.ArgumentParser()
+    p.add_argument("--n", type=int, default=61)
+    p.add_argument("--order", type=int, default=5)
+    p.add_argument("--steps", type=int, default=400)
+    p.add_argument("--every", type=int, default=20)
+    p.add_argument("--dirs", type=int, default=32)
+    a = p.parse_args(argv)
+    P = make_wave_inversion_problem(n=a.n, order=a.order)
+    torch = _torch()
+    x = P["discr"].nodes
+    # initial pressure pulse (width 0.2) beside the source
+    q0 = np.stack([np.exp(-((x - 0.3) ** 2).sum(1) / 0.2 ** 2), 0 * x[:, 0], 0 * x[:, 0]])
+    q0 = torch.as_tensor(q0, device=P["discr"].device)
+    r = check_gradients(P, nsteps=a.steps, every=a.every, ndirs=a.dirs, q0=q0)
+    d = P["discr"]
+    r.update({"workload": "varwave2d_K%d_N%d_steps%d" % (d.K, a.order, a.steps),
+              "K": d.K, "order": a.order, "checkpoint_every": a.every, "dtype": "f64",
+              "dof_updates_forward_per_s": d.K * d.Np * 3 * 5 * a.steps / r["t_forward_s"]})
+    print(json.dumps(r), flush=True)
+
+
+if __name__ == "__main__":
+    main()
