@@ -37,6 +37,11 @@ class hb_discr_desc(C.Structure):
                 ("mass", C.c_void_p), ("abs_jacobian", C.c_void_p)]
 
 
+class hb_batch_member(C.Structure):
+    _fields_ = [("op", C.c_void_p), ("q0", C.c_void_p), ("q1", C.c_void_p),
+                ("res", C.c_void_p), ("dt", C.c_double), ("tile_elems", C.c_int32)]
+
+
 class hb_op_desc(C.Structure):
     _fields_ = [("model", C.c_int32), ("num_fields", C.c_int32),
                 ("precision", C.c_int32), ("flux_type", C.c_int32),
@@ -51,7 +56,8 @@ EXPORTED = [
     "hb_discr_create", "hb_discr_destroy", "hb_op_create", "hb_op_destroy",
     "hb_rhs", "hb_lsrk_stage", "hb_lincomb", "hb_gather_map", "hb_op_check",
     "hb_op_launch_info", "hb_norm", "hb_norm_noalloc", "hb_rhs_adjoint_work_size",
-    "hb_rhs_adjoint",
+    "hb_rhs_adjoint", "hb_batch_create", "hb_batch_destroy", "hb_batch_stage",
+    "hb_batch_info", "hb_batch_check",
     "hb_last_error_string",
 ]
 
@@ -86,6 +92,11 @@ def load(path=LIB_PATH):
             "hb_norm_noalloc": [i64, i32, i32, i32, vp, vp, vp, vp, vp],
             "hb_rhs_adjoint_work_size": [vp, vp],
             "hb_rhs_adjoint": [vp, vp, vp, vp, vp, vp, vp, vp],
+            "hb_batch_create": [vp, i32, vp],
+            "hb_batch_destroy": [vp],
+            "hb_batch_stage": [vp, d, d, i32, vp],
+            "hb_batch_info": [vp, vp, i32],
+            "hb_batch_check": [vp, vp],
         }
         for name, args in sig.items():
             fn = getattr(lib, name)

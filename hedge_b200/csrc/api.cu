@@ -26,18 +26,6 @@ hb_status cuda_fail(cudaError_t err, const char* what) {
 
 // Makes `dev` current for the scope of one C-ABI call and restores the
 // caller's device afterwards.
-struct DeviceGuard {
-  int prev = -1;
-  bool ok = false;
-  explicit DeviceGuard(int dev) {
-    if (cudaGetDevice(&prev) != cudaSuccess) return;
-    ok = prev == dev || cudaSetDevice(dev) == cudaSuccess;
-  }
-  ~DeviceGuard() {
-    int cur;
-    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-  }
-};
 
 template <typename T>
 static hb_status upload(T** dst, const T* src, size_t n) {

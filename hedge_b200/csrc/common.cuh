@@ -39,6 +39,20 @@ enum : int {
   DEV_MMA_TIMEOUT = 5
 };
 
+// Makes `dev` current for the guard's lifetime, restoring the caller's device.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = false;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) return;
+    ok = prev == dev || cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    int cur;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
 // Operator data uploaded once per discretization.
 struct Discr {
   int device;

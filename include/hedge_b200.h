@@ -181,6 +181,34 @@ hb_status hb_rhs_adjoint_work_size(hb_op* op, int64_t* bytes);
 hb_status hb_rhs_adjoint(hb_op* op, const double* q, const double* lam, double* q_bar,
                          double* c_bar, const double* coeff, void* work, void* stream);
 
+/* Batched ensemble: one launch per LSRK stage advances many independent
+ * discretizations of uneven size and order.  Each member is a compiled
+ * operator (advection or constant-c wave, HB_PREC_FP32, no given boundary
+ * data) with two FP32 state buffers q0, q1 [F][K*Np], an FP64 residual res
+ * [F][K*Np] (zero before the first stage), its own time step dt and tile
+ * size (elements per tile; 0 = 256 / Np).  A stage with parity p computes,
+ * for every member, res = a*res + dt*RHS(q_p) (RHS in FP32, residual FP64)
+ * and q_(1-p) = q_p + b*res (FP64 arithmetic, stored FP32).  The batch
+ * descriptor owns its instance and tile tables; members' buffers stay the
+ * caller's.  No reference counterpart: the reference advances one
+ * discretization at a time (hedge/timestep/runge_kutta.py:104-131). */
+typedef struct hb_batch hb_batch;
+typedef struct {
+  hb_op* op;
+  float* q0;
+  float* q1;
+  double* res;
+  double dt;
+  int32_t tile_elems;
+} hb_batch_member;
+hb_status hb_batch_create(const hb_batch_member* members, int32_t n, hb_batch** out);
+hb_status hb_batch_destroy(hb_batch* batch);
+hb_status hb_batch_stage(hb_batch* batch, double a, double b, int32_t parity, void* stream);
+/* up to n of {tiles, grid, threads per CTA, dynamic shared bytes, DOFs} */
+hb_status hb_batch_info(hb_batch* batch, int64_t* info, int32_t n);
+/* synchronises `stream`; HB_ERR_DEVICE_FLAG if a stage met bad face data */
+hb_status hb_batch_check(hb_batch* batch, void* stream);
+
 /* Synchronises `stream` and returns HB_ERR_DEVICE_FLAG if a kernel of this
  * operator flagged bad input (out-of-range neighbour or code, missing
  * boundary vector); the flag stays set. */
