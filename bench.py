@@ -48,22 +48,50 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--precision", default="fp16x3", choices=["fp64", "fp32", "bf16x3", "fp16x3"])
+    p.add_argument("--workload", default="maxwell", choices=["maxwell", "wave7"],
+                   help="maxwell: 3D Maxwell N=4 cavity (default); wave7: 3D acoustic "
+                        "wave N=7 Gaussian pulse (the high-order precision workload)")
+    p.add_argument("--accuracy-steps", type=int, default=None,
+                   help="steps of the split-vs-FP64 accuracy run (default steps+warmup)")
     p.add_argument("--no-compare", action="store_true",
                    help="skip the plain-FP64 comparison and the split accuracy check")
     p.add_argument("--n", type=int, default=20, help="cubes per axis")
-    p.add_argument("--order", type=int, default=4)
+    p.add_argument("--order", type=int, default=None, help="default 4 (maxwell), 7 (wave7)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     return p.parse_args()
 
 
-def build_problem(n, order, precision, device=None):
+WORKLOADS = {
+    "maxwell": {"order": 4, "fields": 6,
+                "metric": "DG RHS DOF-updates/s (3D Maxwell N=4, LSRK4)",
+                "label": "maxwell3d_cavity_K%d_N%d"},
+    "wave7": {"order": 7, "fields": 4,
+              "metric": "DG RHS DOF-updates/s (3D acoustic wave N=7, LSRK4)",
+              "label": "wave3d_pulse_K%d_N%d"},
+}
+
+
+def build_problem(n, order, precision, device=None, workload="maxwell"):
     import hedge_b200 as hb
     h = 2.0 / n
     mesh = hb.make_box_tet_mesh(n=(n, n, n), jitter=0.05 * h, seed=1)
     discr = hb.Discretization(mesh, order=order, precision=precision, device=device)
-    op = hb.MaxwellOperator(1.0, 1.0, flux_type=1)
+    if workload == "wave7":
+        # c = 1, upwind, reflecting (Dirichlet) walls
+        op = hb.StrongWaveOperator(1.0, 3, flux_type="upwind")
+    else:
+        op = hb.MaxwellOperator(1.0, 1.0, flux_type=1)
     return hb, mesh, discr, op
+
+
+def initial_state(discr, workload="maxwell"):
+    if workload == "wave7":
+        x = discr.nodes
+        w = np.zeros((4, len(discr)))
+        w[0] = np.exp(-(x ** 2).sum(1) / 0.15 ** 2)   # pressure pulse of width 0.15
+        return w
+    return cavity_ic(discr)
 
 
 def cavity_ic(discr):
@@ -82,13 +110,13 @@ def cavity_ic(discr):
     return w + 1e-3 * rng.uniform(-1, 1, w.shape)
 
 
-def algorithmic_bytes_per_dof_update(discr, state_bytes):
+def algorithmic_bytes_per_dof_update(discr, state_bytes, F=6):
     """read q, read res, write q, write res per DOF-update, plus per-element
     geometry (d^2 metric + Nf (normal, Fscale)) and connectivity (Nf x
     (u32 neighbour, u8 face, u8 perm)) spread over Np*F DOF-updates."""
     d, nf = discr.dimensions, discr.Nfaces
     g_el = 8 * (d * d + nf * (d + 1)) + nf * 6
-    return 4 * state_bytes + g_el / (discr.Np * 6)
+    return 4 * state_bytes + g_el / (discr.Np * F)
 
 
 class ClockSampler:
@@ -187,7 +215,7 @@ def load_traffic(kernel_key):
         return None
 
 
-def cpu_baseline(discr, op, w0, dt, threads=None):
+def cpu_baseline(discr, op, w0, dt, threads=None, F=6):
     """Oracle (CPU port of the jit backend) on a bounded sample: one LSRK
     stage over the whole mesh, all host threads (best of 3 after a warm-up),
     plus the same on one thread (the reference's generated loops are serial)."""
@@ -195,7 +223,7 @@ def cpu_baseline(discr, op, w0, dt, threads=None):
     import oracle as orc_mod
     ncores = os.cpu_count() or 1
     orc = orc_mod.OracleRHS(discr, op.op_template())
-    dofs = discr.K * discr.Np * 6
+    dofs = discr.K * discr.Np * F
 
     def stage_time(nthreads, reps):
         used = orc_mod.set_threads(nthreads)
@@ -223,8 +251,10 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", 0))
     if rank != 0:
         return
-    hb, mesh, discr, op = build_problem(args.n, args.order, "fp64")
-    w0 = cavity_ic(discr)
+    W = WORKLOADS[args.workload]
+    F = W["fields"]
+    hb, mesh, discr, op = build_problem(args.n, args.order, "fp64", workload=args.workload)
+    w0 = initial_state(discr, args.workload)
     dt = op.estimate_timestep(discr)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc_mod
@@ -243,16 +273,16 @@ def run_reference(args):
         res = RK4A[s % 5] * res + dt * r
         y = y + RK4B[s % 5] * res
     el = time.perf_counter() - t0
-    dofs = discr.K * discr.Np * 6 * args.steps
+    dofs = discr.K * discr.Np * F * args.steps
     v = dofs / el
     line = {
-        "impl": "reference", "metric": "DG RHS DOF-updates/s (3D Maxwell N=4, LSRK4)",
+        "impl": "reference", "metric": W["metric"],
         "value": v, "unit": "DOF-updates/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "maxwell3d_cavity_K48000_N4", "K": discr.K,
-                   "order": args.order, "fields": 6, "step": "one LSRK stage per step"},
+        "config": {"workload": W["label"] % (discr.K, args.order), "K": discr.K,
+                   "order": args.order, "fields": F, "step": "one LSRK stage per step"},
         "cpu_baseline": {"value": v, "unit": "DOF-updates/s", "cores": used,
                          "kind": "port",
                          "sample": "one LSRK stage over the full mesh per step; C++ "
@@ -267,13 +297,16 @@ def run_ours(args):
     import torch
     rank, world, local = dist_setup(args.gpus)
     dev = torch.device("cuda", torch.cuda.current_device())
-    hb, mesh, discr, op = build_problem(args.n, args.order, args.precision, device=dev)
-    w0 = cavity_ic(discr)
+    W = WORKLOADS[args.workload]
+    F = W["fields"]
+    hb, mesh, discr, op = build_problem(args.n, args.order, args.precision, device=dev,
+                                        workload=args.workload)
+    w0 = initial_state(discr, args.workload)
     dt = op.estimate_timestep(discr)
     rhs = op.bind(discr)
     comp = rhs.compiled
     stepper = hb.LSRK4TimeStepper()
-    y = discr.to_device(w0).reshape(6, -1)
+    y = discr.to_device(w0).reshape(F, -1)
     # warm-up
     t = 0.0
     for _ in range(args.warmup):
@@ -294,13 +327,13 @@ def run_ours(args):
     ms = ev0.elapsed_time(ev1)
     comp.check()
     ms_max = max_over_ranks(ms, world)
-    dofs_rank = discr.K * discr.Np * 6 * 5 * args.steps
+    dofs_rank = discr.K * discr.Np * F * 5 * args.steps
     value = dofs_rank * world / (ms_max * 1e-3)
     launches = 5 * args.steps
     launch_ms = ms / launches
     state_bytes = 8 if args.precision != "fp32" else 4
-    bpd = algorithmic_bytes_per_dof_update(discr, state_bytes)
-    bytes_per_launch = bpd * discr.K * discr.Np * 6
+    bpd = algorithmic_bytes_per_dof_update(discr, state_bytes, F)
+    bytes_per_launch = bpd * discr.K * discr.Np * F
     achieved = bytes_per_launch / (launch_ms * 1e-3) / 1e9
     peaks = {}
     try:
@@ -311,7 +344,9 @@ def run_ours(args):
     peak = peaks.get("hbm_gbs")
     peak_src = "measured" if peak else "fallback"
     peak = peak or 6650.0
-    kernel_key = "rhs_stage_%s_maxwell3d_N%d" % (args.precision, args.order)
+    kernel_key = "rhs_stage_%s_%s_N%d" % (args.precision,
+                                          "maxwell3d" if args.workload == "maxwell" else "wave3d",
+                                          args.order)
     traffic = load_traffic(kernel_key)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
@@ -323,8 +358,8 @@ def run_ours(args):
     if not args.no_compare and args.precision != "fp64":
         d64 = hb.Discretization(mesh, order=args.order, precision="fp64", device=dev)
         rhs64 = op.bind(d64)
-        y64 = d64.to_device(w0).reshape(6, -1)
-        ys = discr.to_device(w0).reshape(6, -1)
+        y64 = d64.to_device(w0).reshape(F, -1)
+        ys = discr.to_device(w0).reshape(F, -1)
         r_split = rhs(0.0, ys)
         r_64 = rhs64(0.0, y64)
         err_rhs = float(torch.linalg.norm(r_split - r_64) / torch.linalg.norm(r_64))
@@ -342,10 +377,10 @@ def run_ours(args):
         ev1.record(stream)
         barrier(world)
         ms64 = max_over_ranks(ev0.elapsed_time(ev1), world)
-        v64 = discr.K * discr.Np * 6 * 5 * n64 * world / (ms64 * 1e-3)
+        v64 = discr.K * discr.Np * F * 5 * n64 * world / (ms64 * 1e-3)
         # same IC, same number of steps on both paths
-        nacc = args.steps + args.warmup
-        ya, yb, ta = discr.to_device(w0).reshape(6, -1), d64.to_device(w0).reshape(6, -1), 0.0
+        nacc = args.accuracy_steps or (args.steps + args.warmup)
+        ya, yb, ta = discr.to_device(w0).reshape(F, -1), d64.to_device(w0).reshape(F, -1), 0.0
         sa, sb = hb.LSRK4TimeStepper(), hb.LSRK4TimeStepper()
         for _ in range(nacc):
             ya = sa(ya, ta, dt, rhs)
@@ -378,20 +413,20 @@ def run_ours(args):
         barrier(world)
         e_ms = max_over_ranks(ev0.elapsed_time(ev1), world)
         nbytes = host_in.numel() * host_in.element_size()
-        e2e = {"value": discr.K * discr.Np * 6 * 5 * e2e_steps * world / (e_ms * 1e-3),
+        e2e = {"value": discr.K * discr.Np * F * 5 * e2e_steps * world / (e_ms * 1e-3),
                "unit": "DOF-updates/s", "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "steps": e2e_steps}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu, _ = cpu_baseline(discr, op, w0, dt)
+            cpu, _ = cpu_baseline(discr, op, w0, dt, F=F)
         except Exception as exc:   # the baseline must not sink the GPU line
             cpu = {"value": None, "error": str(exc)}
 
     if rank == 0:
         line = {
-            "metric": "DG RHS DOF-updates/s (3D Maxwell N=4, LSRK4)",
+            "metric": W["metric"],
             "value": value, "unit": "DOF-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -399,12 +434,12 @@ def run_ours(args):
             "dtype": {"fp64": "f64", "fp32": "f32", "bf16x3": "bf16x3+f32acc, f64 state",
                       "fp16x3": "fp16x3(scaled)+f32acc, f64 state"}[args.precision],
             "data": "synthetic",
-            "config": {"workload": "maxwell3d_cavity_K48000_N4", "K": discr.K,
-                       "order": args.order, "Np": discr.Np, "fields": 6,
+            "config": {"workload": W["label"] % (discr.K, args.order), "K": discr.K,
+                       "order": args.order, "Np": discr.Np, "fields": F,
                        "precision": args.precision, "stepper": "LSRK4 (5 fused stages)",
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "working set 3 x %.1f MB > 126 MB L2, no flush" %
-                             (discr.K * discr.Np * 6 * state_bytes / 1e6)},
+                             (discr.K * discr.Np * F * state_bytes / 1e6)},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "split_vs_fp64": compare,
             "gpu_launches": launches, "clocks": clk.summary(),
         }
@@ -416,6 +451,8 @@ def run_ours(args):
 
 def main():
     args = parse()
+    if args.order is None:
+        args.order = WORKLOADS[args.workload]["order"]
     if args.impl == "reference":
         run_reference(args)
     else:

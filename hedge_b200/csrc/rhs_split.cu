@@ -957,11 +957,499 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
 }
 
 // ---------------------------------------------------------------------------
+// Streamed-operator variant for high orders, whose operator planes do not fit
+// in shared memory next to the data planes (3D, N >= 6).  Same contraction
+// layout, split, epilogue and stage update as rhs_split_kernel; differences:
+//   * the operator planes stream from global memory (L2-resident) through a
+//     two-buffer ring, one 16-column K chunk at a time; each chunk's MMAs are
+//     committed to that buffer's mbarrier, which is waited on before the
+//     buffer is refilled;
+//   * d*Np may exceed one MMA's N (256): the diff accumulator is then filled
+//     by two MMAs per product (N = ND1 + ND2 columns);
+//   * the state is read from global memory (FP64) in the split and face
+//     phases, the rhs is staged (FP32) in the state-plane area after the diff
+//     MMAs completed, and the FP64 stage update is a coalesced pass;
+//   * all 8 warps run every phase; thread 0 issues the MMAs.
+template <int MODEL, int DIM, int ORDER>
+struct ShapeS {
+  static constexpr int F = Traits<MODEL, DIM>::F;
+  static constexpr int C = Traits<MODEL, DIM>::COEFF;
+  static constexpr int NA = F + C;
+  static constexpr int NP = DIM == 2 ? (ORDER + 1) * (ORDER + 2) / 2
+                                     : (ORDER + 1) * (ORDER + 2) * (ORDER + 3) / 6;
+  static constexpr int NFP = DIM == 2 ? ORDER + 1 : (ORDER + 1) * (ORDER + 2) / 2;
+  static constexpr int NF = DIM + 1;
+  static constexpr int NFPT = NF * NFP;
+  static constexpr int G = DIM * DIM + NF * (DIM + 1);
+  static constexpr int EPW = 32 / F;
+  static constexpr int EB = 4 * EPW;
+  static constexpr int FNP = EB * NP;
+  static constexpr int NVAL = F * FNP;
+  static constexpr int KD = ru16(NP), KL = ru16(NFPT);
+  static constexpr int ND = ru16(DIM * NP), NL = ru16(NP);
+  static constexpr int ND1 = ND <= 256 ? ND : ru16(ND / 2);
+  static constexpr int ND2 = ND - ND1;
+  static constexpr int LIFT_COL = ru32(ND);
+  static constexpr int NKD = KD / 16, NKL = KL / 16;
+  static constexpr int THREADS = 256;
+  static constexpr int NW = THREADS / 32;
+  static constexpr int NPQ = (((NP + 1) / 2) + 3) & ~3;       // nodes per epilogue warp
+  static constexpr int NFACE = EB * NFPT;
+  static constexpr int NFV = (NFACE + THREADS - 1) / THREADS;
+  static constexpr int NITEM = 4 * (KD / 8);
+  static constexpr uint32_t bDc = ND * 16 * 2, bLc = NL * 16 * 2;   // one plane, one chunk
+  static constexpr uint32_t RING = al128(2 * (bDc > bLc ? bDc : bLc));
+  static constexpr uint32_t bAq = 128 * KD * 2, bAf = 128 * KL * 2;
+  static constexpr uint32_t oAqh = 0;
+  static constexpr uint32_t oAql = al128(oAqh + bAq);
+  static constexpr uint32_t oAfh = al128(oAql + bAq);
+  static constexpr uint32_t oAfl = al128(oAfh + bAf);
+  static constexpr uint32_t oR0 = al128(oAfl + bAf);
+  static constexpr uint32_t oR1 = al128(oR0 + RING);
+  static constexpr uint32_t osv = al128(oR1 + RING);                 // FP64 [F][EB][DIM+1]
+  static constexpr uint32_t olam = al16(osv + F * EB * (DIM + 1) * 8);
+  static constexpr uint32_t ogeo = al16(olam + NP * DIM * 8);
+  static constexpr uint32_t oconn = al16(ogeo + EB * G * 4);
+  static constexpr uint32_t ocoef = al16(oconn + EB * NF * 8);       // FP32 c [EB][NP]
+  static constexpr uint32_t ofm = al16(ocoef + (C ? EB * NP * 4 : 0));
+  static constexpr uint32_t osh = al16(ofm + NFPT);
+  static constexpr uint32_t overt = al16(osh + 6 * NFP);
+  static constexpr uint32_t ors = al16(overt + 4);                   // [2][128] row maxima
+  static constexpr uint32_t obar = al16(ors + 256 * 4);              // ring[2], done, slot
+  static constexpr uint32_t total = al16(obar + 48);
+  static constexpr uint32_t LIN_BYTES = 8 + NP * DIM * 8;
+  static constexpr int TMEM_NEED = LIFT_COL + NL;
+  static constexpr uint32_t TMEM_COLS = TMEM_NEED <= 128 ? 128 : TMEM_NEED <= 256 ? 256 : 512;
+  static constexpr bool FITS = ND1 <= 256 && ND2 <= 256 && NL <= 256 && TMEM_NEED <= 512 &&
+                               LIFT_COL + NP + 3 < 512 && total <= SMEM_LIMIT &&
+                               F * FNP * 4 <= (int)(2 * bAq);
+};
+
+template <int MODEL, int DIM, int ORDER, int PT>
+__global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
+  using S = ShapeS<MODEL, DIM, ORDER>;
+  constexpr int F = S::F, C = S::C, NA = S::NA, NP = S::NP, NFP = S::NFP, NF = S::NF;
+  constexpr int NFPT = S::NFPT, G = S::G, EPW = S::EPW, EB = S::EB, FNP = S::FNP;
+  constexpr int KD = S::KD, KL = S::KL, NV1 = DIM + 1;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(128) uint8_t smem[];
+  uint8_t* Aqh = smem + S::oAqh;
+  uint8_t* Aql = smem + S::oAql;
+  uint8_t* Afh = smem + S::oAfh;
+  uint8_t* Afl = smem + S::oAfl;
+  float* sq = reinterpret_cast<float*>(smem + S::oAqh);            // staged rhs (after diff)
+  double* sv = reinterpret_cast<double*>(smem + S::osv);
+  const double* slam = reinterpret_cast<const double*>(smem + S::olam);
+  float* sgeo = reinterpret_cast<float*>(smem + S::ogeo);
+  int2* sconn = reinterpret_cast<int2*>(smem + S::oconn);
+  float* scoef = reinterpret_cast<float*>(smem + S::ocoef);
+  uint8_t* sfm = smem + S::ofm;
+  uint8_t* ssh = smem + S::osh;
+  const uint8_t* svert = smem + S::overt;
+  uint32_t* rsq = reinterpret_cast<uint32_t*>(smem + S::ors);        // state rows
+  uint32_t* rsf = rsq + 128;                                         // flux rows
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + S::obar);      // [0..1] ring, [2] done
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + S::obar + 32);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint8_t* dimg = a.ops;                                       // D chunks
+  const uint8_t* limg = a.ops + (size_t)S::NKD * 2 * S::bDc;          // L chunks
+  const uint8_t* tail = limg + (size_t)S::NKL * 2 * S::bLc;
+
+  {
+    if (tid < 4) smem[S::overt + tid] = tail[tid];
+    double* lam = reinterpret_cast<double*>(smem + S::olam);
+    const double* lsrcd = reinterpret_cast<const double*>(tail + 8);
+    for (int x = tid; x < NP * DIM; x += S::THREADS) lam[x] = lsrcd[x];
+    for (int x = tid; x < NFPT; x += S::THREADS) sfm[x] = (uint8_t)a.fmask[x];
+    for (int x = tid; x < a.nperm * NFP; x += S::THREADS) ssh[x] = (uint8_t)a.shuffle[x];
+    // the lift planes' K padding and unused rows are never written again
+    const uint4 z = make_uint4(0, 0, 0, 0);
+    for (uint32_t o = S::oAfh + tid * 16; o < S::oR0; o += S::THREADS * 16)
+      *reinterpret_cast<uint4*>(smem + o) = z;
+    if (tid == 0) {
+      tc::mbar_init(&mbar[0], 1);
+      tc::mbar_init(&mbar[1], 1);
+      tc::mbar_init(&mbar[2], 1);
+    }
+    if (warp == 0) tc::tmem_alloc(tmem_slot, S::TMEM_COLS);
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+  }
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t tmem_diff = tmem, tmem_lift = tmem + S::LIFT_COL;
+  constexpr uint32_t ID_D1 = tc::idesc_16bit(128, S::ND1, PT == PT_BF16);
+  constexpr uint32_t ID_D2 = tc::idesc_16bit(128, S::ND2 > 0 ? S::ND2 : 16, PT == PT_BF16);
+  constexpr uint32_t ID_L = tc::idesc_16bit(128, S::NL, PT == PT_BF16);
+  const int64_t Knp = a.K * NP;
+  const int quad = warp & 3, part = warp >> 2;
+  const int lf = lane / F, fown = lane - lf * F;
+  const bool lane_used = lf < EPW;
+  const int e_lane = quad * EPW + lf;
+  const uint32_t lane_addr = (uint32_t)(quad * 32) << 16;
+  const int row = quad * 32 + lane;
+  uint32_t ring_uses[2] = {0u, 0u};   // commits so far on each ring buffer
+  uint32_t chunk = 0;                 // running chunk counter (ring buffer = chunk & 1)
+  int bad = 0;
+
+  // refill ring buffer (chunk & 1) with `bytes` from src once its previous
+  // MMAs completed; thread 0 then issues `issue()` and commits to the buffer
+  auto stream_chunk = [&](const uint8_t* src, uint32_t bytes, auto issue) -> bool {
+    const int b = (int)(chunk & 1u);
+    uint8_t* buf = smem + (b ? S::oR1 : S::oR0);
+    int late = 0;
+    if (tid == 0 && ring_uses[b] > 0)
+      late = !tc::mbar_wait(&mbar[b], (ring_uses[b] - 1) & 1u, MBAR_MAX_NS);
+    if (__syncthreads_or(late)) return false;
+    const uint4* s4 = reinterpret_cast<const uint4*>(src);
+    for (uint32_t x = tid; x < bytes / 16; x += S::THREADS)
+      reinterpret_cast<uint4*>(buf)[x] = __ldg(s4 + x);
+    tc::fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+      issue(tc::smem_u32(buf));
+      tc::mma_commit(&mbar[b]);
+    }
+    ++ring_uses[b];
+    ++chunk;
+    return true;
+  };
+
+  uint32_t it = 0;
+  for (int64_t batch = blockIdx.x; batch < a.nbatch; batch += gridDim.x, ++it) {
+    const int64_t el0 = batch * EB;
+    const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
+    const bool valid = lane_used && e_lane < ne;
+    const int e_own = valid ? e_lane : 0;
+    uint32_t* rmx = rsq;
+    uint32_t* fmx = rsf;
+
+    // ---- A: element data, vertex values, split state planes ----
+    for (int x = tid; x < ne * G; x += S::THREADS) sgeo[x] = a.geo32[el0 * G + x];
+    for (int x = tid; x < ne * NF; x += S::THREADS) sconn[x] = a.conn[el0 * NF + x];
+    if constexpr (C != 0)
+      for (int x = tid; x < ne * NP; x += S::THREADS) scoef[x] = (float)a.coeff[el0 * NP + x];
+    for (int x = tid; x < F * EB * NV1; x += S::THREADS) {
+      const int fe = x / NV1, vv = x % NV1, f = fe / EB, e = fe % EB;
+      const int node = vv == 0 ? 0 : svert[vv - 1];
+      sv[x] = e < ne ? a.q_in[f * Knp + (el0 + e) * NP + node] : 0.0;
+    }
+    if (tid < 256) rsq[tid] = 0u;   // both row-maxima arrays
+    __syncthreads();
+    float lin[DIM];
+    {
+      const double* v = sv + (fown * EB + e_own) * NV1;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) lin[d] = valid ? (float)(0.5 * (v[1 + d] - v[0])) : 0.f;
+    }
+    auto remainder = [&](int j) -> float {
+      const double* v = sv + (fown * EB + e_own) * NV1;
+      double l = v[0];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) l += slam[j * DIM + d] * (v[1 + d] - v[0]);
+      return (float)(a.q_in[fown * Knp + (el0 + e_own) * NP + j] - l);
+    };
+    float inv = 1.0f;
+    if constexpr (PT == PT_FP16) {
+      uint32_t m = 0u;
+      for (int item = warp; item < S::NITEM; item += S::NW) {
+        const int chunk8 = item >> 2;
+        if ((item & 3) != quad) continue;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          const int j = chunk8 * 8 + c;
+          if (valid && j < NP) m = max(m, __float_as_uint(fabsf(remainder(j))));
+        }
+      }
+      atomicMax(&rmx[row], m);
+      __syncthreads();
+      inv = row_scale_inv(rmx[row]);
+    }
+    for (int item = warp; item < S::NITEM; item += S::NW) {
+      if ((item & 3) != quad) continue;
+      const int chunk8 = item >> 2;
+      uint32_t hw[4], lw[4];
+#pragma unroll
+      for (int c = 0; c < 8; c += 2) {
+        const int j = chunk8 * 8 + c;
+        const float x0 = (valid && j < NP) ? remainder(j) * inv : 0.f;
+        const float x1 = (valid && j + 1 < NP) ? remainder(j + 1) * inv : 0.f;
+        if constexpr (PT == PT_BF16) {
+          const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+          const float2 hf = __bfloat1622float2(h);
+          const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+          hw[c / 2] = *reinterpret_cast<const uint32_t*>(&h);
+          lw[c / 2] = *reinterpret_cast<const uint32_t*>(&l);
+        } else {
+          const __half2 h = __floats2half2_rn(x0, x1);
+          const float2 hf = __half22float2(h);
+          const __half2 l = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+          hw[c / 2] = *reinterpret_cast<const uint32_t*>(&h);
+          lw[c / 2] = *reinterpret_cast<const uint32_t*>(&l);
+        }
+      }
+      const uint32_t off = kmajor_off(row, chunk8 * 8, KD);
+      *reinterpret_cast<uint4*>(Aqh + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+      *reinterpret_cast<uint4*>(Aql + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+    }
+    tc::fence_proxy_async();
+    __syncthreads();
+
+    // ---- B: diff MMAs, operator chunks streamed ----
+    {
+      const uint32_t aq_h = tc::smem_u32(Aqh), aq_l = tc::smem_u32(Aql);
+      for (int kk = 0; kk < S::NKD && !bad; ++kk) {
+        const bool ok = stream_chunk(dimg + (size_t)kk * 2 * S::bDc, 2 * S::bDc,
+                                     [&](uint32_t buf) {
+          const uint32_t bh = buf, bl = buf + S::bDc;
+          const uint64_t ah = tc::smem_desc(aq_h + kk * 256, 128, KD * 16);
+          const uint64_t al = tc::smem_desc(aq_l + kk * 256, 128, KD * 16);
+          const uint32_t acc0 = kk > 0 ? 1u : 0u;
+          tc::mma_bf16(tmem_diff, ah, tc::smem_desc(bh, 128, 256), ID_D1, acc0);
+          tc::mma_bf16(tmem_diff, ah, tc::smem_desc(bl, 128, 256), ID_D1, 1u);
+          tc::mma_bf16(tmem_diff, al, tc::smem_desc(bh, 128, 256), ID_D1, 1u);
+          if constexpr (S::ND2 > 0) {
+            const uint32_t o2 = (S::ND1 / 8) * 256;
+            tc::mma_bf16(tmem_diff + S::ND1, ah, tc::smem_desc(bh + o2, 128, 256), ID_D2, acc0);
+            tc::mma_bf16(tmem_diff + S::ND1, ah, tc::smem_desc(bl + o2, 128, 256), ID_D2, 1u);
+            tc::mma_bf16(tmem_diff + S::ND1, al, tc::smem_desc(bh + o2, 128, 256), ID_D2, 1u);
+          }
+        });
+        if (!ok) bad = 1;
+      }
+    }
+    if (bad) {
+      if (tid == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+      break;
+    }
+
+    // ---- C: face fluxes (FP32 on jumps formed in FP64) -> lift planes ----
+    auto face_flux = [&](int x, float (&fl)[F]) -> bool {
+      const int e = x / NFPT, p = x % NFPT, face = p / NFP, k = p % NFP;
+#pragma unroll
+      for (int f = 0; f < F; ++f) fl[f] = 0.f;
+      if (x >= S::NFACE || e >= ne) return false;
+      const int lnode = sfm[p];
+      float uM[NA], uP[NA], n[DIM];
+      const float* gf = sgeo + e * G + DIM * DIM + face * (DIM + 1);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) n[d] = gf[d];
+      const float fscale = gf[DIM];
+      const int2 cn = sconn[e * NF + face];
+      const int nb = cn.x;
+      const int64_t gm = (el0 + e) * NP + lnode;
+      bool have = true, bdry = false;
+      if (nb >= 0) {
+        const int nface = cn.y & 3, perm = cn.y >> 2;
+        if (!(nface < NF && perm < a.nperm && nb < a.K)) {
+          atomicCAS(a.err, 0, DEV_BAD_CODE);
+          return false;
+        }
+        const int nn = sfm[nface * NFP + ssh[perm * NFP + k]];
+        const int64_t gp = (int64_t)nb * NP + nn;
+        if constexpr (JumpLinear<MODEL>::value) {
+#pragma unroll
+          for (int f = 0; f < F; ++f) {
+            uM[f] = (float)(__ldg(a.q_in + f * Knp + gm) - __ldg(a.q_in + f * Knp + gp));
+            uP[f] = 0.f;
+          }
+        } else {
+          if constexpr (C != 0) {
+            uM[0] = scoef[e * NP + lnode];
+            uP[0] = (float)__ldg(a.coeff + gp);
+          }
+#pragma unroll
+          for (int f = 0; f < F; ++f) {
+            uM[C + f] = (float)__ldg(a.q_in + f * Knp + gm);
+            uP[C + f] = (float)__ldg(a.q_in + f * Knp + gp);
+          }
+        }
+      } else {
+        bdry = true;
+        if constexpr (C != 0) uM[0] = scoef[e * NP + lnode];
+#pragma unroll
+        for (int f = 0; f < F; ++f) uM[C + f] = (float)__ldg(a.q_in + f * Knp + gm);
+        float given = 0.f;
+        if (cn.y == HB_BC_GIVEN) {
+          const int64_t bi = (int64_t)(-1 - nb) * NFP + k;
+          if (a.bdry == nullptr || bi >= a.n_given) {
+            atomicCAS(a.err, 0, a.bdry == nullptr ? DEV_MISSING_INPUT : DEV_BAD_BDRY_INDEX);
+            have = false;
+          } else {
+            given = (float)__ldg(a.bdry + bi);
+          }
+        }
+        if (have) have = model_bc<MODEL, DIM, float>(a.mp, cn.y, uM, n, given, uP);
+      }
+      if (!have) return false;
+      model_flux<MODEL, DIM, float>(a.mp, bdry, uM, uP, n, fl);
+#pragma unroll
+      for (int f = 0; f < F; ++f) fl[f] *= fscale;
+      return true;
+    };
+    if constexpr (PT == PT_FP16) {
+      for (int u = 0; u < S::NFV; ++u) {
+        const int x = tid + u * S::THREADS;
+        float fl[F];
+        face_flux(x, fl);
+        const int e = x < S::NFACE ? x / NFPT : -1;
+        const unsigned grp = __match_any_sync(FULL, e);
+        const bool leader = (__ffs(grp) - 1) == lane;
+#pragma unroll
+        for (int f = 0; f < F; ++f) {
+          const unsigned m = __reduce_max_sync(grp, __float_as_uint(fabsf(fl[f])));
+          if (leader && e >= 0 && e < ne) atomicMax(&fmx[(e / EPW) * 32 + (e % EPW) * F + f], m);
+        }
+      }
+      __syncthreads();
+    }
+    for (int u = 0; u < S::NFV; ++u) {
+      const int x = tid + u * S::THREADS;
+      float fl[F];
+      face_flux(x, fl);
+      const int e = x / NFPT, p = x % NFPT;
+      if (x < S::NFACE && e < ne) {
+        const int rowb = (e / EPW) * 32 + (e % EPW) * F;
+#pragma unroll
+        for (int f = 0; f < F; ++f) {
+          float v = fl[f];
+          if constexpr (PT == PT_FP16) v *= row_scale_inv(fmx[rowb + f]);
+          store_split<PT>(Afh, Afl, kmajor_off(rowb + f, p, KL), v);
+        }
+      }
+    }
+    tc::fence_proxy_async();
+    __syncthreads();
+
+    // ---- D: lift MMAs, operator chunks streamed ----
+    {
+      const uint32_t af_h = tc::smem_u32(Afh), af_l = tc::smem_u32(Afl);
+      for (int kk = 0; kk < S::NKL && !bad; ++kk) {
+        const bool ok = stream_chunk(limg + (size_t)kk * 2 * S::bLc, 2 * S::bLc,
+                                     [&](uint32_t buf) {
+          const uint32_t bh = buf, bl = buf + S::bLc;
+          const uint64_t ah = tc::smem_desc(af_h + kk * 256, 128, KL * 16);
+          const uint64_t al = tc::smem_desc(af_l + kk * 256, 128, KL * 16);
+          tc::mma_bf16(tmem_lift, ah, tc::smem_desc(bh, 128, 256), ID_L, kk > 0 ? 1u : 0u);
+          tc::mma_bf16(tmem_lift, ah, tc::smem_desc(bl, 128, 256), ID_L, 1u);
+          tc::mma_bf16(tmem_lift, al, tc::smem_desc(bh, 128, 256), ID_L, 1u);
+        });
+        if (!ok) bad = 1;
+      }
+      if (!bad && tid == 0) tc::mma_commit(&mbar[2]);   // all of this batch's MMAs
+    }
+    if (bad) {
+      if (tid == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+      break;
+    }
+
+    // ---- E: TMEM -> chain rule, volume terms, + lift -> staged rhs ----
+    {
+      int late = 0;
+      if (tid == 0) late = !tc::mbar_wait(&mbar[2], it & 1u, MBAR_MAX_NS);
+      if (__syncthreads_or(late)) {
+        if (tid == 0) {
+          atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+          tc::mbar_wait(&mbar[2], it & 1u, MBAR_MAX_NS);
+        }
+        __syncthreads();
+        break;
+      }
+    }
+    tc::fence_after_sync();
+    {
+      const float* ge = sgeo + e_own * G;
+      float gm[DIM][DIM];
+#pragma unroll
+      for (int r = 0; r < DIM; ++r)
+#pragma unroll
+        for (int x = 0; x < DIM; ++x) gm[r][x] = ge[r * DIM + x];
+      const int base = lf * F;
+      float sdiff = a.op_scale_d, slift = a.op_scale_l;
+      if constexpr (PT == PT_FP16) {
+        sdiff *= row_scale(rmx[row]);
+        slift *= row_scale(fmx[row]);
+      }
+      const int i_lo = part * S::NPQ;
+      const int i_hi = (part + 1) * S::NPQ < NP ? (part + 1) * S::NPQ : NP;
+      constexpr int CHK = 8;
+#pragma unroll 1
+      for (int c0 = i_lo; c0 < i_hi; c0 += CHK) {
+        float dv[DIM][CHK], lv[CHK];
+#pragma unroll
+        for (int g = 0; g < CHK / 4; ++g) {
+          if (c0 + 4 * g < i_hi) {
+#pragma unroll
+            for (int r = 0; r < DIM; ++r)
+              tc::tmem_ld4(tmem_diff + lane_addr + r * NP + c0 + 4 * g,
+                           *reinterpret_cast<float(*)[4]>(&dv[r][4 * g]));
+            tc::tmem_ld4(tmem_lift + lane_addr + c0 + 4 * g,
+                         *reinterpret_cast<float(*)[4]>(&lv[4 * g]));
+          }
+        }
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int c = 0; c < CHK; ++c) {
+          const int i = c0 + c;
+          if (i >= i_hi) break;
+          float g[DIM];
+#pragma unroll
+          for (int x = 0; x < DIM; ++x) {
+            float s = 0.f;
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) s += gm[r][x] * (dv[r][c] * sdiff + lin[r]);
+            g[x] = s;
+          }
+          const float cnode = C ? scoef[e_own * NP + i] : 0.f;
+          const float mine = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
+          if (valid) {
+            const float src = a.source ? (float)a.source[(el0 + e_own) * NP + i] : 0.f;
+            sq[fown * FNP + e_own * NP + i] =
+                model_finish<MODEL, DIM, float>(a.mp, fown, mine, lv[c] * slift, src);
+          }
+        }
+      }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+
+    // ---- F: FP64 stage update (coalesced) ----
+    for (int x = tid; x < S::NVAL; x += S::THREADS) {
+      const int f = x / FNP, r = x - f * FNP;
+      if (r < ne * NP) {
+        const int64_t idx = f * Knp + el0 * NP + r;
+        const double rr = (double)sq[x];
+        if (a.mode == 0) {
+          a.q_out[idx] = rr;
+        } else {
+          const double nr = a.ra * a.res[idx] + a.dt * rr;
+          a.res[idx] = nr;
+          a.q_out[idx] = a.q_in[idx] + a.rb * nr;
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- tear-down: wait for any MMAs still reading the ring, release TMEM ----
+  if (tid == 0) {
+    for (int b = 0; b < 2; ++b)
+      if (ring_uses[b] > 0) tc::mbar_wait(&mbar[b], (ring_uses[b] - 1) & 1u, MBAR_MAX_NS);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, S::TMEM_COLS);
+}
+
+// ---------------------------------------------------------------------------
 // host side
 
 struct SplitOps {
   uint8_t* dev = nullptr;
   int order = 0;
+  int stream = 0;   // 1: streamed-operator variant
   float scale_d = 1.f, scale_l = 1.f;
 };
 
@@ -1190,6 +1678,155 @@ static hb_status launch_split_t(Op* op, int mode, double ra, double rb, double d
   }
 }
 
+
+// ---- streamed-operator variant (high orders) ----
+
+// one 16-column K chunk [k0, k0 + 16) of a (rows x cols) FP64 matrix (scaled
+// by 1/scale) as hi/lo planes of rp rows in the canonical K-major layout
+static void build_chunk(const std::vector<double>& m, int rows, int cols, int rp, int k0,
+                        int pt, double scale, uint8_t* hi, uint8_t* lo) {
+  std::memset(hi, 0, (size_t)rp * 16 * 2);
+  std::memset(lo, 0, (size_t)rp * 16 * 2);
+  for (int r = 0; r < rows; ++r)
+    for (int k = k0; k < cols && k < k0 + 16; ++k) {
+      const double v = m[(size_t)r * cols + k] / scale;
+      uint16_t h, l;
+      if (pt == PT_BF16) {
+        h = host_bf16((float)v);
+        l = host_bf16((float)(v - (double)host_bf16_to_float(h)));
+      } else {
+        h = host_fp16((float)v);
+        l = host_fp16((float)(v - (double)host_fp16_to_float(h)));
+      }
+      const uint32_t off = kmajor_off(r, k - k0, 16);
+      std::memcpy(hi + off, &h, 2);
+      std::memcpy(lo + off, &l, 2);
+    }
+}
+
+template <int MODEL, int DIM, int ORDER, int PT>
+static hb_status configure_stream(Op* op) {
+  using S = ShapeS<MODEL, DIM, ORDER>;
+  Discr* d = op->d;
+  if constexpr (!S::FITS) {
+    return fail(HB_ERR_UNSUPPORTED, "split kernel: element too large for the streamed variant");
+  } else {
+    if (d->np != S::NP || d->nfp != S::NFP)
+      return fail(HB_ERR_INVALID_ARGUMENT, "element sizes do not match the order");
+    auto kern = rhs_split_stream_kernel<MODEL, DIM, ORDER, PT>;
+    int dev, max_optin = 0, sms = 0;
+    HB_CUDA(cudaGetDevice(&dev));
+    HB_CUDA(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    HB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (S::total > (uint32_t)max_optin)
+      return fail(HB_ERR_UNSUPPORTED, "split kernel: streamed variant exceeds shared memory");
+    // one CTA per SM: pad the request so that TMEM is never oversubscribed
+    int smem_sm = 0;
+    HB_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    size_t smem = S::total;
+    const int max_ctas = 512 / (int)S::TMEM_COLS;
+    if ((size_t)smem_sm / (smem + 1024) > (size_t)max_ctas)
+      smem = std::min<size_t>((size_t)smem_sm / max_ctas - 1024 + 16, (size_t)max_optin);
+    HB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int64_t nbatch = (d->K + S::EB - 1) / S::EB;
+    op->threads = S::THREADS;
+    op->blocks_per_sm = 1;
+    op->smem = smem;
+    op->grid = (int)std::min<int64_t>(nbatch, (int64_t)sms);
+    op->elems_per_block = S::EB;
+    const int np = S::NP, nfpt = S::NFPT;
+    const double* h = reinterpret_cast<const double*>(d->host_blob.data());
+    const size_t ndm = (size_t)DIM * np * np;
+    std::vector<double> Dt((size_t)DIM * np * np);
+    for (int r = 0; r < DIM; ++r)
+      for (int j = 0; j < np; ++j)
+        for (int i = 0; i < np; ++i)
+          Dt[((size_t)r * np + i) * np + j] = h[((size_t)r * np + j) * np + i];
+    std::vector<double> Lt((size_t)np * nfpt);
+    for (int k = 0; k < nfpt; ++k)
+      for (int i = 0; i < np; ++i) Lt[(size_t)i * nfpt + k] = h[ndm + (size_t)k * np + i];
+    const size_t dbytes = (size_t)S::NKD * 2 * S::bDc, lbytes = (size_t)S::NKL * 2 * S::bLc;
+    std::vector<uint8_t> img(dbytes + lbytes + S::LIN_BYTES);
+    const double sd = plane_scale(Dt, PT), sl = plane_scale(Lt, PT);
+    for (int kk = 0; kk < S::NKD; ++kk) {
+      uint8_t* c = img.data() + (size_t)kk * 2 * S::bDc;
+      build_chunk(Dt, DIM * np, np, S::ND, 16 * kk, PT, sd, c, c + S::bDc);
+    }
+    for (int kk = 0; kk < S::NKL; ++kk) {
+      uint8_t* c = img.data() + dbytes + (size_t)kk * 2 * S::bLc;
+      build_chunk(Lt, np, nfpt, S::NL, 16 * kk, PT, sl, c, c + S::bLc);
+    }
+    {
+      uint8_t vert[4] = {0, 0, 0, 0};
+      for (int dd = 0; dd < DIM; ++dd) {
+        int best = -1;
+        for (int j = 0; j < np; ++j) {
+          bool hit = true;
+          for (int c = 0; c < DIM; ++c) {
+            const double want = (c == dd) ? 1.0 : -1.0;
+            if (std::fabs(d->unit_nodes[(size_t)j * DIM + c] - want) > 1e-12) hit = false;
+          }
+          if (hit) best = j;
+        }
+        if (best < 0) return fail(HB_ERR_INVALID_ARGUMENT, "reference element lacks vertex nodes");
+        vert[dd] = (uint8_t)best;
+      }
+      uint8_t* t = img.data() + dbytes + lbytes;
+      std::memcpy(t, vert, 4);
+      double* lam = reinterpret_cast<double*>(t + 8);
+      for (int j = 0; j < np; ++j)
+        for (int dd = 0; dd < DIM; ++dd)
+          lam[j * DIM + dd] = 0.5 * (1.0 + d->unit_nodes[(size_t)j * DIM + dd]);
+    }
+    SplitOps* so = static_cast<SplitOps*>(op->split_ops);
+    so->scale_d = (float)sd;
+    so->scale_l = (float)sl;
+    so->stream = 1;
+    if (cudaMalloc(&so->dev, img.size()) != cudaSuccess ||
+        cudaMemcpy(so->dev, img.data(), img.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(HB_ERR_CUDA, "cannot upload the split operator planes");
+    return HB_OK;
+  }
+}
+
+template <int MODEL, int DIM, int ORDER, int PT>
+static hb_status launch_stream_t(Op* op, int mode, double ra, double rb, double dt,
+                                 const void* q_in, void* q_out, void* res,
+                                 const double* coeff, const double* bdry,
+                                 const double* source, cudaStream_t s) {
+  using S = ShapeS<MODEL, DIM, ORDER>;
+  if constexpr (!S::FITS) {
+    return fail(HB_ERR_UNSUPPORTED, "split kernel: element too large for the streamed variant");
+  } else {
+    Discr* d = op->d;
+    SplitOps* so = static_cast<SplitOps*>(op->split_ops);
+    SplitArgs a;
+    a.K = d->K;
+    a.nbatch = (d->K + S::EB - 1) / S::EB;
+    a.n_given = op->n_given;
+    a.nperm = d->nperm;
+    a.ops = so->dev;
+    a.geo32 = d->geo32;
+    a.conn = op->conn; a.fmask = d->fmask; a.shuffle = d->shuffle;
+    a.q_in = static_cast<const double*>(q_in);
+    a.q_out = static_cast<double*>(q_out);
+    a.res = static_cast<double*>(res);
+    a.coeff = coeff; a.bdry = bdry; a.source = source;
+    a.ra = ra; a.rb = rb; a.dt = dt; a.mode = mode;
+    a.op_scale_d = so->scale_d;
+    a.op_scale_l = so->scale_l;
+    a.mp = op->mp;
+    a.err = op->err_flag;
+    rhs_split_stream_kernel<MODEL, DIM, ORDER, PT><<<op->grid, op->threads, op->smem, s>>>(a);
+    HB_CUDA(cudaGetLastError());
+    return HB_OK;
+  }
+}
+
+// high-order instances of the streamed variant
+#define HB_SPLIT_STREAM_INSTANCES(X) \
+  X(HB_MODEL_WAVE, 3, 6) X(HB_MODEL_WAVE, 3, 7) X(HB_MODEL_MAXWELL, 3, 6)
+
 // (model, dim, order) instances built into the library
 #define HB_SPLIT_INSTANCES(X)                                                          \
   X(HB_MODEL_ADVECTION, 2, 3) X(HB_MODEL_ADVECTION, 2, 4) X(HB_MODEL_ADVECTION, 2, 5)  \
@@ -1215,9 +1852,15 @@ hb_status prepare_split(Op* op) {
                          : configure_split<M, D, O, PT_BF16>(op);
   HB_SPLIT_INSTANCES(HB_CASE)
 #undef HB_CASE
+#define HB_CASE(M, D, O)                                                       \
+  if (op->model == M && dim == D && order == O)                                \
+    return pt == PT_FP16 ? configure_stream<M, D, O, PT_FP16>(op)              \
+                         : configure_stream<M, D, O, PT_BF16>(op);
+  HB_SPLIT_STREAM_INSTANCES(HB_CASE)
+#undef HB_CASE
   return fail(HB_ERR_UNSUPPORTED,
-              "BF16x3 path: this (model, dimension, order) is not built (see "
-              "HB_SPLIT_INSTANCES)");
+              "split path: this (model, dimension, order) is not built (see "
+              "HB_SPLIT_INSTANCES, HB_SPLIT_STREAM_INSTANCES)");
 }
 
 hb_status launch_split(Op* op, int mode, double ra, double rb, double dt,
@@ -1233,6 +1876,15 @@ hb_status launch_split(Op* op, int mode, double ra, double rb, double dt,
                : launch_split_t<M, D, O, PT_BF16>(op, mode, ra, rb, dt, q_in, q_out,  \
                                                   res, coeff, bdry, source, s);
   HB_SPLIT_INSTANCES(HB_CASE)
+#undef HB_CASE
+#define HB_CASE(M, D, O)                                                              \
+  if (op->model == M && dim == D && order == O)                                       \
+    return pt == PT_FP16                                                              \
+               ? launch_stream_t<M, D, O, PT_FP16>(op, mode, ra, rb, dt, q_in, q_out, \
+                                                   res, coeff, bdry, source, s)       \
+               : launch_stream_t<M, D, O, PT_BF16>(op, mode, ra, rb, dt, q_in, q_out, \
+                                                   res, coeff, bdry, source, s);
+  HB_SPLIT_STREAM_INSTANCES(HB_CASE)
 #undef HB_CASE
   return fail(HB_ERR_UNSUPPORTED, "model/dimension/order combination not built");
 }

@@ -106,3 +106,52 @@ def test_split_lsrk_steps(cuda_device, precision):
     err = rel_l2(y.cpu().numpy().reshape(yo.shape), yo)
     print("%s 5 LSRK4 steps rel-L2 %.3e" % (precision, err))
     assert err <= 2e-4
+
+
+# ---- streamed-operator variant (3D, N >= 6: operator planes stream through
+# shared memory; diff accumulator split over two MMAs at N = 7) ----
+
+@pytest.mark.parametrize("precision", PRECS)
+@pytest.mark.parametrize("order", [6, 7])
+def test_split_stream_wave_3d(cuda_device, order, precision):
+    d = hb.Discretization(box(2, 0.05, 3), order=order)
+    err = _split_err(d, hb.StrongWaveOperator(1.0, 3, flux_type="upwind"), precision=precision)
+    print("%s wave3d N=%d (streamed) rel-L2 %.3e" % (precision, order, err))
+    assert err <= TOL[precision]
+
+
+@pytest.mark.parametrize("precision", PRECS)
+def test_split_stream_maxwell(cuda_device, precision):
+    d = hb.Discretization(box(2, 0.05, 5), order=6)
+    err = _split_err(d, hb.MaxwellOperator(1.0, 1.0, flux_type=1), precision=precision)
+    print("%s maxwell N=6 (streamed) rel-L2 %.3e" % (precision, err))
+    assert err <= TOL[precision]
+
+
+def test_split_stream_pulse_steps(cuda_device):
+    """Wave N = 7, Gaussian pulse on a coarse box: FP16x3 within 5e-6 of the
+    oracle after one RHS and after 5 fused LSRK4 steps."""
+    from oracle import OracleRHS
+    from hedge_b200.timestep import RK4A, RK4B
+    d = hb.Discretization(box(2, 0.05, 3), order=7)
+    op = hb.StrongWaveOperator(1.0, 3, flux_type="upwind")
+    x = d.nodes
+    q = np.zeros((4, len(d)))
+    q[0] = np.exp(-(x ** 2).sum(1) / 0.15 ** 2 * 0.25)
+    orc = OracleRHS(d, op.op_template())
+    rhs = op.bind(hb.Discretization(d.mesh, order=7, precision="fp16x3"))
+    err1 = rel_l2(rhs(0.0, q).cpu().numpy(), orc(q))
+    print("fp16x3 wave3d N=7 pulse: 1 RHS rel-L2 %.3e" % err1)
+    assert err1 <= 5e-6, err1
+    dt = op.estimate_timestep(d)
+    st = hb.LSRK4TimeStepper()
+    y = rhs.discr.to_device(q)
+    ref, res = q.copy(), np.zeros_like(q)
+    for _ in range(5):
+        y = st(y, 0.0, dt, rhs)
+        for s in range(5):
+            res = RK4A[s] * res + dt * orc(ref)
+            ref = ref + RK4B[s] * res
+    err5 = rel_l2(y.cpu().numpy(), ref)
+    print("fp16x3 wave3d N=7 pulse: 5 steps rel-L2 %.3e" % err5)
+    assert err5 <= 5e-6, err5
