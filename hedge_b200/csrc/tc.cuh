@@ -124,9 +124,10 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// Waits for the completion of the mbarrier phase with parity `parity`
-// (try_wait lets the hardware suspend the thread between polls); gives up
-// after `max_ns` nanoseconds and returns false.
+// Waits for the completion of the mbarrier phase with parity `parity`; gives
+// up after `max_ns` nanoseconds and returns false.  Each try_wait may suspend
+// the thread in hardware for up to ~1 ms (it resumes as soon as the phase
+// completes), so a waiting warp does not spin on the issue slots.
 __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint64_t max_ns) {
   const uint32_t a = smem_u32(mbar);
   const uint64_t t0 = global_ns();
@@ -134,10 +135,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint6
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}\n"
         : "=r"(done)
-        : "r"(a), "r"(parity)
+        : "r"(a), "r"(parity), "r"(1000000u)
         : "memory");
     if (done) return true;
     if (global_ns() - t0 > max_ns) return false;
