@@ -49,7 +49,8 @@ class hb_op_desc(C.Structure):
                 ("v", C.c_double * 3), ("c", C.c_double), ("eps", C.c_double),
                 ("mu", C.c_double), ("alpha", C.c_double), ("bdry_alpha", C.c_double),
                 ("time_sign", C.c_double),
-                ("conn", C.c_void_p), ("num_given_bdry_nodes", C.c_int64)]
+                ("conn", C.c_void_p), ("num_given_bdry_nodes", C.c_int64),
+                ("num_halo_faces", C.c_int64)]
 
 
 EXPORTED = [
@@ -57,7 +58,7 @@ EXPORTED = [
     "hb_rhs", "hb_lsrk_stage", "hb_lincomb", "hb_gather_map", "hb_op_check",
     "hb_op_launch_info", "hb_norm", "hb_norm_noalloc", "hb_rhs_adjoint_work_size",
     "hb_rhs_adjoint", "hb_batch_create", "hb_batch_destroy", "hb_batch_stage",
-    "hb_batch_info", "hb_batch_check",
+    "hb_batch_info", "hb_batch_check", "hb_op_set_halo", "hb_pack",
     "hb_last_error_string",
 ]
 
@@ -97,6 +98,8 @@ def load(path=LIB_PATH):
             "hb_batch_stage": [vp, d, d, i32, vp],
             "hb_batch_info": [vp, vp, i32],
             "hb_batch_check": [vp, vp],
+            "hb_op_set_halo": [vp, vp, vp],
+            "hb_pack": [i64, i32, i32, i64, vp, vp, vp, vp],
         }
         for name, args in sig.items():
             fn = getattr(lib, name)

@@ -183,11 +183,16 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
     return fail(HB_ERR_INVALID_ARGUMENT, "Maxwell material must be positive");
   // host validation of the face table (the kernels also flag bad entries)
   const int64_t nfc = d->K * d->nfaces;
+  if (desc->num_halo_faces < 0) return fail(HB_ERR_INVALID_ARGUMENT, "negative halo face count");
+  if (desc->num_halo_faces > 0 && desc->precision != HB_PREC_FP64 &&
+      desc->precision != HB_PREC_FP32)
+    return fail(HB_ERR_UNSUPPORTED, "halo faces: FP64 and FP32 paths only");
+  const int64_t nb_end = d->K + desc->num_halo_faces;   // neighbours K.. are halo slots
   int64_t max_given = 0;
   for (int64_t x = 0; x < nfc; ++x) {
     const int nbr = desc->conn[2 * x], code = desc->conn[2 * x + 1];
     if (nbr >= 0) {
-      if (nbr >= d->K || (code & 3) >= d->nfaces || (code >> 2) >= d->nperm || code < 0)
+      if (nbr >= nb_end || (code & 3) >= d->nfaces || (code >> 2) >= d->nperm || code < 0)
         return fail(HB_ERR_INVALID_ARGUMENT, "connectivity entry out of range");
     } else {
       if (code < HB_BC_NONE || code > HB_BC_ABSORB)
@@ -207,6 +212,7 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
   op->F = F;
   op->precision = desc->precision;
   op->n_given = desc->num_given_bdry_nodes;
+  op->n_halo = desc->num_halo_faces;
   ModelParams& mp = op->mp;
   for (int k = 0; k < 3; ++k) mp.v[k] = desc->v[k];
   mp.c = desc->c; mp.eps = desc->eps; mp.mu = desc->mu;
@@ -252,6 +258,8 @@ static hb_status check_inputs(Op* op, const void* q_in, const void* q_out,
                               const double* coeff) {
   if (!q_in || !q_out) return fail(HB_ERR_INVALID_ARGUMENT, "null state pointer");
   if (q_in == q_out) return fail(HB_ERR_INVALID_ARGUMENT, "output aliases the input state");
+  if (op->n_halo > 0 && !op->halo)
+    return fail(HB_ERR_INVALID_ARGUMENT, "halo faces but no halo buffer (hb_op_set_halo)");
   if (op->model == HB_MODEL_VARWAVE && !coeff)
     return fail(HB_ERR_INVALID_ARGUMENT, "variable-velocity wave needs the c field");
   return HB_OK;
@@ -345,6 +353,28 @@ hb_status hb_rhs_adjoint(hb_op* handle, const double* q, const double* lam, doub
   if (!g.ok) return fail(HB_ERR_CUDA, "cannot select the CUDA device");
   return launch_adjoint(op, q, lam, q_bar, c_bar, coeff, static_cast<double*>(work),
                         reinterpret_cast<cudaStream_t>(stream));
+}
+
+hb_status hb_op_set_halo(hb_op* handle, const void* halo, const double* halo_coeff) {
+  if (!handle) return fail(HB_ERR_INVALID_ARGUMENT, "null operator");
+  Op* op = reinterpret_cast<Op*>(handle);
+  if (op->n_halo == 0) return fail(HB_ERR_INVALID_ARGUMENT, "operator has no halo faces");
+  if (!halo) return fail(HB_ERR_INVALID_ARGUMENT, "null halo buffer");
+  if (op->model == HB_MODEL_VARWAVE && !halo_coeff)
+    return fail(HB_ERR_INVALID_ARGUMENT, "variable-velocity wave needs the halo c values");
+  op->halo = halo;
+  op->halo_c = halo_coeff;
+  return HB_OK;
+}
+
+hb_status hb_pack(int64_t n, int32_t dtype, int32_t nfields, int64_t field_stride,
+                  const int64_t* idx, const void* src, void* dst, void* stream) {
+  if (n < 0 || nfields < 1 || (dtype != 0 && dtype != 1))
+    return fail(HB_ERR_INVALID_ARGUMENT, "bad pack size, field count or dtype");
+  if (n == 0) return HB_OK;
+  if (!idx || !src || !dst) return fail(HB_ERR_INVALID_ARGUMENT, "null argument");
+  return launch_pack(n, dtype, nfields, field_stride, idx, src, dst,
+                     reinterpret_cast<cudaStream_t>(stream));
 }
 
 hb_status hb_op_check(hb_op* handle, void* stream) {

@@ -83,6 +83,9 @@ struct Op {
   ModelParams mp;
   int2* conn = nullptr;        // [K][nfaces] (nbr, code)
   int64_t n_given;
+  int64_t n_halo = 0;          // halo faces (neighbours K .. K + n_halo - 1)
+  const void* halo = nullptr;  // [n_halo * nfp][F] ext values, state dtype (caller's)
+  const double* halo_c = nullptr;  // [n_halo * nfp] ext c values (var-c wave)
   int* err_flag = nullptr;     // device int
   // launch configuration chosen at create time
   int elems_per_block = 0;
@@ -108,6 +111,10 @@ hb_status launch_norm(int64_t K, int np, int nfields, int dtype, const double* m
 int64_t adjoint_work_bytes(const Op* op);
 hb_status launch_adjoint(Op* op, const double* q, const double* lam, double* q_bar,
                          double* c_bar, const double* coeff, double* work, cudaStream_t s);
+
+// gather for halo exchange (rhs_simt.cu): dst[j][f] = src[f][idx[j]]
+hb_status launch_pack(int64_t n, int dtype, int nfields, int64_t field_stride,
+                      const int64_t* idx, const void* src, void* dst, cudaStream_t s);
 
 // kernel launchers (rhs_simt.cu)
 hb_status launch_simt(Op* op, int mode, double a, double b, double dt,

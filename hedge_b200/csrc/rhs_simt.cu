@@ -43,6 +43,9 @@ struct SimtArgs {
   const double* coeff;
   const double* bdry;
   const double* source;
+  const S* halo;            // [n_halo * nfp][F] ext values of halo faces
+  const double* halo_c;     // [n_halo * nfp] ext c (var-c wave)
+  int64_t n_halo;
   double ra, rb, dt;
   int mode;  // 0: write rhs, 1: LSRK stage
   int ops_in_smem;  // operators staged in shared memory (else read via L1)
@@ -201,11 +204,23 @@ __global__ void __launch_bounds__(256) rhs_simt_kernel(SimtArgs<T, S> a) {
         const int2 cn = sconn[e * nf + face];
         bool have = true;
         bool bdry = false;
-        if (cn.x >= 0) {
+        if (cn.x >= a.K) {
+          // neighbour on another partition: ext values from the halo buffer
+          const int64_t h = (int64_t)cn.x - a.K;
+          if (h >= a.n_halo || a.halo == nullptr) {
+            flag(a.err, DEV_BAD_NEIGHBOUR);
+            have = false;
+          } else {
+            const int64_t hi = h * nfp + k;
+            if constexpr (C != 0) uP[0] = T(a.halo_c[hi]);
+#pragma unroll
+            for (int f = 0; f < F; ++f) uP[C + f] = T(a.halo[hi * F + f]);
+          }
+        } else if (cn.x >= 0) {
           bool ok;
           const int nn = ext_node(cn.y, k, nfp, nf, a.nperm, sfm, ssh, ok);
-          if (!ok || cn.x >= a.K) {
-            flag(a.err, ok ? DEV_BAD_NEIGHBOUR : DEV_BAD_CODE);
+          if (!ok) {
+            flag(a.err, DEV_BAD_CODE);
             have = false;
           } else {
             const int64_t gi = (int64_t)cn.x * np + nn;
@@ -336,6 +351,9 @@ static hb_status launch_one(Op* op, int mode, double ra, double rb, double dt,
   a.res = static_cast<S*>(res);
   a.rhs_out = static_cast<S*>(q_out);
   a.coeff = coeff; a.bdry = bdry; a.source = source;
+  a.halo = static_cast<const S*>(op->halo);
+  a.halo_c = op->halo_c;
+  a.n_halo = op->n_halo;
   a.ra = ra; a.rb = rb; a.dt = dt; a.mode = mode;
   a.ops_in_smem = op->ops_in_smem;
   a.mp = op->mp;
@@ -442,6 +460,35 @@ hb_status launch_lincomb(int64_t n, int dtype, double a, const void* x, double b
   else
     lincomb_kernel<float><<<grid, 256, 0, s>>>(n, (float)a, (const float*)x, (float)b,
                                                (const float*)y, (float*)out);
+  HB_CUDA(cudaGetLastError());
+  return HB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// halo exchange pack: dst[j][f] = src[f][idx[j]] (thread per (j, f) pair)
+template <typename T>
+__global__ void pack_kernel(int64_t n, int nfields, int64_t field_stride,
+                            const int64_t* __restrict__ idx, const T* __restrict__ src,
+                            T* __restrict__ dst) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * nfields) return;
+  const int64_t j = t / nfields;
+  const int f = (int)(t - j * nfields);
+  dst[t] = src[f * field_stride + idx[j]];
+}
+
+hb_status launch_pack(int64_t n, int dtype, int nfields, int64_t field_stride,
+                      const int64_t* idx, const void* src, void* dst, cudaStream_t s) {
+  const int64_t total = n * nfields;
+  const unsigned grid = (unsigned)((total + 255) / 256);
+  if (dtype == 0)
+    pack_kernel<double><<<grid, 256, 0, s>>>(n, nfields, field_stride, idx,
+                                             static_cast<const double*>(src),
+                                             static_cast<double*>(dst));
+  else
+    pack_kernel<float><<<grid, 256, 0, s>>>(n, nfields, field_stride, idx,
+                                            static_cast<const float*>(src),
+                                            static_cast<float*>(dst));
   HB_CUDA(cudaGetLastError());
   return HB_OK;
 }

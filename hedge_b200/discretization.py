@@ -310,6 +310,50 @@ class PointEvaluator:
         return np.asarray(field)[..., s] @ self.coeff
 
 
+def build_face_table(discr, ot):
+    """Host face table of an operator: [K][Nf][2] int32, interior faces
+    (neighbour, nbr_face | perm << 2), boundary faces (-1 - b, BC kind) with
+    b numbering the BC_GIVEN faces; and the number of given boundary nodes
+    and the given tag."""
+    mesh = discr.mesh
+    model = ot.operator
+    if model is not None and hasattr(model, "bc_tags"):
+        check_bc_coverage(mesh, model.bc_tags())
+    nbr = discr.nbr.astype(np.int64).copy()
+    code = discr.nbr_code.astype(np.int64).copy()
+    bdry_faces = nbr < 0
+    # boundary faces without a BC of this operator contribute no flux
+    code[bdry_faces] = BC_NONE
+    given_tag = None
+    n_given = 0
+    for tag, kind in ot.bcs:
+        if tag is TAG_NONE:
+            continue
+        ef = mesh.boundary_faces(tag)
+        if len(ef) == 0:
+            continue
+        code[ef[:, 0], ef[:, 1]] = kind
+        if kind == BC_GIVEN:
+            nbr[ef[:, 0], ef[:, 1]] = -1 - np.arange(len(ef))
+            given_tag = tag
+            n_given = len(ef) * discr.Nfp
+    conn = np.ascontiguousarray(np.stack([nbr, code], axis=-1).astype(np.int32))
+    return conn, n_given, given_tag
+
+
+def op_descriptor(ot, prec, conn, n_given, num_halo_faces=0):
+    """hb_op_desc of a model operator over a face table."""
+    p = ot.params
+    v = np.zeros(3)
+    if "v" in p:
+        v[:len(p["v"])] = p["v"]
+    return _native.hb_op_desc(
+        ot.model, ot.n_fields, prec, ot.flux_type, p.get("bdry_flux_type", ot.flux_type),
+        (C.c_double * 3)(*v), p.get("c", 0.0), p.get("eps", 1.0), p.get("mu", 1.0),
+        p.get("alpha", 1.0), p.get("bdry_alpha", p.get("alpha", 1.0)),
+        p.get("time_sign", 1.0), conn.ctypes.data, n_given, int(num_halo_faces))
+
+
 class CompiledOperator:
     """A model right-hand side compiled for the device.
 
@@ -323,43 +367,14 @@ class CompiledOperator:
         self.ot = ot
         self.precision = precision
         self.F = ot.n_fields
-        mesh = discr.mesh
-        model = ot.operator
-        if model is not None and hasattr(model, "bc_tags"):
-            check_bc_coverage(mesh, model.bc_tags())
-        nbr = discr.nbr.astype(np.int64).copy()
-        code = discr.nbr_code.astype(np.int64).copy()
-        bdry_faces = nbr < 0
-        # boundary faces without a BC of this operator contribute no flux
-        code[bdry_faces] = BC_NONE
-        self.given_tag = None
-        n_given = 0
-        for tag, kind in ot.bcs:
-            if tag is TAG_NONE:
-                continue
-            ef = mesh.boundary_faces(tag)
-            if len(ef) == 0:
-                continue
-            code[ef[:, 0], ef[:, 1]] = kind
-            if kind == BC_GIVEN:
-                nbr[ef[:, 0], ef[:, 1]] = -1 - np.arange(len(ef))
-                self.given_tag = tag
-                n_given = len(ef) * discr.Nfp
-        self.conn = np.ascontiguousarray(np.stack([nbr, code], axis=-1).astype(np.int32))
-        self.n_given = n_given
-        p = ot.params
-        v = np.zeros(3)
-        if "v" in p:
-            v[:len(p["v"])] = p["v"]
+        self.conn, self.n_given, self.given_tag = build_face_table(discr, ot)
         prec = PRECISIONS[precision] if precision != "plain" else (
             _native.PREC_FP64 if discr.default_scalar_type == np.float64
             else _native.PREC_FP32)
         self.prec_code = prec
-        desc = _native.hb_op_desc(
-            ot.model, ot.n_fields, prec, ot.flux_type, p.get("bdry_flux_type", ot.flux_type),
-            (C.c_double * 3)(*v), p.get("c", 0.0), p.get("eps", 1.0), p.get("mu", 1.0),
-            p.get("alpha", 1.0), p.get("bdry_alpha", p.get("alpha", 1.0)),
-            p.get("time_sign", 1.0), self.conn.ctypes.data, n_given)
+        model = ot.operator
+        p = ot.params
+        desc = op_descriptor(ot, prec, self.conn, self.n_given)
         lib = _native.load()
         h = C.c_void_p()
         _native.check(lib.hb_op_create(discr._native_handle(), C.byref(desc), C.byref(h)))

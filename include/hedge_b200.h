@@ -92,6 +92,9 @@ typedef struct {
   double time_sign;        /* variable-velocity wave */
   const int32_t* conn;
   int64_t num_given_bdry_nodes;
+  int64_t num_halo_faces;  /* faces whose neighbour lives on another partition
+                              (conn neighbour K + h, h < num_halo_faces); their
+                              ext values come from hb_op_set_halo; 0 = none */
 } hb_op_desc;
 
 /* Replaces Discretization.compile -> jit Executor construction
@@ -208,6 +211,24 @@ hb_status hb_batch_stage(hb_batch* batch, double a, double b, int32_t parity, vo
 hb_status hb_batch_info(hb_batch* batch, int64_t* info, int32_t n);
 /* synchronises `stream`; HB_ERR_DEVICE_FLAG if a stage met bad face data */
 hb_status hb_batch_check(hb_batch* batch, void* stream);
+
+/* Element-partitioned operators (several devices or processes, one
+ * partition each): a face whose neighbour lives on another partition is
+ * coded (K + h, nbr_face | perm << 2) with h < num_halo_faces, and its ext
+ * values are read from a halo buffer [num_halo_faces * nfp][F] (state dtype;
+ * row h*nfp + k = the neighbour's values at this face's node k, already in
+ * this face's node order) and, for the variable-velocity wave, halo_coeff
+ * [num_halo_faces * nfp].  Both are device buffers of the caller, refreshed
+ * between stages (typically by hb_pack on the owner + a point-to-point
+ * exchange).  FP64 / FP32 paths.  Replaces the reference's MPI face-trace
+ * exchange (hedge/backends/mpi/__init__.py:184-216, 284-340). */
+hb_status hb_op_set_halo(hb_op* op, const void* halo, const double* halo_coeff);
+
+/* dst[j * nfields + f] = src[f * field_stride + idx[j]], j < n: packs the
+ * volume values a peer needs (idx device int64) for the halo exchange;
+ * dtype 0 = FP64, 1 = FP32. */
+hb_status hb_pack(int64_t n, int32_t dtype, int32_t nfields, int64_t field_stride,
+                  const int64_t* idx, const void* src, void* dst, void* stream);
 
 /* Synchronises `stream` and returns HB_ERR_DEVICE_FLAG if a kernel of this
  * operator flagged bad input (out-of-range neighbour or code, missing
