@@ -51,6 +51,10 @@ def parse():
     p.add_argument("--workload", default="maxwell", choices=["maxwell", "wave7"],
                    help="maxwell: 3D Maxwell N=4 cavity (default); wave7: 3D acoustic "
                         "wave N=7 Gaussian pulse (the high-order precision workload)")
+    p.add_argument("--layout", default="partitioned", choices=["partitioned", "replicas"],
+                   help="N > 1: partitioned = one mesh of N x the per-GPU size, "
+                        "element-partitioned with a face-trace exchange every stage "
+                        "(weak scaling); replicas = N independent copies")
     p.add_argument("--accuracy-steps", type=int, default=None,
                    help="steps of the split-vs-FP64 accuracy run (default steps+warmup)")
     p.add_argument("--no-compare", action="store_true",
@@ -293,20 +297,63 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def partitioned_problem(args, rank, world, dev):
+    """One mesh of world x the per-GPU workload (the box stretched along x),
+    element-partitioned across the ranks; this rank's operator exchanges its
+    cut-face traces with its neighbours (NCCL point-to-point) every stage."""
+    import torch
+    import torch.distributed as dist
+    import hedge_b200 as hb
+    from hedge_b200.partition import DistExchange, PartitionPlan, PartitionedOperator
+    from hedge_b200.timestep import RK4A, RK4B
+    n = args.n
+    h = 2.0 / n
+    mesh = hb.make_box_tet_mesh(a=(-1, -1, -1), b=(-1 + 2 * world, 1, 1), n=(n * world, n, n),
+                                jitter=0.05 * h, seed=1)
+    discr = hb.Discretization(mesh, order=args.order, precision=args.precision, device=dev)
+    _, _, _, op = build_problem(2, args.order, "fp64", device=dev, workload=args.workload)
+    plan = PartitionPlan(discr, op.op_template(), world)
+    part = PartitionedOperator(discr, op, plan, rank, precision=args.precision, device=dev,
+                               exchange=DistExchange(plan, rank))
+    dist.barrier()
+    w0 = initial_state(discr, args.workload)
+    dt = op.estimate_timestep(discr)
+    res = torch.zeros((part.F, part.K * part.Np), dtype=part.dtype, device=dev)
+
+    def stepper(y, t, dt_, rhs_):
+        cur = y
+        for s_ in range(5):
+            nxt = torch.empty_like(cur)
+            part.lsrk_stage(RK4A[s_], RK4B[s_], dt_, cur, nxt, res)
+            cur = nxt
+        return cur
+
+    return hb, discr, op, part, part.scatter(w0), dt, stepper
+
+
 def run_ours(args):
     import torch
     rank, world, local = dist_setup(args.gpus)
     dev = torch.device("cuda", torch.cuda.current_device())
     W = WORKLOADS[args.workload]
     F = W["fields"]
-    hb, mesh, discr, op = build_problem(args.n, args.order, args.precision, device=dev,
-                                        workload=args.workload)
-    w0 = initial_state(discr, args.workload)
-    dt = op.estimate_timestep(discr)
-    rhs = op.bind(discr)
-    comp = rhs.compiled
-    stepper = hb.LSRK4TimeStepper()
-    y = discr.to_device(w0).reshape(F, -1)
+    partitioned = world > 1 and args.layout == "partitioned"
+    if partitioned:
+        hb, discr, op, comp, y, dt, stepper = partitioned_problem(args, rank, world, dev)
+        rhs = None
+        w0 = y.cpu().numpy()
+        K_rank, K_total = comp.K, discr.K
+        args.no_compare = True
+    else:
+        hb, mesh, discr, op = build_problem(args.n, args.order, args.precision, device=dev,
+                                            workload=args.workload)
+        w0 = initial_state(discr, args.workload)
+        dt = op.estimate_timestep(discr)
+        rhs = op.bind(discr)
+        comp = rhs.compiled
+        stepper = hb.LSRK4TimeStepper()
+        y = discr.to_device(w0).reshape(F, -1)
+        K_rank, K_total = discr.K, discr.K * world
     # warm-up
     t = 0.0
     for _ in range(args.warmup):
@@ -327,13 +374,12 @@ def run_ours(args):
     ms = ev0.elapsed_time(ev1)
     comp.check()
     ms_max = max_over_ranks(ms, world)
-    dofs_rank = discr.K * discr.Np * F * 5 * args.steps
-    value = dofs_rank * world / (ms_max * 1e-3)
+    value = K_total * discr.Np * F * 5 * args.steps / (ms_max * 1e-3)
     launches = 5 * args.steps
     launch_ms = ms / launches
     state_bytes = 8 if args.precision != "fp32" else 4
     bpd = algorithmic_bytes_per_dof_update(discr, state_bytes, F)
-    bytes_per_launch = bpd * discr.K * discr.Np * F
+    bytes_per_launch = bpd * K_rank * discr.Np * F
     achieved = bytes_per_launch / (launch_ms * 1e-3) / 1e9
     peaks = {}
     try:
@@ -413,7 +459,7 @@ def run_ours(args):
         barrier(world)
         e_ms = max_over_ranks(ev0.elapsed_time(ev1), world)
         nbytes = host_in.numel() * host_in.element_size()
-        e2e = {"value": discr.K * discr.Np * F * 5 * e2e_steps * world / (e_ms * 1e-3),
+        e2e = {"value": K_total * discr.Np * F * 5 * e2e_steps / (e_ms * 1e-3),
                "unit": "DOF-updates/s", "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "steps": e2e_steps}
 
@@ -434,14 +480,16 @@ def run_ours(args):
             "dtype": {"fp64": "f64", "fp32": "f32", "bf16x3": "bf16x3+f32acc, f64 state",
                       "fp16x3": "fp16x3(scaled)+f32acc, f64 state"}[args.precision],
             "data": "synthetic",
-            "config": {"workload": W["label"] % (discr.K, args.order), "K": discr.K,
-                       "order": args.order, "Np": discr.Np, "fields": F,
+            "config": {"workload": W["label"] % (K_rank, args.order), "K": K_total,
+                       "K_per_gpu": K_rank, "order": args.order, "Np": discr.Np, "fields": F,
                        "precision": args.precision, "stepper": "LSRK4 (5 fused stages)",
-                       "parallelism": "replicas" if world > 1 else "single",
+                       "parallelism": ("partitioned, face-trace exchange per stage (NCCL)"
+                                       if partitioned else
+                                       "replicas" if world > 1 else "single"),
                        "l2": "working set 3 x %.1f MB > 126 MB L2, no flush" %
-                             (discr.K * discr.Np * F * state_bytes / 1e6)},
+                             (K_rank * discr.Np * F * state_bytes / 1e6)},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "split_vs_fp64": compare,
-            "gpu_launches": launches, "clocks": clk.summary(),
+            "gpu_launches": launches * (2 if partitioned else 1), "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
     if world > 1:

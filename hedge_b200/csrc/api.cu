@@ -184,9 +184,6 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
   // host validation of the face table (the kernels also flag bad entries)
   const int64_t nfc = d->K * d->nfaces;
   if (desc->num_halo_faces < 0) return fail(HB_ERR_INVALID_ARGUMENT, "negative halo face count");
-  if (desc->num_halo_faces > 0 && desc->precision != HB_PREC_FP64 &&
-      desc->precision != HB_PREC_FP32)
-    return fail(HB_ERR_UNSUPPORTED, "halo faces: FP64 and FP32 paths only");
   const int64_t nb_end = d->K + desc->num_halo_faces;   // neighbours K.. are halo slots
   int64_t max_given = 0;
   for (int64_t x = 0; x < nfc; ++x) {

@@ -161,6 +161,9 @@ struct SplitArgs {
   const double* coeff;
   const double* bdry;
   const double* source;
+  const double* halo;     // [n_halo * nfp][F] ext values of faces on other partitions
+  const double* halo_c;   // [n_halo * nfp] ext c (var-c wave)
+  int64_t n_halo;
   double ra, rb, dt;
   float op_scale_d, op_scale_l;   // operator plane scales (powers of two)
   int mode;
@@ -742,7 +745,25 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
           if (j < NEPW && e < ne && p < NFPT) {
             const int2 cn = sconn[e * NF + face];
             const int nb = cn.x;
-            if (nb >= 0) {
+            if (nb >= a.K) {
+              // neighbour on another partition: ext values from the halo buffer
+              const int64_t hk = ((int64_t)nb - a.K) * NFP + k;
+              if (nb - a.K < a.n_halo && a.halo != nullptr) {
+                const int lnode = sfm[p];
+                if constexpr (JumpLinear<MODEL>::value) {
+#pragma unroll
+                  for (int f = 0; f < F; ++f)
+                    uPs[u][f] = (float)(st[f * FNP + e * NP + lnode] - a.halo[hk * F + f]);
+                } else {
+                  if constexpr (C != 0) uPs[u][0] = (float)a.halo_c[hk];
+#pragma unroll
+                  for (int f = 0; f < F; ++f) uPs[u][C + f] = (float)a.halo[hk * F + f];
+                }
+                okp[u] = true;
+              } else {
+                atomicCAS(a.err, 0, DEV_BAD_NEIGHBOUR);
+              }
+            } else if (nb >= 0) {
               const int code = cn.y;
               const int nface = code & 3, perm = code >> 2;
               if (nface < NF && perm < a.nperm && nb < a.K) {
@@ -1667,6 +1688,9 @@ static hb_status launch_split_t(Op* op, int mode, double ra, double rb, double d
     a.q_out = static_cast<double*>(q_out);
     a.res = static_cast<double*>(res);
     a.coeff = coeff; a.bdry = bdry; a.source = source;
+    a.halo = static_cast<const double*>(op->halo);
+    a.halo_c = op->halo_c;
+    a.n_halo = op->n_halo;
     a.ra = ra; a.rb = rb; a.dt = dt; a.mode = mode;
     a.op_scale_d = so->scale_d;
     a.op_scale_l = so->scale_l;
@@ -1713,6 +1737,8 @@ static hb_status configure_stream(Op* op) {
   } else {
     if (d->np != S::NP || d->nfp != S::NFP)
       return fail(HB_ERR_INVALID_ARGUMENT, "element sizes do not match the order");
+    if (op->n_halo > 0)
+      return fail(HB_ERR_UNSUPPORTED, "halo faces: not on the streamed high-order split kernel");
     auto kern = rhs_split_stream_kernel<MODEL, DIM, ORDER, PT>;
     int dev, max_optin = 0, sms = 0;
     HB_CUDA(cudaGetDevice(&dev));

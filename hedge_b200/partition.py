@@ -182,7 +182,7 @@ class LocalExchange:
 
 class PartitionedOperator:
     """One part of an element-partitioned model operator on one device
-    (FP64 or FP32 path)."""
+    (any precision path; the split ones below order 6 in 3D)."""
 
     def __init__(self, discr, model, plan, rank, precision="fp64", device=None, exchange=None):
         torch = _torch()
@@ -193,8 +193,9 @@ class PartitionedOperator:
         self.Np = discr.Np
         self.K = len(p.elements)
         self.device = torch.device(device) if device is not None else discr.device
-        prec = {"fp64": _native.PREC_FP64, "fp32": _native.PREC_FP32}[precision]
-        self.dtype = torch.float64 if precision == "fp64" else torch.float32
+        prec = {"fp64": _native.PREC_FP64, "fp32": _native.PREC_FP32,
+                "bf16x3": _native.PREC_BF16X3, "fp16x3": _native.PREC_FP16X3}[precision]
+        self.dtype = torch.float32 if precision == "fp32" else torch.float64
         self.lib = lib = _native.load()
         ld = discr.ldis
         E = p.elements

@@ -220,7 +220,8 @@ hb_status hb_batch_check(hb_batch* batch, void* stream);
  * this face's node order) and, for the variable-velocity wave, halo_coeff
  * [num_halo_faces * nfp].  Both are device buffers of the caller, refreshed
  * between stages (typically by hb_pack on the owner + a point-to-point
- * exchange).  FP64 / FP32 paths.  Replaces the reference's MPI face-trace
+ * exchange).  All paths except the streamed high-order split kernel (3D,
+ * N >= 6).  Replaces the reference's MPI face-trace
  * exchange (hedge/backends/mpi/__init__.py:184-216, 284-340). */
 hb_status hb_op_set_halo(hb_op* op, const void* halo, const double* halo_coeff);
 
