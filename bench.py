@@ -253,11 +253,21 @@ def cpu_baseline(discr, op, w0, dt, threads=None, F=6):
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
     if rank != 0:
         return
     W = WORKLOADS[args.workload]
     F = W["fields"]
-    hb, mesh, discr, op = build_problem(args.n, args.order, "fp64", workload=args.workload)
+    if world > 1 and args.layout == "partitioned":
+        # the same mesh as our partitioned arm: world x the per-GPU workload
+        import hedge_b200 as hb
+        h = 2.0 / args.n
+        mesh = hb.make_box_tet_mesh(a=(-1, -1, -1), b=(-1 + 2 * world, 1, 1),
+                                    n=(args.n * world, args.n, args.n), jitter=0.05 * h, seed=1)
+        discr = hb.Discretization(mesh, order=args.order)
+        _, _, _, op = build_problem(2, args.order, "fp64", workload=args.workload)
+    else:
+        hb, mesh, discr, op = build_problem(args.n, args.order, "fp64", workload=args.workload)
     w0 = initial_state(discr, args.workload)
     dt = op.estimate_timestep(discr)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -285,8 +295,11 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": W["label"] % (discr.K, args.order), "K": discr.K,
-                   "order": args.order, "fields": F, "step": "one LSRK stage per step"},
+        "config": {"workload": W["label"] % (discr.K // max(world, 1)
+                                             if args.layout == "partitioned" else discr.K,
+                                             args.order),
+                   "K": discr.K, "order": args.order, "fields": F,
+                   "step": "one LSRK stage per step"},
         "cpu_baseline": {"value": v, "unit": "DOF-updates/s", "cores": used,
                          "kind": "port",
                          "sample": "one LSRK stage over the full mesh per step; C++ "
