@@ -8,7 +8,7 @@ graph; since a step's five stages flip the state buffers an odd number of
 times, two graphs are kept (the step starting from buffer 0 or buffer 1).
 
 ``autotune`` picks the tile size (elements per tile) for each (order, field
-count) by timing the candidates on a synthetic member; ``make_c5_members``
+count) by timing the candidates on the ensemble itself; ``make_c5_members``
 builds the ensemble workload (256 2D advection / wave members of K
 log-uniform in [500, 20000], orders 3..6).
 """
@@ -188,39 +188,45 @@ def make_c5_members(n=256, seed=6, ic_seed=7, kmin=500, kmax=20000, orders=(3, 4
     return [_rect_member(int(k), int(o), str(m), ic, device) for k, o, m in zip(ks, ords, kinds)]
 
 
-def autotune(orders=(3, 4, 5, 6), kinds=("advection", "wave"), K=40000, reps=10,
-             budgets=(128, 256, 512, 1024), table=None, device=None):
-    """Tile size per (order, F, dim): for each candidate (elements per tile =
-    budget // Np, budget = nodes per tile) time `reps` stages of a synthetic
-    K-element member and keep the fastest.  Fills and returns `table`."""
+def autotune(members, budgets=(128, 256, 512, 1024), steps=5, passes=1, table=None):
+    """Tile size (elements per tile) per (order, F, dim) for this ensemble:
+    coordinate descent over the keys present, each candidate (budget // Np
+    elements, budget = nodes per tile) timed by `steps` LSRK4 steps of the
+    whole ensemble with CUDA events, the other keys held at their current
+    best.  Fills and returns `table` (default: the module's TILE_TABLE) and
+    the timings {key: {elements: ms per step}}."""
     torch = _torch()
     table = TILE_TABLE if table is None else table
-    rng = np.random.default_rng(1234)
-    results = {}
-    for order in orders:
-        for kind in kinds:
-            m = _rect_member(K, order, kind, rng, device)
-            best, best_t = None, None
-            timings = {}
+    keys = sorted({m.key for m in members})
+    np_of = {m.key: m.discr.Np for m in members}
+    cur = {k: table.get(k, max(1, 256 // np_of[k])) for k in keys}
+    timings = {}
+
+    def measure(tiles):
+        ens = Ensemble(members, tiles=tiles)
+        ens.step(1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ens.step(steps)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    for _ in range(passes):
+        for k in keys:
+            res = {}
             for b in budgets:
-                E = max(1, b // m.discr.Np)
-                ens = Ensemble([m], tiles={m.key: E})
-                ens.step(2)
-                torch.cuda.synchronize()
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record()
-                ens.step(reps)
-                e1.record()
-                torch.cuda.synchronize()
-                t = e0.elapsed_time(e1)
-                timings[E] = t
-                if best_t is None or t < best_t:
-                    best, best_t = E, t
-                del ens
-            table[m.key] = best
-            results[m.key] = timings
-    return table, results
+                E = max(1, b // np_of[k])
+                if E in res:
+                    continue
+                trial = dict(cur)
+                trial[k] = E
+                res[E] = measure(trial)
+            cur[k] = min(res, key=res.get)
+            timings[k] = res
+    table.update(cur)
+    return table, timings
 
 
 def main(argv=None):
@@ -236,12 +242,12 @@ def main(argv=None):
     p.add_argument("--steps", type=int, default=100)
     p.add_argument("--no-autotune", action="store_true")
     a = p.parse_args(argv)
+    members = make_c5_members(a.members)
     t0 = time.perf_counter()
     tuned = None
     if not a.no_autotune:
-        _, tuned = autotune()
+        _, tuned = autotune(members)
     t_tune = time.perf_counter() - t0
-    members = make_c5_members(a.members)
     ens = Ensemble(members)
     info = ens.info()
     ens.step(3)

@@ -80,10 +80,11 @@ def test_ensemble_tile_sizes_do_not_change_results(cuda_device):
 
 def test_autotune_small(cuda_device):
     from hedge_b200.ensemble import autotune
-    table, res = autotune(orders=(3,), kinds=("advection",), K=400, reps=2, table={})
-    ((key, E),) = table.items()
-    assert key == (3, 1, 2)
-    assert E in res[key]
+    ms = _members(9)[:3]
+    table, res = autotune(ms, budgets=(64, 256), steps=1, table={})
+    assert set(table) == {m.key for m in ms}
+    for k, E in table.items():
+        assert E in res[k]
 
 
 def test_ensemble_refuses_unsupported_member(cuda_device):
