@@ -21,6 +21,8 @@ import numpy as np
 from . import _native
 from .facegroups import Boundary, build_compact_connectivity, build_interior_face_group
 from .mesh import Mesh, TAG_ALL, TAG_NONE, check_bc_coverage
+from .lowering import as_descriptor
+from .optemplate import Expr
 from .models import (BC_GIVEN, BC_NONE, MODEL_MAXWELL, MODEL_VARWAVE, MODEL_WAVE,
                      MODEL_ADVECTION, OpTemplate)
 from .refelem import make_element
@@ -293,8 +295,12 @@ class Discretization:
         except Exception:
             pass
 
-    def compile(self, optemplate: OpTemplate, precision=None):
-        return CompiledOperator(self, optemplate, precision or self.precision)
+    def compile(self, optemplate, precision=None):
+        """Compile an operator template (``hedge_b200.optemplate``; lowered
+        by ``hedge_b200.lowering.lower``) or an already lowered
+        :class:`OpTemplate` (discretization/__init__.py:1288-1302)."""
+        return CompiledOperator(self, as_descriptor(optemplate, self.dimensions),
+                                precision or self.precision)
 
 
 class PointEvaluator:
@@ -315,6 +321,7 @@ def build_face_table(discr, ot):
     (neighbour, nbr_face | perm << 2), boundary faces (-1 - b, BC kind) with
     b numbering the BC_GIVEN faces; and the number of given boundary nodes
     and the given tag."""
+    ot = as_descriptor(ot, discr.dimensions)
     mesh = discr.mesh
     model = ot.operator
     if model is not None and hasattr(model, "bc_tags"):
@@ -382,12 +389,30 @@ class CompiledOperator:
         self._lib = lib
         self._coeff = None
         self._source = None
+        names = ot.fields or {}
         if ot.model == MODEL_VARWAVE:
-            self.set_coefficient(model.c if model is not None else 1.0)
-        src = p.get("source", 0) if ot.model == MODEL_WAVE else (
-            getattr(model, "source", 0) if ot.model == MODEL_VARWAVE else 0)
-        if not (np.isscalar(src) and src == 0):
-            self.set_source(src)
+            c = model.c if model is not None else (None if names.get("coeff") else 1.0)
+            if c is not None and not isinstance(c, Expr):
+                self.set_coefficient(c)
+        if names:
+            # lowered from a template: source = sign * (const + coef * field)
+            self._src_spec = (-1.0 if ot.model == MODEL_VARWAVE else 1.0,
+                              float(names.get("source_const", 0.0)), names.get("source"),
+                              float(names.get("source_coef", 0.0)))
+            val = None
+            if self._src_spec[2] is not None and model is not None:
+                val = model.source if ot.model == MODEL_VARWAVE else \
+                    getattr(model, "source_f", None)
+                if isinstance(val, Expr):
+                    val = None
+            src = self._source_from(val)
+            if src is not None:
+                self._source = src
+        else:
+            src = p.get("source", 0) if ot.model == MODEL_WAVE else (
+                getattr(model, "source", 0) if ot.model == MODEL_VARWAVE else 0)
+            if not (np.isscalar(src) and src == 0):
+                self.set_source(src)
 
     @property
     def state_dtype(self):
@@ -405,6 +430,22 @@ class CompiledOperator:
         if t.shape != (len(d),):
             raise ValueError("c must be a volume vector of length %d" % len(d))
         self._coeff = t
+
+    def _source_from(self, value):
+        """Device source vector of a lowered template for the value of its
+        source field (None: the field's value is not known yet)."""
+        sign, const, name, coef = self._src_spec
+        if name is None:
+            if const == 0:
+                return None
+            value, coef = 0.0, 0.0
+        elif value is None:
+            return None
+        torch = _torch()
+        d = self.discr
+        v = torch.full((len(d),), float(value), dtype=torch.float64, device=d.device) \
+            if np.isscalar(value) else d.to_device(value, torch.float64).reshape(-1)
+        return (sign * (const + coef * v)).contiguous()
 
     def set_source(self, s):
         torch = _torch()
@@ -529,11 +570,37 @@ class CompiledOperator:
         return ii, ee
 
     def __call__(self, w=None, t=0.0, bc_in=None, u=None, **kwargs):
+        """Evaluate the RHS.  A compiled template takes its fields by the
+        names it uses (state, given boundary data, coefficient, source),
+        like the reference's compiled templates (``op(w=..., c=...)``)."""
+        names = self.ot.fields or {}
+        coeff = source = None
+        if names.get("state") in kwargs:
+            w = kwargs.pop(names["state"])
+        elif names.get("state_keys") and names["state_keys"][0][0] in kwargs:
+            # state components named one by one
+            w = [kwargs[n] if i is None else kwargs[n][i] for n, i in names["state_keys"]]
+        if names.get("given") in kwargs:
+            bc_in = kwargs.pop(names["given"])
+        if names.get("coeff") in kwargs:
+            coeff = self.discr.to_device(kwargs.pop(names["coeff"]), _torch().float64)
+            coeff = coeff.reshape(-1).contiguous()
+        src_name = names.get("source")
+        if src_name is not None and src_name[0] in kwargs:
+            val = kwargs.pop(src_name[0])
+            if src_name[1] is not None:
+                val = val[src_name[1]]
+            source = self._source_from(val)
         if w is None:
             w = u
+        if self.ot.model == MODEL_VARWAVE and coeff is None and self._coeff is None:
+            raise ValueError("this template needs its coefficient field %r"
+                             % names.get("coeff", "c"))
+        if src_name is not None and source is None and self._source is None:
+            raise ValueError("this template needs its source field %r" % src_name[0])
         q = self.as_state(w)
         out = self.discr.volume_empty((self.F,), self.state_dtype)
-        self.rhs_into(q, out, bc_in=bc_in)
+        self.rhs_into(q, out, bc_in=bc_in, coeff=coeff, source=source)
         return out[0] if self.F == 1 and self.ot.model == MODEL_ADVECTION else out
 
     def bind_model(self, model):

@@ -1,0 +1,643 @@
+"""Lowering of symbolic operator templates onto the fused kernels.
+
+The reference compiles an op template into instructions (diff batches, flux
+batches, vector expressions; hedge/optemplate/tools.py:255-326 and
+hedge/compiler.py:547-1103) and runs them one by one.  Here the kernels are
+fused per model, so compiling a template means recognising which kernel
+model, with which parameters and which boundary condition on each tag, it
+is equal to.  ``lower(template)`` does that in four steps:
+
+1. structure: flux operators appear only inside one inverse mass, the
+   inverse mass holds nothing but fluxes, derivatives act on fields only,
+   and every operator is one the path supports (else ``NotImplementedError``);
+2. roles: the interior flux argument names the state fields (differentiated)
+   and at most one coefficient field (not differentiated, first); fields in
+   boundary data outside ``BoundarizeOperator`` are given boundary data;
+   remaining fields outside the fluxes are sources;
+3. parameters: the template is evaluated pointwise on probe values, with each
+   derivative, interior / exterior value and face normal an independent
+   random number (the inverse mass and the lift act on every flux term
+   alike, so they drop out).  Unit derivative probes give the volume
+   coefficients, from which the model's parameters follow (advection
+   velocity, wave speed, time sign, permittivity and permeability);
+4. verification: the model's own template with those parameters (and each
+   candidate flux type / boundary kind) is evaluated on the same probes, in
+   the volume, on interior faces and on each boundary tag's faces.  The first
+   candidate that agrees everywhere to rounding gives the lowered
+   :class:`~hedge_b200.models.OpTemplate`.
+
+A template that no kernel model reproduces raises ``NotImplementedError``
+naming the part that differs.
+"""
+
+from __future__ import annotations
+
+import numbers
+import zlib
+
+import numpy as np
+
+from . import flux as fl
+from . import optemplate as ot
+from .mesh import TAG_ALL, TAG_NONE
+from .models import (BC_ABSORB, BC_DIRICHLET, BC_GIVEN, BC_NEUMANN, BC_PEC, BC_PMC,
+                     BC_RADIATION, MODEL_ADVECTION, MODEL_MAXWELL, MODEL_VARWAVE,
+                     MODEL_WAVE, MaxwellOperator, OpTemplate, StrongAdvectionOperator,
+                     StrongWaveOperator, VariableVelocityStrongWaveOperator)
+
+PROBES = 16
+TOL = 1e-10
+
+
+def _is_num(x):
+    return isinstance(x, numbers.Number) and not isinstance(x, bool)
+
+
+def _comps(x):
+    if isinstance(x, np.ndarray):
+        return list(x.reshape(-1))
+    if isinstance(x, (list, tuple)):
+        return list(x)
+    return [x]
+
+
+# --------------------------------------------------------------------------
+# structure and roles
+
+class _Scan:
+    """One pass over a template: checks the structure and records the
+    interior flux arguments, boundary pairs and field roles."""
+
+    def __init__(self):
+        self.interior_args = []
+        self.pairs = []
+        self.diff_keys = []
+        self.outside_fields = {}    # fields outside any flux argument
+        self.given_fields = {}      # fields in boundary data, not boundarized
+        self.flux_fields = {}
+
+    def run(self, outs):
+        for x in outs:
+            self._visit(x, in_minv=False, in_flux=False, in_bnd=False)
+
+    def _visit(self, x, in_minv, in_flux, in_bnd, in_bfield=False):
+        if _is_num(x):
+            return
+        if isinstance(x, np.ndarray):
+            for c in x.reshape(-1):
+                self._visit(c, in_minv, in_flux, in_bnd, in_bfield)
+            return
+        if isinstance(x, ot.Field):
+            if in_minv and not in_flux:
+                raise NotImplementedError(
+                    "inverse mass of a volume term (%s): only fluxes are lifted" % x)
+            if in_flux:
+                self.flux_fields[x.key] = x
+                if in_bfield and not in_bnd:
+                    self.given_fields[x.key] = x
+            else:
+                self.outside_fields[x.key] = x
+            return
+        if isinstance(x, (ot.Sum, ot.Product)):
+            for c in x.children:
+                self._visit(c, in_minv, in_flux, in_bnd, in_bfield)
+            return
+        if isinstance(x, ot.Quotient):
+            self._visit(x.num, in_minv, in_flux, in_bnd, in_bfield)
+            self._visit(x.den, in_minv, in_flux, in_bnd, in_bfield)
+            return
+        if isinstance(x, ot.Power):
+            self._visit(x.base, in_minv, in_flux, in_bnd, in_bfield)
+            self._visit(x.exponent, in_minv, in_flux, in_bnd, in_bfield)
+            return
+        if isinstance(x, ot.BoundaryNormalComponent):
+            if not in_bfield:
+                raise NotImplementedError("boundary normal outside boundary data")
+            return
+        if isinstance(x, ot.OperatorBinding):
+            op = x.op
+            if isinstance(op, ot.DifferentiationOperator):
+                if in_flux or in_minv:
+                    raise NotImplementedError("derivative inside a flux or an inverse mass")
+                if not isinstance(x.field, ot.Field):
+                    raise NotImplementedError(
+                        "derivative of an expression (%s): only fields are "
+                        "differentiated on this path" % x.field)
+                self.diff_keys.append(x.field.key)
+                return
+            if isinstance(op, ot.InverseMassOperator):
+                if in_minv or in_flux:
+                    raise NotImplementedError("nested inverse mass")
+                self._visit(x.field, True, False, False)
+                return
+            if isinstance(op, ot.BoundarizeOperator):
+                if not in_bfield:
+                    raise NotImplementedError("boundary restriction outside boundary data")
+                self._visit(x.field, in_minv, in_flux, True, in_bfield)
+                return
+            if isinstance(op, ot.FluxOperator):
+                if not in_minv or in_flux:
+                    raise NotImplementedError(
+                        "flux outside an inverse mass: only the strong-form lift "
+                        "M^-1 (flux) is on this path")
+                arg = x.field
+                if isinstance(arg, ot.BoundaryPair):
+                    if arg.tag is TAG_NONE:
+                        return
+                    self.pairs.append((op, arg))
+                    self._visit(arg.field, in_minv, True, False, False)
+                    self._visit(arg.bfield, in_minv, True, False, True)
+                else:
+                    self.interior_args.append(_comps(arg))
+                    self._visit(arg, in_minv, True, False, False)
+                return
+            raise NotImplementedError("operator %s is not on this path" % op)
+        raise NotImplementedError("template node %r is not on this path" % (x,))
+
+
+# --------------------------------------------------------------------------
+# pointwise evaluation
+
+def _rand(key, lo, hi, n):
+    seed = zlib.crc32(repr(key).encode())
+    return np.random.default_rng(seed).uniform(lo, hi, n)
+
+
+class _Ctx:
+    """Probe values: fields (interior / exterior), derivatives, normals and
+    the face kind evaluated (None: volume terms only; "interior"; or a
+    boundary tag).  ``fixed`` overrides values by key."""
+
+    def __init__(self, dims, face=None, coeff_keys=(), zero_state=False, fixed=None,
+                 deriv=None, P=PROBES, salt=0):
+        self.dims, self.face, self.P, self.salt = dims, face, P, salt
+        self.coeff_keys = set(coeff_keys)
+        self.fixed = fixed or {}
+        self.deriv = deriv
+        self.zero_state = zero_state
+        n = _rand(("normal", salt), -1, 1, dims * P).reshape(dims, P)
+        self.n = n / np.linalg.norm(n, axis=0)
+
+    def val(self, key, interior):
+        if (key, interior) in self.fixed:
+            return self.fixed[(key, interior)]
+        if key in self.fixed:
+            return self.fixed[key]
+        if key in self.coeff_keys:
+            return _rand((key, interior, self.salt), 0.5, 1.5, self.P)
+        if self.zero_state:
+            return np.zeros(self.P)
+        return _rand((key, interior, self.salt), -1, 1, self.P)
+
+    def der(self, key, axis):
+        if self.deriv is not None:
+            return self.deriv(key, axis)
+        return _rand(("d", key, axis, self.salt), -1, 1, self.P)
+
+
+def _ev(x, ctx, interior=True):
+    if _is_num(x):
+        return float(x)
+    if isinstance(x, ot.Field):
+        return ctx.val(x.key, interior)
+    if isinstance(x, ot.Sum):
+        r = 0.0
+        for c in x.children:
+            r = r + _ev(c, ctx, interior)
+        return r
+    if isinstance(x, ot.Product):
+        r = 1.0
+        for c in x.children:
+            r = r * _ev(c, ctx, interior)
+        return r
+    if isinstance(x, ot.Quotient):
+        return _ev(x.num, ctx, interior) / _ev(x.den, ctx, interior)
+    if isinstance(x, ot.Power):
+        return _ev(x.base, ctx, interior) ** _ev(x.exponent, ctx, interior)
+    if isinstance(x, ot.BoundaryNormalComponent):
+        return ctx.n[x.axis]
+    if isinstance(x, ot.OperatorBinding):
+        op = x.op
+        if isinstance(op, ot.DifferentiationOperator):
+            return ctx.der(x.field.key, op.xyz_axis)
+        if isinstance(op, (ot.InverseMassOperator, ot.BoundarizeOperator)):
+            return _ev(x.field, ctx, interior)
+        if isinstance(op, ot.FluxOperator):
+            return _ev_binding(op, x.field, ctx)
+    raise NotImplementedError("cannot evaluate %r" % (x,))
+
+
+def _ev_binding(op, arg, ctx):
+    if isinstance(arg, ot.BoundaryPair):
+        if ctx.face is None or ctx.face == "interior" or arg.tag is TAG_NONE:
+            return 0.0
+        if not (arg.tag is TAG_ALL or arg.tag == ctx.face):
+            return 0.0
+        iv = [_ev(c, ctx, True) for c in _comps(arg.field)]
+        ev = [_ev(c, ctx, True) for c in _comps(arg.bfield)]
+        if len(iv) != len(ev):
+            raise ValueError("boundary pair: %d volume vs %d boundary components"
+                             % (len(iv), len(ev)))
+    else:
+        if ctx.face != "interior":
+            return 0.0
+        iv = [_ev(c, ctx, True) for c in _comps(arg)]
+        ev = [_ev(c, ctx, False) for c in _comps(arg)]
+    return _ev_flux(op.flux, iv, ev, ctx.n)
+
+
+def _ev_flux(x, iv, ev, n):
+    if _is_num(x):
+        return float(x)
+    if isinstance(x, fl.FieldComponent):
+        vals = iv if x.is_interior else ev
+        if not 0 <= x.index < len(vals):
+            raise ValueError("flux refers to component %d of a %d-vector"
+                             % (x.index, len(vals)))
+        v = vals[x.index]
+        return v if not _is_num(v) else np.full(n.shape[1], float(v))
+    if isinstance(x, fl.Normal):
+        return n[x.axis]
+    if isinstance(x, ot.Sum):
+        r = 0.0
+        for c in x.children:
+            r = r + _ev_flux(c, iv, ev, n)
+        return r
+    if isinstance(x, ot.Product):
+        r = 1.0
+        for c in x.children:
+            r = r * _ev_flux(c, iv, ev, n)
+        return r
+    if isinstance(x, ot.Quotient):
+        return _ev_flux(x.num, iv, ev, n) / _ev_flux(x.den, iv, ev, n)
+    if isinstance(x, ot.Power):
+        return _ev_flux(x.base, iv, ev, n) ** _ev_flux(x.exponent, iv, ev, n)
+    if isinstance(x, fl.IfPositive):
+        c = np.broadcast_to(_ev_flux(x.criterion, iv, ev, n), (n.shape[1],))
+        return np.where(c > 0, _ev_flux(x.then, iv, ev, n), _ev_flux(x.else_, iv, ev, n))
+    if isinstance(x, fl.FunctionCall):
+        a = [_ev_flux(y, iv, ev, n) for y in x.args]
+        return {"abs": lambda: np.abs(a[0]), "max": lambda: np.maximum(a[0], a[1]),
+                "min": lambda: np.minimum(a[0], a[1])}[x.name]()
+    raise NotImplementedError("flux term %s is not on this path" % (x,))
+
+
+def evaluate(outs, ctx):
+    """Outputs of a template at the probes of ``ctx``: [n_outputs, P]."""
+    return np.stack([np.broadcast_to(np.asarray(_ev(x, ctx), dtype=np.float64), (ctx.P,))
+                     for x in outs])
+
+
+def _close(a, b):
+    return np.max(np.abs(a - b)) <= TOL * (1.0 + np.max(np.abs(a)))
+
+
+# --------------------------------------------------------------------------
+# kernel models
+
+class _Roles:
+    def __init__(self, state, coeff, given, source):
+        self.state = state          # object array of the state Fields
+        self.coeff = coeff          # Field or None
+        self.given = given          # Field or None
+        self.source = source        # expression of the user's source (or 0)
+
+    def names(self):
+        st = self.state
+        names = {st[0].name} if all(f.name == st[0].name for f in st) else None
+        d = {"state": st[0].name if names else None,
+             "state_keys": [f.key for f in st]}
+        if self.coeff is not None:
+            d["coeff"] = self.coeff.name
+        if self.given is not None:
+            d["given"] = self.given.name
+        return d
+
+
+class _Family:
+    model = None
+    kinds = ()
+
+    def applies(self, dims, F, ncoeff):
+        return False
+
+    def volume_params(self, V):
+        return None
+
+    def flux_choices(self, user, roles, params, dims):
+        return []
+
+    def bdry_choices(self, user, roles, params, dims, tag, kind):
+        return [None]
+
+    def build(self, roles, params, bc):
+        raise NotImplementedError
+
+
+class _Advection(_Family):
+    model = MODEL_ADVECTION
+    kinds = (BC_GIVEN,)
+
+    def applies(self, dims, F, ncoeff):
+        return F == 1 and ncoeff == 0
+
+    def volume_params(self, V):
+        return {"v": -V[0, 0, :]}
+
+    def flux_choices(self, user, roles, params, dims):
+        return [dict(params, flux_type=t) for t in ("central", "upwind", "lf")]
+
+    def build(self, roles, p, bc):
+        tag = bc[0] if bc is not None else TAG_NONE
+        m = StrongAdvectionOperator(p["v"], inflow_tag=tag, flux_type=p["flux_type"])
+        if bc is not None and roles.given is None:
+            return None
+        return m, _comps(m.op_template(u=roles.state[0],
+                                       bc_in=roles.given if roles.given is not None
+                                       else ot.Field("bc_in")))
+
+
+class _Wave(_Family):
+    model = MODEL_WAVE
+    kinds = (BC_DIRICHLET, BC_NEUMANN, BC_RADIATION)
+
+    def applies(self, dims, F, ncoeff):
+        return F == dims + 1 and ncoeff == 0
+
+    def volume_params(self, V):
+        c = V[0, 1, 0]
+        return {"c": c} if c != 0 else None
+
+    def flux_choices(self, user, roles, params, dims):
+        return [dict(params, flux_type=t) for t in ("upwind", "central")]
+
+    def _tags(self, bc):
+        t = {BC_DIRICHLET: TAG_NONE, BC_NEUMANN: TAG_NONE, BC_RADIATION: TAG_NONE}
+        if bc is not None:
+            t[bc[1]] = bc[0]
+        return dict(dirichlet_tag=t[BC_DIRICHLET], neumann_tag=t[BC_NEUMANN],
+                    radiation_tag=t[BC_RADIATION])
+
+    def build(self, roles, p, bc):
+        dims = len(roles.state) - 1
+        m = StrongWaveOperator(p["c"], dims, source_f=0, flux_type=p["flux_type"],
+                               **self._tags(bc))
+        m.source_f = roles.source
+        return m, _comps(m.op_template(w=roles.state))
+
+
+class _VarWave(_Wave):
+    model = MODEL_VARWAVE
+
+    def applies(self, dims, F, ncoeff):
+        return F == dims + 1 and ncoeff == 1
+
+    def volume_params(self, V):
+        ts = V[0, 1, 0]      # time_sign * c with the coefficient probed at 1
+        return {"time_sign": ts} if ts != 0 else None
+
+    def build(self, roles, p, bc):
+        dims = len(roles.state) - 1
+        m = VariableVelocityStrongWaveOperator(
+            roles.coeff, dims, source=0, flux_type=p["flux_type"],
+            time_sign=p["time_sign"], **self._tags(bc))
+        m.source = -1 * roles.source if not ot.is_zero(roles.source) else 0
+        return m, _comps(m.op_template(w=roles.state))
+
+
+class _Maxwell(_Family):
+    model = MODEL_MAXWELL
+    kinds = (BC_PEC, BC_PMC, BC_ABSORB)
+
+    def applies(self, dims, F, ncoeff):
+        return dims == 3 and F == 6 and ncoeff == 0
+
+    def volume_params(self, V):
+        a, b = V[0, 5, 1], V[3, 2, 1]
+        if a <= 0 or b >= 0:
+            return None
+        return {"eps": 1.0 / a, "mu": -1.0 / b}
+
+    def _fit(self, user, roles, p, ctx, key, bc):
+        """Numeric flux types enter affinely: fit from the templates at 0, 1."""
+        ys = []
+        for alpha in (0.0, 1.0):
+            q = dict(p, **{key: alpha})
+            ys.append(evaluate(self.build(roles, q, bc)[1], ctx))
+        y = evaluate(user, ctx)
+        dy = ys[1] - ys[0]
+        den = float(np.sum(dy * dy))
+        return float(np.sum((y - ys[0]) * dy) / den) if den > 0 else 0.0
+
+    def flux_choices(self, user, roles, params, dims):
+        ctx = _Ctx(dims, face="interior")
+        alpha = self._fit(user, roles, dict(params, bdry_flux_type=0.0), ctx, "flux_type",
+                          None)
+        return [dict(params, flux_type="lf", bdry_flux_type="lf"),
+                dict(params, flux_type=alpha, bdry_flux_type=alpha)]
+
+    def bdry_choices(self, user, roles, params, dims, tag, kind):
+        ctx = _Ctx(dims, face=tag)
+        return ["lf", self._fit(user, roles, params, ctx, "bdry_flux_type", (tag, kind))]
+
+    def build(self, roles, p, bc):
+        t = {BC_PEC: TAG_NONE, BC_PMC: TAG_NONE, BC_ABSORB: TAG_NONE}
+        if bc is not None:
+            t[bc[1]] = bc[0]
+        m = MaxwellOperator(p["eps"], p["mu"], p["flux_type"],
+                            bdry_flux_type=p.get("bdry_flux_type", p["flux_type"]),
+                            pec_tag=t[BC_PEC], pmc_tag=t[BC_PMC],
+                            absorb_tag=t[BC_ABSORB])
+        return m, _comps(m.op_template(w=roles.state))
+
+
+_FAMILIES = (_Advection(), _Wave(), _VarWave(), _Maxwell())
+
+
+# --------------------------------------------------------------------------
+
+def _source(user, roles_keys, src_fields, dims):
+    """The template's source: output values with the state, derivatives and
+    fluxes at zero, as const + sum coef_k * field_k on output 0."""
+    zero = {k: np.zeros(PROBES) for k in roles_keys}
+
+    def at(fixed):
+        ctx = _Ctx(dims, face=None, fixed={**zero, **fixed},
+                   deriv=lambda k, a: np.zeros(PROBES))
+        return evaluate(user, ctx)
+
+    allzero = {k: np.zeros(PROBES) for k in src_fields}
+    base = at(allzero)
+    const = base[0, 0]
+    expr = const if const != 0 else 0
+    terms = []
+    for k, f in src_fields.items():
+        one = at({**allzero, k: np.ones(PROBES)})
+        coef = one[0, 0] - const
+        if coef != 0:
+            expr = expr + coef * f
+            terms.append((f.name, f.index, coef))
+    if np.any(base[1:] != 0) or np.any(base[0] != const):
+        raise NotImplementedError("source terms on fields other than the first")
+    return expr, const, terms
+
+
+def lower(template, dimensions):
+    """The :class:`~hedge_b200.models.OpTemplate` a symbolic template equals
+    (see the module docstring); raises ``NotImplementedError`` when no
+    kernel model reproduces it."""
+    outs = _comps(template)
+    F = len(outs)
+    scan = _Scan()
+    scan.run(outs)
+    if not scan.interior_args:
+        raise NotImplementedError("template has no interior flux")
+    arg = scan.interior_args[0]
+    for a in scan.interior_args[1:]:
+        if [getattr(x, "key", x) for x in a] != [getattr(x, "key", x) for x in arg]:
+            raise NotImplementedError("interior fluxes of different arguments")
+    if not all(isinstance(x, ot.Field) for x in arg):
+        raise NotImplementedError("flux argument components must be fields")
+    diff = set(scan.diff_keys)
+    state = [x for x in arg if x.key in diff]
+    coeff = [x for x in arg if x.key not in diff]
+    if len(coeff) > 1 or (coeff and arg[0] is not coeff[0]):
+        raise NotImplementedError("at most one coefficient field, first in the flux argument")
+    if len(state) != F:
+        raise NotImplementedError("%d outputs but %d differentiated state fields in the "
+                                  "flux argument" % (F, len(state)))
+    st_keys = {x.key for x in state}
+    co_keys = {x.key for x in coeff}
+    given = [f for k, f in scan.given_fields.items() if k not in st_keys | co_keys]
+    if len(given) > 1:
+        raise NotImplementedError("more than one given boundary field")
+    src_fields = {k: f for k, f in scan.outside_fields.items()
+                  if k not in st_keys | co_keys and k not in diff}
+    roles_keys = st_keys | co_keys | {f.key for f in given}
+    src_expr, src_const, src_terms = _source(outs, roles_keys, src_fields, dimensions)
+    if len(src_terms) > 1:
+        raise NotImplementedError("more than one source field")
+    state_arr = ot.join_fields(state)
+    roles = _Roles(state_arr, coeff[0] if coeff else None, given[0] if given else None,
+                   src_expr)
+
+    # volume coefficients V[f, g, x]: unit derivative probes less the
+    # zero-derivative value (the constant source), coefficient fields = 1
+    keys = [x.key for x in state]
+    fixed = {k: np.zeros(PROBES) for k in st_keys}
+    fixed.update({k: np.ones(PROBES) for k in co_keys})
+    fixed.update({k: np.zeros(PROBES) for k in src_fields})
+    V0 = evaluate(outs, _Ctx(dimensions, face=None, fixed=fixed,
+                             deriv=lambda k, a: np.zeros(PROBES)))[:, 0]
+    V = np.zeros((F, F, dimensions))
+    for g, kg in enumerate(keys):
+        for x in range(dimensions):
+            def der(k, a, kg=kg, x=x):
+                return np.full(PROBES, 1.0 if (k == kg and a == x) else 0.0)
+            ctx = _Ctx(dimensions, face=None, fixed=fixed, deriv=der)
+            V[:, g, x] = evaluate(outs, ctx)[:, 0] - V0
+
+    tags = []
+    for _, pair in scan.pairs:
+        if not any(pair.tag is t or pair.tag == t for t in tags):
+            tags.append(pair.tag)
+    if len(tags) > 1 and any(t is TAG_ALL for t in tags):
+        raise NotImplementedError("TAG_ALL together with other boundary tags")
+
+    # the reason reported is the one from the furthest stage reached
+    why = [0, "no kernel model has %d fields in %dD" % (F, dimensions)]
+
+    def fail(stage, msg):
+        if stage >= why[0]:
+            why[:] = [stage, msg]
+    for fam in _FAMILIES:
+        if not fam.applies(dimensions, F, len(coeff)):
+            continue
+        params = fam.volume_params(V)
+        if params is None:
+            fail(1, "volume terms match no kernel model")
+            continue
+        vol_ctx = _Ctx(dimensions, face=None, coeff_keys=co_keys)
+        int_ctx = _Ctx(dimensions, face="interior", coeff_keys=co_keys)
+        y_vol, y_int = evaluate(outs, vol_ctx), evaluate(outs, int_ctx)
+        for choice in fam.flux_choices(outs, roles, params, dimensions):
+            built = fam.build(roles, choice, None)
+            if built is None:
+                continue
+            canon = built[1]
+            if not _close(y_vol, evaluate(canon, vol_ctx)):
+                fail(1, "volume terms differ from the %s kernel's" % type(fam).__name__[1:])
+                break
+            if not _close(y_int, evaluate(canon, int_ctx)):
+                fail(2, "interior flux matches no flux type of the %s kernel"
+                     % type(fam).__name__[1:])
+                continue
+            bcs, bft = [], None
+            ok = True
+            for tag in tags:
+                b_ctx = _Ctx(dimensions, face=tag, coeff_keys=co_keys)
+                y_b = evaluate(outs, b_ctx)
+                hit = None
+                for kind in fam.kinds:
+                    for bchoice in fam.bdry_choices(outs, roles, choice, dimensions, tag, kind):
+                        q = dict(choice) if bchoice is None else dict(choice, bdry_flux_type=bchoice)
+                        b = fam.build(roles, q, (tag, kind))
+                        if b is not None and _close(y_b, evaluate(b[1], b_ctx)):
+                            hit = (kind, bchoice)
+                            break
+                    if hit:
+                        break
+                if hit is None:
+                    fail(3, "boundary %s: no boundary condition of the %s kernel matches" % (
+                        getattr(tag, "__name__", tag), type(fam).__name__[1:]))
+                    ok = False
+                    break
+                if hit[1] is not None:
+                    if bft is not None and not _same_ft(bft, hit[1]):
+                        fail(3, "boundary fluxes of different flux types")
+                        ok = False
+                        break
+                    bft = hit[1]
+                bcs.append((tag, hit[0]))
+            if not ok:
+                continue
+            final = dict(choice)
+            if bft is not None:
+                final["bdry_flux_type"] = bft
+            model = fam.build(roles, final, None)[0]
+            desc = model.descriptor()
+            names = roles.names()
+            if src_terms:
+                names["source"] = src_terms[0][:2]
+                names["source_coef"] = src_terms[0][2]
+            names["source_const"] = src_const
+            return OpTemplate(desc.model, desc.dimensions, desc.n_fields, desc.flux_type,
+                              _lowered_params(desc, src_const), bcs, None, names)
+    raise NotImplementedError("op template is not one the B200 kernels implement: " + why[1])
+
+
+def as_descriptor(template, dimensions):
+    """A lowered :class:`OpTemplate` for a template or an OpTemplate (the
+    model that made the template, if any, attached as its operator)."""
+    if isinstance(template, OpTemplate):
+        return template
+    from .models import template_model
+    desc = lower(template, dimensions)
+    desc.operator = template_model(template)
+    return desc
+
+
+def _same_ft(a, b):
+    if isinstance(a, str) or isinstance(b, str):
+        return a == b
+    return abs(a - b) <= 1e-9
+
+
+def _lowered_params(desc, src_const):
+    p = dict(desc.params)
+    if "source" in p:
+        p["source"] = src_const
+    return p
+
+
+__all__ = ["lower", "as_descriptor", "evaluate", "PROBES"]

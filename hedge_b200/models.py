@@ -1,9 +1,11 @@
 """Hyperbolic DG operators: advection, wave, variable-velocity wave, Maxwell.
 
-Constructor signatures and ``bind(discr) -> rhs(t, w)`` mirror the
-reference's models.  pymbolic (the reference's op-template language) is not
-available, so ``op_template()`` returns an :class:`OpTemplate` descriptor of
-the same right-hand side instead of a symbolic tree:
+Constructor signatures, ``op_template()`` and ``bind(discr) -> rhs(t, w)``
+mirror the reference's models.  ``op_template()`` builds the reference's
+symbolic template in this package's template language
+(``hedge_b200.optemplate`` / ``hedge_b200.flux``); ``Discretization.compile``
+lowers any such template onto the fused kernels.  ``descriptor()`` gives the
+lowered form (:class:`OpTemplate`) directly:
 
 * StrongAdvectionOperator  hedge/models/advection.py:124-149
   rhs = -v.grad u + M^-1 (flux(u) + flux(BoundaryPair(u, bc_in, inflow)))
@@ -17,11 +19,14 @@ the same right-hand side instead of a symbolic tree:
 
 from __future__ import annotations
 
+import weakref
 from dataclasses import dataclass, field
 from math import sqrt
 
 import numpy as np
 
+from . import flux as fl
+from . import optemplate as ot
 from .mesh import TAG_ALL, TAG_NONE, check_bc_coverage
 
 # model ids shared with the C-ABI (include/hedge_b200.h)
@@ -43,7 +48,10 @@ BC_ABSORB = 7      # Maxwell: first-order absorbing
 
 @dataclass
 class OpTemplate:
-    """Typed description of a model's right-hand side."""
+    """Lowered right-hand side: the kernel model, its parameters and the
+    boundary kind of each tag.  ``fields`` names the template's volume
+    fields when it was lowered from a symbolic template (state, given
+    boundary data, coefficient, source)."""
 
     model: int
     dimensions: int
@@ -52,10 +60,30 @@ class OpTemplate:
     params: dict
     bcs: list                 # [(tag, bc_kind)], disjoint tags
     operator: object = field(repr=False, default=None)
+    fields: dict = field(default_factory=dict)
 
     @property
     def n_flux_args(self):
         return self.n_fields + (1 if self.model == MODEL_VARWAVE else 0)
+
+
+# templates made by a model's op_template(): id -> (weak reference, model),
+# so that compiling one binds the model's data (variable c, source vectors)
+_ORIGIN = {}
+
+
+def _remember(model, tree):
+    key = id(tree)
+    ref = weakref.ref(tree, lambda r, k=key: _ORIGIN.pop(k, None))
+    _ORIGIN[key] = (ref, model)
+    return tree
+
+
+def template_model(tree):
+    """The model whose op_template() made ``tree`` (None for a template
+    built by hand)."""
+    e = _ORIGIN.get(id(tree))
+    return e[1] if e is not None and e[0]() is tree else None
 
 
 class HyperbolicOperator:
@@ -70,6 +98,9 @@ class HyperbolicOperator:
                 * discr.dt_geometric_factor())
 
     def bind(self, discr):
+        """hedge/models/*.py bind(): coverage check, then the compiled
+        template with this model's data (boundary values, c, sources)."""
+        check_bc_coverage(discr.mesh, self.bc_tags())
         return discr.compile(self.op_template()).bind_model(self)
 
 
@@ -119,7 +150,35 @@ class StrongAdvectionOperator(HyperbolicOperator):
     def max_eigenvalue(self, t=None, fields=None, discr=None):
         return float(np.linalg.norm(self.v))
 
-    def op_template(self):
+    def weak_flux(self):
+        """advection.py:58-80"""
+        u = fl.FluxScalarPlaceholder(0)
+        normal = fl.make_normal(self.dimensions)
+        nv = np.dot(normal, self.v)
+        if self.flux_type == "central":
+            return u.avg * nv
+        if self.flux_type == "lf":
+            return u.avg * nv + 0.5 * float(np.linalg.norm(self.v)) * (u.int - u.ext)
+        return nv * fl.IfPositive(nv, u.int, u.ext)
+
+    def flux(self):
+        """advection.py:125-131"""
+        u = fl.FluxScalarPlaceholder(0)
+        normal = fl.make_normal(self.dimensions)
+        return u.int * np.dot(normal, self.v) - self.weak_flux()
+
+    def op_template(self, u=None, bc_in=None):
+        """advection.py:133-149"""
+        u = ot.Field("u") if u is None else u
+        bc_in = ot.Field("bc_in") if bc_in is None else bc_in
+        nabla = ot.make_nabla(self.dimensions)
+        m_inv = ot.InverseMassOperator()
+        flux_op = ot.get_flux_operator(self.flux())
+        return _remember(self, -np.dot(self.v, nabla * u)
+                         + m_inv(flux_op(u) + flux_op(ot.BoundaryPair(u, bc_in,
+                                                                      self.inflow_tag))))
+
+    def descriptor(self):
         return OpTemplate(MODEL_ADVECTION, self.dimensions, 1,
                           self.flux_types.index(self.flux_type),
                           {"v": self.v.copy()},
@@ -154,7 +213,43 @@ class StrongWaveOperator(HyperbolicOperator):
     def max_eigenvalue(self, t=None, fields=None, discr=None):
         return abs(self.c)
 
-    def op_template(self):
+    def flux(self):
+        """wave.py:80-108"""
+        dim = self.dimensions
+        w = fl.FluxVectorPlaceholder(1 + dim)
+        u, v = w[0], w[1:]
+        normal = fl.make_normal(dim)
+        flux_weak = ot.join_fields(np.dot(v.avg, normal), u.avg * normal)
+        if self.flux_type == "upwind":
+            flux_weak = flux_weak - self.sign * ot.join_fields(
+                0.5 * (u.int - u.ext), 0.5 * (normal * np.dot(normal, v.int - v.ext)))
+        flux_strong = ot.join_fields(np.dot(v.int, normal), u.int * normal) - flux_weak
+        return -self.c * flux_strong
+
+    def op_template(self, w=None):
+        """wave.py:110-180"""
+        d = self.dimensions
+        w = ot.make_sym_vector("w", d + 1) if w is None else w
+        u, v = w[0], w[1:]
+        B = ot.BoundarizeOperator
+        dir_bc = ot.join_fields(-(B(self.dirichlet_tag) * u), B(self.dirichlet_tag) * v)
+        neu_bc = ot.join_fields(B(self.neumann_tag) * u, -(B(self.neumann_tag) * v))
+        rn = ot.normal(self.radiation_tag, d)
+        rad_u, rad_v = B(self.radiation_tag) * u, B(self.radiation_tag) * v
+        rad_bc = ot.join_fields(0.5 * (rad_u - self.sign * np.dot(rn, rad_v)),
+                                0.5 * rn * (np.dot(rn, rad_v) - self.sign * rad_u))
+        nabla = ot.make_nabla(d)
+        flux_op = ot.get_flux_operator(self.flux())
+        result = (-ot.join_fields(-self.c * np.dot(nabla, v), -self.c * (nabla * u))
+                  + ot.InverseMassOperator() * (
+                      flux_op(w)
+                      + flux_op(ot.BoundaryPair(w, dir_bc, self.dirichlet_tag))
+                      + flux_op(ot.BoundaryPair(w, neu_bc, self.neumann_tag))
+                      + flux_op(ot.BoundaryPair(w, rad_bc, self.radiation_tag))))
+        result[0] = result[0] + _template_value(self.source_f, "source")
+        return _remember(self, result)
+
+    def descriptor(self):
         return OpTemplate(MODEL_WAVE, self.dimensions, self.dimensions + 1,
                           1 if self.flux_type == "upwind" else 0,
                           {"c": self.c, "source": self.source_f},
@@ -190,7 +285,50 @@ class VariableVelocityStrongWaveOperator(HyperbolicOperator):
     def max_eigenvalue(self, t=None, fields=None, discr=None):
         return float(np.max(np.abs(np.asarray(_to_numpy(self.c)))))
 
-    def op_template(self):
+    def flux(self):
+        """wave.py:246-273"""
+        dim = self.dimensions
+        w = fl.FluxVectorPlaceholder(2 + dim)
+        c, u, v = w[0], w[1], w[2:]
+        normal = fl.make_normal(dim)
+        flux = self.time_sign * 0.5 * ot.join_fields(
+            c.ext * np.dot(v.ext, normal) - c.int * np.dot(v.int, normal),
+            normal * (c.ext * u.ext - c.int * u.int))
+        if self.flux_type == "upwind":
+            flux = flux + ot.join_fields(
+                c.ext * u.ext - c.int * u.int,
+                c.ext * normal * np.dot(normal, v.ext) - c.int * normal * np.dot(normal, v.int))
+        return flux
+
+    def op_template(self, w=None):
+        """wave.py:287-395 without artificial diffusion; a numeric or array
+        ``c`` (``source``) enters as the field "c" ("source")."""
+        d = self.dimensions
+        w = ot.make_sym_vector("w", d + 1) if w is None else w
+        u, v = w[0], w[1:]
+        c = _template_value(self.c, "c")
+        flux_w = ot.join_fields(c, w)
+        B = ot.BoundarizeOperator
+        dt_, nt_, rt_ = self.dirichlet_tag, self.neumann_tag, self.radiation_tag
+        dir_bc = ot.join_fields(B(dt_) * c, -(B(dt_) * u), B(dt_) * v)
+        neu_bc = ot.join_fields(B(nt_) * c, B(nt_) * u, -(B(nt_) * v))
+        rn = ot.normal(rt_, d)
+        rad_u, rad_v = B(rt_) * u, B(rt_) * v
+        rad_bc = ot.join_fields(B(rt_) * c,
+                                0.5 * (rad_u - self.time_sign * np.dot(rn, rad_v)),
+                                0.5 * rn * (np.dot(rn, rad_v) - self.time_sign * rad_u))
+        nabla = ot.make_nabla(d)
+        flux_op = ot.get_flux_operator(self.flux())
+        src = _template_value(self.source, "source")
+        return _remember(self, -ot.join_fields(-self.time_sign * c * np.dot(nabla, v) + src,
+                                               -self.time_sign * c * (nabla * u))
+                         + ot.InverseMassOperator() * (
+                             flux_op(flux_w)
+                             + flux_op(ot.BoundaryPair(flux_w, dir_bc, dt_))
+                             + flux_op(ot.BoundaryPair(flux_w, neu_bc, nt_))
+                             + flux_op(ot.BoundaryPair(flux_w, rad_bc, rt_))))
+
+    def descriptor(self):
         return OpTemplate(MODEL_VARWAVE, self.dimensions, self.dimensions + 1,
                           1 if self.flux_type == "upwind" else 0,
                           {"time_sign": float(self.time_sign)},
@@ -215,6 +353,8 @@ class MaxwellOperator(HyperbolicOperator):
             raise NotImplementedError("only fixed material")
         if current != 0:
             raise NotImplementedError("source currents are not on this path")
+        if incident_tag is not TAG_NONE:
+            raise NotImplementedError("incident boundary data is not on this path")
         self.epsilon, self.mu = float(epsilon), float(mu)
         self.flux_type = flux_type
         self.bdry_flux_type = flux_type if bdry_flux_type is None else bdry_flux_type
@@ -231,7 +371,52 @@ class MaxwellOperator(HyperbolicOperator):
     def max_eigenvalue(self, t=None, fields=None, discr=None):
         return 1 / sqrt(self.epsilon * self.mu)
 
-    def op_template(self):
+    def flux(self, flux_type):
+        """em.py:118-190, fixed material"""
+        normal = fl.make_normal(3)
+        w = fl.FluxVectorPlaceholder(6)
+        e, h = w[0:3], w[3:6]
+        epsilon = fl.FluxConstantPlaceholder(self.epsilon)
+        mu = fl.FluxConstantPlaceholder(self.mu)
+        Z_int = (mu.int / epsilon.int) ** 0.5
+        Y_int = 1 / Z_int
+        Z_ext = (mu.ext / epsilon.ext) ** 0.5
+        Y_ext = 1 / Z_ext
+        de, dh = e.int - e.ext, h.int - h.ext
+        if flux_type == "lf":
+            return ot.join_fields(0.5 * -ot.cross(normal, dh), 0.5 * ot.cross(normal, de))
+        return ot.join_fields(
+            -1 / (Z_int + Z_ext) * ot.cross(normal, Z_ext * dh - flux_type * ot.cross(normal, de)),
+            1 / (Y_int + Y_ext) * ot.cross(normal, Y_ext * de + flux_type * ot.cross(normal, dh)))
+
+    def local_derivatives(self, w):
+        """em.py:192-214: (current - curl H, curl E)"""
+        e, h = w[0:3], w[3:6]
+        nabla = ot.make_nabla(3)
+        return ot.join_fields(-ot.cross(nabla, h), ot.cross(nabla, e))
+
+    def op_template(self, w=None):
+        """em.py:226-371, fixed material"""
+        w = ot.make_sym_vector("w", 6) if w is None else w
+        e, h = w[0:3], w[3:6]
+        B = ot.BoundarizeOperator
+        pec = ot.join_fields(-(B(self.pec_tag) * e), B(self.pec_tag) * h)
+        pmc = ot.join_fields(B(self.pmc_tag) * e, -(B(self.pmc_tag) * h))
+        an = ot.normal(self.absorb_tag, 3)
+        Z = (self.mu / self.epsilon) ** 0.5
+        ae, ah = B(self.absorb_tag) * e, B(self.absorb_tag) * h
+        absorb = ot.join_fields(
+            ae + 0.5 * (ot.cross(an, ot.cross(an, ae)) - Z * ot.cross(an, ah)),
+            ah + 0.5 * (ot.cross(an, ot.cross(an, ah)) + (1 / Z) * ot.cross(an, ae)))
+        flux_op = ot.get_flux_operator(self.flux(self.flux_type))
+        bdry_flux_op = ot.get_flux_operator(self.flux(self.bdry_flux_type))
+        divisor = np.array([self.epsilon] * 3 + [self.mu] * 3)
+        bdry = sum(bdry_flux_op(ot.BoundaryPair(w, bc, tag)) for tag, bc in
+                   [(self.pec_tag, pec), (self.pmc_tag, pmc), (self.absorb_tag, absorb)])
+        return _remember(self, (-self.local_derivatives(w)
+                                + ot.InverseMassOperator()(flux_op(w) + bdry)) / divisor)
+
+    def descriptor(self):
         def code(ft):
             return (1, 0.0) if ft == "lf" else (0, float(ft))
         ft, alpha = code(self.flux_type)
@@ -247,6 +432,16 @@ class MaxwellOperator(HyperbolicOperator):
         return [self.pec_tag, self.absorb_tag, self.incident_tag]
 
 
+def _template_value(x, name):
+    """A model datum as a template term: expressions and numbers as they
+    are, volume vectors as the field ``name`` (bound when the model binds)."""
+    if isinstance(x, ot.Expr):
+        return x
+    if np.isscalar(x):
+        return float(x) if x != 0 else 0
+    return ot.Field(name)
+
+
 def _to_numpy(x):
     try:
         import torch
@@ -257,7 +452,7 @@ def _to_numpy(x):
     return x
 
 
-__all__ = ["StrongAdvectionOperator", "StrongWaveOperator",
+__all__ = ["template_model", "StrongAdvectionOperator", "StrongWaveOperator",
            "VariableVelocityStrongWaveOperator", "MaxwellOperator",
            "OpTemplate", "make_tdep_constant", "TimeConstantGivenFunction",
            "TimeDependentGivenFunction",

@@ -30,6 +30,7 @@ import numpy as np
 
 from . import _native
 from .discretization import build_face_table, op_descriptor
+from .lowering import as_descriptor
 from .models import MODEL_VARWAVE
 
 
@@ -78,6 +79,7 @@ class PartPlan:
 
 class PartitionPlan:
     def __init__(self, discr, ot, nparts, owner=None):
+        ot = as_descriptor(ot, discr.dimensions)
         conn, n_given, _ = build_face_table(discr, ot)
         if n_given:
             raise NotImplementedError("partitions with given boundary data")
@@ -186,7 +188,7 @@ class PartitionedOperator:
 
     def __init__(self, discr, model, plan, rank, precision="fp64", device=None, exchange=None):
         torch = _torch()
-        ot = model.op_template()
+        ot = as_descriptor(model.op_template(), discr.dimensions)
         self.ot, self.plan, self.rank = ot, plan, rank
         self.part = p = plan.parts[rank]
         self.F = ot.n_fields

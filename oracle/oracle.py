@@ -112,8 +112,9 @@ class OracleRHS:
     read: reference matrices, geometry, face groups, boundaries)."""
 
     def __init__(self, discr, optemplate, c_field=None, source=None):
+        from hedge_b200.lowering import as_descriptor
         self.discr = discr
-        self.ot = ot = optemplate
+        self.ot = ot = as_descriptor(optemplate, discr.dimensions)
         ld = discr.ldis
         self.dim = discr.dimensions
         self.K, self.Np = discr.K, discr.Np

@@ -45,7 +45,7 @@ def _check_adjoint(d, op, bc_in=None, c_field=None, source=None, seed=0):
     comp = d.compile(ot, precision="fp64")
     if c_field is not None:
         comp.set_coefficient(c_field)
-    F = ot.n_fields
+    F = op.descriptor().n_fields
     orc = OracleRHS(d, ot, c_field=c_field, source=source)
     orc.F = F
     n = F * len(d)

@@ -29,7 +29,7 @@ def _check(discr, op, precision, seed=0, bc_in=None, c_field=None, source=None):
         comp.set_coefficient(c_field)
     if source is not None:
         comp.set_source(source)
-    q = _fields(discr, ot.n_fields, seed)
+    q = _fields(discr, op.descriptor().n_fields, seed)
     orc = OracleRHS(discr, ot, c_field=c_field, source=source)
     ref = orc(q, bc_in=bc_in)
     qs = q.astype(np.float32).astype(np.float64) if precision == "fp32" else q
@@ -179,10 +179,10 @@ def test_fused_lsrk_matches_oracle(cuda_device, model):
         op = hb.MaxwellOperator(1.0, 1.0, flux_type=1)
     ot = op.op_template()
     rhs = op.bind(d)
-    q = _fields(d, ot.n_fields, 9)
+    q = _fields(d, op.descriptor().n_fields, 9)
     dt = op.estimate_timestep(d) * 0.5
     stepper = hb.LSRK4TimeStepper()
-    y = d.to_device(q).reshape(ot.n_fields, -1)
+    y = d.to_device(q).reshape(op.descriptor().n_fields, -1)
     orc = OracleRHS(d, ot)
     yo, res = q.copy(), np.zeros_like(q)
     t = 0.0

@@ -31,7 +31,7 @@ def _setup(kind, nparts, precision):
 def test_partitioned_rhs_equals_global(cuda_device, kind, precision):
     import torch
     d, model, plan, parts, ex = _setup(kind, 3, precision)
-    F = model.op_template().n_fields
+    F = model.descriptor().n_fields
     q = np.random.default_rng(1).standard_normal((F, len(d)))
     comp = d.compile(model.op_template(), precision=precision)
     if kind == "varwave":
@@ -90,7 +90,7 @@ def test_halo_op_refusals(cuda_device):
     p = PartitionedOperator(d, model, plan, 0)
     part = plan.parts[0]
     # an operator with halo faces refuses to run before it has a halo buffer
-    od = op_descriptor(model.op_template(), _native.PREC_FP64, part.conn, 0, part.n_halo_faces)
+    od = op_descriptor(model.descriptor(), _native.PREC_FP64, part.conn, 0, part.n_halo_faces)
     h = C.c_void_p()
     assert lib.hb_op_create(p._dh, C.byref(od), C.byref(h)) == _native.HB_OK
     q = torch.zeros((3, p.K * p.Np), dtype=torch.float64, device=p.device)
@@ -99,6 +99,6 @@ def test_halo_op_refusals(cuda_device):
     assert st == _native.HB_ERR_INVALID_ARGUMENT
     lib.hb_op_destroy(h)
     # halo slots beyond num_halo_faces are refused at creation
-    od = op_descriptor(model.op_template(), _native.PREC_FP64, part.conn, 0,
+    od = op_descriptor(model.descriptor(), _native.PREC_FP64, part.conn, 0,
                        max(part.n_halo_faces - 1, 0))
     assert lib.hb_op_create(p._dh, C.byref(od), C.byref(h)) == _native.HB_ERR_INVALID_ARGUMENT

@@ -26,7 +26,7 @@ def _split_err(discr, op, seed=0, bc_in=None, c_field=None, precision="bf16x3"):
     comp = discr.compile(ot, precision=precision)
     if c_field is not None:
         comp.set_coefficient(c_field)
-    q = _fields(discr, ot.n_fields, seed)
+    q = _fields(discr, op.descriptor().n_fields, seed)
     ref = OracleRHS(discr, ot, c_field=c_field)(q, bc_in=bc_in)
     got = comp(w=q, bc_in=bc_in)
     comp.check()

@@ -1,0 +1,336 @@
+"""Operator templates (CPU): the models' symbolic templates, their lowering
+onto the kernel models, and hand-written templates.
+
+* every model template lowers to the model's own descriptor;
+* the CPU template executor (oracle/optemplate_exec.py), which evaluates a
+  tree node by node like the reference's jit executor, agrees with the C
+  oracle on the model templates (rel-L2 <= 1e-12) -- this pins the
+  templates to the reference formulas the oracle restates;
+* hand-written templates (other field names, rearranged algebra, per-tag
+  boundary conditions) lower to the right kernel model, and the oracle run
+  on the lowered descriptor agrees with the executor run on the tree -- this
+  pins the lowering;
+* templates outside the path raise NotImplementedError.
+"""
+import numpy as np
+import pytest
+
+import hedge_b200 as hb
+from hedge_b200 import flux as fl
+from hedge_b200 import optemplate as ot
+from hedge_b200.lowering import lower
+from hedge_b200.mesh import TAG_ALL, TAG_NONE
+from hedge_b200.models import (BC_ABSORB, BC_DIRICHLET, BC_GIVEN, BC_NEUMANN, BC_PEC,
+                               BC_PMC, BC_RADIATION, MODEL_ADVECTION, MODEL_MAXWELL,
+                               MODEL_VARWAVE, MODEL_WAVE)
+
+from conftest import rel_l2
+
+
+def rect(n=6, periodic=False, jitter=0.02, seed=0, tagger=None):
+    kw = {"boundary_tagger": tagger} if tagger else {}
+    return hb.make_regular_rect_mesh((-1, -1), (1, 1), (n, n),
+                                     periodicity=(periodic, periodic) if periodic else None,
+                                     jitter=jitter, seed=seed, **kw)
+
+
+def box(n=2, jitter=0.03, seed=1, tagger=None):
+    kw = {"boundary_tagger": tagger} if tagger else {}
+    return hb.make_box_tet_mesh(n=(n, n, n), jitter=jitter, seed=seed, **kw)
+
+
+def _fields(d, F, seed):
+    rng = np.random.default_rng(seed)
+    x = d.nodes
+    return np.stack([np.sin(1.1 * (f + 1) * x[:, 0] + 0.4 * f) * np.cos(0.8 * x[:, -1])
+                     + 0.1 * rng.uniform(-1, 1, len(d)) for f in range(F)])
+
+
+def _same_descriptor(a, b):
+    assert a.model == b.model and a.n_fields == b.n_fields and a.flux_type == b.flux_type
+    for k, v in b.params.items():
+        if k == "source":
+            continue
+        assert np.allclose(a.params[k], v, rtol=1e-12, atol=1e-12), (k, a.params[k], v)
+    keep = {(t, k) for t, k in b.bcs if t is not TAG_NONE and k != 0}
+    assert set(a.bcs) <= {(t, k) for t, k in b.bcs}
+    # every tag the model gives a flux-carrying condition appears
+    assert {t for t, k in keep} <= {t for t, _ in a.bcs} | {
+        t for t, k in keep if k == BC_GIVEN and t is TAG_NONE}
+
+
+def _tagger_lr(names):
+    def tagger(fvi, el, fn, allv):
+        x = allv[list(fvi)].mean(0)
+        if x[0] < -0.99:
+            return [names[0]]
+        if x[0] > 0.99:
+            return [names[1]]
+        return [names[2]]
+    return tagger
+
+
+MODELS = [
+    lambda: hb.StrongAdvectionOperator(np.array([1.0, 0.5]), flux_type="upwind"),
+    lambda: hb.StrongAdvectionOperator(np.array([0.6, -0.8]), flux_type="central",
+                                       inflow_tag=TAG_ALL),
+    lambda: hb.StrongAdvectionOperator(np.array([0.3, 0.2, -0.4]), flux_type="lf"),
+    lambda: hb.StrongWaveOperator(-0.7, 2, flux_type="upwind"),
+    lambda: hb.StrongWaveOperator(1.0, 2, flux_type="central", dirichlet_tag="dir",
+                                  neumann_tag="neu", radiation_tag="rad", source_f=0.25),
+    lambda: hb.StrongWaveOperator(1.3, 3),
+    lambda: hb.VariableVelocityStrongWaveOperator(np.ones(3), 2, time_sign=-1,
+                                                  radiation_tag="rad", dirichlet_tag="dir"),
+    lambda: hb.MaxwellOperator(1.0, 1.0, flux_type=1),
+    lambda: hb.MaxwellOperator(2.0, 0.5, flux_type=0.5, bdry_flux_type="lf",
+                               pec_tag="pec", pmc_tag="pmc", absorb_tag="abs"),
+]
+
+
+@pytest.mark.parametrize("make", MODELS)
+def test_model_templates_lower_to_their_descriptors(make):
+    m = make()
+    _same_descriptor(lower(m.op_template(), m.dimensions), m.descriptor())
+
+
+def _executor_vs_oracle(d, template, desc, env, q, bc_in=None, c_field=None, source=None):
+    from oracle import OracleRHS
+    from optemplate_exec import TemplateExecutor
+    got = TemplateExecutor(d)(template, **env)
+    ref = OracleRHS(d, desc, c_field=c_field, source=source)(q, bc_in=bc_in)
+    assert got.shape == ref.shape
+    return rel_l2(got, ref)
+
+
+CASES = ["adv_periodic", "adv_inflow", "wave_mixed", "wave3d", "varwave", "maxwell_pec",
+         "maxwell_mixed"]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_model_templates_match_oracle(case):
+    """The model templates, executed as trees, equal the C oracle's RHS."""
+    bc = c = src = None
+    if case == "adv_periodic":
+        d = hb.Discretization(rect(6, True, 0.0), order=3)
+        op = hb.StrongAdvectionOperator(np.array([1.0, 0.5]), flux_type="upwind")
+    elif case == "adv_inflow":
+        d = hb.Discretization(rect(5, tagger=lambda *a: ["inflow"]), order=3)
+        op = hb.StrongAdvectionOperator(np.array([0.6, -0.8]), flux_type="lf",
+                                        inflow_tag="inflow")
+        bc = np.sin(3 * d.get_boundary("inflow").nodes[:, 0])
+    elif case == "wave_mixed":
+        d = hb.Discretization(rect(5, tagger=_tagger_lr(["neu", "rad", "dir"])), order=3)
+        op = hb.StrongWaveOperator(-0.8, 2, dirichlet_tag="dir", neumann_tag="neu",
+                                   radiation_tag="rad", source_f=0.3)
+    elif case == "wave3d":
+        d = hb.Discretization(box(2), order=2)
+        op = hb.StrongWaveOperator(1.0, 3, flux_type="central")
+    elif case == "varwave":
+        d = hb.Discretization(rect(5, tagger=_tagger_lr(["dir", "rad", "dir"])), order=3)
+        rng = np.random.default_rng(4)
+        c = np.repeat(rng.uniform(0.8, 1.2, d.K), d.Np)
+        src = np.exp(-4 * (d.nodes ** 2).sum(1))
+        op = hb.VariableVelocityStrongWaveOperator(c, 2, source=src, dirichlet_tag="dir",
+                                                   radiation_tag="rad", time_sign=-1)
+    elif case == "maxwell_pec":
+        d = hb.Discretization(box(2), order=2)
+        op = hb.MaxwellOperator(1.0, 1.0, flux_type=1)
+    else:
+        def tagger(fvi, el, fn, allv):
+            x = allv[list(fvi)].mean(0)
+            return ["abs"] if x[2] > 0.99 else (["pmc"] if x[2] < -0.99 else ["pec"])
+        d = hb.Discretization(box(2, tagger=tagger), order=2)
+        op = hb.MaxwellOperator(2.0, 0.5, flux_type=0.5, bdry_flux_type="lf",
+                                pec_tag="pec", pmc_tag="pmc", absorb_tag="abs")
+    desc = op.descriptor()
+    q = _fields(d, desc.n_fields, 3)
+    if desc.model == MODEL_ADVECTION:
+        env = {"u": q[0], "bc_in": bc if bc is not None else 0.0}
+    else:
+        env = {"w": q}
+    if c is not None:
+        env["c"] = c
+    if src is not None:
+        env["source"] = src
+    err = _executor_vs_oracle(d, op.op_template(), desc, env, q, bc_in=bc, c_field=c,
+                              source=src)
+    assert err <= 1e-12, err
+
+
+# --------------------------------------------------------------------------
+# hand-written templates
+
+def advection_by_hand(v, tag):
+    """Upwind advection written out: field 'phi', inflow data 'g'."""
+    phi, g = ot.Field("phi"), ot.Field("g")
+    u = fl.FluxScalarPlaceholder(0)
+    n = fl.make_normal(len(v))
+    nv = n[0] * v[0] + n[1] * v[1]
+    flux = nv * (u.int - fl.IfPositive(nv, u.int, u.ext))
+    F = ot.FluxOperator(flux)
+    grad = [ot.DifferentiationOperator(i)(phi) for i in range(2)]
+    return -(v[0] * grad[0] + v[1] * grad[1]) + ot.InverseMassOperator()(
+        F(phi) + F(ot.BoundaryPair(phi, g, tag)))
+
+
+def wave_by_hand(c, tags):
+    """2D wave with separately named fields (p, vx, vy), central flux,
+    Dirichlet on tags[0] and Neumann on tags[1]."""
+    p, vx, vy = ot.Field("p"), ot.Field("vx"), ot.Field("vy")
+    w = ot.join_fields(p, vx, vy)
+    W = fl.FluxVectorPlaceholder(3)
+    n = fl.make_normal(2)
+    # c * (jump terms) of the central strong-form flux, written per component
+    fu = -c * 0.5 * ((W[1].int - W[1].ext) * n[0] + (W[2].int - W[2].ext) * n[1])
+    fv = [-c * 0.5 * (W[0].int - W[0].ext) * n[i] for i in range(2)]
+    Fop = ot.get_flux_operator(ot.join_fields(fu, fv[0], fv[1]))
+    B0, B1 = ot.BoundarizeOperator(tags[0]), ot.BoundarizeOperator(tags[1])
+    dir_bc = ot.join_fields(-B0(p), B0(vx), B0(vy))
+    neu_bc = ot.join_fields(B1(p), -B1(vx), -B1(vy))
+    D = ot.make_nabla(2)
+    vol = ot.join_fields(c * (D[0](vx) + D[1](vy)), c * D[0](p), c * D[1](p))
+    return vol + ot.InverseMassOperator()(
+        Fop(w) + Fop(ot.BoundaryPair(w, dir_bc, tags[0]))
+        + Fop(ot.BoundaryPair(w, neu_bc, tags[1])))
+
+
+def varwave_by_hand():
+    """Variable-speed wave with coefficient 'speed' and source 2*f."""
+    w = ot.make_sym_vector("q", 3)
+    speed = ot.Field("speed")
+    m = hb.VariableVelocityStrongWaveOperator(speed, 2, flux_type="upwind",
+                                              source=2 * ot.Field("f"))
+    return m.op_template(w=w)
+
+
+def maxwell_by_hand(alpha):
+    """Maxwell with eps = mu = 1 written with explicit curls, PEC walls."""
+    w = ot.make_sym_vector("em", 6)
+    e, h = w[:3], w[3:]
+    D = ot.make_nabla(3)
+    curl = ot.cross
+    W = fl.FluxVectorPlaceholder(6)
+    n = fl.make_normal(3)
+    de = W[0:3].int - W[0:3].ext
+    dh = W[3:6].int - W[3:6].ext
+    fe = -0.5 * curl(n, dh - alpha * curl(n, de))
+    fh = 0.5 * curl(n, de + alpha * curl(n, dh))
+    Fop = ot.get_flux_operator(ot.join_fields(fe, fh))
+    B = ot.BoundarizeOperator(TAG_ALL)
+    pec = ot.join_fields(-B(e), B(h))
+    return ot.join_fields(curl(D, h), -curl(D, e)) + ot.InverseMassOperator()(
+        Fop(w) + Fop(ot.BoundaryPair(w, pec, TAG_ALL)))
+
+
+def test_hand_written_advection():
+    d = hb.Discretization(rect(5, tagger=lambda *a: ["in"]), order=3)
+    tpl = advection_by_hand(np.array([0.7, -0.4]), "in")
+    desc = lower(tpl, 2)
+    assert desc.model == MODEL_ADVECTION and desc.flux_type == 1
+    assert np.allclose(desc.params["v"], [0.7, -0.4]) and desc.bcs == [("in", BC_GIVEN)]
+    assert desc.fields["state"] == "phi" and desc.fields["given"] == "g"
+    q = _fields(d, 1, 5)
+    bc = np.cos(2 * d.get_boundary("in").nodes[:, 1])
+    err = _executor_vs_oracle(d, tpl, desc, {"phi": q[0], "g": bc}, q, bc_in=bc)
+    assert err <= 1e-12, err
+
+
+def test_hand_written_wave_named_fields():
+    d = hb.Discretization(rect(5, tagger=_tagger_lr(["neu", "dir", "dir"])), order=3)
+    tpl = wave_by_hand(1.2, ("dir", "neu"))
+    desc = lower(tpl, 2)
+    assert desc.model == MODEL_WAVE and desc.flux_type == 0
+    assert np.isclose(desc.params["c"], 1.2)
+    assert set(desc.bcs) == {("dir", BC_DIRICHLET), ("neu", BC_NEUMANN)}
+    assert desc.fields["state_keys"] == [("p", None), ("vx", None), ("vy", None)]
+    q = _fields(d, 3, 6)
+    err = _executor_vs_oracle(d, tpl, desc, {"p": q[0], "vx": q[1], "vy": q[2]}, q)
+    assert err <= 1e-12, err
+
+
+def test_hand_written_varwave_source():
+    d = hb.Discretization(rect(5), order=3)
+    desc = lower(varwave_by_hand(), 2)
+    assert desc.model == MODEL_VARWAVE and desc.fields["coeff"] == "speed"
+    # the template's output 0 carries -2 f (the model subtracts its source)
+    assert desc.fields["source"] == ("f", None) and desc.fields["source_coef"] == -2.0
+    rng = np.random.default_rng(2)
+    c = np.repeat(rng.uniform(0.8, 1.2, d.K), d.Np)
+    f = np.sin(d.nodes[:, 0])
+    q = _fields(d, 3, 7)
+    err = _executor_vs_oracle(d, varwave_by_hand(), desc,
+                              {"q": q, "speed": c, "f": f}, q, c_field=c, source=2 * f)
+    assert err <= 1e-12, err
+
+
+@pytest.mark.parametrize("alpha", [1.0, 0.25])
+def test_hand_written_maxwell(alpha):
+    d = hb.Discretization(box(2), order=2)
+    tpl = maxwell_by_hand(alpha)
+    desc = lower(tpl, 3)
+    assert desc.model == MODEL_MAXWELL and desc.flux_type == 0
+    assert np.isclose(desc.params["alpha"], alpha) and np.isclose(desc.params["bdry_alpha"], alpha)
+    assert desc.bcs == [(TAG_ALL, BC_PEC)]
+    q = _fields(d, 6, 8)
+    err = _executor_vs_oracle(d, tpl, desc, {"em": q}, q)
+    assert err <= 1e-12, err
+
+
+def test_per_tag_conditions_beyond_one_tag_per_kind():
+    """Two Dirichlet tags and a radiation tag (the model class has one tag
+    per kind; the lowered table has any number)."""
+    w = ot.make_sym_vector("w", 3)
+    parts = []
+    for tag in ("a", "b"):
+        m = hb.StrongWaveOperator(1.0, 2, dirichlet_tag=tag)
+        parts.append(m.op_template(w=w))
+    m = hb.StrongWaveOperator(1.0, 2, dirichlet_tag=TAG_NONE, radiation_tag="r")
+    bare = hb.StrongWaveOperator(1.0, 2, dirichlet_tag=TAG_NONE).op_template(w=w)
+    # interior and volume terms once, boundary terms of the three templates
+    tpl = m.op_template(w=w) + (parts[0] - bare) + (parts[1] - bare)
+    desc = lower(tpl, 2)
+    assert set(desc.bcs) == {("a", BC_DIRICHLET), ("b", BC_DIRICHLET), ("r", BC_RADIATION)}
+
+
+def test_nonmodel_templates_raise():
+    u = ot.Field("u")
+    U = fl.FluxScalarPlaceholder(0)
+    n = fl.make_normal(2)
+    D = ot.make_nabla(2)
+    central = ot.FluxOperator(0.5 * (U.int - U.ext) * n[0])
+    M = ot.InverseMassOperator()
+    bad = {
+        "mass operator": -D[0](u) + ot.MassOperator()(u),
+        "flux outside the inverse mass": -D[0](u) + central(u),
+        "derivative of a product": -D[0](2 * u * u) + M(central(u)),
+        "nonlinear flux": -D[0](u) + M(ot.FluxOperator(U.int * U.ext * n[0])(u)),
+        "penalty term": -D[0](u) + M(ot.FluxOperator(fl.PenaltyTerm() * (U.int - U.ext))(u)),
+        "volume term under the inverse mass": M(D[0](u) + central(u)),
+        "nonlinear volume term": -D[0](u) * u + M(central(u)),
+        "extrapolation boundary": -D[0](u) + M(central(u) + central(
+            ot.BoundaryPair(u, ot.BoundarizeOperator("out")(u), "out"))),
+    }
+    for what, tpl in bad.items():
+        with pytest.raises(NotImplementedError):
+            lower(tpl, 2)
+            pytest.fail(what)
+
+
+def test_wrong_wave_boundary_raises():
+    w = ot.make_sym_vector("w", 3)
+    m = hb.StrongWaveOperator(1.0, 2, dirichlet_tag=TAG_NONE)
+    tpl = m.op_template(w=w)
+    Fop = ot.get_flux_operator(m.flux())
+    B = ot.BoundarizeOperator("x")
+    tpl = tpl + ot.InverseMassOperator()(Fop(ot.BoundaryPair(w, 2.0 * B(w), "x")))
+    with pytest.raises(NotImplementedError, match="boundary"):
+        lower(tpl, 2)
+
+
+def test_template_arithmetic_prunes_zeros():
+    u = ot.Field("u")
+    assert ot.is_zero(0 * u) and (0 + u) is u and (u * 1) is u
+    D = ot.make_nabla(2)
+    e = np.dot(np.array([0.0, 2.0]), D * u)
+    assert isinstance(e, ot.OperatorBinding) or isinstance(e, ot.Product)
+    assert "d/dx0" not in str(e)

@@ -47,7 +47,7 @@ def test_plan_consistent(dim, nparts):
     from hedge_b200.discretization import build_face_table
     gconn, _, _ = build_face_table(d, op.op_template())
     rng = np.random.default_rng(0)
-    F = op.op_template().n_fields
+    F = op.descriptor().n_fields
     q = rng.standard_normal((F, len(d)))
     for r, p in enumerate(plan.parts):
         Kr = len(p.elements)
@@ -105,7 +105,7 @@ def _gloo_worker(rank, world, port, result_path):
         d, op = _discr(2)
         plan = PartitionPlan(d, op.op_template(), world)
         p = plan.parts[rank]
-        F = op.op_template().n_fields
+        F = op.descriptor().n_fields
         q = np.random.default_rng(7).standard_normal((F, len(d)))
         nodes = (p.elements[:, None] * d.Np + np.arange(d.Np)).reshape(-1)
         ql = q[:, nodes]
