@@ -14,6 +14,8 @@ from .models import (StrongAdvectionOperator, StrongWaveOperator,
                      TimeDependentGivenFunction)
 from .discretization import Discretization, CompiledOperator, BoundRHS
 from .timestep import LSRK4TimeStepper, RK4TimeStepper
+from .nd_calculus import GradientOperator, DivergenceOperator
+from .visualization import VtkVisualizer, LegacyVtkVisualizer
 
 __all__ = [
     "Mesh", "TAG_ALL", "TAG_NONE", "make_regular_rect_mesh", "make_box_tet_mesh",
@@ -21,5 +23,6 @@ __all__ = [
     "StrongAdvectionOperator", "StrongWaveOperator",
     "VariableVelocityStrongWaveOperator", "MaxwellOperator", "make_tdep_constant",
     "TimeConstantGivenFunction", "TimeDependentGivenFunction", "Discretization", "CompiledOperator", "BoundRHS",
-    "LSRK4TimeStepper", "RK4TimeStepper",
+    "LSRK4TimeStepper", "RK4TimeStepper", "GradientOperator", "DivergenceOperator",
+    "VtkVisualizer", "LegacyVtkVisualizer",
 ]

@@ -368,6 +368,20 @@ class MaxwellOperator(HyperbolicOperator):
     def c(self):
         return 1 / sqrt(self.mu * self.epsilon)
 
+    def get_eh_subset(self):
+        """em.py: which of (Ex, Ey, Ez, Hx, Hy, Hz) the operator carries."""
+        return (True,) * 6
+
+    def split_eh(self, w):
+        """(E, H) of a field vector [6, ...]."""
+        return w[0:3], w[3:6]
+
+    def assemble_eh(self, e, h):
+        import torch
+        if isinstance(e, torch.Tensor):
+            return torch.cat([e.reshape(3, -1), h.reshape(3, -1)])
+        return np.concatenate([np.asarray(e).reshape(3, -1), np.asarray(h).reshape(3, -1)])
+
     def max_eigenvalue(self, t=None, fields=None, discr=None):
         return 1 / sqrt(self.epsilon * self.mu)
 

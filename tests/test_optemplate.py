@@ -334,3 +334,31 @@ def test_template_arithmetic_prunes_zeros():
     e = np.dot(np.array([0.0, 2.0]), D * u)
     assert isinstance(e, ot.OperatorBinding) or isinstance(e, ot.Product)
     assert "d/dx0" not in str(e)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_nd_calculus_templates_equal_wave_pieces(dim):
+    """The DG gradient (divergence) template equals the v-part (u-part) of
+    the central-flux wave template with c = 1 and Neumann (Dirichlet) walls,
+    which is how nd_calculus evaluates them."""
+    from optemplate_exec import TemplateExecutor
+    d = hb.Discretization(rect(5) if dim == 2 else box(2), order=3)
+    ex = TemplateExecutor(d)
+    b = d.get_boundary(TAG_ALL).vol_indices
+    x = d.nodes
+    u = np.sin(x[:, 0]) * np.cos(x[:, 1]) + x[:, -1] ** 3
+    w = np.zeros((dim + 1, len(d)))
+    w[0] = u
+    g = ex(hb.GradientOperator(dim).op_template(), u=u, bc=u[b])
+    wave_n = hb.StrongWaveOperator(1.0, dim, flux_type="central", dirichlet_tag=TAG_NONE,
+                                   neumann_tag=TAG_ALL)
+    assert rel_l2(g, ex(wave_n.op_template(), w=w)[1:]) <= 1e-14
+    v = np.stack([np.cos(x[:, k]) * x[:, (k + 1) % dim] for k in range(dim)])
+    w = np.zeros((dim + 1, len(d)))
+    w[1:] = v
+    dv = ex(hb.DivergenceOperator(dim).op_template(), v=v, bc=v[:, b])
+    wave_d = hb.StrongWaveOperator(1.0, dim, flux_type="central", dirichlet_tag=TAG_ALL)
+    assert rel_l2(dv[0], ex(wave_d.op_template(), w=w)[0]) <= 1e-13
+    # linear fields are differentiated exactly
+    gx = ex(hb.GradientOperator(dim).op_template(), u=x[:, 0], bc=x[b, 0])
+    assert np.abs(gx[0] - 1).max() < 1e-12 and np.abs(gx[1:]).max() < 1e-12
