@@ -8,7 +8,7 @@ right-hand-side evaluation and LSRK stage runs in hand-written CUDA kernels
 from .mesh import (Mesh, TAG_ALL, TAG_NONE, make_regular_rect_mesh,
                    make_box_tet_mesh, check_bc_coverage)
 from .refelem import TriangleElement, TetrahedronElement, make_element
-from .models import (StrongAdvectionOperator, StrongWaveOperator,
+from .models import (StrongAdvectionOperator, WeakAdvectionOperator, StrongWaveOperator,
                      VariableVelocityStrongWaveOperator, MaxwellOperator,
                      make_tdep_constant, TimeConstantGivenFunction,
                      TimeDependentGivenFunction)
@@ -20,7 +20,7 @@ from .visualization import VtkVisualizer, LegacyVtkVisualizer
 __all__ = [
     "Mesh", "TAG_ALL", "TAG_NONE", "make_regular_rect_mesh", "make_box_tet_mesh",
     "check_bc_coverage", "TriangleElement", "TetrahedronElement", "make_element",
-    "StrongAdvectionOperator", "StrongWaveOperator",
+    "StrongAdvectionOperator", "WeakAdvectionOperator", "StrongWaveOperator",
     "VariableVelocityStrongWaveOperator", "MaxwellOperator", "make_tdep_constant",
     "TimeConstantGivenFunction", "TimeDependentGivenFunction", "Discretization", "CompiledOperator", "BoundRHS",
     "LSRK4TimeStepper", "RK4TimeStepper", "GradientOperator", "DivergenceOperator",

@@ -299,7 +299,7 @@ class Discretization:
         """Compile an operator template (``hedge_b200.optemplate``; lowered
         by ``hedge_b200.lowering.lower``) or an already lowered
         :class:`OpTemplate` (discretization/__init__.py:1288-1302)."""
-        return CompiledOperator(self, as_descriptor(optemplate, self.dimensions),
+        return CompiledOperator(self, as_descriptor(optemplate, self.dimensions, self.mesh),
                                 precision or self.precision)
 
 
@@ -321,7 +321,7 @@ def build_face_table(discr, ot):
     (neighbour, nbr_face | perm << 2), boundary faces (-1 - b, BC kind) with
     b numbering the BC_GIVEN faces; and the number of given boundary nodes
     and the given tag."""
-    ot = as_descriptor(ot, discr.dimensions)
+    ot = as_descriptor(ot, discr.dimensions, discr.mesh)
     mesh = discr.mesh
     model = ot.operator
     if model is not None and hasattr(model, "bc_tags"):

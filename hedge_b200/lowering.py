@@ -26,6 +26,19 @@ is equal to.  ``lower(template)`` does that in four steps:
    candidate that agrees everywhere to rounding gives the lowered
    :class:`~hedge_b200.models.OpTemplate`.
 
+Two rewrites come first.  Weak-form derivatives: inside the inverse mass,
+``S_x^T f`` (the weak derivative, int f d(phi)/dx) becomes
+``-M D_x f + int_faces n_x f.int phi``, so that ``M^-1 S_x^T f`` is
+``-D_x f + M^-1 (flux n_x f.int on every face)``.  That is summation by
+parts, which the nodal mass, stiffness and face-mass matrices satisfy
+exactly on affine simplices, so weak-form templates (the reference's
+WeakAdvectionOperator) run on the strong-form kernels.  Over-integration:
+the quadrature up-samplers and the quadrature stiffness operator are
+dropped when every integrand they feed is a polynomial of degree <= 2N
+(state fields with constant coefficients, flux coefficients constant per
+face), which the nodal operators integrate exactly; a template with a
+coefficient field under a quadrature operator is refused.
+
 A template that no kernel model reproduces raises ``NotImplementedError``
 naming the part that differs.
 """
@@ -40,7 +53,7 @@ import numpy as np
 from . import flux as fl
 from . import optemplate as ot
 from .mesh import TAG_ALL, TAG_NONE
-from .models import (BC_ABSORB, BC_DIRICHLET, BC_GIVEN, BC_NEUMANN, BC_PEC, BC_PMC,
+from .models import (BC_ABSORB, BC_DIRICHLET, BC_GIVEN, BC_NEUMANN, BC_NONE, BC_PEC, BC_PMC,
                      BC_RADIATION, MODEL_ADVECTION, MODEL_MAXWELL, MODEL_VARWAVE,
                      MODEL_WAVE, MaxwellOperator, OpTemplate, StrongAdvectionOperator,
                      StrongWaveOperator, VariableVelocityStrongWaveOperator)
@@ -153,6 +166,146 @@ class _Scan:
                 return
             raise NotImplementedError("operator %s is not on this path" % op)
         raise NotImplementedError("template node %r is not on this path" % (x,))
+
+
+# --------------------------------------------------------------------------
+# rewrites: over-integration and weak-form derivatives
+
+_QUAD_SAMPLERS = (ot.QuadratureGridUpsampler, ot.QuadratureInteriorFacesGridUpsampler,
+                  ot.QuadratureBoundaryGridUpsampler)
+
+
+def _rebuild(x, f):
+    """Copy of a template with ``f`` applied bottom-up to every node."""
+    if isinstance(x, np.ndarray):
+        out = np.empty(x.shape, dtype=object)
+        for i in np.ndindex(x.shape):
+            out[i] = _rebuild(x[i], f)
+        return out
+    if isinstance(x, ot.Sum):
+        r = 0
+        for c in x.children:
+            r = ot.add(r, _rebuild(c, f))
+        return f(r)
+    if isinstance(x, ot.Product):
+        r = 1
+        for c in x.children:
+            r = ot.mul(r, _rebuild(c, f))
+        return f(r)
+    if isinstance(x, ot.Quotient):
+        return f(ot.div(_rebuild(x.num, f), _rebuild(x.den, f)))
+    if isinstance(x, ot.Power):
+        return f(ot.power(_rebuild(x.base, f), _rebuild(x.exponent, f)))
+    if isinstance(x, ot.BoundaryPair):
+        return ot.BoundaryPair(_rebuild(x.field, f), _rebuild(x.bfield, f), x.tag)
+    if isinstance(x, ot.OperatorBinding):
+        return f(ot.OperatorBinding(x.op, _rebuild(x.field, f)))
+    return f(x)
+
+
+def _linear_terms(x):
+    """x as [(number, node)] with x = sum number * node, nodes free of
+    top-level sums and numeric factors; None if x is not of that form."""
+    if _is_num(x):
+        return None if x != 0 else []
+    if isinstance(x, ot.Sum):
+        out = []
+        for c in x.children:
+            t = _linear_terms(c)
+            if t is None:
+                return None
+            out.extend(t)
+        return out
+    if isinstance(x, ot.Product):
+        coef, rest = 1.0, []
+        for c in x.children:
+            if _is_num(c):
+                coef *= c
+            else:
+                rest.append(c)
+        if len(rest) != 1:
+            return None
+        t = _linear_terms(rest[0])
+        return None if t is None else [(coef * c, n) for c, n in t]
+    if isinstance(x, ot.Quotient) and _is_num(x.den):
+        t = _linear_terms(x.num)
+        return None if t is None else [(c / x.den, n) for c, n in t]
+    return [(1.0, x)]
+
+
+def _linear_in_fields(x):
+    """Linear combination of fields (possibly restricted to a boundary)
+    with numeric coefficients."""
+    if isinstance(x, np.ndarray):
+        return all(_linear_in_fields(c) for c in x.reshape(-1))
+    t = _linear_terms(x)
+    if t is None:
+        return False
+    for _, n in t:
+        if isinstance(n, ot.Field):
+            continue
+        if isinstance(n, ot.OperatorBinding) and isinstance(
+                n.op, (ot.BoundarizeOperator,) + _QUAD_SAMPLERS) and _linear_in_fields(n.field):
+            continue
+        return False
+    return True
+
+
+class _Rewrites:
+    def __init__(self):
+        self.quadrature = False
+        self.weak = False
+
+    def run(self, outs):
+        outs = [_rebuild(x, self._strip_quadrature) for x in outs]
+        return [_rebuild(x, self._weak_to_strong) for x in outs]
+
+    def _strip_quadrature(self, node):
+        if not isinstance(node, ot.OperatorBinding):
+            return node
+        op = node.op
+        if isinstance(op, _QUAD_SAMPLERS):
+            if not _linear_in_fields(node.field):
+                raise NotImplementedError(
+                    "over-integration of %s: only fields with constant coefficients are "
+                    "integrated exactly without quadrature on this path" % (node.field,))
+            self.quadrature = True
+            return node.field
+        if isinstance(op, ot.QuadratureStiffnessTOperator):
+            if not _linear_in_fields(node.field):
+                raise NotImplementedError("quadrature stiffness of a non-linear integrand")
+            self.quadrature = True
+            return ot.OperatorBinding(ot.StiffnessTOperator(op.xyz_axis), node.field)
+        return node
+
+    def _weak_to_strong(self, node):
+        if not (isinstance(node, ot.OperatorBinding)
+                and isinstance(node.op, ot.InverseMassOperator)):
+            return node
+        terms = _linear_terms(node.field) if not isinstance(node.field, np.ndarray) else None
+        if terms is None or not any(
+                isinstance(n, ot.OperatorBinding) and isinstance(n.op, ot.StiffnessTOperator)
+                for _, n in terms):
+            return node
+        self.weak = True
+        vol, rest = 0, 0
+        U = fl.FluxScalarPlaceholder(0)
+        for c, n in terms:
+            if not (isinstance(n, ot.OperatorBinding)
+                    and isinstance(n.op, ot.StiffnessTOperator)):
+                rest = ot.add(rest, ot.mul(c, n))
+                continue
+            x = n.op.xyz_axis
+            inner = _linear_terms(n.field)
+            if inner is None or not all(isinstance(g, ot.Field) for _, g in inner):
+                raise NotImplementedError("weak derivative of %s: only of fields" % (n.field,))
+            face = ot.FluxOperator(fl.Normal(x) * U.int)
+            for cf, g in inner:
+                vol = ot.add(vol, ot.mul(-c * cf, ot.DifferentiationOperator(x)(g)))
+                both = ot.add(face(g), face(ot.BoundaryPair(
+                    g, ot.BoundarizeOperator(TAG_ALL)(g), TAG_ALL)))
+                rest = ot.add(rest, ot.mul(c * cf, both))
+        return ot.add(vol, ot.InverseMassOperator()(rest))
 
 
 # --------------------------------------------------------------------------
@@ -482,11 +635,14 @@ def _source(user, roles_keys, src_fields, dims):
     return expr, const, terms
 
 
-def lower(template, dimensions):
+def lower(template, dimensions, mesh=None):
     """The :class:`~hedge_b200.models.OpTemplate` a symbolic template equals
     (see the module docstring); raises ``NotImplementedError`` when no
-    kernel model reproduces it."""
-    outs = _comps(template)
+    kernel model reproduces it.  With ``mesh``, boundary faces that carry
+    none of the template's specific tags are known to exist or not (else a
+    TAG_ALL-only boundary condition must match too)."""
+    rw = _Rewrites()
+    outs = rw.run(_comps(template))
     F = len(outs)
     scan = _Scan()
     scan.run(outs)
@@ -537,12 +693,20 @@ def lower(template, dimensions):
             ctx = _Ctx(dimensions, face=None, fixed=fixed, deriv=der)
             V[:, g, x] = evaluate(outs, ctx)[:, 0] - V0
 
+    if rw.quadrature and coeff:
+        raise NotImplementedError("over-integration with a coefficient field")
     tags = []
     for _, pair in scan.pairs:
         if not any(pair.tag is t or pair.tag == t for t in tags):
             tags.append(pair.tag)
-    if len(tags) > 1 and any(t is TAG_ALL for t in tags):
-        raise NotImplementedError("TAG_ALL together with other boundary tags")
+    specific = [t for t in tags if t is not TAG_ALL]
+    if specific and any(t is TAG_ALL for t in tags):
+        # TAG_ALL pairs act on every boundary face: in each specific tag's
+        # context together with that tag's pairs, and alone on the faces
+        # no specific tag covers (if the mesh has any)
+        tags = specific[:]
+        if mesh is None or _uncovered(mesh, specific):
+            tags.insert(0, TAG_ALL)
 
     # the reason reported is the one from the furthest stage reached
     why = [0, "no kernel model has %d fields in %dD" % (F, dimensions)]
@@ -578,7 +742,9 @@ def lower(template, dimensions):
                 b_ctx = _Ctx(dimensions, face=tag, coeff_keys=co_keys)
                 y_b = evaluate(outs, b_ctx)
                 hit = None
-                for kind in fam.kinds:
+                if _close(y_b, evaluate(canon, b_ctx)):
+                    hit = (BC_NONE, None)     # no boundary flux on these faces
+                for kind in ([] if hit else fam.kinds):
                     for bchoice in fam.bdry_choices(outs, roles, choice, dimensions, tag, kind):
                         q = dict(choice) if bchoice is None else dict(choice, bdry_flux_type=bchoice)
                         b = fam.build(roles, q, (tag, kind))
@@ -606,6 +772,7 @@ def lower(template, dimensions):
                 final["bdry_flux_type"] = bft
             model = fam.build(roles, final, None)[0]
             desc = model.descriptor()
+            bcs = [(t, k) for t, k in bcs if not (k == BC_NONE and t is TAG_ALL)]
             names = roles.names()
             if src_terms:
                 names["source"] = src_terms[0][:2]
@@ -616,13 +783,21 @@ def lower(template, dimensions):
     raise NotImplementedError("op template is not one the B200 kernels implement: " + why[1])
 
 
-def as_descriptor(template, dimensions):
+def _uncovered(mesh, tags):
+    """Whether some boundary face carries none of ``tags``."""
+    covered = set()
+    for t in tags:
+        covered.update(map(tuple, mesh.boundary_faces(t).tolist()))
+    return any(tuple(f) not in covered for f in mesh.boundary_faces(TAG_ALL).tolist())
+
+
+def as_descriptor(template, dimensions, mesh=None):
     """A lowered :class:`OpTemplate` for a template or an OpTemplate (the
     model that made the template, if any, attached as its operator)."""
     if isinstance(template, OpTemplate):
         return template
     from .models import template_model
-    desc = lower(template, dimensions)
+    desc = lower(template, dimensions, mesh)
     desc.operator = template_model(template)
     return desc
 

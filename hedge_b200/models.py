@@ -192,6 +192,27 @@ class StrongAdvectionOperator(HyperbolicOperator):
         return {"bc_in": self.inflow_u.boundary_interpolant(t, discr, self.inflow_tag)}
 
 
+class WeakAdvectionOperator(StrongAdvectionOperator):
+    """advection.py:153-187: M^-1 (v . S^T u - fluxes), the weak form with
+    the weak flux and outflow data taken from the interior.  Lowered onto
+    the strong-form advection kernel (summation by parts; see
+    hedge_b200.lowering), hence the same descriptor."""
+
+    def flux(self):
+        return self.weak_flux()
+
+    def op_template(self, u=None, bc_in=None):
+        u = ot.Field("u") if u is None else u
+        bc_in = ot.Field("bc_in") if bc_in is None else bc_in
+        bc_out = ot.BoundarizeOperator(self.outflow_tag) * u
+        stiff_t = ot.make_stiffness_t(self.dimensions)
+        flux_op = ot.get_flux_operator(self.flux())
+        return _remember(self, ot.InverseMassOperator()(
+            np.dot(self.v, stiff_t * u)
+            - (flux_op(u) + flux_op(ot.BoundaryPair(u, bc_in, self.inflow_tag))
+               + flux_op(ot.BoundaryPair(u, bc_out, self.outflow_tag)))))
+
+
 class StrongWaveOperator(HyperbolicOperator):
     def __init__(self, c, dimensions, source_f=0, flux_type="upwind",
                  dirichlet_tag=TAG_ALL, dirichlet_bc_f=0,
@@ -466,7 +487,7 @@ def _to_numpy(x):
     return x
 
 
-__all__ = ["template_model", "StrongAdvectionOperator", "StrongWaveOperator",
+__all__ = ["template_model", "StrongAdvectionOperator", "WeakAdvectionOperator", "StrongWaveOperator",
            "VariableVelocityStrongWaveOperator", "MaxwellOperator",
            "OpTemplate", "make_tdep_constant", "TimeConstantGivenFunction",
            "TimeDependentGivenFunction",

@@ -19,6 +19,11 @@ Operator (call / ``op * f``)   operators.py:36-74
 DifferentiationOperator        operators.py:107-139
 MassOperator,                  operators.py:389-415
 InverseMassOperator
+StiffnessOperator,             operators.py:133-143 (S_x = M D_x and the
+StiffnessTOperator,            weak derivative S_x^T)
+make_stiffness(_t)
+Quadrature*Upsampler,          operators.py:149-168, 262-314
+QuadratureStiffnessTOperator   (over-integration)
 BoundarizeOperator             operators.py:488-495
 FluxOperator,                  operators.py:529-657
 VectorFluxOperator
@@ -329,6 +334,72 @@ class MassOperator(Operator):
     pass
 
 
+class StiffnessOperator(Operator):
+    """S_x = M D_x (operators.py:133-135)."""
+
+    def __init__(self, xyz_axis):
+        self.xyz_axis = xyz_axis
+
+    def _args(self):
+        return (self.xyz_axis,)
+
+
+class StiffnessTOperator(Operator):
+    """Weak derivative S_x^T: (S_x^T u)_i = int u d(phi_i)/dx
+    (operators.py:141-143)."""
+
+    def __init__(self, xyz_axis):
+        self.xyz_axis = xyz_axis
+
+    def _args(self):
+        return (self.xyz_axis,)
+
+    def __str__(self):
+        return "ST%d" % self.xyz_axis
+
+
+class QuadratureGridUpsampler(Operator):
+    """A volume (or, applied to boundary data, boundary) field sampled at
+    the quadrature nodes of ``quadrature_tag`` (operators.py:262-276)."""
+
+    def __init__(self, quadrature_tag):
+        self.quadrature_tag = quadrature_tag
+
+    def _args(self):
+        return (self.quadrature_tag,)
+
+
+class QuadratureInteriorFacesGridUpsampler(Operator):
+    """Face traces sampled at the face quadrature nodes
+    (operators.py:278-292)."""
+
+    def __init__(self, quadrature_tag):
+        self.quadrature_tag = quadrature_tag
+
+    def _args(self):
+        return (self.quadrature_tag,)
+
+
+class QuadratureBoundaryGridUpsampler(Operator):
+    def __init__(self, quadrature_tag, boundary_tag):
+        self.quadrature_tag = quadrature_tag
+        self.boundary_tag = boundary_tag
+
+    def _args(self):
+        return (self.quadrature_tag, self.boundary_tag)
+
+
+class QuadratureStiffnessTOperator(Operator):
+    """S_x^T with the integral taken by quadrature (operators.py:149-168)."""
+
+    def __init__(self, xyz_axis, quadrature_tag):
+        self.xyz_axis = xyz_axis
+        self.quadrature_tag = quadrature_tag
+
+    def _args(self):
+        return (self.xyz_axis, self.quadrature_tag)
+
+
 class InverseMassOperator(Operator):
     def __str__(self):
         return "MInv"
@@ -390,6 +461,14 @@ def get_flux_operator(flux):
 
 def make_nabla(dim):
     return np.array([DifferentiationOperator(i) for i in range(dim)], dtype=object)
+
+
+def make_stiffness(dim):
+    return np.array([StiffnessOperator(i) for i in range(dim)], dtype=object)
+
+
+def make_stiffness_t(dim):
+    return np.array([StiffnessTOperator(i) for i in range(dim)], dtype=object)
 
 
 def join_fields(*args):
@@ -454,6 +533,9 @@ def pretty(template):
 __all__ = ["Field", "make_field", "make_sym_vector", "make_vector_field",
            "BoundaryPair", "BoundaryNormalComponent", "normal", "make_normal",
            "OperatorBinding", "Operator", "DifferentiationOperator", "MassOperator",
+           "StiffnessOperator", "StiffnessTOperator", "QuadratureGridUpsampler",
+           "QuadratureInteriorFacesGridUpsampler", "QuadratureBoundaryGridUpsampler",
+           "QuadratureStiffnessTOperator", "make_stiffness", "make_stiffness_t",
            "InverseMassOperator", "BoundarizeOperator", "FluxOperator",
            "VectorFluxOperator", "get_flux_operator", "make_nabla", "join_fields",
            "make_obj_array", "cse", "cross", "is_zero", "pretty", "walk"]

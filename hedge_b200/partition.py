@@ -79,7 +79,7 @@ class PartPlan:
 
 class PartitionPlan:
     def __init__(self, discr, ot, nparts, owner=None):
-        ot = as_descriptor(ot, discr.dimensions)
+        ot = as_descriptor(ot, discr.dimensions, discr.mesh)
         conn, n_given, _ = build_face_table(discr, ot)
         if n_given:
             raise NotImplementedError("partitions with given boundary data")
@@ -188,7 +188,7 @@ class PartitionedOperator:
 
     def __init__(self, discr, model, plan, rank, precision="fp64", device=None, exchange=None):
         torch = _torch()
-        ot = as_descriptor(model.op_template(), discr.dimensions)
+        ot = as_descriptor(model.op_template(), discr.dimensions, discr.mesh)
         self.ot, self.plan, self.rank = ot, plan, rank
         self.part = p = plan.parts[rank]
         self.F = ot.n_fields

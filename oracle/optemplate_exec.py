@@ -18,7 +18,18 @@ lowering.
   lift E (face_operators.hpp:154-263);
 * inverse mass: M^-1 (1/J u) per element (jit/__init__.py:249-258);
 * BoundarizeOperator: the volume vector at the boundary's nodes
-  (discretization/__init__.py:1055-1093); boundary normals per boundary node.
+  (discretization/__init__.py:1055-1093); boundary normals per boundary node;
+* weak derivative S_x^T u: per element (M D_r)^T u times dr/dx |J|
+  (operators.py:141-143 with the reference element's matrices);
+* over-integration (operators.py:149-168, 262-314, 593-631): where a
+  stiffness-transpose or a flux operator acts on up-sampled fields, the
+  integrals are taken with collapsed Gauss-Jacobi rules (Duffy transform,
+  Gauss-Legendre x Gauss-Jacobi(1,0) [x Gauss-Jacobi(2,0)] points, exact to
+  degree 2(N+2)-1 per direction) on the elements and on every face, with the
+  interior / exterior traces evaluated from each element's own polynomial at
+  the physical quadrature points and boundary data interpolated from the
+  face nodes.  This is an independent evaluation of the integrals the
+  nodal operators compute in closed form.
 """
 
 from __future__ import annotations
@@ -29,7 +40,40 @@ import numpy as np
 
 from hedge_b200 import flux as fl
 from hedge_b200 import optemplate as ot
-from hedge_b200.mesh import TAG_NONE
+from hedge_b200.mesh import TAG_ALL, TAG_NONE, face_vertex_table
+from hedge_b200.refelem import make_element
+
+_QUAD = (ot.QuadratureGridUpsampler, ot.QuadratureInteriorFacesGridUpsampler,
+         ot.QuadratureBoundaryGridUpsampler)
+
+
+def _has_quad(x):
+    return any(isinstance(n, ot.OperatorBinding) and isinstance(n.op, _QUAD)
+               for n in ot.walk(x))
+
+
+def _gauss_jacobi(n, alpha):
+    from scipy.special import roots_jacobi
+    return roots_jacobi(n, alpha, 0.0)
+
+
+def simplex_rule(dim, n):
+    """Collapsed Gauss-Jacobi rule on the reference simplex (vertices -1 /
+    unit vectors scaled to [-1, 1]); weights sum to its volume."""
+    a, wa = np.polynomial.legendre.leggauss(n)
+    if dim == 1:
+        return a[:, None], wa
+    b, wb = _gauss_jacobi(n, 1.0)
+    if dim == 2:
+        A, B = np.meshgrid(a, b, indexing="ij")
+        r = (1 + A) * (1 - B) / 2 - 1
+        return np.stack([r.ravel(), B.ravel()], 1), (wa[:, None] * wb[None, :]).ravel() / 2
+    c, wc = _gauss_jacobi(n, 2.0)
+    A, B, Cc = np.meshgrid(a, b, c, indexing="ij")
+    r = (1 + A) * (1 - B) * (1 - Cc) / 4 - 1
+    s_ = (1 + B) * (1 - Cc) / 2 - 1
+    w = (wa[:, None, None] * wb[None, :, None] * wc[None, None, :]).ravel() / 8
+    return np.stack([r.ravel(), s_.ravel(), Cc.ravel()], 1), w
 
 
 def _num(x):
@@ -48,12 +92,201 @@ class TemplateExecutor:
         self.imd = discr.mesh.inv_map_a                             # [K, r, x]
         self.absj = np.abs(discr.mesh.jacobians)
         self._groups = {}
+        self._quad = None
+
+    # -- nodal basis at arbitrary points ----------------------------------------------
+    def _phi(self, r):
+        """Nodal basis values [P, Np] (and reference gradients [d, P, Np]) at
+        reference points r [P, d]."""
+        ld = self.d.ldis
+        modes = ld.mode_ids()
+        vinv = np.linalg.inv(ld.vandermonde)
+        P = np.stack([ld.basis(m, r) for m in modes], 1)
+        G = [ld.grad_basis(m, r) for m in modes]
+        dP = np.stack([np.stack([g[k] for g in G], 1) for k in range(self.dim)])
+        return P @ vinv, dP @ vinv
+
+    def _to_ref(self, k, x):
+        m = self.d.mesh
+        return (x - m.map_b[k]) @ m.inv_map_a[k].T
+
+    def _setup_quadrature(self):
+        """Volume and face quadrature of degree 2 (N + 2) - 1 per direction."""
+        if self._quad is not None:
+            return self._quad
+        d, N, m = self.dim, self.d.order, self.d.mesh
+        n = N + 2
+        rq, wq = simplex_rule(d, n)
+        phi_q, dphi_q = self._phi(rq)
+        # faces: physical points, weights, normals, int / ext basis values
+        fr, fw = simplex_rule(d - 1, n)
+        nf = d + 1
+        ftab = face_vertex_table(d)
+        K = self.K
+        nbr = {}
+        for el_l, f_l, el_n, f_n in m.interfaces:
+            nbr[(int(el_l), int(f_l))] = int(el_n)
+            nbr[(int(el_n), int(f_n))] = int(el_l)
+        faces = []
+        for k in range(K):
+            verts = m.points[m.elements[k]]
+            for f in range(nf):
+                P = verts[list(ftab[f])]
+                if d == 2:
+                    x = P[0] + (fr[:, :1] + 1) / 2 * (P[1] - P[0])
+                    dA = fw * np.linalg.norm(P[1] - P[0]) / 2
+                else:
+                    x = P[0] + (fr[:, :1] + 1) / 2 * (P[1] - P[0]) + \
+                        (fr[:, 1:2] + 1) / 2 * (P[2] - P[0])
+                    dA = fw * np.linalg.norm(np.cross(P[1] - P[0], P[2] - P[0])) / 4
+                phi_i, _ = self._phi(self._to_ref(k, x))
+                e = nbr.get((k, f))
+                phi_e = self._phi(self._to_ref(e, x))[0] if e is not None else None
+                faces.append(dict(k=k, f=f, x=x, dA=dA, n=m.face_normals[k, f],
+                                  phi_i=phi_i, ext=e, phi_e=phi_e, P=P))
+        self._quad = dict(wq=wq, phi_q=phi_q, dphi_q=dphi_q, faces=faces)
+        return self._quad
 
     # -- element-local operators ---------------------------------------------------
     def grad(self, u, axis):
         ue = u.reshape(self.K, self.Np)
         dr = np.einsum("rij,kj->kri", self.dmats, ue)                # [K, r, Np]
         return np.einsum("kr,kri->ki", self.imd[:, :, axis], dr).reshape(-1)
+
+    def stiffness_t(self, f, axis):
+        """Nodal S_x^T f per element: dr/dx |J| (M D_r)^T f."""
+        M = self.d.ldis.mass_matrix
+        fe = f.reshape(self.K, self.Np)
+        out = np.zeros_like(fe)
+        for r in range(self.dim):
+            S = M @ self.dmats[r]
+            out += (self.imd[:, r, axis] * self.absj)[:, None] * (fe @ S)
+        return out.reshape(-1)
+
+    def _qvol(self, x, env):
+        """An up-sampled expression at the volume quadrature points [K, Q]."""
+        q = self._setup_quadrature()
+        if _num(x):
+            return np.full((self.K, len(q["wq"])), float(x))
+        if isinstance(x, ot.Field):
+            return self.vol(x, env).reshape(self.K, self.Np) @ q["phi_q"].T
+        if isinstance(x, ot.Sum):
+            return sum(self._qvol(c, env) for c in x.children)
+        if isinstance(x, ot.Product):
+            r = 1.0
+            for c in x.children:
+                r = r * self._qvol(c, env)
+            return r
+        if isinstance(x, ot.OperatorBinding) and isinstance(x.op, ot.QuadratureGridUpsampler):
+            return self._qvol(x.field, env)
+        raise NotImplementedError("quadrature-grid node %r" % (x,))
+
+    def quad_stiffness_t(self, x, axis, env):
+        q = self._setup_quadrature()
+        fq = self._qvol(x, env)                                     # [K, Q]
+        dphi = np.einsum("kr,rqi->kqi", self.imd[:, :, axis], q["dphi_q"])
+        return (np.einsum("q,kq,kqi->ki", q["wq"], fq, dphi) * self.absj[:, None]).reshape(-1)
+
+    def _strip(self, x):
+        """Template with the up-samplers removed (their operands' values at
+        a point are the same polynomial's)."""
+        if isinstance(x, np.ndarray):
+            return np.array([self._strip(c) for c in x.reshape(-1)], dtype=object)
+        if isinstance(x, ot.OperatorBinding) and isinstance(x.op, _QUAD):
+            return self._strip(x.field)
+        if isinstance(x, ot.Sum):
+            r = 0
+            for c in x.children:
+                r = ot.add(r, self._strip(c))
+            return r
+        if isinstance(x, ot.Product):
+            r = 1
+            for c in x.children:
+                r = ot.mul(r, self._strip(c))
+            return r
+        if isinstance(x, ot.OperatorBinding):
+            return ot.OperatorBinding(x.op, self._strip(x.field))
+        return x
+
+    def _face_interp(self, face, vals_at_nodes):
+        """Boundary data given at a face's nodes -> its quadrature points
+        (polynomial of degree N in the face's own coordinates)."""
+        d, N = self.dim, self.d.order
+        k, f = face["k"], face["f"]
+        xn = self.d.nodes[k * self.Np + self.d.ldis.fmask[f]]
+        P = face["P"]
+
+        def coords(x):
+            A = (P[1:] - P[0]).T                                   # [d, d-1]
+            ab = np.linalg.lstsq(A, (x - P[0]).T, rcond=None)[0].T
+            return 2 * ab - 1
+        if d == 2:
+            vn = np.polynomial.legendre.legvander(coords(xn)[:, 0], N)
+            vq = np.polynomial.legendre.legvander(coords(face["x"])[:, 0], N)
+        else:
+            tri = make_element(2, N)
+            modes = tri.mode_ids()
+            vn = np.stack([tri.basis(m, coords(xn)) for m in modes], 1)
+            vq = np.stack([tri.basis(m, coords(face["x"])) for m in modes], 1)
+        return vq @ np.linalg.solve(vn, vals_at_nodes)
+
+    def _bq(self, x, env, face, bpos):
+        """Boundary data at a face's quadrature points."""
+        if _num(x):
+            return np.full(len(face["dA"]), float(x))
+        if isinstance(x, ot.Field):
+            v = env[x.name]
+            v = v[x.index] if x.index is not None else v
+            v = np.broadcast_to(np.asarray(v, dtype=np.float64), (bpos[1],))
+            return self._face_interp(face, v[bpos[0]:bpos[0] + self.d.Nfp])
+        if isinstance(x, ot.Sum):
+            return sum(self._bq(c, env, face, bpos) for c in x.children)
+        if isinstance(x, ot.Product):
+            r = 1.0
+            for c in x.children:
+                r = r * self._bq(c, env, face, bpos)
+            return r
+        if isinstance(x, ot.BoundaryNormalComponent):
+            return np.full(len(face["dA"]), face["n"][x.axis])
+        if isinstance(x, ot.OperatorBinding):
+            if isinstance(x.op, _QUAD):
+                return self._bq(x.field, env, face, bpos)
+            if isinstance(x.op, ot.BoundarizeOperator):
+                return face["phi_i"] @ self.vol(self._strip(x.field), env).reshape(
+                    self.K, self.Np)[face["k"]]
+        raise NotImplementedError("boundary quadrature node %r" % (x,))
+
+    def quad_flux(self, flux, arg, env):
+        """Face integrals of the flux against the test functions, by face
+        quadrature, on interior faces (arg a volume vector) or on a
+        boundary pair's faces."""
+        q = self._setup_quadrature()
+        out = np.zeros((self.K, self.Np))
+        pair = arg if isinstance(arg, ot.BoundaryPair) else None
+        field = self._strip(pair.field if pair is not None else arg)
+        vals = [self.vol(c, env).reshape(self.K, self.Np) for c in _comps(field)]
+        bfaces = None
+        if pair is not None:
+            if pair.tag is TAG_NONE:
+                return out.reshape(-1)
+            ef = self.d.mesh.boundary_faces(pair.tag)
+            nb = len(ef) * self.d.Nfp
+            bfaces = {(int(a), int(b)): i * self.d.Nfp for i, (a, b) in enumerate(ef)}
+        for face in q["faces"]:
+            k, f = face["k"], face["f"]
+            iv = [face["phi_i"] @ v[k] for v in vals]
+            if pair is None:
+                if face["ext"] is None:
+                    continue
+                ev = [face["phi_e"] @ v[face["ext"]] for v in vals]
+            else:
+                if (k, f) not in bfaces:
+                    continue
+                ev = [self._bq(c, env, face, (bfaces[(k, f)], nb)) for c in _comps(pair.bfield)]
+            nvec = np.broadcast_to(face["n"], (len(face["dA"]), self.dim))
+            fv = self._flux_vals(flux, iv, ev, nvec)
+            out[k] += (face["dA"] * fv) @ face["phi_i"]
+        return out.reshape(-1)
 
     def inverse_mass(self, v):
         ve = v.reshape(self.K, self.Np) / self.absj[:, None]
@@ -156,6 +389,15 @@ class TemplateExecutor:
                 return self.grad(self.vol(x.field, env), op.xyz_axis)
             if isinstance(op, ot.InverseMassOperator):
                 return self.inverse_mass(self.vol(x.field, env))
+            if isinstance(op, ot.QuadratureStiffnessTOperator):
+                return self.quad_stiffness_t(x.field, op.xyz_axis, env)
+            if isinstance(op, ot.StiffnessTOperator):
+                if _has_quad(x.field):
+                    return self.quad_stiffness_t(x.field, op.xyz_axis, env)
+                return self.stiffness_t(self.vol(x.field, env), op.xyz_axis)
+            if isinstance(op, ot.FluxOperator) and _has_quad(
+                    x.field.field if isinstance(x.field, ot.BoundaryPair) else x.field):
+                return self.quad_flux(op.flux, x.field, env)
             if isinstance(op, ot.FluxOperator):
                 arg = x.field
                 if isinstance(arg, ot.BoundaryPair):

@@ -114,7 +114,7 @@ class OracleRHS:
     def __init__(self, discr, optemplate, c_field=None, source=None):
         from hedge_b200.lowering import as_descriptor
         self.discr = discr
-        self.ot = ot = as_descriptor(optemplate, discr.dimensions)
+        self.ot = ot = as_descriptor(optemplate, discr.dimensions, discr.mesh)
         ld = discr.ldis
         self.dim = discr.dimensions
         self.K, self.Np = discr.K, discr.Np

@@ -87,3 +87,21 @@ def test_bound_model_through_its_template(cuda_device):
     got = op.bind(d)(0.0, q).cpu().numpy()
     ref = _exec(d, op.op_template(), {"w": q, "c": c, "source": src})
     assert rel_l2(got, ref) <= 1e-12
+
+
+@pytest.mark.parametrize("quadrature", [False, True])
+def test_compiled_weak_advection(cuda_device, quadrature):
+    """The weak form (nodal or over-integrated) compiled onto the strong
+    advection kernel equals the executor run on the weak tree."""
+    from test_optemplate import _in_out_tagger, weak_quadrature_advection
+    v = np.array([0.7, -0.4])
+    d = hb.Discretization(rect(6, tagger=_in_out_tagger(v)), order=4)
+    tpl = weak_quadrature_advection(v, "upwind") if quadrature else \
+        hb.WeakAdvectionOperator(v, inflow_tag="in", outflow_tag="out",
+                                 flux_type="upwind").op_template()
+    q = _fields(d, 1, 11)
+    bc = np.cos(2 * d.get_boundary("in").nodes[:, 1])
+    comp = d.compile(tpl, precision="fp64")
+    got = comp(u=q[0], bc_in=bc).cpu().numpy()
+    comp.check()
+    assert rel_l2(got, _exec(d, tpl, {"u": q[0], "bc_in": bc})[0]) <= 1e-12

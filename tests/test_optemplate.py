@@ -307,13 +307,29 @@ def test_nonmodel_templates_raise():
         "penalty term": -D[0](u) + M(ot.FluxOperator(fl.PenaltyTerm() * (U.int - U.ext))(u)),
         "volume term under the inverse mass": M(D[0](u) + central(u)),
         "nonlinear volume term": -D[0](u) * u + M(central(u)),
-        "extrapolation boundary": -D[0](u) + M(central(u) + central(
-            ot.BoundaryPair(u, ot.BoundarizeOperator("out")(u), "out"))),
+        "boundary data a multiple of the interior": -D[0](u) + M(central(u) + central(
+            ot.BoundaryPair(u, 3 * ot.BoundarizeOperator("out")(u), "out"))),
+        "weak derivative outside the inverse mass": ot.StiffnessTOperator(0)(u)
+        + M(central(u)),
+        "weak derivative of a product": M(ot.StiffnessTOperator(0)(ot.Field("c") * u)
+                                          + central(u)),
     }
     for what, tpl in bad.items():
         with pytest.raises(NotImplementedError):
             lower(tpl, 2)
             pytest.fail(what)
+
+
+def test_zero_boundary_flux_lowers_to_no_condition():
+    """Extrapolated boundary data (ext = int) gives a zero central flux."""
+    u = ot.Field("u")
+    U = fl.FluxScalarPlaceholder(0)
+    n = fl.make_normal(2)
+    central = ot.FluxOperator(0.5 * (U.int - U.ext) * n[0])
+    tpl = -ot.DifferentiationOperator(0)(u) + ot.InverseMassOperator()(
+        central(u) + central(ot.BoundaryPair(u, ot.BoundarizeOperator("out")(u), "out")))
+    desc = lower(tpl, 2)
+    assert desc.model == MODEL_ADVECTION and desc.bcs == [("out", 0)]
 
 
 def test_wrong_wave_boundary_raises():
@@ -362,3 +378,75 @@ def test_nd_calculus_templates_equal_wave_pieces(dim):
     # linear fields are differentiated exactly
     gx = ex(hb.GradientOperator(dim).op_template(), u=x[:, 0], bc=x[b, 0])
     assert np.abs(gx[0] - 1).max() < 1e-12 and np.abs(gx[1:]).max() < 1e-12
+
+
+# --------------------------------------------------------------------------
+# weak form and over-integration
+
+def _in_out_tagger(v):
+    """Boundary faces with v.n < 0 'in', the others 'out' (unit square)."""
+    def tagger(fvi, el, fn, allv):
+        x = allv[list(fvi)].mean(0)
+        n = np.array([-1.0, 0.0]) if x[0] < -0.99 else np.array([1.0, 0.0]) if x[0] > 0.99 \
+            else np.array([0.0, -1.0]) if x[1] < -0.99 else np.array([0.0, 1.0])
+        return ["in"] if np.dot(n, v) < 0 else ["out"]
+    return tagger
+
+
+def weak_quadrature_advection(v, flux_type):
+    """The weak-form advection written with over-integration: the
+    stiffness acts on up-sampled u, the fluxes on face-quadrature traces."""
+    u, bc = ot.Field("u"), ot.Field("bc_in")
+    to_quad = ot.QuadratureGridUpsampler("quad")
+    to_if = ot.QuadratureInteriorFacesGridUpsampler("quad")
+    m = hb.WeakAdvectionOperator(v, inflow_tag="in", outflow_tag="out", flux_type=flux_type)
+    flux_op = ot.get_flux_operator(m.flux())
+    st = ot.make_stiffness_t(2)
+    bc_out = to_quad(ot.BoundarizeOperator("out")(u))
+    return ot.InverseMassOperator()(
+        np.dot(v, st * to_quad(u))
+        - (flux_op(to_if(u)) + flux_op(ot.BoundaryPair(to_if(u), to_quad(bc), "in"))
+           + flux_op(ot.BoundaryPair(to_if(u), bc_out, "out"))))
+
+
+@pytest.mark.parametrize("flux_type", ["upwind", "central", "lf"])
+@pytest.mark.parametrize("quadrature", [False, True])
+def test_weak_advection_equals_strong_kernel_model(flux_type, quadrature):
+    """The weak form (nodal or over-integrated), evaluated as a tree, equals
+    the oracle's strong-form advection it is lowered to."""
+    v = np.array([0.7, -0.4])
+    d = hb.Discretization(rect(5, tagger=_in_out_tagger(v)), order=3)
+    tpl = weak_quadrature_advection(v, flux_type) if quadrature else \
+        hb.WeakAdvectionOperator(v, inflow_tag="in", outflow_tag="out",
+                                 flux_type=flux_type).op_template()
+    desc = lower(tpl, 2, d.mesh)
+    assert desc.model == MODEL_ADVECTION and np.allclose(desc.params["v"], v)
+    assert desc.flux_type == ["central", "upwind", "lf"].index(flux_type)
+    assert set(desc.bcs) == {("in", BC_GIVEN), ("out", 0)}
+    q = _fields(d, 1, 4)
+    bc = np.cos(2 * d.get_boundary("in").nodes[:, 1])
+    err = _executor_vs_oracle(d, tpl, desc, {"u": q[0], "bc_in": bc}, q, bc_in=bc)
+    assert err <= 1e-12, err
+
+
+def test_weak_form_needs_every_boundary_face_tagged():
+    """Without the mesh (or with untagged boundary faces) the weak form's
+    face term on the remaining boundary faces has no kernel condition."""
+    v = np.array([0.7, -0.4])
+    tpl = hb.WeakAdvectionOperator(v, inflow_tag="in", outflow_tag="out").op_template()
+    with pytest.raises(NotImplementedError, match="boundary"):
+        lower(tpl, 2)
+
+
+def test_over_integration_with_a_coefficient_field_is_refused():
+    """Variable-velocity advection (the velocity a field under the
+    quadrature stiffness, advection.py:300-368) is not integrated exactly by
+    the nodal operators."""
+    u, vx = ot.Field("u"), ot.Field("vx")
+    to_quad = ot.QuadratureGridUpsampler("quad")
+    U = fl.FluxScalarPlaceholder(0)
+    flux = ot.FluxOperator(0.5 * (U.int - U.ext) * fl.make_normal(2)[0])
+    tpl = ot.InverseMassOperator()(ot.StiffnessTOperator(0)(to_quad(vx) * to_quad(u))
+                                   - flux(u))
+    with pytest.raises(NotImplementedError):
+        lower(tpl, 2)
