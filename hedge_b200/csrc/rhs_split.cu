@@ -199,6 +199,42 @@ __device__ __forceinline__ void store_split(uint8_t* hi, uint8_t* lo, uint32_t o
   }
 }
 
+// A plane pair (hi, lo) holds 32 bits per entry: before the FP16 row scale
+// is known, an entry's raw FP32 bits are parked there (upper half in hi, lower
+// half in lo) and split in place once the row maximum is known.
+__device__ __forceinline__ void park_f32(uint8_t* hi, uint8_t* lo, uint32_t off, float v) {
+  const uint32_t b = __float_as_uint(v);
+  *reinterpret_cast<uint16_t*>(hi + off) = (uint16_t)(b >> 16);
+  *reinterpret_cast<uint16_t*>(lo + off) = (uint16_t)(b & 0xffffu);
+}
+__device__ __forceinline__ float unpark_f32(const uint8_t* hi, const uint8_t* lo, uint32_t off) {
+  return __uint_as_float(((uint32_t)*reinterpret_cast<const uint16_t*>(hi + off) << 16) |
+                         *reinterpret_cast<const uint16_t*>(lo + off));
+}
+// the same for 8 consecutive K entries (one 16-byte chunk per plane)
+__device__ __forceinline__ void park8(uint8_t* hi, uint8_t* lo, uint32_t off, const float (&v)[8]) {
+  uint32_t hw[4], lw[4];
+#pragma unroll
+  for (int c = 0; c < 8; c += 2) {
+    const uint32_t b0 = __float_as_uint(v[c]), b1 = __float_as_uint(v[c + 1]);
+    hw[c / 2] = (b1 & 0xffff0000u) | (b0 >> 16);
+    lw[c / 2] = (b1 << 16) | (b0 & 0xffffu);
+  }
+  *reinterpret_cast<uint4*>(hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+  *reinterpret_cast<uint4*>(lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+}
+__device__ __forceinline__ void unpark8(const uint8_t* hi, const uint8_t* lo, uint32_t off,
+                                        float (&v)[8]) {
+  const uint4 h = *reinterpret_cast<const uint4*>(hi + off);
+  const uint4 l = *reinterpret_cast<const uint4*>(lo + off);
+  const uint32_t hw[4] = {h.x, h.y, h.z, h.w}, lw[4] = {l.x, l.y, l.z, l.w};
+#pragma unroll
+  for (int c = 0; c < 8; c += 2) {
+    v[c] = __uint_as_float((hw[c / 2] << 16) | (lw[c / 2] & 0xffffu));
+    v[c + 1] = __uint_as_float((hw[c / 2] & 0xffff0000u) | (lw[c / 2] >> 16));
+  }
+}
+
 // power-of-two row scale from the bit pattern of the row's largest |value|
 __device__ __forceinline__ float row_scale(uint32_t maxbits) {
   int e = (int)((maxbits >> 23) & 0xffu) - 13;   // max / 2^(e-127) in [2^13, 2^14)
@@ -1174,15 +1210,19 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
     };
     float inv = 1.0f;
     if constexpr (PT == PT_FP16) {
+      // remainders once: row maxima, raw values parked in the planes
       uint32_t m = 0u;
       for (int item = warp; item < S::NITEM; item += S::NW) {
         const int chunk8 = item >> 2;
         if ((item & 3) != quad) continue;
+        float v[8];
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
           const int j = chunk8 * 8 + c;
-          if (valid && j < NP) m = max(m, __float_as_uint(fabsf(remainder(j))));
+          v[c] = (valid && j < NP) ? remainder(j) : 0.f;
+          m = max(m, __float_as_uint(fabsf(v[c])));
         }
+        park8(Aqh, Aql, kmajor_off(row, chunk8 * 8, KD), v);
       }
       atomicMax(&rmx[row], m);
       __syncthreads();
@@ -1192,11 +1232,19 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
       if ((item & 3) != quad) continue;
       const int chunk8 = item >> 2;
       uint32_t hw[4], lw[4];
+      float parked[8];
+      if constexpr (PT == PT_FP16) unpark8(Aqh, Aql, kmajor_off(row, chunk8 * 8, KD), parked);
 #pragma unroll
       for (int c = 0; c < 8; c += 2) {
         const int j = chunk8 * 8 + c;
-        const float x0 = (valid && j < NP) ? remainder(j) * inv : 0.f;
-        const float x1 = (valid && j + 1 < NP) ? remainder(j + 1) * inv : 0.f;
+        float x0, x1;
+        if constexpr (PT == PT_FP16) {
+          x0 = parked[c] * inv;
+          x1 = parked[c + 1] * inv;
+        } else {
+          x0 = (valid && j < NP) ? remainder(j) : 0.f;
+          x1 = (valid && j + 1 < NP) ? remainder(j + 1) : 0.f;
+        }
         if constexpr (PT == PT_BF16) {
           const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
           const float2 hf = __bfloat1622float2(h);
@@ -1311,6 +1359,8 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
       return true;
     };
     if constexpr (PT == PT_FP16) {
+      // fluxes once: row maxima, raw values parked in the planes; then
+      // every thread splits its own entries with the row scale
       for (int u = 0; u < S::NFV; ++u) {
         const int x = tid + u * S::THREADS;
         float fl[F];
@@ -1323,21 +1373,37 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
           const unsigned m = __reduce_max_sync(grp, __float_as_uint(fabsf(fl[f])));
           if (leader && e >= 0 && e < ne) atomicMax(&fmx[(e / EPW) * 32 + (e % EPW) * F + f], m);
         }
+        if (e >= 0 && e < ne) {
+          const int p = x % NFPT, rowb = (e / EPW) * 32 + (e % EPW) * F;
+#pragma unroll
+          for (int f = 0; f < F; ++f) park_f32(Afh, Afl, kmajor_off(rowb + f, p, KL), fl[f]);
+        }
       }
       __syncthreads();
-    }
-    for (int u = 0; u < S::NFV; ++u) {
-      const int x = tid + u * S::THREADS;
-      float fl[F];
-      face_flux(x, fl);
-      const int e = x / NFPT, p = x % NFPT;
-      if (x < S::NFACE && e < ne) {
-        const int rowb = (e / EPW) * 32 + (e % EPW) * F;
+      for (int u = 0; u < S::NFV; ++u) {
+        const int x = tid + u * S::THREADS;
+        const int e = x / NFPT, p = x % NFPT;
+        if (x < S::NFACE && e < ne) {
+          const int rowb = (e / EPW) * 32 + (e % EPW) * F;
 #pragma unroll
-        for (int f = 0; f < F; ++f) {
-          float v = fl[f];
-          if constexpr (PT == PT_FP16) v *= row_scale_inv(fmx[rowb + f]);
-          store_split<PT>(Afh, Afl, kmajor_off(rowb + f, p, KL), v);
+          for (int f = 0; f < F; ++f) {
+            const uint32_t off = kmajor_off(rowb + f, p, KL);
+            store_split<PT>(Afh, Afl, off,
+                            unpark_f32(Afh, Afl, off) * row_scale_inv(fmx[rowb + f]));
+          }
+        }
+      }
+    } else {
+      for (int u = 0; u < S::NFV; ++u) {
+        const int x = tid + u * S::THREADS;
+        float fl[F];
+        face_flux(x, fl);
+        const int e = x / NFPT, p = x % NFPT;
+        if (x < S::NFACE && e < ne) {
+          const int rowb = (e / EPW) * 32 + (e % EPW) * F;
+#pragma unroll
+          for (int f = 0; f < F; ++f)
+            store_split<PT>(Afh, Afl, kmajor_off(rowb + f, p, KL), fl[f]);
         }
       }
     }
