@@ -1201,50 +1201,66 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
 #pragma unroll
       for (int d = 0; d < DIM; ++d) lin[d] = valid ? (float)(0.5 * (v[1 + d] - v[0])) : 0.f;
     }
-    auto remainder = [&](int j) -> float {
-      const double* v = sv + (fown * EB + e_own) * NV1;
-      double l = v[0];
+    // remainders of 8 consecutive nodes of this thread's row (item chunk8):
+    // the 8 state loads are issued before any is used
+    auto rem8 = [&](int chunk8, float (&v)[8]) {
+      const double* v3 = sv + (fown * EB + e_own) * NV1;
+      const double* src = a.q_in + fown * Knp + (el0 + e_own) * NP;
+      double q[8];
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) l += slam[j * DIM + d] * (v[1 + d] - v[0]);
-      return (float)(a.q_in[fown * Knp + (el0 + e_own) * NP + j] - l);
+      for (int c = 0; c < 8; ++c) {
+        const int j = chunk8 * 8 + c;
+        q[c] = (valid && j < NP) ? __ldg(src + j) : 0.0;
+      }
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const int j = chunk8 * 8 + c;
+        const int jj = j < NP ? j : 0;
+        double l = v3[0];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) l += slam[jj * DIM + d] * (v3[1 + d] - v3[0]);
+        v[c] = (valid && j < NP) ? (float)(q[c] - l) : 0.f;
+      }
     };
+    // this warp's items are warp + k * NW (all in its TMEM quadrant), two
+    // at a time so that 16 state loads are in flight
+    static_assert((S::NITEM / S::NW) % 2 == 0, "items per warp must be even");
     float inv = 1.0f;
     if constexpr (PT == PT_FP16) {
       // remainders once: row maxima, raw values parked in the planes
       uint32_t m = 0u;
-      for (int item = warp; item < S::NITEM; item += S::NW) {
-        const int chunk8 = item >> 2;
-        if ((item & 3) != quad) continue;
-        float v[8];
+#pragma unroll 1
+      for (int k = 0; k < S::NITEM / S::NW; k += 2) {
+        const int c0 = (warp + k * S::NW) >> 2, c1 = (warp + (k + 1) * S::NW) >> 2;
+        float v0[8], v1[8];
+        rem8(c0, v0);
+        rem8(c1, v1);
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          const int j = chunk8 * 8 + c;
-          v[c] = (valid && j < NP) ? remainder(j) : 0.f;
-          m = max(m, __float_as_uint(fabsf(v[c])));
-        }
-        park8(Aqh, Aql, kmajor_off(row, chunk8 * 8, KD), v);
+        for (int c = 0; c < 8; ++c)
+          m = max(m, max(__float_as_uint(fabsf(v0[c])), __float_as_uint(fabsf(v1[c]))));
+        park8(Aqh, Aql, kmajor_off(row, c0 * 8, KD), v0);
+        park8(Aqh, Aql, kmajor_off(row, c1 * 8, KD), v1);
       }
       atomicMax(&rmx[row], m);
       __syncthreads();
       inv = row_scale_inv(rmx[row]);
     }
-    for (int item = warp; item < S::NITEM; item += S::NW) {
-      if ((item & 3) != quad) continue;
-      const int chunk8 = item >> 2;
+#pragma unroll 1
+    for (int k = 0; k < S::NITEM / S::NW; ++k) {
+      const int chunk8 = (warp + k * S::NW) >> 2;
+      const uint32_t off = kmajor_off(row, chunk8 * 8, KD);
+      float v[8];
+      if constexpr (PT == PT_FP16) {
+        unpark8(Aqh, Aql, off, v);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) v[c] *= inv;
+      } else {
+        rem8(chunk8, v);
+      }
       uint32_t hw[4], lw[4];
-      float parked[8];
-      if constexpr (PT == PT_FP16) unpark8(Aqh, Aql, kmajor_off(row, chunk8 * 8, KD), parked);
 #pragma unroll
       for (int c = 0; c < 8; c += 2) {
-        const int j = chunk8 * 8 + c;
-        float x0, x1;
-        if constexpr (PT == PT_FP16) {
-          x0 = parked[c] * inv;
-          x1 = parked[c + 1] * inv;
-        } else {
-          x0 = (valid && j < NP) ? remainder(j) : 0.f;
-          x1 = (valid && j + 1 < NP) ? remainder(j + 1) : 0.f;
-        }
+        const float x0 = v[c], x1 = v[c + 1];
         if constexpr (PT == PT_BF16) {
           const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
           const float2 hf = __bfloat1622float2(h);
@@ -1259,7 +1275,6 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
           lw[c / 2] = *reinterpret_cast<const uint32_t*>(&l);
         }
       }
-      const uint32_t off = kmajor_off(row, chunk8 * 8, KD);
       *reinterpret_cast<uint4*>(Aqh + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
       *reinterpret_cast<uint4*>(Aql + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
     }
@@ -1502,18 +1517,36 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
     tc::fence_before_sync();
     __syncthreads();
 
-    // ---- F: FP64 stage update (coalesced) ----
-    for (int x = tid; x < S::NVAL; x += S::THREADS) {
-      const int f = x / FNP, r = x - f * FNP;
-      if (r < ne * NP) {
-        const int64_t idx = f * Knp + el0 * NP + r;
-        const double rr = (double)sq[x];
-        if (a.mode == 0) {
-          a.q_out[idx] = rr;
-        } else {
-          const double nr = a.ra * a.res[idx] + a.dt * rr;
-          a.res[idx] = nr;
-          a.q_out[idx] = a.q_in[idx] + a.rb * nr;
+    // ---- F: FP64 stage update (coalesced; UF values per thread in flight) ----
+    {
+      constexpr int UF = 6;
+      for (int x0 = tid; x0 < S::NVAL; x0 += UF * S::THREADS) {
+        double r0[UF], q0[UF];
+        int64_t idx[UF];
+        bool ok[UF];
+#pragma unroll
+        for (int u = 0; u < UF; ++u) {
+          const int x = x0 + u * S::THREADS;
+          const int f = x / FNP, r = x - f * FNP;
+          ok[u] = x < S::NVAL && r < ne * NP;
+          idx[u] = f * Knp + el0 * NP + r;
+          r0[u] = q0[u] = 0.0;
+          if (ok[u] && a.mode != 0) {
+            r0[u] = a.res[idx[u]];
+            q0[u] = __ldg(a.q_in + idx[u]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < UF; ++u) {
+          if (!ok[u]) continue;
+          const double rr = (double)sq[x0 + u * S::THREADS];
+          if (a.mode == 0) {
+            a.q_out[idx[u]] = rr;
+          } else {
+            const double nr = a.ra * r0[u] + a.dt * rr;
+            a.res[idx[u]] = nr;
+            a.q_out[idx[u]] = q0[u] + a.rb * nr;
+          }
         }
       }
     }
