@@ -346,6 +346,12 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
                ::"r"(tc::smem_u32(mbar)), "r"(bytes)
                : "memory");
 }
+// one arrival on `mbar` that also announces `bytes` of transactions
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+               ::"r"(tc::smem_u32(mbar)), "r"(bytes)
+               : "memory");
+}
 __device__ __forceinline__ void bulk_load(void* sdst, const void* gsrc, uint32_t bytes,
                                           uint64_t* mbar) {
   asm volatile(
@@ -1072,8 +1078,10 @@ struct ShapeS {
   static constexpr uint32_t osh = al16(ofm + NFPT);
   static constexpr uint32_t overt = al16(osh + 6 * NFP);
   static constexpr uint32_t ors = al16(overt + 4);                   // [2][128] row maxima
-  static constexpr uint32_t obar = al16(ors + 256 * 4);              // ring[2], done, slot
-  static constexpr uint32_t total = al16(obar + 48);
+  // mbarriers: [0..1] ring MMAs done, [2] batch MMAs done, [5..6] ring copy
+  // landed; the TMEM address word sits at byte 32
+  static constexpr uint32_t obar = al16(ors + 256 * 4);
+  static constexpr uint32_t total = al16(obar + 64);
   static constexpr uint32_t LIN_BYTES = 8 + NP * DIM * 8;
   static constexpr int TMEM_NEED = LIFT_COL + NL;
   static constexpr uint32_t TMEM_COLS = TMEM_NEED <= 128 ? 128 : TMEM_NEED <= 256 ? 256 : 512;
@@ -1105,7 +1113,7 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
   const uint8_t* svert = smem + S::overt;
   uint32_t* rsq = reinterpret_cast<uint32_t*>(smem + S::ors);        // state rows
   uint32_t* rsf = rsq + 128;                                         // flux rows
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + S::obar);      // [0..1] ring, [2] done
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + S::obar);      // see ShapeS::obar
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + S::obar + 32);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint8_t* dimg = a.ops;                                       // D chunks
@@ -1127,6 +1135,8 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
       tc::mbar_init(&mbar[0], 1);
       tc::mbar_init(&mbar[1], 1);
       tc::mbar_init(&mbar[2], 1);
+      tc::mbar_init(&mbar[5], 1);
+      tc::mbar_init(&mbar[6], 1);
     }
     if (warp == 0) tc::tmem_alloc(tmem_slot, S::TMEM_COLS);
     tc::fence_proxy_async();
@@ -1146,31 +1156,38 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
   const int e_lane = quad * EPW + lf;
   const uint32_t lane_addr = (uint32_t)(quad * 32) << 16;
   const int row = quad * 32 + lane;
-  uint32_t ring_uses[2] = {0u, 0u};   // commits so far on each ring buffer
+  uint32_t ring_uses[2] = {0u, 0u};   // MMA commits so far on each ring buffer
+  uint32_t ring_fills[2] = {0u, 0u};  // bulk copies started into each ring buffer
+  uint32_t ring_waits[2] = {0u, 0u};  // copies waited for on each ring buffer
   uint32_t chunk = 0;                 // running chunk counter (ring buffer = chunk & 1)
   int bad = 0;
 
-  // refill ring buffer (chunk & 1) with `bytes` from src once its previous
-  // MMAs completed; thread 0 then issues `issue()` and commits to the buffer
-  auto stream_chunk = [&](const uint8_t* src, uint32_t bytes, auto issue) -> bool {
-    const int b = (int)(chunk & 1u);
-    uint8_t* buf = smem + (b ? S::oR1 : S::oR0);
-    int late = 0;
-    if (tid == 0 && ring_uses[b] > 0)
-      late = !tc::mbar_wait(&mbar[b], (ring_uses[b] - 1) & 1u, MBAR_MAX_NS);
-    if (__syncthreads_or(late)) return false;
-    const uint4* s4 = reinterpret_cast<const uint4*>(src);
-    for (uint32_t x = tid; x < bytes / 16; x += S::THREADS)
-      reinterpret_cast<uint4*>(buf)[x] = __ldg(s4 + x);
-    tc::fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) {
-      tc::fence_after_sync();
-      issue(tc::smem_u32(buf));
+  // Thread 0 only: streams n operator chunks of `bytes` (at src + k * bytes)
+  // through the two ring buffers with bulk copies, the copy of chunk k + 1
+  // in flight while chunk k's MMAs (issue(k, buffer)) run.  A buffer is
+  // refilled once the MMAs that read it completed.  False on a timeout.
+  auto stream_chunks = [&](const uint8_t* src, int n, uint32_t bytes, auto issue) -> bool {
+    const uint32_t c0 = chunk;          // running number of this stream's chunk 0
+    auto fill = [&](int k) -> bool {
+      const int b = (int)((c0 + (uint32_t)k) & 1u);
+      if (ring_uses[b] > 0 && !tc::mbar_wait(&mbar[b], (ring_uses[b] - 1) & 1u, MBAR_MAX_NS))
+        return false;
+      mbar_arrive_expect_tx(&mbar[5 + b], bytes);
+      bulk_load(smem + (b ? S::oR1 : S::oR0), src + (size_t)k * bytes, bytes, &mbar[5 + b]);
+      ++ring_fills[b];
+      return true;
+    };
+    if (n > 0 && !fill(0)) return false;
+    for (int k = 0; k < n; ++k) {
+      const int b = (int)(chunk & 1u);
+      if (k + 1 < n && !fill(k + 1)) return false;
+      if (!tc::mbar_wait(&mbar[5 + b], ring_waits[b] & 1u, MBAR_MAX_NS)) return false;
+      ++ring_waits[b];
+      issue(k, tc::smem_u32(smem + (b ? S::oR1 : S::oR0)));
       tc::mma_commit(&mbar[b]);
+      ++ring_uses[b];
+      ++chunk;
     }
-    ++ring_uses[b];
-    ++chunk;
     return true;
   };
 
@@ -1281,12 +1298,13 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
     tc::fence_proxy_async();
     __syncthreads();
 
-    // ---- B: diff MMAs, operator chunks streamed ----
-    {
-      const uint32_t aq_h = tc::smem_u32(Aqh), aq_l = tc::smem_u32(Aql);
-      for (int kk = 0; kk < S::NKD && !bad; ++kk) {
-        const bool ok = stream_chunk(dimg + (size_t)kk * 2 * S::bDc, 2 * S::bDc,
-                                     [&](uint32_t buf) {
+    // ---- B: diff MMAs, operator chunks streamed by warp 0 (lane 0) while
+    // the other warps start on the face fluxes, which do not need them ----
+    if (warp == 0) {
+      int ok = 1;
+      if (lane == 0) {
+        const uint32_t aq_h = tc::smem_u32(Aqh), aq_l = tc::smem_u32(Aql);
+        ok = stream_chunks(dimg, S::NKD, 2 * S::bDc, [&](int kk, uint32_t buf) {
           const uint32_t bh = buf, bl = buf + S::bDc;
           const uint64_t ah = tc::smem_desc(aq_h + kk * 256, 128, KD * 16);
           const uint64_t al = tc::smem_desc(aq_l + kk * 256, 128, KD * 16);
@@ -1300,13 +1318,10 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
             tc::mma_bf16(tmem_diff + S::ND1, ah, tc::smem_desc(bl + o2, 128, 256), ID_D2, 1u);
             tc::mma_bf16(tmem_diff + S::ND1, al, tc::smem_desc(bh + o2, 128, 256), ID_D2, 1u);
           }
-        });
-        if (!ok) bad = 1;
+        }) ? 1 : 0;
       }
-    }
-    if (bad) {
-      if (tid == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
-      break;
+      __syncwarp();
+      if (!__shfl_sync(FULL, ok, 0)) bad = 1;
     }
 
     // ---- C: face fluxes (FP32 on jumps formed in FP64) -> lift planes ----
@@ -1423,28 +1438,32 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
       }
     }
     tc::fence_proxy_async();
-    __syncthreads();
+    // (every thread learns whether the diff stream gave up)
+    if (__syncthreads_or(bad)) {
+      if (tid == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+      break;
+    }
 
-    // ---- D: lift MMAs, operator chunks streamed ----
+    // ---- D: lift MMAs, operator chunks streamed by thread 0 ----
     {
-      const uint32_t af_h = tc::smem_u32(Afh), af_l = tc::smem_u32(Afl);
-      for (int kk = 0; kk < S::NKL && !bad; ++kk) {
-        const bool ok = stream_chunk(limg + (size_t)kk * 2 * S::bLc, 2 * S::bLc,
-                                     [&](uint32_t buf) {
+      int ok = 1;
+      if (tid == 0) {
+        tc::fence_after_sync();
+        const uint32_t af_h = tc::smem_u32(Afh), af_l = tc::smem_u32(Afl);
+        ok = stream_chunks(limg, S::NKL, 2 * S::bLc, [&](int kk, uint32_t buf) {
           const uint32_t bh = buf, bl = buf + S::bLc;
           const uint64_t ah = tc::smem_desc(af_h + kk * 256, 128, KL * 16);
           const uint64_t al = tc::smem_desc(af_l + kk * 256, 128, KL * 16);
           tc::mma_bf16(tmem_lift, ah, tc::smem_desc(bh, 128, 256), ID_L, kk > 0 ? 1u : 0u);
           tc::mma_bf16(tmem_lift, ah, tc::smem_desc(bl, 128, 256), ID_L, 1u);
           tc::mma_bf16(tmem_lift, al, tc::smem_desc(bh, 128, 256), ID_L, 1u);
-        });
-        if (!ok) bad = 1;
+        }) ? 1 : 0;
+        if (ok) tc::mma_commit(&mbar[2]);   // all of this batch's MMAs
       }
-      if (!bad && tid == 0) tc::mma_commit(&mbar[2]);   // all of this batch's MMAs
-    }
-    if (bad) {
-      if (tid == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
-      break;
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+        break;
+      }
     }
 
     // ---- E: TMEM -> chain rule, volume terms, + lift -> staged rhs ----
@@ -1553,10 +1572,13 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
     __syncthreads();
   }
 
-  // ---- tear-down: wait for any MMAs still reading the ring, release TMEM ----
+  // ---- tear-down: wait for copies and MMAs still using the ring, release TMEM ----
   if (tid == 0) {
-    for (int b = 0; b < 2; ++b)
+    for (int b = 0; b < 2; ++b) {
+      for (uint32_t w = ring_waits[b]; w < ring_fills[b]; ++w)
+        tc::mbar_wait(&mbar[5 + b], w & 1u, MBAR_MAX_NS);
       if (ring_uses[b] > 0) tc::mbar_wait(&mbar[b], (ring_uses[b] - 1) & 1u, MBAR_MAX_NS);
+    }
   }
   tc::fence_before_sync();
   __syncthreads();
