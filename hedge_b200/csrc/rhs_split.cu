@@ -928,10 +928,65 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
       warp_arrive(&mbar[MB_FREADY]);
 
       // ---- E: TMEM -> chain rule, volume terms, + lift -> FP64 stage update
-      // in place (the I/O warp stores the buffers out) ----
+      // in place (the I/O warp stores the buffers out).  With few nodes per
+      // warp the volume terms (diff accumulators only) are formed first and
+      // kept in registers, so the wait for the lift MMA overlaps them ----
+      constexpr int CHK = S::NPQ < 8 ? S::NPQ : 8;   // TMEM columns per wait
+      constexpr int NCH = (S::NPQ + CHK - 1) / CHK;
+      constexpr bool VOL_FIRST = S::NPQ <= 16;
+      const int i_lo = part * S::NPQ;
+      const int i_hi = (part + 1) * S::NPQ < NP ? (part + 1) * S::NPQ : NP;
+      const int base = lf * F;
+      float vol[VOL_FIRST ? NCH * CHK : 1];
+      float gm[DIM][DIM];
+      float sdiff = a.op_scale_d;
+      if constexpr (VOL_FIRST) {
+        if (!warp_wait(&mbar[MB_DIFF], par)) {
+          if (lane == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+          bad = 1;
+          if (PT == PT_BF16) break;
+          continue;   // leaves at the next batch's barrier (or the loop's end)
+        }
+        tc::fence_after_sync();
+        const float* ge = sgeo + e_own * G;
+#pragma unroll
+        for (int r = 0; r < DIM; ++r)
+#pragma unroll
+          for (int x = 0; x < DIM; ++x) gm[r][x] = ge[r * DIM + x];
+        if constexpr (PT == PT_FP16) sdiff *= row_scale(rmx[row]);
+#pragma unroll
+        for (int kc = 0; kc < NCH; ++kc) {
+          const int c0 = i_lo + kc * CHK;
+          if (c0 >= i_hi) break;         // warp-uniform
+          float dv[DIM][CHK];
+#pragma unroll
+          for (int g = 0; g < CHK / 4; ++g)
+            if (c0 + 4 * g < i_hi)       // warp-uniform
+#pragma unroll
+              for (int r = 0; r < DIM; ++r)
+                tc::tmem_ld4(tmem_diff + lane_addr + r * NP + c0 + 4 * g,
+                             *reinterpret_cast<float(*)[4]>(&dv[r][4 * g]));
+          tc::tmem_wait_ld();
+#pragma unroll
+          for (int c = 0; c < CHK; ++c) {
+            const int i = c0 + c;
+            if (i >= i_hi) break;        // warp-uniform
+            float g[DIM];
+#pragma unroll
+            for (int x = 0; x < DIM; ++x) {
+              float t = 0.f;
+#pragma unroll
+              for (int r = 0; r < DIM; ++r) t += gm[r][x] * (dv[r][c] * sdiff + lin[r]);
+              g[x] = t;
+            }
+            const float cnode = C ? (float)scoef[e_own * NP + i] : 0.f;
+            vol[kc * CHK + c] = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
+          }
+        }
+      }
       // (FREADY also orders the flux row maxima the other warps wrote)
       const bool wf = PT == PT_BF16 || warp_wait(&mbar[MB_FREADY], par);
-      const bool w0 = wf && warp_wait(&mbar[MB_DIFF], par);
+      const bool w0 = wf && (VOL_FIRST || warp_wait(&mbar[MB_DIFF], par));
       const bool w1 = w0 && warp_wait(&mbar[MB_LIFT], par);
       const bool wr = !stage_res || (w1 && warp_wait(&mbar[MB_RES_FULL], par));
       if (!(w0 && w1 && wr)) {
@@ -942,35 +997,33 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
       }
       tc::fence_after_sync();
       {
-        const float* ge = sgeo + e_own * G;
-        float gm[DIM][DIM];
+        if constexpr (!VOL_FIRST) {
+          const float* ge = sgeo + e_own * G;
 #pragma unroll
-        for (int r = 0; r < DIM; ++r)
+          for (int r = 0; r < DIM; ++r)
 #pragma unroll
-          for (int x = 0; x < DIM; ++x) gm[r][x] = ge[r * DIM + x];
-        const int base = lf * F;
-        float sdiff = a.op_scale_d, slift = a.op_scale_l;
-        if constexpr (PT == PT_FP16) {
-          sdiff *= row_scale(rmx[row]);
-          slift *= row_scale(fmx[row]);   // written in C by the row's owner warp
+            for (int x = 0; x < DIM; ++x) gm[r][x] = ge[r * DIM + x];
+          if constexpr (PT == PT_FP16) sdiff *= row_scale(rmx[row]);
         }
+        float slift = a.op_scale_l;
+        if constexpr (PT == PT_FP16)
+          slift *= row_scale(fmx[row]);   // written in C by the row's owner warp
         double* qo = st + fown * FNP + e_own * NP;
         double* ro = rbuf + fown * FNP + e_own * NP;
         const int64_t gidx = fown * Knp + (el0 + e_own) * NP;
-        const int i_lo = part * S::NPQ;
-        const int i_hi = (part + 1) * S::NPQ < NP ? (part + 1) * S::NPQ : NP;
-        // TMEM columns are read CHK at a time (one wait per chunk)
-        constexpr int CHK = S::NPQ < 8 ? S::NPQ : 8;
-#pragma unroll 1
-        for (int c0 = i_lo; c0 < i_hi; c0 += CHK) {
+#pragma unroll
+        for (int kc = 0; kc < NCH; ++kc) {
+          const int c0 = i_lo + kc * CHK;
+          if (c0 >= i_hi) break;         // warp-uniform
           float dv[DIM][CHK], lv[CHK];
 #pragma unroll
           for (int g = 0; g < CHK / 4; ++g) {
-            if (c0 + 4 * g < i_hi) {   // warp-uniform
+            if (c0 + 4 * g < i_hi) {     // warp-uniform
+              if constexpr (!VOL_FIRST)
 #pragma unroll
-              for (int r = 0; r < DIM; ++r)
-                tc::tmem_ld4(tmem_diff + lane_addr + r * NP + c0 + 4 * g,
-                             *reinterpret_cast<float(*)[4]>(&dv[r][4 * g]));
+                for (int r = 0; r < DIM; ++r)
+                  tc::tmem_ld4(tmem_diff + lane_addr + r * NP + c0 + 4 * g,
+                               *reinterpret_cast<float(*)[4]>(&dv[r][4 * g]));
               tc::tmem_ld4(tmem_lift + lane_addr + c0 + 4 * g,
                            *reinterpret_cast<float(*)[4]>(&lv[4 * g]));
             }
@@ -980,16 +1033,21 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
           for (int c = 0; c < CHK; ++c) {
             const int i = c0 + c;
             if (i >= i_hi) break;        // warp-uniform
-            float g[DIM];
+            float mine;
+            if constexpr (VOL_FIRST) {
+              mine = vol[kc * CHK + c];
+            } else {
+              float g[DIM];
 #pragma unroll
-            for (int x = 0; x < DIM; ++x) {
-              float s = 0.f;
+              for (int x = 0; x < DIM; ++x) {
+                float t = 0.f;
 #pragma unroll
-              for (int r = 0; r < DIM; ++r) s += gm[r][x] * (dv[r][c] * sdiff + lin[r]);
-              g[x] = s;
+                for (int r = 0; r < DIM; ++r) t += gm[r][x] * (dv[r][c] * sdiff + lin[r]);
+                g[x] = t;
+              }
+              const float cnode = C ? (float)scoef[e_own * NP + i] : 0.f;
+              mine = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
             }
-            const float cnode = C ? (float)scoef[e_own * NP + i] : 0.f;
-            const float mine = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
             if (valid) {
               const float src = a.source ? (float)a.source[(el0 + e_own) * NP + i] : 0.f;
               const double rr =
