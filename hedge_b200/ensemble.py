@@ -275,12 +275,14 @@ def main(argv=None):
             peak = json.load(f).get("hbm_gbs")
     except (OSError, ValueError):
         pass
+    peak_source = "measured" if peak else "fallback"
+    peak = peak or 6650.0      # earlier STREAM-copy measurement on B200, GB/s
     gbs = ens.algorithmic_bytes_per_step() / (ms * 1e-3) / 1e9
     out = {"workload": "ensemble2d_%d_members" % a.members, "members": a.members,
            "dofs": info["dofs"], "steps": a.steps, "ms_per_step": ms,
            "dof_updates_per_s": ens.dof_updates_per_step() / (ms * 1e-3),
            "eager_ms_per_step": eager_ms, "achieved_gbs": gbs,
-           "peak_gbs": peak, "frac": gbs / peak if peak else None,
+           "peak_gbs": peak, "peak_source": peak_source, "frac": gbs / peak,
            "launch": info, "tiles": {"%d,%d,%d" % k: v for k, v in TILE_TABLE.items()},
            "autotune_s": t_tune,
            "autotune_ms": {"%d,%d,%d" % k: v for k, v in (tuned or {}).items()}}
