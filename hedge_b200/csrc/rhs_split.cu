@@ -1297,24 +1297,26 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
         v[c] = (valid && j < NP) ? (float)(q[c] - l) : 0.f;
       }
     };
-    // this warp's items are warp + k * NW (all in its TMEM quadrant), two
-    // at a time so that 16 state loads are in flight
-    static_assert((S::NITEM / S::NW) % 2 == 0, "items per warp must be even");
+    // this warp's items are warp + k * NW (all in its TMEM quadrant), NI
+    // at a time so that 8 NI state loads are in flight
+    constexpr int IPWS = S::NITEM / S::NW;
+    constexpr int NI = IPWS % 4 == 0 ? 4 : 2;
+    static_assert(IPWS % 2 == 0, "items per warp must be even");
     float inv = 1.0f;
     if constexpr (PT == PT_FP16) {
       // remainders once: row maxima, raw values parked in the planes
       uint32_t m = 0u;
 #pragma unroll 1
-      for (int k = 0; k < S::NITEM / S::NW; k += 2) {
-        const int c0 = (warp + k * S::NW) >> 2, c1 = (warp + (k + 1) * S::NW) >> 2;
-        float v0[8], v1[8];
-        rem8(c0, v0);
-        rem8(c1, v1);
+      for (int k = 0; k < IPWS; k += NI) {
+        float v[NI][8];
 #pragma unroll
-        for (int c = 0; c < 8; ++c)
-          m = max(m, max(__float_as_uint(fabsf(v0[c])), __float_as_uint(fabsf(v1[c]))));
-        park8(Aqh, Aql, kmajor_off(row, c0 * 8, KD), v0);
-        park8(Aqh, Aql, kmajor_off(row, c1 * 8, KD), v1);
+        for (int t = 0; t < NI; ++t) rem8((warp + (k + t) * S::NW) >> 2, v[t]);
+#pragma unroll
+        for (int t = 0; t < NI; ++t) {
+#pragma unroll
+          for (int c = 0; c < 8; ++c) m = max(m, __float_as_uint(fabsf(v[t][c])));
+          park8(Aqh, Aql, kmajor_off(row, ((warp + (k + t) * S::NW) >> 2) * 8, KD), v[t]);
+        }
       }
       atomicMax(&rmx[row], m);
       __syncthreads();
@@ -1596,7 +1598,7 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
 
     // ---- F: FP64 stage update (coalesced; UF values per thread in flight) ----
     {
-      constexpr int UF = 6;
+      constexpr int UF = 10;
       for (int x0 = tid; x0 < S::NVAL; x0 += UF * S::THREADS) {
         double r0[UF], q0[UF];
         int64_t idx[UF];
