@@ -1448,11 +1448,16 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
       for (int f = 0; f < F; ++f) fl[f] *= fscale;
       return true;
     };
+    // warps 1.. compute the fluxes (warp 0 drives the diff stream meanwhile);
+    // face point x of thread ct is ct + u * CT
+    constexpr int CT = S::THREADS - 32;
+    constexpr int NFVC = (S::NFACE + CT - 1) / CT;
+    const int ct = tid - 32;
     if constexpr (PT == PT_FP16) {
       // fluxes once: row maxima, raw values parked in the planes; then
       // every thread splits its own entries with the row scale
-      for (int u = 0; u < S::NFV; ++u) {
-        const int x = tid + u * S::THREADS;
+      for (int u = 0; u < NFVC && warp != 0; ++u) {
+        const int x = ct + u * CT;
         float fl[F];
         face_flux(x, fl);
         const int e = x < S::NFACE ? x / NFPT : -1;
@@ -1470,8 +1475,8 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
         }
       }
       __syncthreads();
-      for (int u = 0; u < S::NFV; ++u) {
-        const int x = tid + u * S::THREADS;
+      for (int u = 0; u < NFVC && warp != 0; ++u) {
+        const int x = ct + u * CT;
         const int e = x / NFPT, p = x % NFPT;
         if (x < S::NFACE && e < ne) {
           const int rowb = (e / EPW) * 32 + (e % EPW) * F;
@@ -1484,8 +1489,8 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
         }
       }
     } else {
-      for (int u = 0; u < S::NFV; ++u) {
-        const int x = tid + u * S::THREADS;
+      for (int u = 0; u < NFVC && warp != 0; ++u) {
+        const int x = ct + u * CT;
         float fl[F];
         face_flux(x, fl);
         const int e = x / NFPT, p = x % NFPT;
