@@ -123,7 +123,7 @@ struct Shape {
   static constexpr uint32_t oAfh = al128(oAql + bAq);
   static constexpr uint32_t oAfl = al128(oAfh + bAf);
   static constexpr uint32_t ostg = al128(oAfl + bAf);
-  static constexpr uint32_t SMALL = 1024 + NP * DIM * 8 + NFPT + 6 * NFP + 4 + 512 * 4 + 96;
+  static constexpr uint32_t SMALL = 1024 + NP * DIM * 8 + NFPT + 6 * NF * NFP + 4 + 512 * 4 + 96;
   // double-buffered stages and a residual buffer when they fit, else fewer
   static constexpr bool fits(int nstg, bool res) {
     return ostg + nstg * bStage + (res ? bState : 0) + SMALL <= SMEM_LIMIT;
@@ -133,8 +133,10 @@ struct Shape {
   static constexpr uint32_t ores = ostg + NSTG * bStage;
   static constexpr uint32_t olam = al16(ores + (RES ? bState : 0));   // FP64 weights
   static constexpr uint32_t ofm = al16(olam + NP * DIM * 8);           // uint8 fmask
-  static constexpr uint32_t osh = al16(ofm + NFPT);                    // uint8 shuffles
-  static constexpr uint32_t overt = al16(osh + 6 * NFP);               // uint8 vertex nodes
+  // uint8 neighbour node of face node k seen through (perm, neighbour face):
+  // fmask[nface][shuffle[perm][k]] at [(perm * NF + nface) * NFP + k]
+  static constexpr uint32_t osh = al16(ofm + NFPT);
+  static constexpr uint32_t overt = al16(osh + 6 * NF * NFP);          // uint8 vertex nodes
   // row maxima (FP16 planes): state rows [2][128] then flux rows [2][128]
   static constexpr uint32_t ors = al16(overt + 4);
   static constexpr uint32_t obar = al16(ors + 512 * 4);                // mbarriers + TMEM slot
@@ -474,7 +476,11 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
       for (int x = tid; x < NP * DIM; x += SPLIT_THREADS) lam[x] = lsrcd[x];
     }
     for (int x = tid; x < NFPT; x += SPLIT_THREADS) sfm[x] = (uint8_t)a.fmask[x];
-    for (int x = tid; x < a.nperm * NFP; x += SPLIT_THREADS) ssh[x] = (uint8_t)a.shuffle[x];
+    for (int x = tid; x < a.nperm * NF * NFP; x += SPLIT_THREADS) {
+      const int perm = x / (NF * NFP), r = x - perm * (NF * NFP);
+      const int nface = r / NFP, k = r - nface * NFP;
+      ssh[x] = (uint8_t)a.fmask[nface * NFP + a.shuffle[perm * NFP + k]];
+    }
     for (int x = tid; x < 512; x += SPLIT_THREADS) rsq[x] = 0u;
     if (tid == 0) {
       tc::mbar_init(&mbar[MB_DIFF], 1);
@@ -809,7 +815,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
               const int code = cn.y;
               const int nface = code & 3, perm = code >> 2;
               if (nface < NF && perm < a.nperm && nb < a.K) {
-                const int nn = sfm[nface * NFP + ssh[perm * NFP + k]];
+                const int nn = ssh[(perm * NF + nface) * NFP + k];
                 const int64_t gi = (int64_t)nb * NP + nn;
                 const int lnode = sfm[p];
                 const int lb = (int)(nb - el0);   // neighbour inside this batch?
