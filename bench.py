@@ -466,26 +466,52 @@ def run_ours(args):
     # ---- end to end through the public API with host buffers ----
     e2e = None
     if not args.no_e2e:
+        # Every step copies its input in from pinned host memory, advances it
+        # one LSRK4 step and copies the result back.  The steps are independent
+        # (the same host input each time), so they are pipelined: the copy in
+        # of step i+1 and the copy out of step i-1 (the two PCIe directions,
+        # each on its own stream) overlap the compute of step i.
         host_in = torch.from_numpy(np.ascontiguousarray(w0)).pin_memory()
-        host_out = torch.empty_like(host_in).pin_memory()
+        host_out = [torch.empty_like(host_in).pin_memory() for _ in range(2)]
+        dev_in = [torch.empty(host_in.shape, dtype=host_in.dtype, device=dev) for _ in range(2)]
+        s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        ev = lambda: torch.cuda.Event()  # noqa: E731
+        in_done, used, comp_done, out_done = ([ev(), ev()] for _ in range(4))
+
+        def e2e_run(n):
+            for i in range(n):
+                b = i & 1
+                with torch.cuda.stream(s_in):
+                    s_in.wait_event(used[b])       # step i-2 is done with dev_in[b]
+                    dev_in[b].copy_(host_in, non_blocking=True)
+                    in_done[b].record(s_in)
+                stream.wait_event(in_done[b])
+                yd = stepper(dev_in[b], 0.0, dt, rhs)
+                used[b].record(stream)
+                comp_done[b].record(stream)
+                with torch.cuda.stream(s_out):
+                    s_out.wait_event(comp_done[b])
+                    s_out.wait_event(out_done[b])  # host_out[b] of step i-2 was read
+                    yd.record_stream(s_out)
+                    host_out[b].copy_(yd, non_blocking=True)
+                    out_done[b].record(s_out)
+            stream.wait_stream(s_in)
+            stream.wait_stream(s_out)
+
         e2e_steps = max(1, min(args.steps, 10))
-        for _ in range(2):
-            yd = host_in.to(dev, non_blocking=True)
-            yd = stepper(yd, 0.0, dt, rhs)
-            host_out.copy_(yd, non_blocking=True)
+        e2e_run(2)
+        torch.cuda.synchronize(dev)
         barrier(world)
         ev0.record(stream)
-        for _ in range(e2e_steps):
-            yd = host_in.to(dev, non_blocking=True)
-            yd = stepper(yd, 0.0, dt, rhs)
-            host_out.copy_(yd, non_blocking=True)
+        e2e_run(e2e_steps)
         ev1.record(stream)
         barrier(world)
         e_ms = max_over_ranks(ev0.elapsed_time(ev1), world)
         nbytes = host_in.numel() * host_in.element_size()
         e2e = {"value": K_total * discr.Np * F * 5 * e2e_steps / (e_ms * 1e-3),
                "unit": "DOF-updates/s", "h2d_bytes_per_step": nbytes,
-               "d2h_bytes_per_step": nbytes, "steps": e2e_steps}
+               "d2h_bytes_per_step": nbytes, "steps": e2e_steps,
+               "overlap": "copy in / compute / copy out of consecutive steps on three streams"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
