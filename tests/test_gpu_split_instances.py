@@ -1,0 +1,53 @@
+"""Every compiled split-precision kernel instance (resident operators for
+3D orders <= 5 / 2D <= 6, streamed operators for 3D orders 6-7) on a small
+mesh against the FP64 oracle, in both split precisions: relative L2 of one
+RHS <= 1e-5 on rough fields (smooth modes + 10 % noise)."""
+import numpy as np
+import pytest
+
+import hedge_b200 as hb
+from conftest import rel_l2
+from test_gpu_parity import _fields, rect, box
+
+pytestmark = pytest.mark.gpu
+
+RESIDENT = [("advection", 2, o) for o in (3, 4, 5, 6)] + [("advection", 3, o) for o in (3, 4)] \
+    + [("wave", 2, o) for o in (3, 4, 5, 6)] + [("wave", 3, o) for o in (3, 4, 5)] \
+    + [("varwave", 2, o) for o in (3, 4, 5, 6)] + [("varwave", 3, o) for o in (3, 4)] \
+    + [("maxwell", 3, o) for o in (3, 4, 5)]
+STREAMED = [("wave", 3, 6), ("wave", 3, 7), ("maxwell", 3, 6)]
+
+
+def _case(model, dim, order):
+    d = hb.Discretization(rect(5, False, 0.03, 1) if dim == 2 else box(2, 0.04, 2),
+                          order=order)
+    bc = c = None
+    if model == "advection":
+        op = hb.StrongAdvectionOperator(np.array([0.8, -0.5, 0.3][:dim]), flux_type="upwind",
+                                        inflow_tag=hb.TAG_ALL)
+        bc = np.sin(2 * d.get_boundary(hb.TAG_ALL).nodes[:, 0])
+    elif model == "wave":
+        op = hb.StrongWaveOperator(1.1, dim, flux_type="upwind")
+    elif model == "varwave":
+        c = np.repeat(np.random.default_rng(3).uniform(0.8, 1.2, d.K), d.Np)
+        op = hb.VariableVelocityStrongWaveOperator(c, dim, flux_type="upwind")
+    else:
+        op = hb.MaxwellOperator(1.0, 1.0, flux_type=1)
+    return d, op, bc, c
+
+
+@pytest.mark.parametrize("precision", ["fp16x3", "bf16x3"])
+@pytest.mark.parametrize("model,dim,order", RESIDENT + STREAMED)
+def test_split_instance(cuda_device, model, dim, order, precision):
+    from oracle import OracleRHS
+    d, op, bc, c = _case(model, dim, order)
+    comp = d.compile(op.op_template(), precision=precision)
+    if c is not None:
+        comp.set_coefficient(c)
+    q = _fields(d, op.descriptor().n_fields, 7)
+    ref = OracleRHS(d, op.descriptor(), c_field=c)(q, bc_in=bc)
+    got = comp(w=q, bc_in=bc)
+    comp.check()
+    err = rel_l2(got.cpu().numpy().reshape(ref.shape), ref)
+    print("%s %s %dD N=%d rel-L2 %.3e" % (precision, model, dim, order, err))
+    assert err <= 1e-5
