@@ -155,3 +155,23 @@ def test_split_stream_pulse_steps(cuda_device):
     err5 = rel_l2(y.cpu().numpy(), ref)
     print("fp16x3 wave3d N=7 pulse: 5 steps rel-L2 %.3e" % err5)
     assert err5 <= 5e-6, err5
+
+
+@pytest.mark.parametrize("precision", PRECS)
+def test_split_fields_of_very_different_magnitude(cuda_device, precision):
+    """E ~ 1e4 and H ~ 1e-4: every (element, field) row has its own FP16
+    scale, so each field keeps its relative accuracy."""
+    from oracle import OracleRHS
+    d = hb.Discretization(box(2, 0.05, 5), order=4)
+    op = hb.MaxwellOperator(1.0, 1.0, flux_type=1)
+    q = _fields(d, 6, 3)
+    q[:3] *= 1e4
+    q[3:] *= 1e-4
+    comp = d.compile(op.op_template(), precision=precision)
+    got = comp(w=q).cpu().numpy()
+    comp.check()
+    ref = OracleRHS(d, op.descriptor())(q)
+    for f in range(6):
+        err = rel_l2(got[f], ref[f])
+        print("%s field %d rel-L2 %.3e" % (precision, f, err))
+        assert err <= TOL[precision]
