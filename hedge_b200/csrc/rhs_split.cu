@@ -93,7 +93,31 @@ struct Shape {
   static constexpr int KD = ru16(NP), KL = ru16(NFPT);
   static constexpr int ND = ru16(DIM * NP), NL = ru16(NP);
   static constexpr int LIFT_COL = ru32(ND);
-  static constexpr int FNP = EB * NP;              // values of one field in a batch
+  // Field stride (in doubles) of the staged state and residual: the EB * NP
+  // values of a field, padded so that the consumer lanes' rows (lane =
+  // element * F + field) at one node hit distinct shared-memory banks as far
+  // as the layout allows (worst lanes per 8-byte bank pair in a half-warp).
+  static constexpr int bank_collisions(int stride) {
+    int worst = 0;
+    for (int half = 0; half < 2; ++half) {
+      int count[16] = {};
+      for (int l = 16 * half; l < 16 * half + 16; ++l) {
+        if (l / F >= EPW) continue;
+        const int b = ((l % F) * stride + (l / F) * NP) % 16;
+        if (++count[b] > worst) worst = count[b];
+      }
+    }
+    return worst;
+  }
+  static constexpr int padded_fnp() {
+    int best = EB * NP, bw = bank_collisions(EB * NP);
+    for (int p = 2; p < 32; p += 2) {
+      const int c = bank_collisions(EB * NP + p);
+      if (c < bw) { bw = c; best = EB * NP + p; }
+    }
+    return best;
+  }
+  static constexpr int FNP = padded_fnp();        // >= EB * NP, even (16-byte rows)
   static constexpr int NVAL = F * FNP;
   static constexpr int NFACE = EB * NFPT;
   static constexpr int NFV = (NFACE + CONSUMERS - 1) / CONSUMERS;
