@@ -158,6 +158,26 @@ class DistExchange:
                 req.wait()
 
 
+def sum_over_ranks(value, group=None, device=None):
+    """A float summed over the ranks of ``group`` (all-reduce); the value
+    itself without an initialised process group.  NCCL reduces a tensor on
+    ``device``, other backends on the host."""
+    import torch.distributed as dist
+    torch = _torch()
+    if not (dist.is_available() and dist.is_initialized()):
+        return float(value)
+    on_dev = dist.get_backend(group) == "nccl"
+    t = torch.tensor([float(value)], dtype=torch.float64,
+                     device=device if on_dev else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return float(t.item())
+
+
+def partitioned_norm(parts, qs):
+    """Energy norm of a field held as several parts in one process."""
+    return sum(p.norm_sq(q) for p, q in zip(parts, qs)) ** 0.5
+
+
 class LocalExchange:
     """All parts in one process (one device): copies each source's send
     slice into each destination's halo slice.  ``parts`` are the
@@ -310,3 +330,22 @@ class PartitionedOperator:
 
     def check(self):
         _native.check(self.lib.hb_op_check(self._h, self._stream()))
+
+    # -- reductions ------------------------------------------------------------
+    def norm_sq(self, q):
+        """Squared energy norm of this part's elements, all fields:
+        sum_k |J_k| q_k^T M q_k, FP64 on the device (hb_norm)."""
+        torch = _torch()
+        qq = q.reshape(self.F, -1).contiguous()
+        out = torch.empty(1, dtype=torch.float64, device=self.device)
+        _native.check(self.lib.hb_norm(self._dh, self.F,
+                                       0 if qq.dtype == torch.float64 else 1,
+                                       qq.data_ptr(), out.data_ptr(), self._stream()))
+        return float(out.item()) ** 2
+
+    def norm(self, q, group=None):
+        """Energy norm of the whole partitioned field: every rank's squared
+        norm summed over the ranks (all-reduce; NCCL between GPUs), then the
+        square root -- the reference's nodal sum plus allreduce
+        (backends/mpi/__init__.py:266-280)."""
+        return sum_over_ranks(self.norm_sq(q), group, self.device) ** 0.5

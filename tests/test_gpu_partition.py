@@ -102,3 +102,18 @@ def test_halo_op_refusals(cuda_device):
     od = op_descriptor(model.descriptor(), _native.PREC_FP64, part.conn, 0,
                        max(part.n_halo_faces - 1, 0))
     assert lib.hb_op_create(p._dh, C.byref(od), C.byref(h)) == _native.HB_ERR_INVALID_ARGUMENT
+
+
+def test_partitioned_norm_equals_global(cuda_device):
+    """Per-part squared energy norms summed (as the all-reduce does across
+    ranks) equal the norm of the whole field."""
+    from hedge_b200.partition import partitioned_norm, sum_over_ranks
+    d, model, plan, parts, ex = _setup("maxwell", 3, "fp64")
+    q = np.random.default_rng(5).standard_normal((6, len(d)))
+    want = d.norm(d.to_device(q))
+    got = partitioned_norm(parts, [p.scatter(q) for p in parts])
+    assert abs(got - want) <= 1e-13 * want
+    # without a process group, a part's norm is its own
+    x = parts[0].scatter(q)
+    assert sum_over_ranks(parts[0].norm_sq(x)) == parts[0].norm_sq(x)
+    assert abs(parts[0].norm(x) - parts[0].norm_sq(x) ** 0.5) <= 1e-15 * parts[0].norm(x)

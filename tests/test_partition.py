@@ -95,6 +95,7 @@ def test_partition_is_balanced():
 
 
 def _gloo_worker(rank, world, port, result_path):
+    """One gloo rank: face-trace exchange and the rank sum of norms."""
     import torch
     import torch.distributed as dist
     from hedge_b200.partition import DistExchange
@@ -114,6 +115,9 @@ def _gloo_worker(rank, world, port, result_path):
         halo = torch.zeros((p.n_halo_faces * d.Nfp, F), dtype=torch.float64)
         DistExchange(plan, rank)(send, halo)
         ok = np.array_equal(halo.numpy(), q[:, p.halo_global].T)
+        # the norm reduction: every rank's share summed over the ranks
+        from hedge_b200.partition import sum_over_ranks
+        ok = ok and sum_over_ranks(float(rank + 1)) == world * (world + 1) / 2
         with open("%s.%d" % (result_path, rank), "w") as fh:
             fh.write("ok" if ok else "mismatch")
     finally:
