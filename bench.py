@@ -249,9 +249,22 @@ def cpu_baseline(discr, op, w0, dt, threads=None, F=6):
     _, el1 = stage_time(1, 1)
     orc_mod.set_threads(ncores)
     return {"value": dofs / el, "unit": "DOF-updates/s", "cores": used,
-            "kind": "port", "single_thread_value": dofs / el1,
+            "cpu_model": cpu_model(), "kind": "port", "single_thread_value": dofs / el1,
             "sample": "one LSRK stage (RHS + update) over the full K=%d mesh, "
                       "%d OpenMP threads, best of 3; C++ oracle -O3" % (discr.K, used)}, el
+
+
+def cpu_model():
+    """The host CPU's model name (Linux /proc/cpuinfo), else the platform's."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or platform.machine()
 
 
 def run_reference(args):
@@ -304,7 +317,7 @@ def run_reference(args):
                    "K": discr.K, "order": args.order, "fields": F,
                    "step": "one LSRK stage per step"},
         "cpu_baseline": {"value": v, "unit": "DOF-updates/s", "cores": used,
-                         "kind": "port",
+                         "cpu_model": cpu_model(), "kind": "port",
                          "sample": "one LSRK stage over the full mesh per step; C++ "
                                    "oracle (restated jit loops), OpenMP"},
         "e2e": {"value": v, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0,
