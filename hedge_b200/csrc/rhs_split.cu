@@ -372,6 +372,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, uint32_t bytes) {
                ::"r"(tc::smem_u32(mbar)), "r"(bytes)
                : "memory");
 }
+// pull a 16-byte-aligned range into L2 in the background (no destination)
+__device__ __forceinline__ void prefetch_l2(const void* gsrc, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(gsrc), "r"(bytes) : "memory");
+}
 // one arrival on `mbar` that also announces `bytes` of transactions
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
@@ -1393,6 +1397,22 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
     if (warp == 0) {
       int ok = 1;
       if (lane == 0) {
+        // L2 prefetch of the next batch's state (its remainders) and of this
+        // batch's residual (the stage update), overlapping this batch's work
+        const int64_t nxt = batch + gridDim.x;
+        if (nxt < a.nbatch) {
+          const int64_t n0 = nxt * EB;
+          const int nn = (int)((a.K - n0) < EB ? (a.K - n0) : EB);
+          for (int f = 0; f < F; ++f) {
+            const double* src = a.q_in + f * Knp + n0 * NP;
+            if (aligned16(src, (uint32_t)(nn * NP * 8))) prefetch_l2(src, (uint32_t)(nn * NP * 8));
+          }
+        }
+        if (a.mode != 0)
+          for (int f = 0; f < F; ++f) {
+            const double* src = a.res + f * Knp + el0 * NP;
+            if (aligned16(src, (uint32_t)(ne * NP * 8))) prefetch_l2(src, (uint32_t)(ne * NP * 8));
+          }
         const uint32_t aq_h = tc::smem_u32(Aqh), aq_l = tc::smem_u32(Aql);
         ok = stream_chunks(dimg, S::NKD, 2 * S::bDc, [&](int kk, uint32_t buf) {
           const uint32_t bh = buf, bl = buf + S::bDc;
