@@ -650,6 +650,20 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
     for (int64_t i = 0; i < nb_cta; ++i) {
       const int b = NSTG == 2 ? (int)(i & 1) : 0;
       if (NSTG == 2 && i + 1 < nb_cta) load_stage(i + 1);   // its buffer was stored out
+      // L2 prefetch of the state two batches ahead and of the next residual,
+      // so that their bulk loads are served from L2
+      if (lane == 0) {
+        for (int64_t j = i + 1; j <= i + 2 && j < nb_cta; ++j) {
+          const int64_t e0 = batch_el0(j);
+          const uint32_t bytes = (uint32_t)batch_ne(e0) * NP * 8u;
+          for (int f = 0; f < F; ++f) {
+            const double* q = a.q_in + f * Knp + e0 * NP;
+            if (j == i + 2 && aligned16(q, bytes)) prefetch_l2(q, bytes);
+            const double* r = a.res + f * Knp + e0 * NP;
+            if (j == i + 1 && stage_res && aligned16(r, bytes)) prefetch_l2(r, bytes);
+          }
+        }
+      }
       // results: the stage buffer holds q_out (or the rhs), the residual buffer res
       if (!warp_wait(&mbar[MB_DONE + b], (uint32_t)((i / NSTG) & 1))) {
         ok = false;
