@@ -11,9 +11,10 @@ from test_gpu_parity import _fields, rect, box
 pytestmark = pytest.mark.gpu
 
 # Tolerance of one split-precision RHS against the FP64 oracle (relative L2)
-# on rough fields (smooth modes + 10% uniform noise: large face jumps, where
-# the BF16 lift contraction dominates the error of both variants)
-TOL = {"bf16x3": 1e-5, "fp16x3": 1e-5}
+# on rough fields (smooth modes + 10% uniform noise: large face jumps).  The
+# scaled FP16 split meets the 1e-6 contract on every case (worst 6e-7, wave
+# N = 7); BF16x3 resolves 16 bits per plane and stays within 1e-5.
+TOL = {"bf16x3": 1e-5, "fp16x3": 1e-6}
 # ... and on the benchmark's smooth cavity field, where the differentiation
 # dominates and the scaled FP16 split meets 1e-6
 TOL_SMOOTH = {"bf16x3": 1e-5, "fp16x3": 1e-6}
@@ -83,9 +84,13 @@ def test_split_cavity_rhs(cuda_device, precision):
     assert err <= TOL_SMOOTH[precision]
 
 
+@pytest.mark.parametrize("dt_factor", [1.0, 0.5])
 @pytest.mark.parametrize("precision", PRECS)
-def test_split_lsrk_steps(cuda_device, precision):
-    """Fused split RHS + FP64 stage update over 5 steps vs the FP64 oracle."""
+def test_split_lsrk_steps(cuda_device, precision, dt_factor):
+    """Fused split RHS + FP64 stage update over 5 steps vs the FP64 oracle, at
+    the CFL estimate and at half of it (the estimate lies beyond the LSRK4
+    stability limit of the upwind Maxwell operator at N = 4, which amplifies
+    the rounding differences)."""
     import torch
     from oracle import OracleRHS
     d = hb.Discretization(box(2, 0.05, 1), order=4, precision=precision)
@@ -94,7 +99,7 @@ def test_split_lsrk_steps(cuda_device, precision):
     x = d.nodes
     q = np.stack([np.sin(np.pi * x[:, (f + 1) % 3] / 2) * np.cos(0.5 * x[:, f % 3])
                   for f in range(6)])
-    dt = op.estimate_timestep(d)
+    dt = dt_factor * op.estimate_timestep(d)
     y = d.to_device(q).reshape(6, -1)
     orc = OracleRHS(d, op.op_template())
     yo, res = q.copy(), np.zeros_like(q)
@@ -104,8 +109,9 @@ def test_split_lsrk_steps(cuda_device, precision):
         yo, res = orc.lsrk4_step(yo, s * dt, dt, res)
     rhs.compiled.check()
     err = rel_l2(y.cpu().numpy().reshape(yo.shape), yo)
-    print("%s 5 LSRK4 steps rel-L2 %.3e" % (precision, err))
-    assert err <= 2e-4
+    print("%s 5 LSRK4 steps at %.1f dt rel-L2 %.3e" % (precision, dt_factor, err))
+    # within the stability limit the steps keep one RHS's accuracy
+    assert err <= (2e-4 if dt_factor == 1.0 else TOL[precision])
 
 
 # ---- streamed-operator variant (3D, N >= 6: operator planes stream through

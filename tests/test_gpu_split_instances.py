@@ -1,7 +1,8 @@
 """Every compiled split-precision kernel instance (resident operators for
 3D orders <= 5 / 2D <= 6, streamed operators for 3D orders 6-7) on a small
 mesh against the FP64 oracle, in both split precisions: relative L2 of one
-RHS <= 1e-5 on rough fields (smooth modes + 10 % noise)."""
+RHS on rough fields (smooth modes + 10 % noise) <= 1e-6 for FP16x3 and
+<= 1e-5 for BF16x3."""
 import numpy as np
 import pytest
 
@@ -50,4 +51,4 @@ def test_split_instance(cuda_device, model, dim, order, precision):
     comp.check()
     err = rel_l2(got.cpu().numpy().reshape(ref.shape), ref)
     print("%s %s %dD N=%d rel-L2 %.3e" % (precision, model, dim, order, err))
-    assert err <= 1e-5
+    assert err <= (1e-6 if precision == "fp16x3" else 1e-5)
