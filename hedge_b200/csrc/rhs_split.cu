@@ -171,7 +171,12 @@ struct Shape {
   static constexpr uint32_t obar = al16(ors + 512 * 4);                // mbarriers + TMEM slot
   static constexpr uint32_t total = al16(obar + 96);
   static constexpr uint32_t LIN_BYTES = 8 + NP * DIM * 8;  // vertex nodes + weights (image)
-  static constexpr int TMEM_NEED = LIFT_COL + NL + 4;
+  // epilogue: with at most 16 nodes per warp the volume terms are formed
+  // before the lift MMA completes and parked in TMEM columns [VCOL, ...),
+  // NPQ per consumer part of a lane quadrant
+  static constexpr bool PARK = NPQ <= 16;
+  static constexpr int VCOL = LIFT_COL + NL + 4;
+  static constexpr int TMEM_NEED = VCOL + (PARK ? (NCW / 4) * NPQ : 0);
   static constexpr uint32_t TMEM_COLS = TMEM_NEED <= 32 ? 32 : TMEM_NEED <= 64 ? 64
                                         : TMEM_NEED <= 128 ? 128 : TMEM_NEED <= 256 ? 256 : 512;
   static constexpr bool FITS = ND <= 256 && NL <= 256 && TMEM_NEED <= 512 &&
@@ -986,15 +991,19 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
 
       // ---- E: TMEM -> chain rule, volume terms, + lift -> FP64 stage update
       // in place (the I/O warp stores the buffers out).  With few nodes per
-      // warp the volume terms (diff accumulators only) are formed first and
-      // kept in registers, so the wait for the lift MMA overlaps them ----
+      // warp (S::PARK) the volume terms (diff accumulators only) are formed
+      // first, 4 nodes per pass, and parked in this warp's own TMEM columns,
+      // so the wait for the lift MMA overlaps them and both loops stay rolled
+      // up (a small instruction footprint) ----
       constexpr int CHK = S::NPQ < 8 ? S::NPQ : 8;   // TMEM columns per wait
       constexpr int NCH = (S::NPQ + CHK - 1) / CHK;
-      constexpr bool VOL_FIRST = S::NPQ <= 16;
+      constexpr bool VOL_FIRST = S::PARK;
       const int i_lo = part * S::NPQ;
       const int i_hi = (part + 1) * S::NPQ < NP ? (part + 1) * S::NPQ : NP;
       const int base = lf * F;
-      float vol[VOL_FIRST ? NCH * CHK : 1];
+      // parked volume terms: columns [VCOL + i_lo, VCOL + i_lo + NPQ), this
+      // warp's lanes only
+      const uint32_t tmem_vol = tmem + S::VCOL + lane_addr;
       float gm[DIM][DIM];
       float sdiff = a.op_scale_d;
       if constexpr (VOL_FIRST) {
@@ -1011,21 +1020,14 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
 #pragma unroll
           for (int x = 0; x < DIM; ++x) gm[r][x] = ge[r * DIM + x];
         if constexpr (PT == PT_FP16) sdiff *= row_scale(rmx[row]);
+#pragma unroll 1
+        for (int c0 = i_lo; c0 < i_hi; c0 += 4) {
+          float dv[DIM][4], v4[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-        for (int kc = 0; kc < NCH; ++kc) {
-          const int c0 = i_lo + kc * CHK;
-          if (c0 >= i_hi) break;         // warp-uniform
-          float dv[DIM][CHK];
-#pragma unroll
-          for (int g = 0; g < CHK / 4; ++g)
-            if (c0 + 4 * g < i_hi)       // warp-uniform
-#pragma unroll
-              for (int r = 0; r < DIM; ++r)
-                tc::tmem_ld4(tmem_diff + lane_addr + r * NP + c0 + 4 * g,
-                             *reinterpret_cast<float(*)[4]>(&dv[r][4 * g]));
+          for (int r = 0; r < DIM; ++r) tc::tmem_ld4(tmem_diff + lane_addr + r * NP + c0, dv[r]);
           tc::tmem_wait_ld();
 #pragma unroll
-          for (int c = 0; c < CHK; ++c) {
+          for (int c = 0; c < 4; ++c) {
             const int i = c0 + c;
             if (i >= i_hi) break;        // warp-uniform
             float g[DIM];
@@ -1037,9 +1039,11 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
               g[x] = t;
             }
             const float cnode = C ? (float)scoef[e_own * NP + i] : 0.f;
-            vol[kc * CHK + c] = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
+            v4[c] = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
           }
+          tc::tmem_st4(tmem_vol + c0, v4);
         }
+        tc::tmem_wait_st();
       }
       // (FREADY also orders the flux row maxima the other warps wrote)
       const bool wf = PT == PT_BF16 || warp_wait(&mbar[MB_FREADY], par);
@@ -1068,32 +1072,58 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
         double* qo = st + fown * FNP + e_own * NP;
         double* ro = rbuf + fown * FNP + e_own * NP;
         const int64_t gidx = fown * Knp + (el0 + e_own) * NP;
+        // rhs of node i -> stage update in place (or the rhs itself)
+        auto finish = [&](int i, float mine, float lift) {
+          if (valid) {
+            const float src = a.source ? (float)a.source[(el0 + e_own) * NP + i] : 0.f;
+            const double rr =
+                (double)model_finish<MODEL, DIM, float>(a.mp, fown, mine, lift * slift, src);
+            if (a.mode == 0) {
+              qo[i] = rr;
+            } else {
+              const double r0 = S::RES ? ro[i] : a.res[gidx + i];
+              const double nr = a.ra * r0 + a.dt * rr;
+              if constexpr (S::RES) ro[i] = nr;
+              else a.res[gidx + i] = nr;
+              qo[i] = qo[i] + a.rb * nr;
+            }
+          }
+        };
+        if constexpr (VOL_FIRST) {
+#pragma unroll 1
+          for (int c0 = i_lo; c0 < i_hi; c0 += 4) {
+            float lv[4], v4[4];
+            tc::tmem_ld4(tmem_lift + lane_addr + c0, lv);
+            tc::tmem_ld4(tmem_vol + c0, v4);
+            tc::tmem_wait_ld();
 #pragma unroll
-        for (int kc = 0; kc < NCH; ++kc) {
-          const int c0 = i_lo + kc * CHK;
-          if (c0 >= i_hi) break;         // warp-uniform
-          float dv[DIM][CHK], lv[CHK];
+            for (int c = 0; c < 4; ++c) {
+              if (c0 + c >= i_hi) break;   // warp-uniform
+              finish(c0 + c, v4[c], lv[c]);
+            }
+          }
+        } else {
 #pragma unroll
-          for (int g = 0; g < CHK / 4; ++g) {
-            if (c0 + 4 * g < i_hi) {     // warp-uniform
-              if constexpr (!VOL_FIRST)
+          for (int kc = 0; kc < NCH; ++kc) {
+            const int c0 = i_lo + kc * CHK;
+            if (c0 >= i_hi) break;         // warp-uniform
+            float dv[DIM][CHK], lv[CHK];
+#pragma unroll
+            for (int g = 0; g < CHK / 4; ++g) {
+              if (c0 + 4 * g < i_hi) {     // warp-uniform
 #pragma unroll
                 for (int r = 0; r < DIM; ++r)
                   tc::tmem_ld4(tmem_diff + lane_addr + r * NP + c0 + 4 * g,
                                *reinterpret_cast<float(*)[4]>(&dv[r][4 * g]));
-              tc::tmem_ld4(tmem_lift + lane_addr + c0 + 4 * g,
-                           *reinterpret_cast<float(*)[4]>(&lv[4 * g]));
+                tc::tmem_ld4(tmem_lift + lane_addr + c0 + 4 * g,
+                             *reinterpret_cast<float(*)[4]>(&lv[4 * g]));
+              }
             }
-          }
-          tc::tmem_wait_ld();
+            tc::tmem_wait_ld();
 #pragma unroll
-          for (int c = 0; c < CHK; ++c) {
-            const int i = c0 + c;
-            if (i >= i_hi) break;        // warp-uniform
-            float mine;
-            if constexpr (VOL_FIRST) {
-              mine = vol[kc * CHK + c];
-            } else {
+            for (int c = 0; c < CHK; ++c) {
+              const int i = c0 + c;
+              if (i >= i_hi) break;        // warp-uniform
               float g[DIM];
 #pragma unroll
               for (int x = 0; x < DIM; ++x) {
@@ -1103,21 +1133,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
                 g[x] = t;
               }
               const float cnode = C ? (float)scoef[e_own * NP + i] : 0.f;
-              mine = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
-            }
-            if (valid) {
-              const float src = a.source ? (float)a.source[(el0 + e_own) * NP + i] : 0.f;
-              const double rr =
-                  (double)model_finish<MODEL, DIM, float>(a.mp, fown, mine, lv[c] * slift, src);
-              if (a.mode == 0) {
-                qo[i] = rr;
-              } else {
-                const double r0 = S::RES ? ro[i] : a.res[gidx + i];
-                const double nr = a.ra * r0 + a.dt * rr;
-                if constexpr (S::RES) ro[i] = nr;
-                else a.res[gidx + i] = nr;
-                qo[i] = qo[i] + a.rb * nr;
-              }
+              finish(i, volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode), lv[c]);
             }
           }
         }
