@@ -52,3 +52,39 @@ def test_split_instance(cuda_device, model, dim, order, precision):
     err = rel_l2(got.cpu().numpy().reshape(ref.shape), ref)
     print("%s %s %dD N=%d rel-L2 %.3e" % (precision, model, dim, order, err))
     assert err <= (1e-6 if precision == "fp16x3" else 1e-5)
+
+
+@pytest.mark.parametrize("precision", ["fp16x3", "bf16x3"])
+@pytest.mark.parametrize("model,dim,order", RESIDENT + STREAMED)
+def test_split_instance_stage(cuda_device, model, dim, order, precision):
+    """One fused LSRK stage of every instance against the oracle's RHS:
+    res1 = a res0 + dt RHS(q0) and q1 = q0 + b res1, with a residual of the
+    size of dt RHS (the FP64 update reads it from shared memory or HBM,
+    depending on the instance)."""
+    import torch
+    from oracle import OracleRHS
+    d, op, bc, c = _case(model, dim, order)
+    comp = d.compile(op.op_template(), precision=precision)
+    F = op.descriptor().n_fields
+    q0 = _fields(d, F, 8)
+    rhs = OracleRHS(d, op.descriptor(), c_field=c)(q0, bc_in=bc).reshape(F, -1)
+    a, b, dt = -0.4, 0.6, 0.01
+    res0 = dt * np.abs(rhs).max() * np.random.default_rng(9).uniform(-1, 1, rhs.shape)
+    ref_res = a * res0 + dt * rhs
+    ref_q = q0 + b * ref_res
+    dev = d.device
+    q_in = torch.tensor(q0, device=dev)
+    q_out = torch.empty_like(q_in)
+    res = torch.tensor(res0, device=dev)
+    cf = torch.tensor(c, device=dev) if c is not None else None
+    bt = torch.tensor(bc, device=dev) if bc is not None else None
+    comp.lsrk_stage(a, b, dt, q_in, q_out, res, bc_in=bt, coeff=cf)
+    comp.check()
+    r1 = res.cpu().numpy()
+    e_res = rel_l2(r1, ref_res)
+    # the FP64 update itself: q1 = q0 + b res1 with the kernel's own res1
+    e_q = rel_l2(q_out.cpu().numpy(), q0 + b * r1)
+    print("%s %s %dD N=%d stage: res rel-L2 %.3e, q rel-L2 %.3e (vs oracle %.3e)"
+          % (precision, model, dim, order, e_res, e_q, rel_l2(q_out.cpu().numpy(), ref_q)))
+    assert e_res <= (2e-6 if precision == "fp16x3" else 2e-5)
+    assert e_q <= 1e-14
