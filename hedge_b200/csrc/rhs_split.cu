@@ -171,11 +171,11 @@ struct Shape {
   static constexpr uint32_t obar = al16(ors + 512 * 4);                // mbarriers + TMEM slot
   static constexpr uint32_t total = al16(obar + 96);
   static constexpr uint32_t LIN_BYTES = 8 + NP * DIM * 8;  // vertex nodes + weights (image)
-  // epilogue: with at most 16 nodes per warp the volume terms are formed
-  // before the lift MMA completes and parked in TMEM columns [VCOL, ...),
-  // NPQ per consumer part of a lane quadrant
-  static constexpr bool PARK = NPQ <= 16;
+  // epilogue: the volume terms are formed before the lift MMA completes and
+  // parked in TMEM columns [VCOL, ...), NPQ per consumer part of a lane
+  // quadrant, wherever those columns fit in TMEM
   static constexpr int VCOL = LIFT_COL + NL + 4;
+  static constexpr bool PARK = VCOL + (NCW / 4) * NPQ <= 512;
   static constexpr int TMEM_NEED = VCOL + (PARK ? (NCW / 4) * NPQ : 0);
   static constexpr uint32_t TMEM_COLS = TMEM_NEED <= 32 ? 32 : TMEM_NEED <= 64 ? 64
                                         : TMEM_NEED <= 128 ? 128 : TMEM_NEED <= 256 ? 256 : 512;
