@@ -117,3 +117,31 @@ def test_partitioned_norm_equals_global(cuda_device):
     x = parts[0].scatter(q)
     assert sum_over_ranks(parts[0].norm_sq(x)) == parts[0].norm_sq(x)
     assert abs(parts[0].norm(x) - parts[0].norm_sq(x) ** 0.5) <= 1e-15 * parts[0].norm(x)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp16x3", "bf16x3"])
+def test_partitioned_maxwell_n5(cuda_device, precision):
+    """3D N = 5: an operator without halo faces takes the streamed-operator
+    split kernel, the parts (with halo faces) the resident one; each part's
+    RHS against the oracle on its elements."""
+    from oracle import OracleRHS
+    from hedge_b200.partition import LocalExchange, PartitionPlan, PartitionedOperator
+    from test_gpu_parity import _fields
+    d = hb.Discretization(hb.make_box_tet_mesh(n=(2, 2, 2), jitter=0.03, seed=5), order=5)
+    model = hb.MaxwellOperator(1.0, 1.0, flux_type=1)
+    plan = PartitionPlan(d, model.op_template(), 3)
+    parts = [PartitionedOperator(d, model, plan, r, precision=precision) for r in range(3)]
+    ex = LocalExchange(plan, parts)
+    q = _fields(d, 6, 12)
+    ref = OracleRHS(d, model.op_template())(q).reshape(6, -1)
+    tol = {"fp64": 1e-12, "fp16x3": 1e-6, "bf16x3": 1e-5}[precision]
+    ql = [p.scatter(q) for p in parts]
+    for p, x in zip(parts, ql):
+        p.pack(x)
+    ex.exchange_all()
+    for p, x in zip(parts, ql):
+        got = p.rhs(x, exchanged=True)
+        p.check()
+        err = rel_l2(got.double().cpu().numpy(), ref[:, p.local_nodes()])
+        print("%s maxwell N=5 part rel-L2 %.3e" % (precision, err))
+        assert err <= tol
