@@ -13,7 +13,7 @@ from .models import (StrongAdvectionOperator, WeakAdvectionOperator, StrongWaveO
                      make_tdep_constant, TimeConstantGivenFunction,
                      TimeDependentGivenFunction)
 from .discretization import Discretization, CompiledOperator, BoundRHS
-from .timestep import LSRK4TimeStepper, RK4TimeStepper
+from .timestep import GraphedLSRK4, LSRK4TimeStepper, RK4TimeStepper
 from .nd_calculus import GradientOperator, DivergenceOperator
 from .visualization import VtkVisualizer, LegacyVtkVisualizer
 
@@ -23,6 +23,6 @@ __all__ = [
     "StrongAdvectionOperator", "WeakAdvectionOperator", "StrongWaveOperator",
     "VariableVelocityStrongWaveOperator", "MaxwellOperator", "make_tdep_constant",
     "TimeConstantGivenFunction", "TimeDependentGivenFunction", "Discretization", "CompiledOperator", "BoundRHS",
-    "LSRK4TimeStepper", "RK4TimeStepper", "GradientOperator", "DivergenceOperator",
+    "LSRK4TimeStepper", "RK4TimeStepper", "GraphedLSRK4", "GradientOperator", "DivergenceOperator",
     "VtkVisualizer", "LegacyVtkVisualizer",
 ]
