@@ -1152,7 +1152,8 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
 
 // ---------------------------------------------------------------------------
 // Streamed-operator variant for high orders, whose operator planes do not fit
-// in shared memory next to the data planes (3D, N >= 6).  Same contraction
+// in shared memory next to the data planes (3D, N >= 6), or leave room for a
+// single state stage only (3D, N = 5, operators without halo faces).  Same contraction
 // layout, split, epilogue and stage update as rhs_split_kernel; differences:
 //   * the operator planes stream from global memory (L2-resident) through a
 //     two-buffer ring, one 16-column K chunk at a time; each chunk's MMAs are
