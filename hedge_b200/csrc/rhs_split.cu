@@ -21,16 +21,19 @@
 // through 16 bits; face jumps are formed in FP64.
 //
 // One CTA per SM runs a persistent loop over batches with warp roles:
-//   * a producer warp streams each batch's FP64 state, geometry and face
-//     table into one of two stage buffers (cp.async, completion counted on
-//     an mbarrier) while the previous batch is computed, and the batch's
-//     residual into a residual buffer once the previous update is done;
-//   * 12 consumer warps split the state, issue the diff MMA (one thread),
-//     evaluate the face fluxes into the lift planes, issue the lift MMA, read
-//     the accumulators back (chain rule, volume terms, + lift: one lane holds
-//     every derivative of its (e, f); the model's curl/div/grad gather the
+//   * an I/O warp streams each batch's FP64 state, geometry and face table
+//     into one of two stage buffers (bulk copies, completion counted on an
+//     mbarrier) while the previous batch is computed, the batch's residual
+//     into a residual buffer once the previous update is done, and the
+//     results back out; it also prefetches upcoming batches into L2;
+//   * an MMA warp issues the diff and lift MMAs once the consumers have
+//     written the state and flux planes;
+//   * 12 consumer warps split the state, evaluate the face fluxes into the
+//     lift planes, read the accumulators back (chain rule and volume terms
+//     first, parked in spare TMEM columns, then + lift: one lane holds every
+//     derivative of its (e, f); the model's curl/div/grad gather the
 //     element's other fields with warp shuffles) and apply the FP64 stage
-//     update from shared memory with coalesced stores.
+//     update in shared memory, which the I/O warp stores out.
 // All waits are bounded (2 s); a timeout sets the device error flag and the
 // CTA leaves after releasing its TMEM.  Element shapes are compile-time
 // (template on the order).  Restated reference loops: jit/diff.py:137-175,
