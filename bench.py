@@ -38,8 +38,6 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-CAVITY_MODE = (1, 1, 1)
-
 # time-step factor of the split-vs-FP64 accuracy run (see run_ours)
 ACC_DT_FACTOR = 0.5
 
@@ -81,40 +79,26 @@ WORKLOADS = {
 
 def build_problem(n, order, precision, device=None, workload="maxwell"):
     import hedge_b200 as hb
-    h = 2.0 / n
-    mesh = hb.make_box_tet_mesh(n=(n, n, n), jitter=0.05 * h, seed=1)
+    from hedge_b200 import workloads
+    mesh = workloads.box_mesh(n)
     discr = hb.Discretization(mesh, order=order, precision=precision, device=device)
-    if workload == "wave7":
-        # c = 1, upwind, reflecting (Dirichlet) walls
-        op = hb.StrongWaveOperator(1.0, 3, flux_type="upwind")
-    else:
-        op = hb.MaxwellOperator(1.0, 1.0, flux_type=1)
-    return hb, mesh, discr, op
+    return hb, mesh, discr, workloads.operator(workload)
 
 
 def initial_state(discr, workload="maxwell"):
-    if workload == "wave7":
-        x = discr.nodes
-        w = np.zeros((4, len(discr)))
-        w[0] = np.exp(-(x ** 2).sum(1) / 0.15 ** 2)   # pressure pulse of width 0.15
-        return w
-    return cavity_ic(discr)
+    from hedge_b200 import workloads
+    return workloads.initial_state(discr, workload)
 
 
-def cavity_ic(discr):
-    """(1,1,1) mode of the cavity [-1,1]^3 (reference
-    examples/maxwell/analytic_solutions.py:240-300, dimensions (2,2,2),
-    coordinates shifted by +1), real part at t=0, plus noise."""
-    x, y, z = (discr.nodes + 1.0).T
-    f, g, h = [np.pi * m / 2.0 for m in CAVITY_MODE]
-    k2 = f * f + g * g
-    # zdep_add = 2 cos(hz), zdep_sub = 2i sin(hz), C = i/(f^2+g^2)
-    ex = -(1.0 / k2) * f * h * np.cos(f * x) * np.sin(g * y) * 2 * np.sin(h * z)
-    ey = -(1.0 / k2) * g * h * np.sin(f * x) * np.cos(g * y) * 2 * np.sin(h * z)
-    ez = np.sin(f * x) * np.sin(g * y) * 2 * np.cos(h * z)
-    w = np.stack([ex, ey, ez, np.zeros_like(x), np.zeros_like(x), np.zeros_like(x)])
-    rng = np.random.default_rng(2)
-    return w + 1e-3 * rng.uniform(-1, 1, w.shape)
+def workload_config(args, K_total, K_rank, Np, F):
+    """The workload as both arms report it (the implementation's precision
+    and layout are reported beside it, in dtype and parallelism)."""
+    W = WORKLOADS[args.workload]
+    return {"workload": W["label"] % (K_rank, args.order), "K": K_total,
+            "K_per_gpu": K_rank, "order": args.order, "Np": Np, "fields": F,
+            "stepper": "LSRK4, one step = 5 RHS + stage updates",
+            "l2": "working set of a stage (q_in, q_out, res) 3 x %.1f MB in FP64 > 126 MB L2, "
+                  "no flush" % (K_rank * Np * F * 8 / 1e6)}
 
 
 def algorithmic_bytes_per_dof_update(discr, state_bytes, F=6):
@@ -268,22 +252,25 @@ def cpu_model():
 
 
 def run_reference(args):
+    """The reference arm: the CPU oracle (the reference jit backend's loops,
+    restated; the reference itself cannot be built here) on all host cores,
+    on the same workload and metric as run_ours.  At N = 1 a step is one
+    LSRK4 step (5 RHS + stage updates) over the whole mesh, as in run_ours.
+    For N > 1 (a mesh N times larger) a step is a bounded sample, one LSRK
+    stage over the whole mesh, so that the run ends within minutes."""
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     if rank != 0:
         return
     W = WORKLOADS[args.workload]
     F = W["fields"]
-    if world > 1 and args.layout == "partitioned":
-        # the same mesh as our partitioned arm: world x the per-GPU workload
-        import hedge_b200 as hb
-        h = 2.0 / args.n
-        mesh = hb.make_box_tet_mesh(a=(-1, -1, -1), b=(-1 + 2 * world, 1, 1),
-                                    n=(args.n * world, args.n, args.n), jitter=0.05 * h, seed=1)
-        discr = hb.Discretization(mesh, order=args.order)
-        _, _, _, op = build_problem(2, args.order, "fp64", workload=args.workload)
-    else:
-        hb, mesh, discr, op = build_problem(args.n, args.order, "fp64", workload=args.workload)
+    from hedge_b200 import workloads
+    import hedge_b200 as hb
+    stretch = world if (world > 1 and args.layout == "partitioned") else 1
+    # the same mesh as our arm: world x the per-GPU workload when partitioned
+    mesh = workloads.box_mesh(args.n, stretch=stretch)
+    discr = hb.Discretization(mesh, order=args.order)
+    op = workloads.operator(args.workload)
     w0 = initial_state(discr, args.workload)
     dt = op.estimate_timestep(discr)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -291,35 +278,39 @@ def run_reference(args):
     ncores = os.cpu_count() or 1
     used = orc_mod.set_threads(ncores)
     orc = orc_mod.OracleRHS(discr, op.op_template())
-    from hedge_b200.timestep import RK4A, RK4B
-    y, res = w0.copy(), np.zeros_like(w0)
-    for s in range(args.warmup):
-        r = orc(y)
-        res = RK4A[s % 5] * res + dt * r
-        y = y + RK4B[s % 5] * res
+    from hedge_b200.timestep import RK4A, RK4B, RK4C
+    stages = 5 if stretch == 1 else 1
+    y, res, t = w0.copy(), np.zeros_like(w0), 0.0
+
+    def step(y, res, t):
+        for s in range(stages):
+            r = orc(y, t + RK4C[s] * dt)
+            res = RK4A[s] * res + dt * r
+            y = y + RK4B[s] * res
+        return y, res, t + dt
+
+    for _ in range(args.warmup):
+        y, res, t = step(y, res, t)
     t0 = time.perf_counter()
-    for s in range(args.steps):
-        r = orc(y)
-        res = RK4A[s % 5] * res + dt * r
-        y = y + RK4B[s % 5] * res
+    for _ in range(args.steps):
+        y, res, t = step(y, res, t)
     el = time.perf_counter() - t0
-    dofs = discr.K * discr.Np * F * args.steps
-    v = dofs / el
+    v = discr.K * discr.Np * F * stages * args.steps / el
+    K_rank = discr.K // world if stretch > 1 else discr.K
+    sample = ("one LSRK4 step (5 RHS + stage updates) over the full K=%d mesh per step"
+              % discr.K if stages == 5 else
+              "one LSRK stage (RHS + update) over the full K=%d mesh per step" % discr.K)
     line = {
         "impl": "reference", "metric": W["metric"],
         "value": v, "unit": "DOF-updates/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": W["label"] % (discr.K // max(world, 1)
-                                             if args.layout == "partitioned" else discr.K,
-                                             args.order),
-                   "K": discr.K, "order": args.order, "fields": F,
-                   "step": "one LSRK stage per step"},
+        "config": workload_config(args, discr.K, K_rank, discr.Np, F),
+        "parallelism": "host cores (%d OpenMP threads)" % used,
         "cpu_baseline": {"value": v, "unit": "DOF-updates/s", "cores": used,
                          "cpu_model": cpu_model(), "kind": "port",
-                         "sample": "one LSRK stage over the full mesh per step; C++ "
-                                   "oracle (restated jit loops), OpenMP"},
+                         "sample": sample + "; C++ oracle (restated jit loops), OpenMP"},
         "e2e": {"value": v, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "per_time_step": {"value": v / 5, "unit": "DOF-steps/s"},
@@ -336,12 +327,10 @@ def partitioned_problem(args, rank, world, dev):
     import hedge_b200 as hb
     from hedge_b200.partition import DistExchange, PartitionPlan, PartitionedOperator
     from hedge_b200.timestep import RK4A, RK4B
-    n = args.n
-    h = 2.0 / n
-    mesh = hb.make_box_tet_mesh(a=(-1, -1, -1), b=(-1 + 2 * world, 1, 1), n=(n * world, n, n),
-                                jitter=0.05 * h, seed=1)
+    from hedge_b200 import workloads
+    mesh = workloads.box_mesh(args.n, stretch=world)
     discr = hb.Discretization(mesh, order=args.order, precision=args.precision, device=dev)
-    _, _, _, op = build_problem(2, args.order, "fp64", device=dev, workload=args.workload)
+    op = workloads.operator(args.workload)
     plan = PartitionPlan(discr, op.op_template(), world)
     part = PartitionedOperator(discr, op, plan, rank, precision=args.precision, device=dev,
                                exchange=DistExchange(plan, rank))
@@ -546,14 +535,10 @@ def run_ours(args):
             "dtype": {"fp64": "f64", "fp32": "f32", "bf16x3": "bf16x3+f32acc, f64 state",
                       "fp16x3": "fp16x3(scaled)+f32acc, f64 state"}[args.precision],
             "data": "synthetic",
-            "config": {"workload": W["label"] % (K_rank, args.order), "K": K_total,
-                       "K_per_gpu": K_rank, "order": args.order, "Np": discr.Np, "fields": F,
-                       "precision": args.precision, "stepper": "LSRK4 (5 fused stages)",
-                       "parallelism": ("partitioned, face-trace exchange per stage (NCCL)"
-                                       if partitioned else
-                                       "replicas" if world > 1 else "single"),
-                       "l2": "working set 3 x %.1f MB > 126 MB L2, no flush" %
-                             (K_rank * discr.Np * F * state_bytes / 1e6)},
+            "config": workload_config(args, K_total, K_rank, discr.Np, F),
+            "precision": args.precision,
+            "parallelism": ("partitioned, face-trace exchange per stage (NCCL)"
+                            if partitioned else "replicas" if world > 1 else "single GPU"),
             # the same rate per LSRK4 time step (5 stages): DOF-steps/s
             "per_time_step": {"value": value / 5, "unit": "DOF-steps/s"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "split_vs_fp64": compare,

@@ -59,7 +59,7 @@ EXPORTED = [
     "hb_op_launch_info", "hb_norm", "hb_norm_noalloc", "hb_rhs_adjoint_work_size",
     "hb_rhs_adjoint", "hb_batch_create", "hb_batch_destroy", "hb_batch_stage",
     "hb_batch_info", "hb_batch_check", "hb_op_set_halo", "hb_pack",
-    "hb_last_error_string",
+    "hb_op_wait_selftest", "hb_last_error_string",
 ]
 
 _lib = None
@@ -100,6 +100,7 @@ def load(path=LIB_PATH):
             "hb_batch_check": [vp, vp],
             "hb_op_set_halo": [vp, vp, vp],
             "hb_pack": [i64, i32, i32, i64, vp, vp, vp, vp],
+            "hb_op_wait_selftest": [vp, i64, vp],
         }
         for name, args in sig.items():
             fn = getattr(lib, name)

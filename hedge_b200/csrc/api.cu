@@ -66,7 +66,12 @@ hb_status check_device_flag(Op* op, cudaStream_t s) {
     static const char* what[] = {"ok", "face neighbour out of range",
                                  "invalid neighbour face / permutation code",
                                  "boundary index out of range", "missing input vector",
-                                 "tensor-core MMA did not complete in time"};
+                                 "a tensor-core kernel's bounded wait ran out "
+                                 "(MMA completion or a data hand-off)"};
+    // reported once: the flag is cleared so that the operator can be used
+    // again once the caller has dealt with the error
+    HB_CUDA(cudaMemsetAsync(op->err_flag, 0, sizeof(int), s));
+    HB_CUDA(cudaStreamSynchronize(s));
     return fail(HB_ERR_DEVICE_FLAG,
                 std::string("device check failed: ") + (flag < 6 ? what[flag] : "unknown"));
   }
@@ -81,6 +86,7 @@ hb_status launch_split(Op* op, int mode, double ra, double rb, double dt,
                        const void* q_in, void* q_out, void* res, const double* coeff,
                        const double* bdry, const double* source, cudaStream_t s);
 void free_split(Op* op);
+hb_status launch_wait_selftest(int* err, uint64_t limit_ns, cudaStream_t s);
 
 }  // namespace hb
 
@@ -379,6 +385,17 @@ hb_status hb_op_check(hb_op* handle, void* stream) {
   Op* op = reinterpret_cast<Op*>(handle);
   DeviceGuard g(op->d->device);
   return check_device_flag(op, reinterpret_cast<cudaStream_t>(stream));
+}
+
+hb_status hb_op_wait_selftest(hb_op* handle, int64_t limit_ns, void* stream) {
+  if (!handle) return fail(HB_ERR_INVALID_ARGUMENT, "null operator");
+  if (limit_ns < 1000 || limit_ns > 2000000000)
+    return fail(HB_ERR_INVALID_ARGUMENT, "wait self-test: limit must be 1 us .. 2 s");
+  Op* op = reinterpret_cast<Op*>(handle);
+  DeviceGuard g(op->d->device);
+  if (!g.ok) return fail(HB_ERR_CUDA, "cannot select the operator's device");
+  return launch_wait_selftest(op->err_flag, (uint64_t)limit_ns,
+                              reinterpret_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

@@ -158,6 +158,29 @@ extern "C" hb_status hb_norm_noalloc(int64_t num_elements, int32_t np, int32_t n
   double* partials = nullptr;
   const hb_status st = noalloc_scratch(&partials);
   if (st != HB_OK) return st;
+  // the scratch address is the current device's: every operand must be
+  // device (or managed) memory of that same device
+  {
+    int dev = -1;
+    HB_CUDA(cudaGetDevice(&dev));
+    const void* ptrs[4] = {mass, abs_jacobian, u, out};
+    const char* names[4] = {"mass", "abs_jacobian", "u", "out"};
+    for (int i = 0; i < 4; ++i) {
+      cudaPointerAttributes attr;
+      const cudaError_t e = cudaPointerGetAttributes(&attr, ptrs[i]);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(HB_ERR_INVALID_ARGUMENT,
+                    std::string("norm_noalloc: cannot query the pointer ") + names[i]);
+      }
+      const bool on_device = attr.type == cudaMemoryTypeDevice ||
+                             attr.type == cudaMemoryTypeManaged;
+      if (!on_device || attr.device != dev)
+        return fail(HB_ERR_INVALID_ARGUMENT,
+                    std::string("norm_noalloc: ") + names[i] +
+                        " is not device memory of the current device");
+    }
+  }
   return launch_norm(num_elements, np, nfields, dtype, mass, abs_jacobian, u, partials,
                      HB_NORM_NOALLOC_MAX_BLOCKS, out, reinterpret_cast<cudaStream_t>(stream));
 }

@@ -2156,14 +2156,28 @@ hb_status prepare_split(Op* op) {
   static_cast<SplitOps*>(op->split_ops)->order = d->order;
   const int dim = d->dim, order = d->order;
   const int pt = op->precision == HB_PREC_FP16X3 ? PT_FP16 : PT_BF16;
-#define HB_CASE(M, D, O)                                                       \
-  if (op->model == M && dim == D && order == O)                                \
-    return pt == PT_FP16 ? configure_stream<M, D, O, PT_FP16>(op)              \
-                         : configure_stream<M, D, O, PT_BF16>(op);
   if (op->n_halo == 0) {
-    HB_SPLIT_STREAM_INSTANCES(HB_CASE)
+    // a streamed variant that this device refuses (e.g. its shared memory)
+    // falls back to the resident kernel where one is built
+    bool tried = false;
+    hb_status sst = HB_ERR_UNSUPPORTED;
+#define HB_CASE(M, D, O)                                                       \
+  if (!tried && op->model == M && dim == D && order == O) {                    \
+    tried = true;                                                              \
+    sst = pt == PT_FP16 ? configure_stream<M, D, O, PT_FP16>(op)               \
+                        : configure_stream<M, D, O, PT_BF16>(op);              \
   }
+    HB_SPLIT_STREAM_INSTANCES(HB_CASE)
 #undef HB_CASE
+    if (tried && sst == HB_OK) return HB_OK;
+    if (tried) {
+      SplitOps* so = static_cast<SplitOps*>(op->split_ops);
+      if (so->dev) cudaFree(so->dev);
+      so->dev = nullptr;
+      so->stream = 0;
+      so->scale_d = so->scale_l = 1.f;
+    }
+  }
 #define HB_CASE(M, D, O)                                                       \
   if (op->model == M && dim == D && order == O)                                \
     return pt == PT_FP16 ? configure_split<M, D, O, PT_FP16>(op)               \

@@ -93,7 +93,16 @@ class GraphedLSRK4:
     ``g = GraphedLSRK4(rhs, y0, dt)``; ``y = g.step()`` advances the state by
     one step and returns the state buffer (overwritten by the next step);
     ``g.state`` is the same buffer.  Same kernels, same order and the same
-    residual as ``LSRK4TimeStepper``, so the states agree bitwise."""
+    residual as ``LSRK4TimeStepper``, so the states agree bitwise.
+
+    The recorded launches read the operator's coefficient field and source
+    vector at their addresses at construction; this object keeps those two
+    tensors alive, and ``step()`` raises if the operator has been given new
+    ones since (``set_coefficient`` / ``set_source``): build a new
+    GraphedLSRK4 then.  A replay does not read the operator's device error
+    flag; ``check()`` does (it synchronises), so call it every so many steps
+    to learn of bad input a kernel flagged (e.g. a halo face without halo
+    data)."""
 
     def __init__(self, rhs, y0, dt):
         from .discretization import BoundRHS
@@ -110,6 +119,8 @@ class GraphedLSRK4:
         self.state = y.clone()
         self._tmp = [torch.empty_like(self.state), torch.empty_like(self.state)]
         self.residual = torch.zeros_like(self.state)
+        # the graph holds these tensors' addresses: keep them alive here
+        self._coeff, self._source = comp._coeff, comp._source
         coeffs = np.array([RK4A, RK4B], dtype=np.float64).T
         # stage s reads bufs[s] and writes bufs[s + 1] (never in place)
         bufs = [self.state, self._tmp[0], self._tmp[1], self._tmp[0], self._tmp[1],
@@ -117,7 +128,8 @@ class GraphedLSRK4:
 
         def stages():
             for s, (a, b) in enumerate(coeffs):
-                comp.lsrk_stage(a, b, self.dt, bufs[s], bufs[s + 1], self.residual)
+                comp.lsrk_stage(a, b, self.dt, bufs[s], bufs[s + 1], self.residual,
+                                coeff=self._coeff, source=self._source)
 
         dev = self.state.device
         side = torch.cuda.Stream(dev)
@@ -134,5 +146,14 @@ class GraphedLSRK4:
         torch.cuda.synchronize(dev)
 
     def step(self):
+        comp = self.compiled
+        if comp._coeff is not self._coeff or comp._source is not self._source:
+            raise RuntimeError("the operator's coefficient or source changed after the "
+                               "step was recorded; build a new GraphedLSRK4")
         self.graph.replay()
         return self.state
+
+    def check(self):
+        """Synchronise and raise if a kernel of the replayed steps flagged bad
+        input (the operator's device error flag)."""
+        self.compiled.check()

@@ -149,7 +149,9 @@ hb_status hb_norm(hb_discr* discr, int32_t nfields, int32_t dtype, const void* u
  * [num_elements] (FP64), inside a time loop that has reserved the device's
  * memory for its fields or must not let an allocation synchronise the device
  * between steps.  Same result and reduction order as hb_norm on the current
- * CUDA device; u and out as for hb_norm, all pointers on the current device.
+ * CUDA device; u and out as for hb_norm, all pointers on the current device
+ * (a pointer that is not device or managed memory of the current device is
+ * rejected with HB_ERR_INVALID_ARGUMENT before any launch).
  *
  * The partial sums go to a fixed device array inside the library of
  * HB_NORM_NOALLOC_MAX_BLOCKS doubles (64 KiB), so the call allocates nothing.
@@ -233,8 +235,21 @@ hb_status hb_pack(int64_t n, int32_t dtype, int32_t nfields, int64_t field_strid
 
 /* Synchronises `stream` and returns HB_ERR_DEVICE_FLAG if a kernel of this
  * operator flagged bad input (out-of-range neighbour or code, missing
- * boundary vector); the flag stays set. */
+ * boundary vector) or a bounded wait of a tensor-core kernel ran out.  The
+ * first flag raised since the last check is reported, once: the check clears
+ * it, so the operator can be launched again afterwards.  The reference
+ * raises a Python exception per call instead (e.g. the generated size checks
+ * of hedge/backends/jit/diff.py:111-126). */
 hb_status hb_op_check(hb_op* op, void* stream);
+
+/* Failure-detection self-test, no reference counterpart: launches one CTA
+ * that allocates tensor memory as the split-precision kernels do, waits on an
+ * mbarrier that nothing arrives on with their bounded wait (limit_ns, 1 us to
+ * 2 s), raises this operator's device error flag when the wait runs out,
+ * releases the tensor memory and returns.  Nothing else is in flight.  A
+ * following hb_op_check returns HB_ERR_DEVICE_FLAG, and the operator (and the
+ * CUDA context) stays usable. */
+hb_status hb_op_wait_selftest(hb_op* op, int64_t limit_ns, void* stream);
 
 /* Launch configuration chosen at hb_op_create, for diagnostics: up to n of
  * {grid, threads per CTA, dynamic shared bytes, elements per batch,

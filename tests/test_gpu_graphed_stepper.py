@@ -73,3 +73,38 @@ def test_graphed_refuses_time_dependent_inflow(cuda_device):
     rhs = op.bind(d)
     with pytest.raises(ValueError):
         hb.GraphedLSRK4(rhs, d.to_device(np.zeros((1, len(d)))).reshape(1, -1), 1e-3)
+
+
+def test_graphed_variable_coefficient_kept_and_guarded(cuda_device):
+    """The recorded stages read the c field and the source at their addresses
+    at construction: the stepper keeps those tensors alive (replays after the
+    caller dropped its own references stay bitwise equal to the eager
+    stepper), and a coefficient set after construction makes step() raise
+    instead of replaying against freed memory."""
+    import gc
+    import torch
+    d = hb.Discretization(rect(7, False, 0.02, 4), order=3)
+    rng = np.random.default_rng(5)
+    c = rng.uniform(0.8, 1.2, len(d))
+    src = 0.1 * rng.uniform(-1, 1, len(d))
+    op = hb.VariableVelocityStrongWaveOperator(c, 2, flux_type="upwind", source=src)
+    rhs = op.bind(d)
+    q = _fields(d, 3, 6)
+    dt = 0.5 * op.estimate_timestep(d)
+    g = hb.GraphedLSRK4(rhs, d.to_device(q).reshape(3, -1), dt)
+    st = hb.LSRK4TimeStepper()
+    y = d.to_device(q).reshape(3, -1)
+    for n in range(5):
+        y = st(y, n * dt, dt, rhs)
+    # churn the caching allocator: freed blocks of the c/source size get reused
+    junk = [torch.full((len(d),), 7.0, dtype=torch.float64, device=d.device)
+            for _ in range(8)]
+    del junk
+    gc.collect()
+    for _ in range(5):
+        yg = g.step()
+    g.check()
+    assert torch.equal(y, yg)
+    rhs.compiled.set_coefficient(np.ones(len(d)))
+    with pytest.raises(RuntimeError):
+        g.step()

@@ -1,8 +1,10 @@
 """hb_norm_noalloc through the C ABI against hb_norm on the same inputs.
 
 Two calls in a row (a larger mesh, then a smaller one, so the second call
-reads a scratch array the first one left full), each within 1e-13 of hb_norm,
-plus the size limit rejected before any launch."""
+reads a scratch array the first one left full), each within 1e-13 of hb_norm
+and, since both run the same kernels in the same reduction order, equal to it
+bit for bit; plus the size limit and operands that are not memory of the
+current device, both rejected before any launch."""
 import numpy as np
 import pytest
 
@@ -42,8 +44,11 @@ def test_noalloc_norm_matches_hb_norm_twice(cuda_device):
         want = d.norm(u)
         got = _noalloc(d, u, mass, absjac)
         assert abs(got - want) <= TOL * want, (got, want)
+        assert got == want, (got, want)
     d, u, mass, absjac = big
-    assert abs(_noalloc(d, u, mass, absjac) - d.norm(u)) <= TOL * d.norm(u)
+    got = _noalloc(d, u, mass, absjac)
+    assert abs(got - d.norm(u)) <= TOL * d.norm(u)
+    assert got == d.norm(u)
 
 
 def test_noalloc_norm_rejects_oversized_mesh(cuda_device):
@@ -57,3 +62,31 @@ def test_noalloc_norm_rejects_oversized_mesh(cuda_device):
                              u.data_ptr(), out.data_ptr(), None)
     assert st == _native.HB_ERR_INVALID_ARGUMENT
     assert b"scratch limit" in lib.hb_last_error_string()
+
+
+def test_noalloc_norm_rejects_host_memory(cuda_device):
+    """The scratch address is the current device's: a field in host memory
+    is refused instead of being read by the kernels."""
+    import torch
+    d, u, mass, absjac = _case(2, 3, 1, 6)
+    host_u = np.ascontiguousarray(u.cpu().numpy())
+    out = torch.zeros(1, dtype=torch.float64, device=d.device)
+    lib = _native.load()
+    st = lib.hb_norm_noalloc(d.K, d.Np, 1, 0, mass.data_ptr(), absjac.data_ptr(),
+                             host_u.ctypes.data, out.data_ptr(), None)
+    assert st == _native.HB_ERR_INVALID_ARGUMENT
+    assert b"not device memory" in lib.hb_last_error_string()
+
+
+def test_noalloc_norm_rejects_other_device(cuda_device):
+    """u on another GPU than the current one is refused (needs two GPUs)."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("one GPU")
+    d, u, mass, absjac = _case(2, 3, 1, 7)
+    u1 = u.to("cuda:1")
+    out = torch.zeros(1, dtype=torch.float64, device=d.device)
+    lib = _native.load()
+    st = lib.hb_norm_noalloc(d.K, d.Np, 1, 0, mass.data_ptr(), absjac.data_ptr(),
+                             u1.data_ptr(), out.data_ptr(), None)
+    assert st == _native.HB_ERR_INVALID_ARGUMENT
