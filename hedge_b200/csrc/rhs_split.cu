@@ -24,16 +24,20 @@
 //   * an I/O warp streams each batch's FP64 state, geometry and face table
 //     into one of two stage buffers (bulk copies, completion counted on an
 //     mbarrier) while the previous batch is computed, the batch's residual
-//     into a residual buffer once the previous update is done, and the
-//     results back out; it also prefetches upcoming batches into L2;
+//     into a residual buffer where one fits, and prefetches the upcoming
+//     states and residuals into L2;
 //   * an MMA warp issues the diff and lift MMAs once the consumers have
 //     written the state and flux planes;
-//   * 12 consumer warps split the state, evaluate the face fluxes into the
+//   * 20 consumer warps split the state, evaluate the face fluxes into the
 //     lift planes, read the accumulators back (chain rule and volume terms
 //     first, parked in spare TMEM columns, then + lift: one lane holds every
 //     derivative of its (e, f); the model's curl/div/grad gather the
-//     element's other fields with warp shuffles) and apply the FP64 stage
-//     update in shared memory, which the I/O warp stores out.
+//     element's other fields with warp shuffles) into FP32 rhs rows in
+//     shared memory, and then apply the FP64 stage update in a coalesced
+//     pass that writes q_out and the residual straight to global memory.
+//     Where the buffers allow, each warp splits batch i + 1 between the
+//     volume terms and the lift epilogue of batch i (software pipeline), so
+//     the lift MMA's latency overlaps that work.
 // All waits are bounded (2 s); a timeout sets the device error flag and the
 // CTA leaves after releasing its TMEM.  Element shapes are compile-time
 // (template on the order).  Restated reference loops: jit/diff.py:137-175,
@@ -43,6 +47,7 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -56,13 +61,15 @@ namespace hb {
 hb_status ensure_fp32(Discr* d);
 
 // Consumer warps (the phases of a batch; a multiple of 4: warp w reads TMEM
-// lane quadrant w % 4), one I/O warp that streams the next batch's state and
-// the current batch's residual into shared memory and the results out, and
-// one warp that issues the tensor-core MMAs.  Registers are split over the
-// SM's 4 sub-partitions (16K each) by warp: 14 warps put at most 4 warps on
-// one, which leaves 128 registers per thread.
+// lane quadrant w % 4), one I/O warp that streams the next batches' state
+// (and residual) into shared memory, and one warp that issues the
+// tensor-core MMAs.  Registers are split over the SM's 4 sub-partitions
+// (16K each) by warp: 22 warps put at most 6 warps on one, which leaves 80
+// registers per thread.  20 consumer warps give one element (face phase) and
+// one state-split item per warp in a 20-element Maxwell batch; across the
+// built instances (K ~ 48000-51000) they run 2-19 % faster than 12.
 #ifndef HB_SPLIT_NCW
-#define HB_SPLIT_NCW 12
+#define HB_SPLIT_NCW 20
 #endif
 constexpr int NCW = HB_SPLIT_NCW;
 // face-flux phase: elements a consumer warp takes per round (0: the default
@@ -83,6 +90,7 @@ __host__ __device__ constexpr int ru16(int x) { return (x + 15) / 16 * 16; }
 __host__ __device__ constexpr int ru32(int x) { return (x + 31) / 32 * 32; }
 __host__ __device__ constexpr uint32_t al128(uint32_t x) { return (x + 127u) & ~127u; }
 __host__ __device__ constexpr uint32_t al16(uint32_t x) { return (x + 15u) & ~15u; }
+__host__ __device__ constexpr uint32_t al1024(uint32_t x) { return (x + 1023u) & ~1023u; }
 
 // Compile-time shape of one (model, dim, order) instance.
 template <int MODEL, int DIM, int ORDER>
@@ -136,6 +144,14 @@ struct Shape {
   static constexpr int NITEM = 4 * (KD / 8);
   static constexpr int IPW = (NITEM + NCW - 1) / NCW;
 
+  // rhs staging rows (FP32, aliasing the state planes once the diff MMA has
+  // read them): NPR floats per (element, field) row, 16-byte aligned
+  static constexpr int NPR = (NP + 3) & ~3;
+  // flux planes in the 128-byte swizzled K-major layout when a row is exactly
+  // one swizzle atom wide (64 K entries): the face phase's stores of one row's
+  // consecutive face points then fall in distinct banks
+  static constexpr bool FSW = KL == 64;
+
   static constexpr uint32_t bD = ND * KD * 2, bL = NL * KL * 2;
   static constexpr uint32_t bAq = 128 * KD * 2, bAf = 128 * KL * 2;
   static constexpr uint32_t bState = NVAL * 8;
@@ -152,26 +168,36 @@ struct Shape {
   static constexpr uint32_t oLl = al128(oLh + bL);
   static constexpr uint32_t oAqh = al128(oLl + bL);
   static constexpr uint32_t oAql = al128(oAqh + bAq);
-  static constexpr uint32_t oAfh = al128(oAql + bAq);
-  static constexpr uint32_t oAfl = al128(oAfh + bAf);
+  static constexpr uint32_t oAfh = FSW ? al1024(oAql + bAq) : al128(oAql + bAq);
+  static constexpr uint32_t oAfl = FSW ? al1024(oAfh + bAf) : al128(oAfh + bAf);
   static constexpr uint32_t ostg = al128(oAfl + bAf);
-  static constexpr uint32_t SMALL = 1024 + NP * DIM * 8 + NFPT + 6 * NF * NFP + 4 + 512 * 4 + 96;
-  // double-buffered stages and a residual buffer when they fit, else fewer
-  static constexpr bool fits(int nstg, bool res) {
-    return ostg + nstg * bStage + (res ? bState : 0) + SMALL <= SMEM_LIMIT;
+  static constexpr uint32_t SMALL = 1024 + NFPT + 6 * NF * NFP + 4 + 768 * 4 + 96;
+  // FP32 rhs rows [128][NPR]: a buffer of their own when it fits next to the
+  // stage buffers, else aliasing the state planes (free once the diff MMA
+  // has read them; the state split rewrites every plane column each batch)
+  static constexpr uint32_t bRhs = al128(128u * NPR * 4u);
+  static_assert(128u * NPR * 4u <= 2u * bAq, "rhs staging must fit in the state planes");
+  // double-buffered stages when they fit, else one; then the rhs rows' own
+  // buffer; then a residual buffer (the I/O warp loads the batch's residual
+  // one batch ahead; without it the update reads the residual from global
+  // memory)
+  static constexpr bool fits(int nstg, bool own_rhs, bool res) {
+    return ostg + nstg * bStage + (own_rhs ? bRhs : 0) + (res ? bState : 0) + SMALL <=
+           SMEM_LIMIT;
   }
-  static constexpr int NSTG = fits(2, false) ? 2 : 1;
-  static constexpr bool RES = fits(NSTG, true);
-  static constexpr uint32_t ores = ostg + NSTG * bStage;
-  static constexpr uint32_t olam = al16(ores + (RES ? bState : 0));   // FP64 weights
-  static constexpr uint32_t ofm = al16(olam + NP * DIM * 8);           // uint8 fmask
+  static constexpr int NSTG = fits(2, false, false) ? 2 : 1;
+  static constexpr bool RHS_OWN = fits(NSTG, true, false);
+  static constexpr bool RES = fits(NSTG, RHS_OWN, true);
+  static constexpr uint32_t orhs = RHS_OWN ? ostg + NSTG * bStage : oAqh;
+  static constexpr uint32_t ores = ostg + NSTG * bStage + (RHS_OWN ? bRhs : 0);
+  static constexpr uint32_t ofm = al16(ores + (RES ? bState : 0));     // uint8 fmask
   // uint8 neighbour node of face node k seen through (perm, neighbour face):
   // fmask[nface][shuffle[perm][k]] at [(perm * NF + nface) * NFP + k]
   static constexpr uint32_t osh = al16(ofm + NFPT);
   static constexpr uint32_t overt = al16(osh + 6 * NF * NFP);          // uint8 vertex nodes
   // row maxima (FP16 planes): state rows [2][128] then flux rows [2][128]
   static constexpr uint32_t ors = al16(overt + 4);
-  static constexpr uint32_t obar = al16(ors + 512 * 4);                // mbarriers + TMEM slot
+  static constexpr uint32_t obar = al16(ors + 768 * 4);                // mbarriers + TMEM slot
   static constexpr uint32_t total = al16(obar + 96);
   static constexpr uint32_t LIN_BYTES = 8 + NP * DIM * 8;  // vertex nodes + weights (image)
   // epilogue: the volume terms are formed before the lift MMA completes and
@@ -458,27 +484,55 @@ enum {
   MB_DIFF = 0,      // diff MMAs done (tcgen05.commit)
   MB_LIFT = 1,      // lift MMAs done
   MB_FULL = 2,      // 2..3: stage buffer loaded
-  MB_RES_FULL = 4,  // residual buffer loaded
-  MB_AREADY = 5,    // every consumer warp wrote its state-plane rows
-  MB_FREADY = 6,    // every consumer warp wrote its flux-plane entries
-  MB_DONE = 7,      // 7..8: every consumer warp left its results in that stage buffer
+  MB_AREADY = 4,    // every consumer warp wrote its state-plane rows
+  MB_FREADY = 5,    // every consumer warp wrote its flux-plane entries
+  MB_DONE = 6,      // 6..7: every consumer warp is done with that stage buffer
+  MB_RES_FULL = 8,  // residual buffer loaded
   MB_COUNT = 9
 };
+
+// FP64 weights (1 + r_d)/2 of every node of the reference element, per
+// (dimension, order) of the resident kernel: the element's linear interpolant
+// through its vertex nodes is v0 + sum_d lam[j][d] (v_d - v0).  Read by the
+// whole warp at one address (constant cache, not the shared-memory pipe).
+constexpr int LAM_MAX = 56 * 3;   // up to 3D N = 5 (Np = 56)
+constexpr int LAM_ORDERS = 7;     // orders 0..6
+__constant__ double c_lam[2][LAM_ORDERS][LAM_MAX];
+
+// byte offset of (row, k) in a flux plane: the 128-byte swizzled K-major
+// layout (8-row atoms of 128-byte rows, 16-byte chunk index XOR row & 7) when
+// SW, else the plain K-major core-matrix layout
+template <bool SW>
+__device__ __forceinline__ uint32_t fplane_off(int row, int k, int kp) {
+  if constexpr (SW)
+    return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + (((k >> 3) ^ (row & 7)) << 4) +
+                      (k & 7) * 2);
+  else
+    return kmajor_off(row, k, kp);
+}
+
+// barrier of the NCW / 4 consumer warps that read one TMEM lane quadrant
+// (named barriers 2..5)
+__device__ __forceinline__ void qbar(int quad) {
+  asm volatile("bar.sync %0, %1;" ::"r"(2 + quad), "n"(32 * (NCW / 4)) : "memory");
+}
 
 template <int MODEL, int DIM, int ORDER, int PT>
 __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a) {
   using S = Shape<MODEL, DIM, ORDER>;
   constexpr int F = S::F, C = S::C, NA = S::NA, NP = S::NP, NFP = S::NFP, NF = S::NF;
   constexpr int NFPT = S::NFPT, G = S::G, EPW = S::EPW, EB = S::EB, FNP = S::FNP;
-  constexpr int KD = S::KD, KL = S::KL, NSTG = S::NSTG;
+  constexpr int KD = S::KD, KL = S::KL, NSTG = S::NSTG, NPR = S::NPR;
+  constexpr bool FSW = S::FSW;
   constexpr unsigned FULL = 0xffffffffu;
-  extern __shared__ __align__(128) uint8_t smem[];
+  extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* Aqh = smem + S::oAqh;
   uint8_t* Aql = smem + S::oAql;
   uint8_t* Afh = smem + S::oAfh;
   uint8_t* Afl = smem + S::oAfl;
+  float* rhs_s = reinterpret_cast<float*>(smem + S::orhs);  // [128][NPR] FP32 rhs rows
   double* rbuf = reinterpret_cast<double*>(smem + S::ores);  // residual [F][EB][NP]
-  const double* slam = reinterpret_cast<const double*>(smem + S::olam);  // [NP][DIM]
+  const double* lamc = &c_lam[DIM - 2][ORDER][0];           // [NP][DIM]
   uint8_t* sfm = smem + S::ofm;
   uint8_t* ssh = smem + S::osh;
   const uint8_t* svert = smem + S::overt;                  // vertex nodes B, C(, D)
@@ -490,7 +544,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
 
-  // ---- one-time set-up: resident operators, zeroed lift planes ----
+  // ---- one-time set-up: resident operators, zeroed operand planes ----
   {
     constexpr uint32_t dD = S::bD, dL = S::bL;
     constexpr uint32_t nchunk = (2 * dD + 2 * dL) / 16;
@@ -504,17 +558,16 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
       else o = S::oLl + (b - 2 * dD - dL);
       *reinterpret_cast<uint4*>(smem + o) = src[x];
     }
-    // the lift planes' K padding and unused rows are never written again
+    // the planes' K padding and unused rows: zero (the flux planes' are never
+    // written again; the state planes' padding chunks are rewritten per batch
+    // only where the rhs rows alias them)
     const uint4 z = make_uint4(0, 0, 0, 0);
-    for (uint32_t o = S::oAfh + tid * 16; o < S::ostg; o += SPLIT_THREADS * 16)
+    for (uint32_t o = S::oAqh + tid * 16; o < S::ostg; o += SPLIT_THREADS * 16)
       *reinterpret_cast<uint4*>(smem + o) = z;
     {
-      // image tail: 4 vertex-node bytes, 4 pad, then the FP64 weights
+      // image tail: 4 vertex-node bytes (the FP64 weights are in c_lam)
       const uint8_t* lsrc = a.ops + 2 * dD + 2 * dL;
       if (tid < 4) smem[S::overt + tid] = lsrc[tid];
-      double* lam = reinterpret_cast<double*>(smem + S::olam);
-      const double* lsrcd = reinterpret_cast<const double*>(lsrc + 8);
-      for (int x = tid; x < NP * DIM; x += SPLIT_THREADS) lam[x] = lsrcd[x];
     }
     for (int x = tid; x < NFPT; x += SPLIT_THREADS) sfm[x] = (uint8_t)a.fmask[x];
     for (int x = tid; x < a.nperm * NF * NFP; x += SPLIT_THREADS) {
@@ -522,17 +575,19 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
       const int nface = r / NFP, k = r - nface * NFP;
       ssh[x] = (uint8_t)a.fmask[nface * NFP + a.shuffle[perm * NFP + k]];
     }
-    for (int x = tid; x < 512; x += SPLIT_THREADS) rsq[x] = 0u;
+    for (int x = tid; x < 768; x += SPLIT_THREADS) rsq[x] = 0u;
     if (tid == 0) {
       tc::mbar_init(&mbar[MB_DIFF], 1);
       tc::mbar_init(&mbar[MB_LIFT], 1);
       tc::mbar_init(&mbar[MB_FULL], 32);
       tc::mbar_init(&mbar[MB_FULL + 1], 32);
-      tc::mbar_init(&mbar[MB_RES_FULL], 32);
       tc::mbar_init(&mbar[MB_AREADY], NCW);
       tc::mbar_init(&mbar[MB_FREADY], NCW);
       tc::mbar_init(&mbar[MB_DONE], NCW);
       tc::mbar_init(&mbar[MB_DONE + 1], NCW);
+      tc::mbar_init(&mbar[MB_RES_FULL], 32);
+      // the swizzled flux planes need 1024-byte aligned atoms
+      if (FSW && (tc::smem_u32(smem) & 1023u) != 0u) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
     }
     if (warp == 0) tc::tmem_alloc(tmem_slot, S::TMEM_COLS);
     tc::fence_proxy_async();
@@ -544,7 +599,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
   const uint32_t tmem_diff = tmem;
   const uint32_t tmem_lift = tmem + S::LIFT_COL;
   const int64_t Knp = a.K * NP;
-  const bool stage_res = a.mode != 0 && S::RES;
+  const bool stage_res = S::RES && a.mode != 0;
   const int64_t nb_cta = a.nbatch > (int64_t)blockIdx.x
                              ? (a.nbatch - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   // bounded wait by lane 0, result shared with (and ordered for) the warp
@@ -560,6 +615,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
     // ================= MMA-issue warp =================
     constexpr uint32_t ID_DIFF = tc::idesc_16bit(128, S::ND, PT == PT_BF16);
     constexpr uint32_t ID_LIFT = tc::idesc_16bit(128, S::NL, PT == PT_BF16);
+    (void)rbuf;
     int64_t diff_issued = -1, lift_issued = -1;
     for (int64_t i = 0; i < nb_cta; ++i) {
       const uint32_t par = (uint32_t)(i & 1);
@@ -591,11 +647,17 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
         const uint32_t l_h = tc::smem_u32(smem + S::oLh), l_l = tc::smem_u32(smem + S::oLl);
 #pragma unroll
         for (int kk = 0; kk < KL / 16; ++kk) {
-          const uint32_t off = kk * 256;
-          const uint64_t ah = tc::smem_desc(af_h + off, 128, KL * 16);
-          const uint64_t al = tc::smem_desc(af_l + off, 128, KL * 16);
-          const uint64_t bh = tc::smem_desc(l_h + off, 128, KL * 16);
-          const uint64_t bl = tc::smem_desc(l_l + off, 128, KL * 16);
+          uint64_t ah, al;
+          if constexpr (FSW) {
+            // K step kk: 32 bytes further into the swizzle atom's rows
+            ah = tc::smem_desc_sw128(af_h + kk * 32, 1024);
+            al = tc::smem_desc_sw128(af_l + kk * 32, 1024);
+          } else {
+            ah = tc::smem_desc(af_h + kk * 256, 128, KL * 16);
+            al = tc::smem_desc(af_l + kk * 256, 128, KL * 16);
+          }
+          const uint64_t bh = tc::smem_desc(l_h + kk * 256, 128, KL * 16);
+          const uint64_t bl = tc::smem_desc(l_l + kk * 256, 128, KL * 16);
           tc::mma_bf16(tmem_lift, ah, bh, ID_LIFT, kk > 0 ? 1u : 0u);
           tc::mma_bf16(tmem_lift, ah, bl, ID_LIFT, 1u);
           tc::mma_bf16(tmem_lift, al, bh, ID_LIFT, 1u);
@@ -614,7 +676,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
     }
     __syncwarp();
   } else if (warp == NCW) {
-    // ====== I/O warp: stage buffers in (bulk copies), results out ======
+    // ====== I/O warp: stage buffers in (bulk copies), L2 prefetches ======
     auto batch_el0 = [&](int64_t i) { return ((int64_t)blockIdx.x + i * gridDim.x) * EB; };
     auto batch_ne = [&](int64_t el0) { return (int)((a.K - el0) < EB ? (a.K - el0) : EB); };
     auto load_stage = [&](int64_t i) {
@@ -655,55 +717,42 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
         stage_in(rbuf + f * FNP, a.res + f * Knp + el0 * NP, ne * NP, lane, mb);
       cp_async_arrive(mb);
     };
+    // pull batch j's state (and residual) into L2 ahead of their reads
+    auto prefetch = [&](int64_t j, bool state, bool res) {
+      if (lane != 0 || j >= nb_cta) return;
+      const int64_t e0 = batch_el0(j);
+      const uint32_t bytes = (uint32_t)batch_ne(e0) * NP * 8u;
+      for (int f = 0; f < F; ++f) {
+        const double* q = a.q_in + f * Knp + e0 * NP;
+        if (state && aligned16(q, bytes)) prefetch_l2(q, bytes);
+        const double* r = a.res + f * Knp + e0 * NP;
+        if (res && a.mode != 0 && aligned16(r, bytes)) prefetch_l2(r, bytes);
+      }
+    };
     bool ok = true;
     if (nb_cta > 0) {
       load_stage(0);
+      if (NSTG == 2 && nb_cta > 1) load_stage(1);
       if (stage_res) load_res(0);
+      else prefetch(0, false, true);
+      prefetch(NSTG, true, false);
     }
     for (int64_t i = 0; i < nb_cta; ++i) {
       const int b = NSTG == 2 ? (int)(i & 1) : 0;
-      if (NSTG == 2 && i + 1 < nb_cta) load_stage(i + 1);   // its buffer was stored out
-      // L2 prefetch of the state two batches ahead and of the next residual,
-      // so that their bulk loads are served from L2
-      if (lane == 0) {
-        for (int64_t j = i + 1; j <= i + 2 && j < nb_cta; ++j) {
-          const int64_t e0 = batch_el0(j);
-          const uint32_t bytes = (uint32_t)batch_ne(e0) * NP * 8u;
-          for (int f = 0; f < F; ++f) {
-            const double* q = a.q_in + f * Knp + e0 * NP;
-            if (j == i + 2 && aligned16(q, bytes)) prefetch_l2(q, bytes);
-            const double* r = a.res + f * Knp + e0 * NP;
-            if (j == i + 1 && stage_res && aligned16(r, bytes)) prefetch_l2(r, bytes);
-          }
-        }
-      }
-      // results: the stage buffer holds q_out (or the rhs), the residual buffer res
+      // the state loaded once this batch is done, and the next batch's
+      // residual (read by the consumers' coalesced update)
+      prefetch(i + NSTG + 1, true, false);
+      prefetch(i + 1, false, true);
       if (!warp_wait(&mbar[MB_DONE + b], (uint32_t)((i / NSTG) & 1))) {
         ok = false;
         break;
       }
-      {
-        const int64_t el0 = batch_el0(i);
-        const int ne = batch_ne(el0);
-        const double* st = reinterpret_cast<const double*>(smem + S::ostg + b * S::bStage);
-        for (int f = 0; f < F; ++f)
-          stage_out(a.q_out + f * Knp + el0 * NP, st + f * FNP, ne * NP, lane);
-        if (stage_res)
-          for (int f = 0; f < F; ++f)
-            stage_out(a.res + f * Knp + el0 * NP, rbuf + f * FNP, ne * NP, lane);
-        if (lane == 0) {
-          bulk_commit();
-          bulk_wait_read();     // the buffers may be refilled now
-        }
-        __syncwarp();
-      }
-      if (NSTG == 1 && i + 1 < nb_cta) load_stage(i + 1);
+      // the consumers are done with this stage buffer (and the residual
+      // buffer): refill them
+      if (i + NSTG < nb_cta) load_stage(i + NSTG);
       if (stage_res && i + 1 < nb_cta) load_res(i + 1);
     }
-    if (lane == 0) {
-      if (!ok) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
-      bulk_wait_all();
-    }
+    if (lane == 0 && !ok) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
     cp_async_drain();
     __syncwarp();
   } else {
@@ -720,13 +769,124 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(mb);
     };
-    // A warp whose bounded wait gave up sets `bad` and does no more work.  With
-    // FP16 planes the consumers meet at one barrier per batch (row maxima of
-    // the state): there every warp learns of it and all leave together, so no
-    // warp is left waiting at a barrier.
+    // A warp whose bounded wait gave up sets `bad` and does no more work, but
+    // still takes every barrier of the batch; at the next batch's consumer
+    // barrier every warp learns of it and all leave together, so no warp is
+    // left waiting at a barrier.
     int bad = 0;
+    // Phase A of the batch with local index `its`: wait for its stage buffer,
+    // split its state into the planes, signal the MMA warp.  Returns true
+    // when the consumers must leave (a warp's bounded wait gave up).
+    auto split = [&](uint32_t its, float (&lin_out)[DIM]) -> bool {
+      const int b = NSTG == 2 ? (int)(its & 1u) : 0;
+      const uint32_t par = its & 1u;
+      const int64_t el0 = ((int64_t)blockIdx.x + (int64_t)its * gridDim.x) * EB;
+      const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
+      double* st = reinterpret_cast<double*>(smem + S::ostg + b * S::bStage);
+      const bool valid = lane_used && e_lane < ne;
+      const int e_own = valid ? e_lane : 0;
+      uint32_t* rmx = rsq + par * 128;
+      if (!bad && !warp_wait(&mbar[MB_FULL + b], (its / NSTG) & 1u)) {
+        if (lane == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+        bad = 1;
+      }
+        // ---- A: remainders after the element's FP64 linear interpolant, split
+        // into the state planes (one row per lane, 8 columns per item) ----
+        {
+          double v0 = 0.0, dv[DIM];
+  #pragma unroll
+          for (int d = 0; d < DIM; ++d) dv[d] = 0.0;
+          if (valid && !bad) {
+            const double* q = st + fown * FNP + e_own * NP;
+            v0 = q[0];
+  #pragma unroll
+            for (int d = 0; d < DIM; ++d) dv[d] = q[svert[d]] - v0;
+          }
+  #pragma unroll
+          for (int d = 0; d < DIM; ++d) lin_out[d] = (float)(0.5 * dv[d]);
+          // chunks wholly in the K padding stay zero from the set-up unless the
+          // rhs rows alias the planes
+          constexpr int NCHUNK = S::RHS_OWN ? (NP + 7) / 8 : KD / 8;
+          constexpr int NITEM = 4 * NCHUNK;
+          constexpr int IPW = (NITEM + NCW - 1) / NCW;
+          float rem[IPW][8];
+          uint32_t rmax = 0u;
+  #pragma unroll
+          for (int k = 0; k < IPW; ++k) {
+            const int item = warp + k * NCW;
+            const int chunk = item >> 2;
+  #pragma unroll
+            for (int c = 0; c < 8; ++c) {
+              const int j = chunk * 8 + c;
+              float v = 0.f;
+              if (item < NITEM && valid && !bad && j < NP) {
+                double l = v0;
+  #pragma unroll
+                for (int d = 0; d < DIM; ++d) l += lamc[j * DIM + d] * dv[d];
+                v = (float)(st[fown * FNP + e_own * NP + j] - l);
+              }
+              rem[k][c] = v;
+              rmax = max(rmax, __float_as_uint(fabsf(v)));
+            }
+          }
+          float inv = 1.0f;
+          if constexpr (PT == PT_FP16) atomicMax(&rmx[row], rmax);
+          // every consumer is past the previous batch's epilogue (the rhs rows
+          // may alias these planes); FP16: the row maxima are complete
+          if (cbar_or(bad)) return true;
+          if constexpr (PT == PT_FP16) {
+            // clear the next batch's maxima
+            if (tid < 128) rsq[(par ^ 1u) * 128 + tid] = 0u;
+            inv = row_scale_inv(rmx[row]);
+          }
+  #pragma unroll
+          for (int k = 0; k < IPW; ++k) {
+            const int item = warp + k * NCW;
+            if (item < NITEM) {
+              const int chunk = item >> 2;
+              uint32_t hw[4], lw[4];
+  #pragma unroll
+              for (int c = 0; c < 8; c += 2) {
+                const float x0 = rem[k][c] * inv, x1 = rem[k][c + 1] * inv;
+                if constexpr (PT == PT_BF16) {
+                  const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+                  const float2 hf = __bfloat1622float2(h);
+                  const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+                  hw[c / 2] = *reinterpret_cast<const uint32_t*>(&h);
+                  lw[c / 2] = *reinterpret_cast<const uint32_t*>(&l);
+                } else {
+                  const __half2 h = __floats2half2_rn(x0, x1);
+                  const float2 hf = __half22float2(h);
+                  const __half2 l = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+                  hw[c / 2] = *reinterpret_cast<const uint32_t*>(&h);
+                  lw[c / 2] = *reinterpret_cast<const uint32_t*>(&l);
+                }
+              }
+              const uint32_t off = kmajor_off(row, chunk * 8, KD);
+              *reinterpret_cast<uint4*>(Aqh + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+              *reinterpret_cast<uint4*>(Aql + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+            }
+          }
+        }
+        // the diff MMA (issued by the MMA warp) reads the planes
+        tc::fence_proxy_async();
+        tc::fence_before_sync();
+        warp_arrive(&mbar[MB_AREADY]);
+      return false;
+    };
+    // Software pipeline (when two stage buffers, an rhs buffer of its own and
+    // parked volume terms allow it): each warp splits batch i + 1 between
+    // the volume terms and the lift epilogue of batch i, so the wait for
+    // batch i's lift MMA overlaps that work.  Otherwise batch i's split
+    // opens its own iteration.
+    constexpr bool PIPE = S::PARK && NSTG == 2 && S::RHS_OWN;
+    float lin[DIM], lin_next[DIM];   // reference derivatives of the removed interpolants
+    bool leave = false;
+    if constexpr (PIPE) {
+      if (nb_cta > 0) leave = split(0u, lin_next);
+    }
     uint32_t it = 0;
-    for (int64_t batch = blockIdx.x; batch < a.nbatch; batch += gridDim.x, ++it) {
+    for (int64_t batch = blockIdx.x; !leave && batch < a.nbatch; batch += gridDim.x, ++it) {
       const int b = NSTG == 2 ? (int)(it & 1u) : 0;
       const uint32_t par = it & 1u;
       const int64_t el0 = batch * EB;
@@ -741,89 +901,11 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
       uint32_t* rmx = rsq + par * 128;     // this batch's state row maxima
       uint32_t* fmx = rsf + par * 128;     // this batch's flux row maxima
 
-      if (!bad && !warp_wait(&mbar[MB_FULL + b], (it / NSTG) & 1u)) {
-        if (lane == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
-        bad = 1;
+      if constexpr (!PIPE) {
+        if (split(it, lin_next)) break;
       }
-      if (PT == PT_BF16 && bad) break;
-
-      // ---- A: remainders after the element's FP64 linear interpolant, split
-      // into the state planes (one row per lane, 8 columns per item) ----
-      float lin[DIM];   // reference derivatives of the removed interpolant
-      {
-        double v0 = 0.0, dv[DIM];
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) dv[d] = 0.0;
-        if (valid && !bad) {
-          const double* q = st + fown * FNP + e_own * NP;
-          v0 = q[0];
-#pragma unroll
-          for (int d = 0; d < DIM; ++d) dv[d] = q[svert[d]] - v0;
-        }
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) lin[d] = (float)(0.5 * dv[d]);
-        float rem[S::IPW][8];
-        uint32_t rmax = 0u;
-#pragma unroll
-        for (int k = 0; k < S::IPW; ++k) {
-          const int item = warp + k * NCW;
-          const int chunk = item >> 2;
-#pragma unroll
-          for (int c = 0; c < 8; ++c) {
-            const int j = chunk * 8 + c;
-            float v = 0.f;
-            if (item < S::NITEM && valid && !bad && j < NP) {
-              double l = v0;
-#pragma unroll
-              for (int d = 0; d < DIM; ++d) l += slam[j * DIM + d] * dv[d];
-              v = (float)(st[fown * FNP + e_own * NP + j] - l);
-            }
-            rem[k][c] = v;
-            rmax = max(rmax, __float_as_uint(fabsf(v)));
-          }
-        }
-        float inv = 1.0f;
-        if constexpr (PT == PT_FP16) {
-          atomicMax(&rmx[row], rmax);
-          if (cbar_or(bad)) break;
-          // every warp is past the previous epilogue: clear the next maxima
-          if (tid < 128) rsq[(par ^ 1u) * 128 + tid] = 0u;
-          inv = row_scale_inv(rmx[row]);
-        }
-#pragma unroll
-        for (int k = 0; k < S::IPW; ++k) {
-          const int item = warp + k * NCW;
-          if (item < S::NITEM) {
-            const int chunk = item >> 2;
-            uint32_t hw[4], lw[4];
-#pragma unroll
-            for (int c = 0; c < 8; c += 2) {
-              const float x0 = rem[k][c] * inv, x1 = rem[k][c + 1] * inv;
-              if constexpr (PT == PT_BF16) {
-                const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
-                const float2 hf = __bfloat1622float2(h);
-                const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
-                hw[c / 2] = *reinterpret_cast<const uint32_t*>(&h);
-                lw[c / 2] = *reinterpret_cast<const uint32_t*>(&l);
-              } else {
-                const __half2 h = __floats2half2_rn(x0, x1);
-                const float2 hf = __half22float2(h);
-                const __half2 l = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
-                hw[c / 2] = *reinterpret_cast<const uint32_t*>(&h);
-                lw[c / 2] = *reinterpret_cast<const uint32_t*>(&l);
-              }
-            }
-            const uint32_t off = kmajor_off(row, chunk * 8, KD);
-            *reinterpret_cast<uint4*>(Aqh + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
-            *reinterpret_cast<uint4*>(Aql + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
-          }
-        }
-      }
-      // the diff MMA (issued by the MMA warp) reads the planes
-      tc::fence_proxy_async();
-      tc::fence_before_sync();
-      warp_arrive(&mbar[MB_AREADY]);
-
+      for (int d = 0; d < DIM; ++d) lin[d] = lin_next[d];
       // ---- C: face fluxes (FP32 on jumps formed in FP64) -> lift planes.
       // Warp w takes the elements w, w + NCW, ... of the batch and lane l
       // their face points l, l + 32, ..., so each flux row (e, f) lies in one
@@ -983,7 +1065,8 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
               for (int sl = 0; sl < SPE; ++sl) {
                 const int p = lane + sl * 32;
                 if (p < NFPT)
-                  store_split<PT>(Afh, Afl, kmajor_off(rowb + f, p, KL), uPs[jj * SPE + sl][f] * inv);
+                  store_split<PT>(Afh, Afl, fplane_off<FSW>(rowb + f, p, KL),
+                                  uPs[jj * SPE + sl][f] * inv);
               }
             }
           }
@@ -992,12 +1075,12 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
       tc::fence_proxy_async();
       warp_arrive(&mbar[MB_FREADY]);
 
-      // ---- E: TMEM -> chain rule, volume terms, + lift -> FP64 stage update
-      // in place (the I/O warp stores the buffers out).  With few nodes per
-      // warp (S::PARK) the volume terms (diff accumulators only) are formed
-      // first, 4 nodes per pass, and parked in this warp's own TMEM columns,
-      // so the wait for the lift MMA overlaps them and both loops stay rolled
-      // up (a small instruction footprint) ----
+      // ---- E1: TMEM -> chain rule, volume terms, + lift -> FP32 rhs rows in
+      // shared memory, 4 nodes per pass.  With few nodes per warp (S::PARK)
+      // the volume terms (diff accumulators only) are formed first and parked
+      // in this warp's own TMEM columns, so the wait for the lift MMA
+      // overlaps them and both loops stay rolled up (a small instruction
+      // footprint) ----
       constexpr int CHK = S::NPQ < 8 ? S::NPQ : 8;   // TMEM columns per wait
       constexpr int NCH = (S::NPQ + CHK - 1) / CHK;
       constexpr bool VOL_FIRST = S::PARK;
@@ -1007,60 +1090,77 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
       // parked volume terms: columns [VCOL + i_lo, VCOL + i_lo + NPQ), this
       // warp's lanes only
       const uint32_t tmem_vol = tmem + S::VCOL + lane_addr;
+      float* rrow = rhs_s + row * NPR;
       float gm[DIM][DIM];
       float sdiff = a.op_scale_d;
+      // Maxwell divides by eps (E) or mu (H): one reciprocal per lane
+      const float inv_m = MODEL == HB_MODEL_MAXWELL
+                              ? 1.0f / (float)(fown < 3 ? a.mp.eps : a.mp.mu) : 1.0f;
+      auto rhs_of = [&](int i, float vol, float lift) -> float {
+        if constexpr (MODEL == HB_MODEL_MAXWELL) {
+          return (vol + lift) * inv_m;
+        } else {
+          const float src = a.source ? (float)a.source[(el0 + e_own) * NP + i] : 0.f;
+          return model_finish<MODEL, DIM, float>(a.mp, fown, vol, lift, src);
+        }
+      };
       if constexpr (VOL_FIRST) {
-        if (!warp_wait(&mbar[MB_DIFF], par)) {
+        if (!bad && !warp_wait(&mbar[MB_DIFF], par)) {
           if (lane == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
           bad = 1;
-          if (PT == PT_BF16) break;
-          continue;   // leaves at the next batch's barrier (or the loop's end)
         }
-        tc::fence_after_sync();
-        const float* ge = sgeo + e_own * G;
+        if (!bad) {
+          tc::fence_after_sync();
+          const float* ge = sgeo + e_own * G;
 #pragma unroll
-        for (int r = 0; r < DIM; ++r)
+          for (int r = 0; r < DIM; ++r)
 #pragma unroll
-          for (int x = 0; x < DIM; ++x) gm[r][x] = ge[r * DIM + x];
-        if constexpr (PT == PT_FP16) sdiff *= row_scale(rmx[row]);
+            for (int x = 0; x < DIM; ++x) gm[r][x] = ge[r * DIM + x];
+          if constexpr (PT == PT_FP16) sdiff *= row_scale(rmx[row]);
 #pragma unroll 1
-        for (int c0 = i_lo; c0 < i_hi; c0 += 4) {
-          float dv[DIM][4], v4[4] = {0.f, 0.f, 0.f, 0.f};
+          for (int c0 = i_lo; c0 < i_hi; c0 += 4) {
+            float dv[DIM][4], v4[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-          for (int r = 0; r < DIM; ++r) tc::tmem_ld4(tmem_diff + lane_addr + r * NP + c0, dv[r]);
-          tc::tmem_wait_ld();
+            for (int r = 0; r < DIM; ++r) tc::tmem_ld4(tmem_diff + lane_addr + r * NP + c0, dv[r]);
+            tc::tmem_wait_ld();
 #pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            const int i = c0 + c;
-            if (i >= i_hi) break;        // warp-uniform
-            float g[DIM];
+            for (int c = 0; c < 4; ++c) {
+              const int i = c0 + c;
+              if (i >= i_hi) break;        // warp-uniform
+              float g[DIM];
 #pragma unroll
-            for (int x = 0; x < DIM; ++x) {
-              float t = 0.f;
+              for (int x = 0; x < DIM; ++x) {
+                float t = 0.f;
 #pragma unroll
-              for (int r = 0; r < DIM; ++r) t += gm[r][x] * (dv[r][c] * sdiff + lin[r]);
-              g[x] = t;
+                for (int r = 0; r < DIM; ++r) t += gm[r][x] * (dv[r][c] * sdiff + lin[r]);
+                g[x] = t;
+              }
+              const float cnode = C ? (float)scoef[e_own * NP + i] : 0.f;
+              v4[c] = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
             }
-            const float cnode = C ? (float)scoef[e_own * NP + i] : 0.f;
-            v4[c] = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
+            tc::tmem_st4(tmem_vol + c0, v4);
           }
-          tc::tmem_st4(tmem_vol + c0, v4);
+          tc::tmem_wait_st();
         }
-        tc::tmem_wait_st();
+      }
+      if constexpr (PIPE) {
+        // the next batch's split, while this batch's lift MMA runs
+        if ((int64_t)it + 1 < nb_cta && split(it + 1u, lin_next)) break;
       }
       // (FREADY also orders the flux row maxima the other warps wrote)
-      const bool wf = PT == PT_BF16 || warp_wait(&mbar[MB_FREADY], par);
-      const bool w0 = wf && (VOL_FIRST || warp_wait(&mbar[MB_DIFF], par));
-      const bool w1 = w0 && warp_wait(&mbar[MB_LIFT], par);
-      const bool wr = !stage_res || (w1 && warp_wait(&mbar[MB_RES_FULL], par));
-      if (!(w0 && w1 && wr)) {
-        if (lane == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
-        bad = 1;
-        if (PT == PT_BF16) break;
-        continue;   // leaves at the next batch's barrier (or the loop's end)
-      }
-      tc::fence_after_sync();
       {
+        bool ok = !bad;
+        if (ok && PT == PT_FP16) ok = warp_wait(&mbar[MB_FREADY], par);
+        if (ok && !VOL_FIRST) ok = warp_wait(&mbar[MB_DIFF], par);
+        if (ok) ok = warp_wait(&mbar[MB_LIFT], par);
+        if (ok && stage_res) ok = warp_wait(&mbar[MB_RES_FULL], par);
+        if (!bad && !ok) {
+          if (lane == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+          bad = 1;
+        }
+      }
+      if (!bad) {
+        tc::fence_after_sync();
         if constexpr (!VOL_FIRST) {
           const float* ge = sgeo + e_own * G;
 #pragma unroll
@@ -1072,45 +1172,25 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
         float slift = a.op_scale_l;
         if constexpr (PT == PT_FP16)
           slift *= row_scale(fmx[row]);   // written in C by the row's owner warp
-        double* qo = st + fown * FNP + e_own * NP;
-        double* ro = rbuf + fown * FNP + e_own * NP;
-        const int64_t gidx = fown * Knp + (el0 + e_own) * NP;
-        // rhs of node i -> stage update in place (or the rhs itself)
-        auto finish = [&](int i, float mine, float lift) {
-          if (valid) {
-            const float src = a.source ? (float)a.source[(el0 + e_own) * NP + i] : 0.f;
-            const double rr =
-                (double)model_finish<MODEL, DIM, float>(a.mp, fown, mine, lift * slift, src);
-            if (a.mode == 0) {
-              qo[i] = rr;
-            } else {
-              const double r0 = S::RES ? ro[i] : a.res[gidx + i];
-              const double nr = a.ra * r0 + a.dt * rr;
-              if constexpr (S::RES) ro[i] = nr;
-              else a.res[gidx + i] = nr;
-              qo[i] = qo[i] + a.rb * nr;
-            }
-          }
-        };
         if constexpr (VOL_FIRST) {
 #pragma unroll 1
           for (int c0 = i_lo; c0 < i_hi; c0 += 4) {
-            float lv[4], v4[4];
+            float lv[4], v4[4], o[4];
             tc::tmem_ld4(tmem_lift + lane_addr + c0, lv);
             tc::tmem_ld4(tmem_vol + c0, v4);
             tc::tmem_wait_ld();
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-              if (c0 + c >= i_hi) break;   // warp-uniform
-              finish(c0 + c, v4[c], lv[c]);
-            }
+            for (int c = 0; c < 4; ++c) o[c] = rhs_of(c0 + c, v4[c], lv[c] * slift);
+            // parts own 4-aligned node ranges; the last part's nodes past
+            // Np land in the row's padding (NPR)
+            if (valid) *reinterpret_cast<float4*>(rrow + c0) = make_float4(o[0], o[1], o[2], o[3]);
           }
         } else {
 #pragma unroll
           for (int kc = 0; kc < NCH; ++kc) {
             const int c0 = i_lo + kc * CHK;
             if (c0 >= i_hi) break;         // warp-uniform
-            float dv[DIM][CHK], lv[CHK];
+            float dv[DIM][CHK], lv[CHK], o[CHK];
 #pragma unroll
             for (int g = 0; g < CHK / 4; ++g) {
               if (c0 + 4 * g < i_hi) {     // warp-uniform
@@ -1126,7 +1206,8 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
 #pragma unroll
             for (int c = 0; c < CHK; ++c) {
               const int i = c0 + c;
-              if (i >= i_hi) break;        // warp-uniform
+              o[c] = 0.f;
+              if (i >= i_hi) continue;     // warp-uniform
               float g[DIM];
 #pragma unroll
               for (int x = 0; x < DIM; ++x) {
@@ -1136,12 +1217,92 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
                 g[x] = t;
               }
               const float cnode = C ? (float)scoef[e_own * NP + i] : 0.f;
-              finish(i, volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode), lv[c]);
+              o[c] = rhs_of(i, volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode),
+                            lv[c] * slift);
+            }
+#pragma unroll
+            for (int g = 0; g < CHK / 4; ++g)
+              if (valid && c0 + 4 * g < i_hi)
+                *reinterpret_cast<float4*>(rrow + c0 + 4 * g) =
+                    make_float4(o[4 * g], o[4 * g + 1], o[4 * g + 2], o[4 * g + 3]);
+          }
+        }
+      }
+      // this warp's TMEM reads are done before the next MMAs may be issued
+      tc::fence_before_sync();
+      // the quadrant's rhs rows are complete
+      qbar(quad);
+
+      // ---- E2: FP64 stage update of the quadrant's elements, coalesced: a
+      // field's values of consecutive elements are contiguous in the state
+      // vectors (q_in from the stage buffer; res and q_out in global memory,
+      // res in place).  Thread t takes positions x = t + QT k of every field,
+      // so its index arithmetic is done once per batch ----
+      if (!bad) {
+        const int e_first = quad * EPW;
+        const int nq = ne - e_first < EPW ? ne - e_first : EPW;
+        if (nq > 0) {
+          constexpr int QT = 32 * (NCW / 4);
+          constexpr int KX = (EPW * NP + QT - 1) / QT;   // positions per thread
+          const int cnt = nq * NP;                       // values per field
+          const int t = part * 32 + lane;
+          const double* qs = st + e_first * NP;
+          const float* rq = rhs_s + quad * 32 * NPR;
+          const int64_t g0 = (el0 + e_first) * NP;
+          // position k of this thread: x = t + QT k; rhs row (el, f) at node
+          // x - el Np is at rhs offset x + el (F NPR - Np) + f NPR
+          if (a.mode == 0) {
+#pragma unroll
+            for (int k = 0; k < KX; ++k) {
+              const int x = t + QT * k;
+              if (x < cnt) {
+                const int ro = x + (x / NP) * (F * NPR - NP);
+#pragma unroll
+                for (int f = 0; f < F; ++f)
+                  a.q_out[(int64_t)f * Knp + g0 + x] = (double)rq[ro + f * NPR];
+              }
+            }
+          } else {
+            const double ra = a.ra, rb = a.rb, dtt = a.dt;
+            double* res0 = a.res + g0;
+            double* qo0 = a.q_out + g0;
+            // every residual load first (they are independent of the stores):
+            // from the residual buffer when it is staged, else global memory
+            double r0[KX][F];
+            if (stage_res) {
+              const double* rs = rbuf + e_first * NP;
+#pragma unroll
+              for (int k = 0; k < KX; ++k) {
+                const int x = t + QT * k;
+#pragma unroll
+                for (int f = 0; f < F; ++f) r0[k][f] = x < cnt ? rs[f * FNP + x] : 0.0;
+              }
+            } else {
+#pragma unroll
+              for (int k = 0; k < KX; ++k) {
+                const int x = t + QT * k;
+#pragma unroll
+                for (int f = 0; f < F; ++f)
+                  r0[k][f] = x < cnt ? res0[(int64_t)f * Knp + x] : 0.0;
+              }
+            }
+#pragma unroll
+            for (int k = 0; k < KX; ++k) {
+              const int x = t + QT * k;
+              if (x < cnt) {
+                const int ro = x + (x / NP) * (F * NPR - NP);
+#pragma unroll
+                for (int f = 0; f < F; ++f) {
+                  const double nr = ra * r0[k][f] + dtt * (double)rq[ro + f * NPR];
+                  res0[(int64_t)f * Knp + x] = nr;
+                  qo0[(int64_t)f * Knp + x] = qs[f * FNP + x] + rb * nr;
+                }
+              }
             }
           }
         }
       }
-      tc::fence_before_sync();
+      // generic reads of the stage buffer before the I/O warp refills it
       tc::fence_proxy_async();
       warp_arrive(&mbar[MB_DONE + b]);
     }
@@ -1232,7 +1393,7 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
   constexpr int NFPT = S::NFPT, G = S::G, EPW = S::EPW, EB = S::EB, FNP = S::FNP;
   constexpr int KD = S::KD, KL = S::KL, NV1 = DIM + 1;
   constexpr unsigned FULL = 0xffffffffu;
-  extern __shared__ __align__(128) uint8_t smem[];
+  extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* Aqh = smem + S::oAqh;
   uint8_t* Aql = smem + S::oAql;
   uint8_t* Afh = smem + S::oAfh;
@@ -1929,6 +2090,11 @@ static hb_status configure_split(Op* op) {
       for (int j = 0; j < np; ++j)
         for (int dd = 0; dd < DIM; ++dd)
           lam[j * DIM + dd] = 0.5 * (1.0 + d->unit_nodes[(size_t)j * DIM + dd]);
+      // the kernel reads the weights from constant memory (per dimension and
+      // order; every discretization of that order writes the same values)
+      static_assert(S::NP * DIM <= LAM_MAX && ORDER < LAM_ORDERS, "weight table too small");
+      HB_CUDA(cudaMemcpyToSymbol(c_lam, lam, sizeof(double) * np * DIM,
+                                 sizeof(double) * (((DIM - 2) * LAM_ORDERS + ORDER) * LAM_MAX)));
     }
     const double sd = plane_scale(Dt, PT), sl = plane_scale(Lt, PT);
     build_planes(Dt, DIM * np, np, S::ND, S::KD, PT, sd, img.data(), img.data() + bD);

@@ -24,6 +24,22 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
   return d;                // base offset 0, layout type 0 (no swizzle)
 }
 
+// Shared-memory matrix descriptor, K-major, 128-byte swizzle: 8-row atoms of
+// 128-byte rows (1024 bytes, 1024-byte aligned), the 16-byte chunk index of
+// a row XORed with the row's index in its atom; `sbo` = byte distance between
+// 8-row groups.  One MMA's 16-bit K slice (32 bytes) lies within an atom row:
+// K steps advance the start address by 32 bytes.  The leading byte offset is
+// unused in this layout.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+  d |= (uint64_t)2 << 61;  // layout type: 128-byte swizzle
+  return d;
+}
+
 // Instruction descriptor of kind::f16: A and B both BF16 (bf16 = true) or
 // both FP16, FP32 accumulation, both operands K-major.
 __host__ __device__ constexpr uint32_t idesc_16bit(int M, int N, bool bf16) {

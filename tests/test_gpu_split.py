@@ -73,10 +73,11 @@ def test_split_varwave_2d(cuda_device, precision):
 @pytest.mark.parametrize("precision", PRECS)
 def test_split_cavity_rhs(cuda_device, precision):
     """The benchmark's field (cavity mode + 1e-3 noise) on a 6^3 box."""
-    import bench
+    from hedge_b200 import workloads
     from oracle import OracleRHS
-    _, _, d, op = bench.build_problem(6, 4, precision)
-    w = bench.cavity_ic(d)
+    d = hb.Discretization(workloads.box_mesh(6), order=4, precision=precision)
+    op = workloads.operator("maxwell")
+    w = workloads.cavity_ic(d)
     ref = OracleRHS(d, op.op_template())(w)
     got = op.bind(d)(0.0, w).cpu().numpy()
     err = rel_l2(got, ref)
