@@ -794,15 +794,15 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
         // into the state planes (one row per lane, 8 columns per item) ----
         {
           double v0 = 0.0, dv[DIM];
-  #pragma unroll
+#pragma unroll
           for (int d = 0; d < DIM; ++d) dv[d] = 0.0;
           if (valid && !bad) {
             const double* q = st + fown * FNP + e_own * NP;
             v0 = q[0];
-  #pragma unroll
+#pragma unroll
             for (int d = 0; d < DIM; ++d) dv[d] = q[svert[d]] - v0;
           }
-  #pragma unroll
+#pragma unroll
           for (int d = 0; d < DIM; ++d) lin_out[d] = (float)(0.5 * dv[d]);
           // chunks wholly in the K padding stay zero from the set-up unless the
           // rhs rows alias the planes
@@ -811,17 +811,17 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
           constexpr int IPW = (NITEM + NCW - 1) / NCW;
           float rem[IPW][8];
           uint32_t rmax = 0u;
-  #pragma unroll
+#pragma unroll
           for (int k = 0; k < IPW; ++k) {
             const int item = warp + k * NCW;
             const int chunk = item >> 2;
-  #pragma unroll
+#pragma unroll
             for (int c = 0; c < 8; ++c) {
               const int j = chunk * 8 + c;
               float v = 0.f;
               if (item < NITEM && valid && !bad && j < NP) {
                 double l = v0;
-  #pragma unroll
+#pragma unroll
                 for (int d = 0; d < DIM; ++d) l += lamc[j * DIM + d] * dv[d];
                 v = (float)(st[fown * FNP + e_own * NP + j] - l);
               }
@@ -839,13 +839,13 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
             if (tid < 128) rsq[(par ^ 1u) * 128 + tid] = 0u;
             inv = row_scale_inv(rmx[row]);
           }
-  #pragma unroll
+#pragma unroll
           for (int k = 0; k < IPW; ++k) {
             const int item = warp + k * NCW;
             if (item < NITEM) {
               const int chunk = item >> 2;
               uint32_t hw[4], lw[4];
-  #pragma unroll
+#pragma unroll
               for (int c = 0; c < 8; c += 2) {
                 const float x0 = rem[k][c] * inv, x1 = rem[k][c + 1] * inv;
                 if constexpr (PT == PT_BF16) {
@@ -873,6 +873,100 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
         tc::fence_before_sync();
         warp_arrive(&mbar[MB_AREADY]);
       return false;
+    };
+    // Phase E2 of the batch with local index `its`, once the quadrant's rhs
+    // rows are complete: the coalesced FP64 update, then the stage buffer
+    // (and the residual buffer) go back to the I/O warp.
+    auto update = [&](uint32_t its) {
+      const int b = NSTG == 2 ? (int)(its & 1u) : 0;
+      const int64_t el0 = ((int64_t)blockIdx.x + (int64_t)its * gridDim.x) * EB;
+      const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
+      double* st = reinterpret_cast<double*>(smem + S::ostg + b * S::bStage);
+      if (!bad && stage_res && !warp_wait(&mbar[MB_RES_FULL], its & 1u)) {
+        if (lane == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
+        bad = 1;
+      }
+        // ---- E2: FP64 stage update of the quadrant's elements, coalesced: a
+        // field's values of consecutive elements are contiguous in the state
+        // vectors (q_in from the stage buffer; res and q_out in global memory,
+        // res in place).  Thread t takes positions x = t + QT k of every field,
+        // so its index arithmetic is done once per batch ----
+        if (!bad) {
+          const int e_first = quad * EPW;
+          const int nq = ne - e_first < EPW ? ne - e_first : EPW;
+          if (nq > 0) {
+            constexpr int QT = 32 * (NCW / 4);
+            constexpr int KX = (EPW * NP + QT - 1) / QT;   // positions per thread
+            const int cnt = nq * NP;                       // values per field
+            const int t = part * 32 + lane;
+            const double* qs = st + e_first * NP;
+            const float* rq = rhs_s + quad * 32 * NPR;
+            const int64_t g0 = (el0 + e_first) * NP;
+            // position k of this thread: x = t + QT k; rhs row (el, f) at node
+            // x - el Np is at rhs offset x + el (F NPR - Np) + f NPR
+            if (a.mode == 0) {
+#pragma unroll
+              for (int k = 0; k < KX; ++k) {
+                const int x = t + QT * k;
+                if (x < cnt) {
+                  const int ro = x + (x / NP) * (F * NPR - NP);
+#pragma unroll
+                  for (int f = 0; f < F; ++f)
+                    a.q_out[(int64_t)f * Knp + g0 + x] = (double)rq[ro + f * NPR];
+                }
+              }
+            } else {
+              const double ra = a.ra, rb = a.rb, dtt = a.dt;
+              double* res0 = a.res + g0;
+              double* qo0 = a.q_out + g0;
+              if constexpr (S::RES) {
+                // residual from the residual buffer (short latency): one
+                // value at a time, few registers live
+                const double* rs = rbuf + e_first * NP;
+#pragma unroll 1
+                for (int k = 0; k < KX; ++k) {
+                  const int x = t + QT * k;
+                  if (x < cnt) {
+                    const int ro = x + (x / NP) * (F * NPR - NP);
+#pragma unroll
+                    for (int f = 0; f < F; ++f) {
+                      const double nr = ra * rs[f * FNP + x] + dtt * (double)rq[ro + f * NPR];
+                      res0[(int64_t)f * Knp + x] = nr;
+                      qo0[(int64_t)f * Knp + x] = qs[f * FNP + x] + rb * nr;
+                    }
+                  }
+                }
+              } else {
+                // residual from global memory: every load first (they are
+                // independent of the stores)
+                double r0[KX][F];
+#pragma unroll
+                for (int k = 0; k < KX; ++k) {
+                  const int x = t + QT * k;
+#pragma unroll
+                  for (int f = 0; f < F; ++f)
+                    r0[k][f] = x < cnt ? res0[(int64_t)f * Knp + x] : 0.0;
+                }
+#pragma unroll
+                for (int k = 0; k < KX; ++k) {
+                  const int x = t + QT * k;
+                  if (x < cnt) {
+                    const int ro = x + (x / NP) * (F * NPR - NP);
+#pragma unroll
+                    for (int f = 0; f < F; ++f) {
+                      const double nr = ra * r0[k][f] + dtt * (double)rq[ro + f * NPR];
+                      res0[(int64_t)f * Knp + x] = nr;
+                      qo0[(int64_t)f * Knp + x] = qs[f * FNP + x] + rb * nr;
+                    }
+                  }
+                }
+              }
+            }
+          }
+        }
+        // generic reads of the stage buffer before the I/O warp refills it
+        tc::fence_proxy_async();
+        warp_arrive(&mbar[MB_DONE + b]);
     };
     // Software pipeline (when two stage buffers, an rhs buffer of its own and
     // parked volume terms allow it): each warp splits batch i + 1 between
@@ -902,7 +996,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
       uint32_t* fmx = rsf + par * 128;     // this batch's flux row maxima
 
       if constexpr (!PIPE) {
-        if (split(it, lin_next)) break;
+        if (split(it, lin_next)) { leave = true; break; }
       }
 #pragma unroll
       for (int d = 0; d < DIM; ++d) lin[d] = lin_next[d];
@@ -1061,12 +1155,42 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
                 if (lane == 0) fmx[rowb + f] = m;
                 inv = row_scale_inv(m);
               }
+              const int frow = rowb + f;
+              // slots in pairs: one packed conversion splits both values
 #pragma unroll
-              for (int sl = 0; sl < SPE; ++sl) {
-                const int p = lane + sl * 32;
+              for (int sl = 0; sl + 1 < SPE; sl += 2) {
+                const int p0 = lane + sl * 32, p1 = p0 + 32;
+                const float x0 = uPs[jj * SPE + sl][f] * inv, x1 = uPs[jj * SPE + sl + 1][f] * inv;
+                uint32_t hh, ll;
+                if constexpr (PT == PT_BF16) {
+                  const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+                  const float2 hf = __bfloat1622float2(h);
+                  const __nv_bfloat162 l = __floats2bfloat162_rn(x0 - hf.x, x1 - hf.y);
+                  hh = *reinterpret_cast<const uint32_t*>(&h);
+                  ll = *reinterpret_cast<const uint32_t*>(&l);
+                } else {
+                  const __half2 h = __floats2half2_rn(x0, x1);
+                  const float2 hf = __half22float2(h);
+                  const __half2 l = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+                  hh = *reinterpret_cast<const uint32_t*>(&h);
+                  ll = *reinterpret_cast<const uint32_t*>(&l);
+                }
+                if (p0 < NFPT) {
+                  const uint32_t o0 = fplane_off<FSW>(frow, p0, KL);
+                  *reinterpret_cast<uint16_t*>(Afh + o0) = (uint16_t)hh;
+                  *reinterpret_cast<uint16_t*>(Afl + o0) = (uint16_t)ll;
+                }
+                if (p1 < NFPT) {
+                  const uint32_t o1 = fplane_off<FSW>(frow, p1, KL);
+                  *reinterpret_cast<uint16_t*>(Afh + o1) = (uint16_t)(hh >> 16);
+                  *reinterpret_cast<uint16_t*>(Afl + o1) = (uint16_t)(ll >> 16);
+                }
+              }
+              if constexpr (SPE % 2 == 1) {
+                const int p = lane + (SPE - 1) * 32;
                 if (p < NFPT)
-                  store_split<PT>(Afh, Afl, fplane_off<FSW>(rowb + f, p, KL),
-                                  uPs[jj * SPE + sl][f] * inv);
+                  store_split<PT>(Afh, Afl, fplane_off<FSW>(frow, p, KL),
+                                  uPs[jj * SPE + SPE - 1][f] * inv);
               }
             }
           }
@@ -1112,40 +1236,93 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
         if (!bad) {
           tc::fence_after_sync();
           const float* ge = sgeo + e_own * G;
-#pragma unroll
-          for (int r = 0; r < DIM; ++r)
-#pragma unroll
-            for (int x = 0; x < DIM; ++x) gm[r][x] = ge[r * DIM + x];
           if constexpr (PT == PT_FP16) sdiff *= row_scale(rmx[row]);
-#pragma unroll 1
-          for (int c0 = i_lo; c0 < i_hi; c0 += 4) {
-            float dv[DIM][4], v4[4] = {0.f, 0.f, 0.f, 0.f};
+          // gradient component x of the lane's field at a node:
+          //   g_x = off_x + sum_r gs[r][x] acc_r, with gs = (dr/dx) * scale
+          //   and off_x = sum_r (dr/dx) lin_r (the removed interpolant)
+          float gs[DIM][DIM], off[DIM];
 #pragma unroll
-            for (int r = 0; r < DIM; ++r) tc::tmem_ld4(tmem_diff + lane_addr + r * NP + c0, dv[r]);
-            tc::tmem_wait_ld();
+          for (int x = 0; x < DIM; ++x) {
+            off[x] = 0.f;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-              const int i = c0 + c;
-              if (i >= i_hi) break;        // warp-uniform
-              float g[DIM];
-#pragma unroll
-              for (int x = 0; x < DIM; ++x) {
-                float t = 0.f;
-#pragma unroll
-                for (int r = 0; r < DIM; ++r) t += gm[r][x] * (dv[r][c] * sdiff + lin[r]);
-                g[x] = t;
-              }
-              const float cnode = C ? (float)scoef[e_own * NP + i] : 0.f;
-              v4[c] = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
+            for (int r = 0; r < DIM; ++r) {
+              const float gmv = ge[r * DIM + x];
+              gs[r][x] = gmv * sdiff;
+              off[x] += gmv * lin[r];
             }
-            tc::tmem_st4(tmem_vol + c0, v4);
+          }
+          if constexpr (MODEL == HB_MODEL_MAXWELL) {
+            // The curls read of each field's gradient only two components,
+            // on other lanes: the lane of field j (E_j or H_j) offers
+            // oA = d/dx_(j+1) and oB = d/dx_(j+2) (indices mod 3), and
+            //   (curl H)_c = oB(H_(c+2)) - oA(H_(c+1)),
+            //   (curl E)_c = oB(E_(c+2)) - oA(E_(c+1));
+            // E_c takes +curl H, H_c takes -curl E.
+            const int cc = fown % 3;
+            const int xa = cc == 2 ? 0 : cc + 1, xb = cc == 0 ? 2 : cc - 1;
+            float cA[3], cB[3];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+              cA[r] = xa == 0 ? gs[r][0] : (xa == 1 ? gs[r][1] : gs[r][2]);
+              cB[r] = xb == 0 ? gs[r][0] : (xb == 1 ? gs[r][1] : gs[r][2]);
+            }
+            const float offA = xa == 0 ? off[0] : (xa == 1 ? off[1] : off[2]);
+            const float offB = xb == 0 ? off[0] : (xb == 1 ? off[1] : off[2]);
+            const int other = fown < 3 ? 3 : 0;
+            const int srcB = base + other + (cc == 0 ? 2 : cc - 1);   // field (c + 2) mod 3
+            const int srcA = base + other + (cc == 2 ? 0 : cc + 1);   // field (c + 1) mod 3
+            const float sgn = fown < 3 ? 1.f : -1.f;
+#pragma unroll 1
+            for (int c0 = i_lo; c0 < i_hi; c0 += 4) {
+              float dv[DIM][4], v4[4];
+#pragma unroll
+              for (int r = 0; r < DIM; ++r) tc::tmem_ld4(tmem_diff + lane_addr + r * NP + c0, dv[r]);
+              tc::tmem_wait_ld();
+#pragma unroll
+              for (int c = 0; c < 4; ++c) {
+                float oA = offA, oB = offB;
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                  oA += cA[r] * dv[r][c];
+                  oB += cB[r] * dv[r][c];
+                }
+                const float t0 = __shfl_sync(FULL, oB, srcB);
+                const float t1 = __shfl_sync(FULL, oA, srcA);
+                v4[c] = sgn * (t0 - t1);
+              }
+              tc::tmem_st4(tmem_vol + c0, v4);
+            }
+          } else {
+#pragma unroll 1
+            for (int c0 = i_lo; c0 < i_hi; c0 += 4) {
+              float dv[DIM][4], v4[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+              for (int r = 0; r < DIM; ++r) tc::tmem_ld4(tmem_diff + lane_addr + r * NP + c0, dv[r]);
+              tc::tmem_wait_ld();
+#pragma unroll
+              for (int c = 0; c < 4; ++c) {
+                const int i = c0 + c;
+                if (i >= i_hi) break;        // warp-uniform
+                float g[DIM];
+#pragma unroll
+                for (int x = 0; x < DIM; ++x) {
+                  float t = off[x];
+#pragma unroll
+                  for (int r = 0; r < DIM; ++r) t += gs[r][x] * dv[r][c];
+                  g[x] = t;
+                }
+                const float cnode = C ? (float)scoef[e_own * NP + i] : 0.f;
+                v4[c] = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
+              }
+              tc::tmem_st4(tmem_vol + c0, v4);
+            }
           }
           tc::tmem_wait_st();
         }
       }
       if constexpr (PIPE) {
         // the next batch's split, while this batch's lift MMA runs
-        if ((int64_t)it + 1 < nb_cta && split(it + 1u, lin_next)) break;
+        if ((int64_t)it + 1 < nb_cta && split(it + 1u, lin_next)) { leave = true; break; }
       }
       // (FREADY also orders the flux row maxima the other warps wrote)
       {
@@ -1153,7 +1330,6 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
         if (ok && PT == PT_FP16) ok = warp_wait(&mbar[MB_FREADY], par);
         if (ok && !VOL_FIRST) ok = warp_wait(&mbar[MB_DIFF], par);
         if (ok) ok = warp_wait(&mbar[MB_LIFT], par);
-        if (ok && stage_res) ok = warp_wait(&mbar[MB_RES_FULL], par);
         if (!bad && !ok) {
           if (lane == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
           bad = 1;
@@ -1233,78 +1409,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
       // the quadrant's rhs rows are complete
       qbar(quad);
 
-      // ---- E2: FP64 stage update of the quadrant's elements, coalesced: a
-      // field's values of consecutive elements are contiguous in the state
-      // vectors (q_in from the stage buffer; res and q_out in global memory,
-      // res in place).  Thread t takes positions x = t + QT k of every field,
-      // so its index arithmetic is done once per batch ----
-      if (!bad) {
-        const int e_first = quad * EPW;
-        const int nq = ne - e_first < EPW ? ne - e_first : EPW;
-        if (nq > 0) {
-          constexpr int QT = 32 * (NCW / 4);
-          constexpr int KX = (EPW * NP + QT - 1) / QT;   // positions per thread
-          const int cnt = nq * NP;                       // values per field
-          const int t = part * 32 + lane;
-          const double* qs = st + e_first * NP;
-          const float* rq = rhs_s + quad * 32 * NPR;
-          const int64_t g0 = (el0 + e_first) * NP;
-          // position k of this thread: x = t + QT k; rhs row (el, f) at node
-          // x - el Np is at rhs offset x + el (F NPR - Np) + f NPR
-          if (a.mode == 0) {
-#pragma unroll
-            for (int k = 0; k < KX; ++k) {
-              const int x = t + QT * k;
-              if (x < cnt) {
-                const int ro = x + (x / NP) * (F * NPR - NP);
-#pragma unroll
-                for (int f = 0; f < F; ++f)
-                  a.q_out[(int64_t)f * Knp + g0 + x] = (double)rq[ro + f * NPR];
-              }
-            }
-          } else {
-            const double ra = a.ra, rb = a.rb, dtt = a.dt;
-            double* res0 = a.res + g0;
-            double* qo0 = a.q_out + g0;
-            // every residual load first (they are independent of the stores):
-            // from the residual buffer when it is staged, else global memory
-            double r0[KX][F];
-            if (stage_res) {
-              const double* rs = rbuf + e_first * NP;
-#pragma unroll
-              for (int k = 0; k < KX; ++k) {
-                const int x = t + QT * k;
-#pragma unroll
-                for (int f = 0; f < F; ++f) r0[k][f] = x < cnt ? rs[f * FNP + x] : 0.0;
-              }
-            } else {
-#pragma unroll
-              for (int k = 0; k < KX; ++k) {
-                const int x = t + QT * k;
-#pragma unroll
-                for (int f = 0; f < F; ++f)
-                  r0[k][f] = x < cnt ? res0[(int64_t)f * Knp + x] : 0.0;
-              }
-            }
-#pragma unroll
-            for (int k = 0; k < KX; ++k) {
-              const int x = t + QT * k;
-              if (x < cnt) {
-                const int ro = x + (x / NP) * (F * NPR - NP);
-#pragma unroll
-                for (int f = 0; f < F; ++f) {
-                  const double nr = ra * r0[k][f] + dtt * (double)rq[ro + f * NPR];
-                  res0[(int64_t)f * Knp + x] = nr;
-                  qo0[(int64_t)f * Knp + x] = qs[f * FNP + x] + rb * nr;
-                }
-              }
-            }
-          }
-        }
-      }
-      // generic reads of the stage buffer before the I/O warp refills it
-      tc::fence_proxy_async();
-      warp_arrive(&mbar[MB_DONE + b]);
+      update(it);
     }
   }
 
