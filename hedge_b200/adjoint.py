@@ -302,8 +302,10 @@ def check_gradients(P, nsteps=400, every=20, ndirs=32, h=1e-6, seed=5, q0=None):
             an = float((gq * dq).sum() + (gc * dc).sum())
             errs["q0" if k % 2 == 0 else "c"].append(abs(fd - an) / max(abs(an), 1e-300))
     allerr = errs["q0"] + errs["c"]
-    return {"loss": L0, "fd_rel_err_max": max(allerr), "fd_rel_err_median": float(np.median(allerr)),
-            "fd_rel_err_max_q0": max(errs["q0"]), "fd_rel_err_max_c": max(errs["c"]),
+    worst = lambda v: max(v) if v else None  # noqa: E731  (fewer than two directions)
+    return {"loss": L0, "fd_rel_err_max": worst(allerr),
+            "fd_rel_err_median": float(np.median(allerr)) if allerr else None,
+            "fd_rel_err_max_q0": worst(errs["q0"]), "fd_rel_err_max_c": worst(errs["c"]),
             "directions": ndirs, "h": h, "t_forward_s": t_fwd, "t_forward_backward_s": t_fb,
             "grad_c_norm": float(gc.norm()), "grad_q0_norm": float(gq.norm())}
 
