@@ -48,7 +48,8 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--precision", default="fp16x3", choices=["fp64", "fp32", "bf16x3", "fp16x3"])
+    p.add_argument("--precision", default="fp16x3",
+                   choices=["fp64", "fp32", "fp32-simt", "bf16x3", "fp16x3"])
     p.add_argument("--workload", default="maxwell", choices=["maxwell", "wave7"],
                    help="maxwell: 3D Maxwell N=4 cavity (default); wave7: 3D acoustic "
                         "wave N=7 Gaussian pulse (the high-order precision workload)")
@@ -382,21 +383,38 @@ def run_ours(args):
     barrier(world)
     stream = torch.cuda.current_stream()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # An FP32 state's stage working set (3 x 40 MB at C2) nearly fits in the
+    # 126 MB L2: those steps are timed one by one, with L2 flushed between
+    # them (a 256 MB write outside the timed events).
+    flush_l2 = args.precision in ("fp32", "fp32-simt")
+    scratch = torch.empty(64 << 20, dtype=torch.float32, device=dev) if flush_l2 else None
     with ClockSampler(dev.index) as clk:
         barrier(world)
-        ev0.record(stream)
-        for _ in range(args.steps):
-            y = stepper(y, t, dt, rhs)
-            t += dt
-        ev1.record(stream)
-        barrier(world)
-    ms = ev0.elapsed_time(ev1)
+        if flush_l2:
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in range(args.steps)]
+            for e_a, e_b in evs:
+                scratch.fill_(1.0)
+                e_a.record(stream)
+                y = stepper(y, t, dt, rhs)
+                t += dt
+                e_b.record(stream)
+            barrier(world)
+            ms = sum(e_a.elapsed_time(e_b) for e_a, e_b in evs)
+        else:
+            ev0.record(stream)
+            for _ in range(args.steps):
+                y = stepper(y, t, dt, rhs)
+                t += dt
+            ev1.record(stream)
+            barrier(world)
+            ms = ev0.elapsed_time(ev1)
     comp.check()
     ms_max = max_over_ranks(ms, world)
     value = K_total * discr.Np * F * 5 * args.steps / (ms_max * 1e-3)
     launches = 5 * args.steps
     launch_ms = ms / launches
-    state_bytes = 8 if args.precision != "fp32" else 4
+    state_bytes = 4 if args.precision in ("fp32", "fp32-simt") else 8
     bpd = algorithmic_bytes_per_dof_update(discr, state_bytes, F)
     bytes_per_launch = bpd * K_rank * discr.Np * F
     achieved = bytes_per_launch / (launch_ms * 1e-3) / 1e9
@@ -532,11 +550,14 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": {"fp64": "f64", "fp32": "f32", "bf16x3": "bf16x3+f32acc, f64 state",
+            "dtype": {"fp64": "f64", "fp32": "f32 state, fp16x3(scaled)+f32acc contractions",
+                      "fp32-simt": "f32", "bf16x3": "bf16x3+f32acc, f64 state",
                       "fp16x3": "fp16x3(scaled)+f32acc, f64 state"}[args.precision],
             "data": "synthetic",
             "config": workload_config(args, K_total, K_rank, discr.Np, F),
             "precision": args.precision,
+            "l2_flush": ("256 MB write before each timed step (FP32 state)" if flush_l2
+                         else "none: working set > L2"),
             "parallelism": ("partitioned, face-trace exchange per stage (NCCL)"
                             if partitioned else "replicas" if world > 1 else "single GPU"),
             # the same rate per LSRK4 time step (5 stages): DOF-steps/s

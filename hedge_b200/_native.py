@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libhedge_b200.so")
 
 HB_OK, HB_ERR_INVALID_ARGUMENT, HB_ERR_UNSUPPORTED, HB_ERR_CUDA, HB_ERR_DEVICE_FLAG = range(5)
-PREC_FP64, PREC_FP32, PREC_BF16X3, PREC_FP16X3 = 0, 1, 2, 3
+PREC_FP64, PREC_FP32, PREC_BF16X3, PREC_FP16X3, PREC_FP32_SIMT = 0, 1, 2, 3, 4
 
 
 class HedgeB200Error(RuntimeError):

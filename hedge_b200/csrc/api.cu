@@ -182,7 +182,7 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
   }
   if (desc->num_fields != F)
     return fail(HB_ERR_INVALID_ARGUMENT, "num_fields does not match the model");
-  if (desc->precision < HB_PREC_FP64 || desc->precision > HB_PREC_FP16X3)
+  if (desc->precision < HB_PREC_FP64 || desc->precision > HB_PREC_FP32_SIMT)
     return fail(HB_ERR_INVALID_ARGUMENT, "unknown precision");
   if (!desc->conn) return fail(HB_ERR_INVALID_ARGUMENT, "null connectivity");
   if (model == HB_MODEL_MAXWELL && !(desc->eps > 0 && desc->mu > 0))
@@ -213,7 +213,8 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
   op->d = d;
   op->model = model;
   op->F = F;
-  op->precision = desc->precision;
+  // FP32_SIMT is the FP32 path kept on the CUDA cores
+  op->precision = desc->precision == HB_PREC_FP32_SIMT ? HB_PREC_FP32 : desc->precision;
   op->n_given = desc->num_given_bdry_nodes;
   op->n_halo = desc->num_halo_faces;
   ModelParams& mp = op->mp;
@@ -237,10 +238,21 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
       cudaMemset(op->err_flag, 0, sizeof(int)) != cudaSuccess)
     return bail(fail(HB_ERR_CUDA, "cannot allocate the device error flag"));
   if (op->precision == HB_PREC_FP32 && (st = ensure_fp32(d))) return bail(st);
-  if (op->precision == HB_PREC_BF16X3 || op->precision == HB_PREC_FP16X3)
+  if (op->precision == HB_PREC_BF16X3 || op->precision == HB_PREC_FP16X3) {
     st = prepare_split(op);
-  else
+    op->split = 1;
+  } else if (op->precision == HB_PREC_FP32 && desc->precision != HB_PREC_FP32_SIMT) {
+    // FP32 state on the tensor cores where a resident kernel is built for
+    // this (model, dimension, order), else on the CUDA cores
+    st = prepare_split(op);
+    op->split = st == HB_OK;
+    if (st == HB_ERR_UNSUPPORTED) {
+      free_split(op);
+      st = prepare_simt(op);
+    }
+  } else {
     st = prepare_simt(op);
+  }
   if (st) return bail(st);
   *out = reinterpret_cast<hb_op*>(op);
   return HB_OK;
@@ -274,7 +286,7 @@ static hb_status run(Op* op, int mode, double a, double b, double dt, const void
   DeviceGuard g(op->d->device);
   if (!g.ok) return fail(HB_ERR_CUDA, "cannot select the CUDA device");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  if (op->precision == HB_PREC_BF16X3 || op->precision == HB_PREC_FP16X3)
+  if (op->split)
     return launch_split(op, mode, a, b, dt, q_in, q_out, res, coeff, bdry, source, s);
   return launch_simt(op, mode, a, b, dt, q_in, q_out, res, coeff, bdry, source, s);
 }

@@ -79,7 +79,8 @@ struct Discr {
 
 struct Op {
   Discr* d;
-  int model, F, precision;
+  int model, F, precision;   // precision: HB_PREC_FP64 .. HB_PREC_FP16X3 (FP32_SIMT is stored as FP32)
+  int split = 0;             // 1: the tensor-core kernels (launch_split), else CUDA cores
   ModelParams mp;
   int2* conn = nullptr;        // [K][nfaces] (nbr, code)
   int64_t n_given;

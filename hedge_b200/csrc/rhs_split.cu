@@ -92,8 +92,9 @@ __host__ __device__ constexpr uint32_t al128(uint32_t x) { return (x + 127u) & ~
 __host__ __device__ constexpr uint32_t al16(uint32_t x) { return (x + 15u) & ~15u; }
 __host__ __device__ constexpr uint32_t al1024(uint32_t x) { return (x + 1023u) & ~1023u; }
 
-// Compile-time shape of one (model, dim, order) instance.
-template <int MODEL, int DIM, int ORDER>
+// Compile-time shape of one (model, dim, order) instance with a state of SB
+// bytes per value (8: FP64, 4: FP32).
+template <int MODEL, int DIM, int ORDER, int SB = 8>
 struct Shape {
   static constexpr int F = Traits<MODEL, DIM>::F;
   static constexpr int C = Traits<MODEL, DIM>::COEFF;
@@ -109,27 +110,31 @@ struct Shape {
   static constexpr int KD = ru16(NP), KL = ru16(NFPT);
   static constexpr int ND = ru16(DIM * NP), NL = ru16(NP);
   static constexpr int LIFT_COL = ru32(ND);
-  // Field stride (in doubles) of the staged state and residual: the EB * NP
+  // Field stride (in values) of the staged state and residual: the EB * NP
   // values of a field, padded so that the consumer lanes' rows (lane =
   // element * F + field) at one node hit distinct shared-memory banks as far
-  // as the layout allows (worst lanes per 8-byte bank pair in a half-warp).
+  // as the layout allows (worst lanes per bank: 8-byte bank pairs in a
+  // half-warp for FP64, 4-byte banks in a warp for FP32), and to 16-byte rows.
+  static constexpr int LPW = SB == 8 ? 16 : 32;   // lanes per wavefront
+  static constexpr int VPR = 16 / SB;             // values per 16 bytes
   static constexpr int bank_collisions(int stride) {
     int worst = 0;
-    for (int half = 0; half < 2; ++half) {
-      int count[16] = {};
-      for (int l = 16 * half; l < 16 * half + 16; ++l) {
+    for (int g = 0; g < 32 / LPW; ++g) {
+      int count[32] = {};
+      for (int l = LPW * g; l < LPW * g + LPW; ++l) {
         if (l / F >= EPW) continue;
-        const int b = ((l % F) * stride + (l / F) * NP) % 16;
+        const int b = ((l % F) * stride + (l / F) * NP) % LPW;
         if (++count[b] > worst) worst = count[b];
       }
     }
     return worst;
   }
   static constexpr int padded_fnp() {
-    int best = EB * NP, bw = bank_collisions(EB * NP);
-    for (int p = 2; p < 32; p += 2) {
-      const int c = bank_collisions(EB * NP + p);
-      if (c < bw) { bw = c; best = EB * NP + p; }
+    const int base = SB == 8 ? EB * NP : (EB * NP + VPR - 1) / VPR * VPR;
+    int best = base, bw = bank_collisions(base);
+    for (int p = VPR; p < 32; p += VPR) {
+      const int c = bank_collisions(base + p);
+      if (c < bw) { bw = c; best = base + p; }
     }
     return best;
   }
@@ -154,7 +159,7 @@ struct Shape {
 
   static constexpr uint32_t bD = ND * KD * 2, bL = NL * KL * 2;
   static constexpr uint32_t bAq = 128 * KD * 2, bAf = 128 * KL * 2;
-  static constexpr uint32_t bState = NVAL * 8;
+  static constexpr uint32_t bState = NVAL * SB;
   // one stage buffer: state [F][EB][NP] FP64, geometry [EB][G] FP32,
   // face table [EB][NF] int2, coefficient [EB][NP] FP64
   static constexpr uint32_t sGeo = bState;
@@ -212,7 +217,8 @@ struct Shape {
                                total <= SMEM_LIMIT;
 };
 
-struct SplitArgs {
+template <typename ST>
+struct SplitArgsT {
   int64_t K, nbatch, n_given;
   int nperm;
   const uint8_t* ops;   // [D_hi | D_lo | L_hi | L_lo] canonical images
@@ -220,13 +226,13 @@ struct SplitArgs {
   const int2* conn;
   const int* fmask;
   const int* shuffle;
-  const double* q_in;
-  double* q_out;
-  double* res;
+  const ST* q_in;
+  ST* q_out;
+  ST* res;
   const double* coeff;
   const double* bdry;
   const double* source;
-  const double* halo;     // [n_halo * nfp][F] ext values of faces on other partitions
+  const ST* halo;         // [n_halo * nfp][F] ext values of faces on other partitions
   const double* halo_c;   // [n_halo * nfp] ext c (var-c wave)
   int64_t n_halo;
   double ra, rb, dt;
@@ -235,6 +241,7 @@ struct SplitArgs {
   ModelParams mp;
   int* err;
 };
+using SplitArgs = SplitArgsT<double>;
 
 // byte offset of element (row, k) in a K-major no-swizzle operand image with
 // K padded to kp: 8x8 core matrices (8 rows x 16 bytes), K chunks 128 B
@@ -498,6 +505,7 @@ enum {
 constexpr int LAM_MAX = 56 * 3;   // up to 3D N = 5 (Np = 56)
 constexpr int LAM_ORDERS = 7;     // orders 0..6
 __constant__ double c_lam[2][LAM_ORDERS][LAM_MAX];
+__constant__ float c_lamf[2][LAM_ORDERS][LAM_MAX];   // the same, FP32 (FP32 state)
 
 // byte offset of (row, k) in a flux plane: the 128-byte swizzled K-major
 // layout (8-row atoms of 128-byte rows, 16-byte chunk index XOR row & 7) when
@@ -517,9 +525,9 @@ __device__ __forceinline__ void qbar(int quad) {
   asm volatile("bar.sync %0, %1;" ::"r"(2 + quad), "n"(32 * (NCW / 4)) : "memory");
 }
 
-template <int MODEL, int DIM, int ORDER, int PT>
-__global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a) {
-  using S = Shape<MODEL, DIM, ORDER>;
+template <int MODEL, int DIM, int ORDER, int PT, typename ST>
+__global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgsT<ST> a) {
+  using S = Shape<MODEL, DIM, ORDER, (int)sizeof(ST)>;
   constexpr int F = S::F, C = S::C, NA = S::NA, NP = S::NP, NFP = S::NFP, NF = S::NF;
   constexpr int NFPT = S::NFPT, G = S::G, EPW = S::EPW, EB = S::EB, FNP = S::FNP;
   constexpr int KD = S::KD, KL = S::KL, NSTG = S::NSTG, NPR = S::NPR;
@@ -531,8 +539,10 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
   uint8_t* Afh = smem + S::oAfh;
   uint8_t* Afl = smem + S::oAfl;
   float* rhs_s = reinterpret_cast<float*>(smem + S::orhs);  // [128][NPR] FP32 rhs rows
-  double* rbuf = reinterpret_cast<double*>(smem + S::ores);  // residual [F][EB][NP]
-  const double* lamc = &c_lam[DIM - 2][ORDER][0];           // [NP][DIM]
+  const ST* lamc;                                            // [NP][DIM] interpolant weights
+  if constexpr (sizeof(ST) == 8) lamc = reinterpret_cast<const ST*>(&c_lam[DIM - 2][ORDER][0]);
+  else lamc = reinterpret_cast<const ST*>(&c_lamf[DIM - 2][ORDER][0]);
+  ST* rbuf = reinterpret_cast<ST*>(smem + S::ores);          // residual [F][EB][NP]
   uint8_t* sfm = smem + S::ofm;
   uint8_t* ssh = smem + S::osh;
   const uint8_t* svert = smem + S::overt;                  // vertex nodes B, C(, D)
@@ -694,7 +704,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
         if (want) mbar_expect_tx(mb, want);
       }
       __syncwarp();
-      double* st = reinterpret_cast<double*>(stg);
+      ST* st = reinterpret_cast<ST*>(stg);
       for (int f = 0; f < F; ++f)
         stage_in(st + f * FNP, a.q_in + f * Knp + el0 * NP, ne * NP, lane, mb);
       stage_in(reinterpret_cast<float*>(stg + S::sGeo), a.geo32 + el0 * G, ne * G, lane, mb);
@@ -721,11 +731,11 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
     auto prefetch = [&](int64_t j, bool state, bool res) {
       if (lane != 0 || j >= nb_cta) return;
       const int64_t e0 = batch_el0(j);
-      const uint32_t bytes = (uint32_t)batch_ne(e0) * NP * 8u;
+      const uint32_t bytes = (uint32_t)batch_ne(e0) * NP * (uint32_t)sizeof(ST);
       for (int f = 0; f < F; ++f) {
-        const double* q = a.q_in + f * Knp + e0 * NP;
+        const ST* q = a.q_in + f * Knp + e0 * NP;
         if (state && aligned16(q, bytes)) prefetch_l2(q, bytes);
-        const double* r = a.res + f * Knp + e0 * NP;
+        const ST* r = a.res + f * Knp + e0 * NP;
         if (res && a.mode != 0 && aligned16(r, bytes)) prefetch_l2(r, bytes);
       }
     };
@@ -782,7 +792,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
       const uint32_t par = its & 1u;
       const int64_t el0 = ((int64_t)blockIdx.x + (int64_t)its * gridDim.x) * EB;
       const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
-      double* st = reinterpret_cast<double*>(smem + S::ostg + b * S::bStage);
+      ST* st = reinterpret_cast<ST*>(smem + S::ostg + b * S::bStage);
       const bool valid = lane_used && e_lane < ne;
       const int e_own = valid ? e_lane : 0;
       uint32_t* rmx = rsq + par * 128;
@@ -793,17 +803,17 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
         // ---- A: remainders after the element's FP64 linear interpolant, split
         // into the state planes (one row per lane, 8 columns per item) ----
         {
-          double v0 = 0.0, dv[DIM];
+          ST v0 = 0, dv[DIM];
 #pragma unroll
           for (int d = 0; d < DIM; ++d) dv[d] = 0.0;
           if (valid && !bad) {
-            const double* q = st + fown * FNP + e_own * NP;
+            const ST* q = st + fown * FNP + e_own * NP;
             v0 = q[0];
 #pragma unroll
             for (int d = 0; d < DIM; ++d) dv[d] = q[svert[d]] - v0;
           }
 #pragma unroll
-          for (int d = 0; d < DIM; ++d) lin_out[d] = (float)(0.5 * dv[d]);
+          for (int d = 0; d < DIM; ++d) lin_out[d] = (float)(ST(0.5) * dv[d]);
           // chunks wholly in the K padding stay zero from the set-up unless the
           // rhs rows alias the planes
           constexpr int NCHUNK = S::RHS_OWN ? (NP + 7) / 8 : KD / 8;
@@ -820,7 +830,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
               const int j = chunk * 8 + c;
               float v = 0.f;
               if (item < NITEM && valid && !bad && j < NP) {
-                double l = v0;
+                ST l = v0;
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) l += lamc[j * DIM + d] * dv[d];
                 v = (float)(st[fown * FNP + e_own * NP + j] - l);
@@ -881,7 +891,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
       const int b = NSTG == 2 ? (int)(its & 1u) : 0;
       const int64_t el0 = ((int64_t)blockIdx.x + (int64_t)its * gridDim.x) * EB;
       const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
-      double* st = reinterpret_cast<double*>(smem + S::ostg + b * S::bStage);
+      ST* st = reinterpret_cast<ST*>(smem + S::ostg + b * S::bStage);
       if (!bad && stage_res && !warp_wait(&mbar[MB_RES_FULL], its & 1u)) {
         if (lane == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
         bad = 1;
@@ -899,7 +909,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
             constexpr int KX = (EPW * NP + QT - 1) / QT;   // positions per thread
             const int cnt = nq * NP;                       // values per field
             const int t = part * 32 + lane;
-            const double* qs = st + e_first * NP;
+            const ST* qs = st + e_first * NP;
             const float* rq = rhs_s + quad * 32 * NPR;
             const int64_t g0 = (el0 + e_first) * NP;
             // position k of this thread: x = t + QT k; rhs row (el, f) at node
@@ -912,17 +922,18 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
                   const int ro = x + (x / NP) * (F * NPR - NP);
 #pragma unroll
                   for (int f = 0; f < F; ++f)
-                    a.q_out[(int64_t)f * Knp + g0 + x] = (double)rq[ro + f * NPR];
+                    a.q_out[(int64_t)f * Knp + g0 + x] = (ST)rq[ro + f * NPR];
                 }
               }
             } else {
-              const double ra = a.ra, rb = a.rb, dtt = a.dt;
-              double* res0 = a.res + g0;
-              double* qo0 = a.q_out + g0;
+              // the stage update in the state's precision (FP64 or FP32)
+              const ST ra = (ST)a.ra, rb = (ST)a.rb, dtt = (ST)a.dt;
+              ST* res0 = a.res + g0;
+              ST* qo0 = a.q_out + g0;
               if constexpr (S::RES) {
                 // residual from the residual buffer (short latency): one
                 // value at a time, few registers live
-                const double* rs = rbuf + e_first * NP;
+                const ST* rs = rbuf + e_first * NP;
 #pragma unroll 1
                 for (int k = 0; k < KX; ++k) {
                   const int x = t + QT * k;
@@ -930,7 +941,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
                     const int ro = x + (x / NP) * (F * NPR - NP);
 #pragma unroll
                     for (int f = 0; f < F; ++f) {
-                      const double nr = ra * rs[f * FNP + x] + dtt * (double)rq[ro + f * NPR];
+                      const ST nr = ra * rs[f * FNP + x] + dtt * (ST)rq[ro + f * NPR];
                       res0[(int64_t)f * Knp + x] = nr;
                       qo0[(int64_t)f * Knp + x] = qs[f * FNP + x] + rb * nr;
                     }
@@ -939,13 +950,13 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
               } else {
                 // residual from global memory: every load first (they are
                 // independent of the stores)
-                double r0[KX][F];
+                ST r0[KX][F];
 #pragma unroll
                 for (int k = 0; k < KX; ++k) {
                   const int x = t + QT * k;
 #pragma unroll
                   for (int f = 0; f < F; ++f)
-                    r0[k][f] = x < cnt ? res0[(int64_t)f * Knp + x] : 0.0;
+                    r0[k][f] = x < cnt ? res0[(int64_t)f * Knp + x] : ST(0);
                 }
 #pragma unroll
                 for (int k = 0; k < KX; ++k) {
@@ -954,7 +965,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
                     const int ro = x + (x / NP) * (F * NPR - NP);
 #pragma unroll
                     for (int f = 0; f < F; ++f) {
-                      const double nr = ra * r0[k][f] + dtt * (double)rq[ro + f * NPR];
+                      const ST nr = ra * r0[k][f] + dtt * (ST)rq[ro + f * NPR];
                       res0[(int64_t)f * Knp + x] = nr;
                       qo0[(int64_t)f * Knp + x] = qs[f * FNP + x] + rb * nr;
                     }
@@ -985,7 +996,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
       const uint32_t par = it & 1u;
       const int64_t el0 = batch * EB;
       const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
-      double* st = reinterpret_cast<double*>(smem + S::ostg + b * S::bStage);  // [F][EB][NP]
+      ST* st = reinterpret_cast<ST*>(smem + S::ostg + b * S::bStage);  // [F][EB][NP]
       const uint8_t* stg = smem + S::ostg + b * S::bStage;
       const float* sgeo = reinterpret_cast<const float*>(stg + S::sGeo);
       const int2* sconn = reinterpret_cast<const int2*>(stg + S::sConn);
@@ -1058,9 +1069,9 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgs a
                 if constexpr (JumpLinear<MODEL>::value) {
 #pragma unroll
                   for (int f = 0; f < F; ++f) {
-                    const double qm = st[f * FNP + e * NP + lnode];
-                    const double qp = inb ? st[f * FNP + lb * NP + nn]
-                                          : __ldg(a.q_in + f * Knp + gi);
+                    const ST qm = st[f * FNP + e * NP + lnode];
+                    const ST qp = inb ? st[f * FNP + lb * NP + nn]
+                                      : __ldg(a.q_in + f * Knp + gi);
                     uPs[u][f] = (float)(qm - qp);
                   }
                 } else {
@@ -2107,16 +2118,16 @@ static double plane_scale(const std::vector<double>& m, int pt) {
   return std::ldexp(1.0, e - 14);
 }
 
-template <int MODEL, int DIM, int ORDER, int PT>
+template <int MODEL, int DIM, int ORDER, int PT, typename ST = double>
 static hb_status configure_split(Op* op) {
-  using S = Shape<MODEL, DIM, ORDER>;
+  using S = Shape<MODEL, DIM, ORDER, (int)sizeof(ST)>;
   Discr* d = op->d;
   if constexpr (!S::FITS) {
     return fail(HB_ERR_UNSUPPORTED, "BF16x3 kernel: element beyond one MMA (N <= 256)");
   } else {
     if (d->np != S::NP || d->nfp != S::NFP)
       return fail(HB_ERR_INVALID_ARGUMENT, "element sizes do not match the order");
-    auto kern = rhs_split_kernel<MODEL, DIM, ORDER, PT>;
+    auto kern = rhs_split_kernel<MODEL, DIM, ORDER, PT, ST>;
     int dev;
     HB_CUDA(cudaGetDevice(&dev));
     int max_optin = 0, sms = 0, smem_sm = 0;
@@ -2198,8 +2209,16 @@ static hb_status configure_split(Op* op) {
       // the kernel reads the weights from constant memory (per dimension and
       // order; every discretization of that order writes the same values)
       static_assert(S::NP * DIM <= LAM_MAX && ORDER < LAM_ORDERS, "weight table too small");
-      HB_CUDA(cudaMemcpyToSymbol(c_lam, lam, sizeof(double) * np * DIM,
-                                 sizeof(double) * (((DIM - 2) * LAM_ORDERS + ORDER) * LAM_MAX)));
+      const size_t slot = ((size_t)(DIM - 2) * LAM_ORDERS + ORDER) * LAM_MAX;
+      if constexpr (sizeof(ST) == 8) {
+        HB_CUDA(cudaMemcpyToSymbol(c_lam, lam, sizeof(double) * np * DIM,
+                                   sizeof(double) * slot));
+      } else {
+        std::vector<float> lamf((size_t)np * DIM);
+        for (size_t x = 0; x < lamf.size(); ++x) lamf[x] = (float)lam[x];
+        HB_CUDA(cudaMemcpyToSymbol(c_lamf, lamf.data(), sizeof(float) * lamf.size(),
+                                   sizeof(float) * slot));
+      }
     }
     const double sd = plane_scale(Dt, PT), sl = plane_scale(Lt, PT);
     build_planes(Dt, DIM * np, np, S::ND, S::KD, PT, sd, img.data(), img.data() + bD);
@@ -2215,18 +2234,18 @@ static hb_status configure_split(Op* op) {
   }
 }
 
-template <int MODEL, int DIM, int ORDER, int PT>
+template <int MODEL, int DIM, int ORDER, int PT, typename ST = double>
 static hb_status launch_split_t(Op* op, int mode, double ra, double rb, double dt,
                                 const void* q_in, void* q_out, void* res,
                                 const double* coeff, const double* bdry,
                                 const double* source, cudaStream_t s) {
-  using S = Shape<MODEL, DIM, ORDER>;
+  using S = Shape<MODEL, DIM, ORDER, (int)sizeof(ST)>;
   if constexpr (!S::FITS) {
     return fail(HB_ERR_UNSUPPORTED, "BF16x3 kernel: element beyond one MMA");
   } else {
     Discr* d = op->d;
     SplitOps* so = static_cast<SplitOps*>(op->split_ops);
-    SplitArgs a;
+    SplitArgsT<ST> a;
     a.K = d->K;
     a.nbatch = (d->K + S::EB - 1) / S::EB;
     a.n_given = op->n_given;
@@ -2234,11 +2253,11 @@ static hb_status launch_split_t(Op* op, int mode, double ra, double rb, double d
     a.ops = so->dev;
     a.geo32 = d->geo32;
     a.conn = op->conn; a.fmask = d->fmask; a.shuffle = d->shuffle;
-    a.q_in = static_cast<const double*>(q_in);
-    a.q_out = static_cast<double*>(q_out);
-    a.res = static_cast<double*>(res);
+    a.q_in = static_cast<const ST*>(q_in);
+    a.q_out = static_cast<ST*>(q_out);
+    a.res = static_cast<ST*>(res);
     a.coeff = coeff; a.bdry = bdry; a.source = source;
-    a.halo = static_cast<const double*>(op->halo);
+    a.halo = static_cast<const ST*>(op->halo);
     a.halo_c = op->halo_c;
     a.n_halo = op->n_halo;
     a.ra = ra; a.rb = rb; a.dt = dt; a.mode = mode;
@@ -2246,7 +2265,7 @@ static hb_status launch_split_t(Op* op, int mode, double ra, double rb, double d
     a.op_scale_l = so->scale_l;
     a.mp = op->mp;
     a.err = op->err_flag;
-    rhs_split_kernel<MODEL, DIM, ORDER, PT><<<op->grid, op->threads, op->smem, s>>>(a);
+    rhs_split_kernel<MODEL, DIM, ORDER, PT, ST><<<op->grid, op->threads, op->smem, s>>>(a);
     HB_CUDA(cudaGetLastError());
     return HB_OK;
   }
@@ -2426,6 +2445,15 @@ hb_status prepare_split(Op* op) {
   op->split_ops = new SplitOps();
   static_cast<SplitOps*>(op->split_ops)->order = d->order;
   const int dim = d->dim, order = d->order;
+  if (op->precision == HB_PREC_FP32) {
+    // FP32 state: resident kernels with FP16 planes
+#define HB_CASE(M, D, O)                                                       \
+  if (op->model == M && dim == D && order == O)                                \
+    return configure_split<M, D, O, PT_FP16, float>(op);
+    HB_SPLIT_INSTANCES(HB_CASE)
+#undef HB_CASE
+    return fail(HB_ERR_UNSUPPORTED, "no FP32-state tensor-core kernel for this instance");
+  }
   const int pt = op->precision == HB_PREC_FP16X3 ? PT_FP16 : PT_BF16;
   if (op->n_halo == 0) {
     // a streamed variant that this device refuses (e.g. its shared memory)
@@ -2474,6 +2502,15 @@ hb_status launch_split(Op* op, int mode, double ra, double rb, double dt,
   const int pt = op->precision == HB_PREC_FP16X3 ? PT_FP16 : PT_BF16;
   const SplitOps* so = static_cast<const SplitOps*>(op->split_ops);
   if (so == nullptr) return fail(HB_ERR_INVALID_ARGUMENT, "split operator not prepared");
+  if (op->precision == HB_PREC_FP32) {
+#define HB_CASE(M, D, O)                                                              \
+  if (op->model == M && dim == D && order == O)                                       \
+    return launch_split_t<M, D, O, PT_FP16, float>(op, mode, ra, rb, dt, q_in, q_out,  \
+                                                   res, coeff, bdry, source, s);
+    HB_SPLIT_INSTANCES(HB_CASE)
+#undef HB_CASE
+    return fail(HB_ERR_UNSUPPORTED, "model/dimension/order combination not built");
+  }
   if (so->stream) {
 #define HB_CASE(M, D, O)                                                              \
   if (op->model == M && dim == D && order == O)                                       \

@@ -28,7 +28,10 @@ from .models import (BC_GIVEN, BC_NONE, MODEL_MAXWELL, MODEL_VARWAVE, MODEL_WAVE
 from .refelem import make_element
 
 PRECISIONS = {"plain": None, "fp64": _native.PREC_FP64, "fp32": _native.PREC_FP32,
+              "fp32-simt": _native.PREC_FP32_SIMT,
               "bf16x3": _native.PREC_BF16X3, "fp16x3": _native.PREC_FP16X3}
+# precisions whose state (and residual) is FP32
+FP32_STATE = ("fp32", "fp32-simt")
 
 
 def _torch():
@@ -43,7 +46,10 @@ class Discretization:
     FP32, and so is the arithmetic), "fp32", "fp64", "bf16x3" (FP64 state,
     differentiation and lift as split-BF16 tensor-core products with FP32
     accumulation) or "fp16x3" (the same with FP16 planes of power-of-two
-    scaled rows: same cost, ~8x smaller error).
+    scaled rows: same cost, ~8x smaller error).  "fp32" runs the two
+    contractions as FP16x3 tensor-core products where a resident tensor-core
+    kernel is built for the (model, dimension, order) and on CUDA cores
+    otherwise; "fp32-simt" keeps them on CUDA cores.
     """
 
     def __init__(self, mesh: Mesh, order=None, local_discretization=None,
@@ -101,7 +107,7 @@ class Discretization:
     @property
     def state_dtype(self):
         torch = _torch()
-        return torch.float32 if self.precision == "fp32" else torch.float64
+        return torch.float32 if self.precision in FP32_STATE else torch.float64
 
     @property
     def device(self):
@@ -417,7 +423,8 @@ class CompiledOperator:
     @property
     def state_dtype(self):
         torch = _torch()
-        return torch.float32 if self.prec_code == _native.PREC_FP32 else torch.float64
+        return torch.float32 if self.prec_code in (_native.PREC_FP32, _native.PREC_FP32_SIMT) \
+            else torch.float64
 
     def set_coefficient(self, c):
         """Variable-velocity wave speed: a number or a volume vector."""

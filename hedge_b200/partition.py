@@ -216,8 +216,9 @@ class PartitionedOperator:
         self.K = len(p.elements)
         self.device = torch.device(device) if device is not None else discr.device
         prec = {"fp64": _native.PREC_FP64, "fp32": _native.PREC_FP32,
+                "fp32-simt": _native.PREC_FP32_SIMT,
                 "bf16x3": _native.PREC_BF16X3, "fp16x3": _native.PREC_FP16X3}[precision]
-        self.dtype = torch.float32 if precision == "fp32" else torch.float64
+        self.dtype = torch.float32 if precision in ("fp32", "fp32-simt") else torch.float64
         self.lib = lib = _native.load()
         ld = discr.ldis
         E = p.elements

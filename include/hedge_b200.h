@@ -40,10 +40,16 @@ enum {
 
 enum {
   HB_PREC_FP64 = 0,   /* FP64 state, FP64 arithmetic */
-  HB_PREC_FP32 = 1,   /* FP32 state, FP32 arithmetic */
+  HB_PREC_FP32 = 1,   /* FP32 state and residual, FP32 arithmetic; where a resident
+                         tensor-core kernel is built for the (model, dimension,
+                         order), the two contractions run as split-FP16 products
+                         (as HB_PREC_FP16X3, FP32 accumulation), else on CUDA cores
+                         (hedge/discretization/__init__.py:217-219,
+                         default_scalar_type float32) */
   HB_PREC_BF16X3 = 2, /* FP64 state, split-BF16 tensor-core products, FP32 accumulation */
-  HB_PREC_FP16X3 = 3  /* FP64 state, split-FP16 products of power-of-two-scaled rows,
+  HB_PREC_FP16X3 = 3, /* FP64 state, split-FP16 products of power-of-two-scaled rows,
                          FP32 accumulation (same cost as BF16X3, ~8x more accurate) */
+  HB_PREC_FP32_SIMT = 4 /* FP32 state, FP32 arithmetic, always on CUDA cores */
 };
 
 enum {

@@ -13,8 +13,8 @@ from test_gpu_parity import _fields
 pytestmark = pytest.mark.gpu
 
 # FP64 / FP32 as in the plain parity tests; the split paths as on rough fields
-TOL = {"fp64": 1e-12, "fp32": 1e-5, "bf16x3": 1e-5, "fp16x3": 1e-6}
-PRECS = ["fp64", "fp32", "bf16x3", "fp16x3"]
+TOL = {"fp64": 1e-12, "fp32": 1e-5, "fp32-simt": 1e-5, "bf16x3": 1e-5, "fp16x3": 1e-6}
+PRECS = ["fp64", "fp32", "fp32-simt", "bf16x3", "fp16x3"]
 
 TRI = np.array([[0.1, -0.2], [1.3, 0.1], [0.2, 0.9]])
 TET = np.array([[0.0, 0.1, -0.1], [1.2, 0.0, 0.1], [0.1, 0.9, 0.0], [0.2, 0.1, 1.1]])
@@ -24,7 +24,7 @@ def _err(d, op, precision, seed):
     from oracle import OracleRHS
     ot = op.op_template()
     q = _fields(d, op.descriptor().n_fields, seed)
-    if precision == "fp32":
+    if precision in ("fp32", "fp32-simt"):
         q = q.astype(np.float32).astype(np.float64)
     ref = OracleRHS(d, ot)(q)
     comp = d.compile(ot, precision=precision)

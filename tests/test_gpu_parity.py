@@ -10,7 +10,9 @@ from conftest import rel_l2
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"fp64": 1e-12, "fp32": 1e-5}
+# "fp32" runs the contractions on the tensor cores (FP16x3) where that
+# instance is built, "fp32-simt" always on CUDA cores
+TOL = {"fp64": 1e-12, "fp32": 1e-5, "fp32-simt": 1e-5}
 
 
 def _fields(discr, F, seed):
@@ -32,8 +34,9 @@ def _check(discr, op, precision, seed=0, bc_in=None, c_field=None, source=None):
     q = _fields(discr, op.descriptor().n_fields, seed)
     orc = OracleRHS(discr, ot, c_field=c_field, source=source)
     ref = orc(q, bc_in=bc_in)
-    qs = q.astype(np.float32).astype(np.float64) if precision == "fp32" else q
-    if precision == "fp32":
+    fp32 = precision in ("fp32", "fp32-simt")
+    qs = q.astype(np.float32).astype(np.float64) if fp32 else q
+    if fp32:
         ref = orc(qs, bc_in=bc_in)
     out = comp(w=qs, bc_in=bc_in)
     comp.check()
@@ -53,7 +56,7 @@ def box(n=3, jitter=0.0, seed=None):
     return hb.make_box_tet_mesh(n=(n, n, n), jitter=jitter, seed=seed)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32-simt"])
 @pytest.mark.parametrize("flux", ["upwind", "central", "lf"])
 def test_advection_2d_periodic(cuda_device, precision, flux):
     d = hb.Discretization(rect(9, True, 0.2 / 8, 0), order=4)
@@ -76,7 +79,7 @@ def test_advection_2d_inflow(cuda_device, order):
     _check(d, op, "fp64", bc_in=bc)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32-simt"])
 @pytest.mark.parametrize("flux", ["upwind", "central"])
 def test_wave_2d_dirichlet(cuda_device, precision, flux):
     d = hb.Discretization(rect(8, False, 0.02, 2), order=5)
@@ -98,7 +101,7 @@ def test_wave_2d_mixed_bcs(cuda_device):
     _check(d, op, "fp64")
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32-simt"])
 def test_wave_3d(cuda_device, precision):
     d = hb.Discretization(box(3, 0.05, 3), order=4)
     _check(d, hb.StrongWaveOperator(1.0, 3, flux_type="upwind"), precision)
@@ -116,7 +119,7 @@ def test_varwave(cuda_device, dim):
     _check(d, op, "fp64", c_field=c, source=src)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32-simt"])
 @pytest.mark.parametrize("flux", [1, 0.5, 0, "lf"])
 def test_maxwell_pec(cuda_device, precision, flux):
     d = hb.Discretization(box(3, 0.05, 5), order=4)

@@ -27,7 +27,7 @@ def _setup(kind, nparts, precision):
 
 
 @pytest.mark.parametrize("kind", ["maxwell", "varwave"])
-@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp16x3", "bf16x3"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32-simt", "fp16x3", "bf16x3"])
 def test_partitioned_rhs_equals_global(cuda_device, kind, precision):
     import torch
     d, model, plan, parts, ex = _setup(kind, 3, precision)
@@ -46,7 +46,7 @@ def test_partitioned_rhs_equals_global(cuda_device, kind, precision):
         p.check()
         want = ref[:, p.local_nodes()]
         g = got.double().cpu().numpy()
-        if precision == "fp32":
+        if precision in ("fp32", "fp32-simt"):
             assert rel_l2(g, want) <= 1e-6
         else:
             # per-row arithmetic does not depend on the batch an element lands in
