@@ -10,6 +10,7 @@ from .mesh import (Mesh, TAG_ALL, TAG_NONE, make_regular_rect_mesh,
 from .refelem import TriangleElement, TetrahedronElement, make_element
 from .models import (StrongAdvectionOperator, WeakAdvectionOperator, StrongWaveOperator,
                      VariableVelocityStrongWaveOperator, MaxwellOperator,
+                     TMMaxwellOperator, TEMaxwellOperator,
                      make_tdep_constant, TimeConstantGivenFunction,
                      TimeDependentGivenFunction)
 from .discretization import Discretization, CompiledOperator, BoundRHS
@@ -21,7 +22,8 @@ __all__ = [
     "Mesh", "TAG_ALL", "TAG_NONE", "make_regular_rect_mesh", "make_box_tet_mesh",
     "check_bc_coverage", "TriangleElement", "TetrahedronElement", "make_element",
     "StrongAdvectionOperator", "WeakAdvectionOperator", "StrongWaveOperator",
-    "VariableVelocityStrongWaveOperator", "MaxwellOperator", "make_tdep_constant",
+    "VariableVelocityStrongWaveOperator", "MaxwellOperator", "TMMaxwellOperator",
+    "TEMaxwellOperator", "make_tdep_constant",
     "TimeConstantGivenFunction", "TimeDependentGivenFunction", "Discretization", "CompiledOperator", "BoundRHS",
     "LSRK4TimeStepper", "RK4TimeStepper", "GraphedLSRK4", "GradientOperator", "DivergenceOperator",
     "VtkVisualizer", "LegacyVtkVisualizer",

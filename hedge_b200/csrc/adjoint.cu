@@ -352,6 +352,10 @@ hb_status launch_adjoint(Op* op, const double* q, const double* lam, double* q_b
     case HB_MODEL_MAXWELL:
       if (dim != 3) return fail(HB_ERR_UNSUPPORTED, "Maxwell adjoint: 3D only");
       return launch_adjoint_t<HB_MODEL_MAXWELL, 3>(op, q, lam, q_bar, c_bar, coeff, work, s);
+    case HB_MODEL_MAXWELL_TM:
+      return launch_adjoint_t<HB_MODEL_MAXWELL_TM, 2>(op, q, lam, q_bar, c_bar, coeff, work, s);
+    case HB_MODEL_MAXWELL_TE:
+      return launch_adjoint_t<HB_MODEL_MAXWELL_TE, 2>(op, q, lam, q_bar, c_bar, coeff, work, s);
     default:
       return fail(HB_ERR_INVALID_ARGUMENT, "unknown model id");
   }

@@ -178,6 +178,9 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
     case HB_MODEL_MAXWELL:
       if (d->dim != 3) return fail(HB_ERR_UNSUPPORTED, "Maxwell needs a 3D mesh");
       F = 6; break;
+    case HB_MODEL_MAXWELL_TM: case HB_MODEL_MAXWELL_TE:
+      if (d->dim != 2) return fail(HB_ERR_UNSUPPORTED, "TM / TE Maxwell needs a 2D mesh");
+      F = 3; break;
     default: return fail(HB_ERR_INVALID_ARGUMENT, "unknown model id");
   }
   if (desc->num_fields != F)
@@ -185,7 +188,8 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
   if (desc->precision < HB_PREC_FP64 || desc->precision > HB_PREC_FP32_SIMT)
     return fail(HB_ERR_INVALID_ARGUMENT, "unknown precision");
   if (!desc->conn) return fail(HB_ERR_INVALID_ARGUMENT, "null connectivity");
-  if (model == HB_MODEL_MAXWELL && !(desc->eps > 0 && desc->mu > 0))
+  if ((model == HB_MODEL_MAXWELL || model == HB_MODEL_MAXWELL_TM ||
+       model == HB_MODEL_MAXWELL_TE) && !(desc->eps > 0 && desc->mu > 0))
     return fail(HB_ERR_INVALID_ARGUMENT, "Maxwell material must be positive");
   // host validation of the face table (the kernels also flag bad entries)
   const int64_t nfc = d->K * d->nfaces;

@@ -23,6 +23,28 @@ template <int DIM>
 struct Traits<HB_MODEL_VARWAVE, DIM> { static constexpr int F = DIM + 1, COEFF = 1; };
 template <int DIM>
 struct Traits<HB_MODEL_MAXWELL, DIM> { static constexpr int F = 6, COEFF = 0; };
+// the 2D TM and TE systems: three of the six components, no z dependence
+template <int DIM>
+struct Traits<HB_MODEL_MAXWELL_TM, DIM> { static constexpr int F = 3, COEFF = 0; };
+template <int DIM>
+struct Traits<HB_MODEL_MAXWELL_TE, DIM> { static constexpr int F = 3, COEFF = 0; };
+
+// Position of field f of a 2D Maxwell system in (Ex Ey Ez Hx Hy Hz): TM
+// carries (Ez, Hx, Hy), TE (Ex, Ey, Hz) (em.py get_eh_subset); and how many
+// of its fields are E components (they come first).
+template <int MODEL>
+__host__ __device__ constexpr int maxwell_slot(int f) {
+  return MODEL == HB_MODEL_MAXWELL_TM ? (f == 0 ? 2 : 2 + f) : (f < 2 ? f : 5);
+}
+template <int MODEL>
+__host__ __device__ constexpr int maxwell_ne() {
+  return MODEL == HB_MODEL_MAXWELL ? 3 : (MODEL == HB_MODEL_MAXWELL_TM ? 1 : 2);
+}
+template <int MODEL>
+struct IsMaxwell {
+  static constexpr bool value = MODEL == HB_MODEL_MAXWELL || MODEL == HB_MODEL_MAXWELL_TM ||
+                                MODEL == HB_MODEL_MAXWELL_TE;
+};
 
 // Flux argument vector: [coeff (var-c wave)] + fields.
 template <int MODEL, int DIM>
@@ -58,6 +80,16 @@ __device__ __forceinline__ void model_volume(const ModelParams& mp,
     vol[0] = c * div;
 #pragma unroll
     for (int x = 0; x < DIM; ++x) vol[1 + x] = c * g[x][0];
+  } else if constexpr (MODEL == HB_MODEL_MAXWELL_TM) {
+    // (Ez, Hx, Hy): (curl H)_z = dx Hy - dy Hx; -curl E = (-dy Ez, dx Ez)
+    vol[0] = g[0][2] - g[1][1];
+    vol[1] = -g[1][0];
+    vol[2] = g[0][0];
+  } else if constexpr (MODEL == HB_MODEL_MAXWELL_TE) {
+    // (Ex, Ey, Hz): curl H = (dy Hz, -dx Hz); -(curl E)_z = -(dx Ey - dy Ex)
+    vol[0] = g[1][2];
+    vol[1] = -g[0][2];
+    vol[2] = -(g[0][1] - g[1][0]);
   } else {  // Maxwell: (curl H, -curl E)
     vol[0] = g[1][5] - g[2][4];
     vol[1] = g[2][3] - g[0][5];
@@ -69,11 +101,14 @@ __device__ __forceinline__ void model_volume(const ModelParams& mp,
 }
 
 // rhs component f from its volume term, lifted flux and optional source
+// (wave, var-c wave: the source of u; Maxwell: the value added to E_f's rhs,
+// -J_f / eps for a current J, zero for the H components)
 template <int MODEL, int DIM, typename T>
 __device__ __forceinline__ T model_finish(const ModelParams& mp, int f, T vol,
                                           T lift, T src) {
-  if constexpr (MODEL == HB_MODEL_MAXWELL) {
-    return (vol + lift) / (f < 3 ? T(mp.eps) : T(mp.mu));
+  if constexpr (IsMaxwell<MODEL>::value) {
+    constexpr int NE = maxwell_ne<MODEL>();
+    return (vol + lift) / (f < NE ? T(mp.eps) : T(mp.mu)) + (f < NE ? src : T(0));
   } else if constexpr (MODEL == HB_MODEL_WAVE) {
     return f == 0 ? vol + lift + src : vol + lift;
   } else if constexpr (MODEL == HB_MODEL_VARWAVE) {
@@ -83,8 +118,50 @@ __device__ __forceinline__ T model_finish(const ModelParams& mp, int f, T vol,
   }
 }
 
+// Index of field f's source value at volume node `node` in the caller's
+// source vector: one [K*Np] vector for the wave models (field 0), [3][K*Np]
+// for Maxwell (the E components); -1 where the field has none.
+template <int MODEL>
+__device__ __forceinline__ int64_t model_src_index(int f, int64_t node, int64_t knp) {
+  if constexpr (IsMaxwell<MODEL>::value) return f < maxwell_ne<MODEL>() ? f * knp + node : -1;
+  else return f == 0 ? node : -1;
+}
+
+// Maxwell boundary states of (E, H) = u[0..3), u[3..6) (em.py:226-287):
+// PEC (-E, H), PMC (E, -H), first-order absorbing.  False: no boundary flux.
+template <typename T>
+__device__ __forceinline__ bool maxwell_bc3(const ModelParams& mp, int kind, const T* u,
+                                            const T* n, T* uP) {
+  const T* e = u;
+  const T* h = u + 3;
+  if (kind == HB_BC_PEC) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { uP[k] = -e[k]; uP[3 + k] = h[k]; }
+  } else if (kind == HB_BC_PMC) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { uP[k] = e[k]; uP[3 + k] = -h[k]; }
+  } else if (kind == HB_BC_ABSORB) {
+    const T Z = T(mp.Z), Y = T(mp.Y);
+    T ne[3], nh[3], nne[3], nnh[3];
+    cross3(n, e, ne);
+    cross3(n, h, nh);
+    cross3(n, ne, nne);
+    cross3(n, nh, nnh);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      uP[k] = e[k] + T(0.5) * (nne[k] - Z * nh[k]);
+      uP[3 + k] = h[k] + T(0.5) * (nnh[k] + Y * ne[k]);
+    }
+  } else {
+    return false;
+  }
+  return true;
+}
+
 // ---- boundary exterior states ---------------------------------------------
-// Returns false when the face carries no boundary flux (BC_NONE).
+// Returns false when the face carries no boundary flux (BC_NONE).  `given`
+// is the caller's boundary datum at the node (HB_BC_GIVEN): the advection
+// inflow value, or the wave's Dirichlet value.
 template <int MODEL, int DIM, typename T>
 __device__ __forceinline__ bool model_bc(const ModelParams& mp, int kind,
                                          const T (&uM)[Args<MODEL, DIM>::N],
@@ -105,6 +182,11 @@ __device__ __forceinline__ bool model_bc(const ModelParams& mp, int kind,
       uP[C] = -u;
 #pragma unroll
       for (int x = 0; x < DIM; ++x) uP[C + 1 + x] = uM[C + 1 + x];
+    } else if (kind == HB_BC_GIVEN && MODEL == HB_MODEL_WAVE) {
+      // inhomogeneous Dirichlet data g (wave.py:133-142): (2 g - u, v)
+      uP[C] = T(2) * given - u;
+#pragma unroll
+      for (int x = 0; x < DIM; ++x) uP[C + 1 + x] = uM[C + 1 + x];
     } else if (kind == HB_BC_NEUMANN) {
       uP[C] = u;
 #pragma unroll
@@ -120,32 +202,56 @@ __device__ __forceinline__ bool model_bc(const ModelParams& mp, int kind,
       return false;
     }
     return true;
-  } else {  // Maxwell
-    const T* e = uM;
-    const T* h = uM + 3;
-    if (kind == HB_BC_PEC) {
+  } else if constexpr (MODEL == HB_MODEL_MAXWELL) {
+    (void)NA;
+    return maxwell_bc3<T>(mp, kind, uM, n, uP);
+  } else {
+    // 2D TM / TE: the 3D conditions on the embedded fields, n_z = 0
+    T u6[6] = {T(0), T(0), T(0), T(0), T(0), T(0)}, p6[6];
+    const T n3[3] = {n[0], n[1], T(0)};
 #pragma unroll
-      for (int k = 0; k < 3; ++k) { uP[k] = -e[k]; uP[3 + k] = h[k]; }
-    } else if (kind == HB_BC_PMC) {
+    for (int f = 0; f < 3; ++f) u6[maxwell_slot<MODEL>(f)] = uM[f];
+    if (!maxwell_bc3<T>(mp, kind, u6, n3, p6)) return false;
 #pragma unroll
-      for (int k = 0; k < 3; ++k) { uP[k] = e[k]; uP[3 + k] = -h[k]; }
-    } else if (kind == HB_BC_ABSORB) {
-      const T Z = T(mp.Z), Y = T(mp.Y);
-      T ne[3], nh[3], nne[3], nnh[3];
-      cross3(&n[0], e, ne);
-      cross3(&n[0], h, nh);
-      cross3(&n[0], ne, nne);
-      cross3(&n[0], nh, nnh);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        uP[k] = e[k] + T(0.5) * (nne[k] - Z * nh[k]);
-        uP[3 + k] = h[k] + T(0.5) * (nnh[k] + Y * ne[k]);
-      }
-    } else {
-      return false;
-    }
+    for (int f = 0; f < 3; ++f) uP[f] = p6[maxwell_slot<MODEL>(f)];
     (void)NA;
     return true;
+  }
+}
+
+// Maxwell numerical flux of the jumps [E] = de, [H] = dh (em.py:145-187,
+// fixed material): "lf" (flux type 1 here) or the numeric flux type alpha.
+template <typename T>
+__device__ __forceinline__ void maxwell_flux3(const ModelParams& mp, bool bdry, const T* de,
+                                              const T* dh, const T* n, T* f) {
+  {
+    const int ft = bdry ? mp.bdry_flux_type : mp.flux_type;
+    const T alpha = T(bdry ? mp.bdry_alpha : mp.alpha);
+    T t[3];
+    if (ft == 1) {
+      cross3(n, dh, t);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) f[k] = T(0.5) * (-t[k]);
+      cross3(n, de, t);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) f[3 + k] = T(0.5) * t[k];
+    } else {
+      const T Z = T(mp.Z), Y = T(mp.Y);
+      T nde[3], ndh[3], a[3];
+      cross3(n, de, nde);
+      cross3(n, dh, ndh);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) a[k] = Z * dh[k] - alpha * nde[k];
+      cross3(n, a, t);
+      const T fe = T(-0.5) * Y, fh = T(0.5) * Z;   // -1/(2Z), 1/(2Y)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) f[k] = fe * t[k];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) a[k] = Y * de[k] + alpha * ndh[k];
+      cross3(n, a, t);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) f[3 + k] = fh * t[k];
+    }
   }
 }
 
@@ -209,37 +315,20 @@ __device__ __forceinline__ void model_flux(const ModelParams& mp, bool bdry,
 #pragma unroll
       for (int x = 0; x < DIM; ++x) f[1 + x] += ce * n[x] * ve_n - ci * n[x] * vi_n;
     }
-  } else {  // Maxwell
-    const int ft = bdry ? mp.bdry_flux_type : mp.flux_type;
-    const T alpha = T(bdry ? mp.bdry_alpha : mp.alpha);
+  } else if constexpr (MODEL == HB_MODEL_MAXWELL) {
     T de[3], dh[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) { de[k] = uM[k] - uP[k]; dh[k] = uM[3 + k] - uP[3 + k]; }
-    T t[3];
-    if (ft == 1) {
-      cross3(&n[0], dh, t);
+    maxwell_flux3<T>(mp, bdry, de, dh, &n[0], f);
+  } else {
+    // 2D TM / TE: the 3D flux of the embedded jumps, n_z = 0
+    T d6[6] = {T(0), T(0), T(0), T(0), T(0), T(0)}, f6[6];
+    const T n3[3] = {n[0], n[1], T(0)};
 #pragma unroll
-      for (int k = 0; k < 3; ++k) f[k] = T(0.5) * (-t[k]);
-      cross3(&n[0], de, t);
+    for (int q = 0; q < 3; ++q) d6[maxwell_slot<MODEL>(q)] = uM[q] - uP[q];
+    maxwell_flux3<T>(mp, bdry, d6, d6 + 3, n3, f6);
 #pragma unroll
-      for (int k = 0; k < 3; ++k) f[3 + k] = T(0.5) * t[k];
-    } else {
-      const T Z = T(mp.Z), Y = T(mp.Y);
-      T nde[3], ndh[3], a[3];
-      cross3(&n[0], de, nde);
-      cross3(&n[0], dh, ndh);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) a[k] = Z * dh[k] - alpha * nde[k];
-      cross3(&n[0], a, t);
-      const T fe = T(-0.5) * Y, fh = T(0.5) * Z;   // -1/(2Z), 1/(2Y)
-#pragma unroll
-      for (int k = 0; k < 3; ++k) f[k] = fe * t[k];
-#pragma unroll
-      for (int k = 0; k < 3; ++k) a[k] = Y * de[k] + alpha * ndh[k];
-      cross3(&n[0], a, t);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) f[3 + k] = fh * t[k];
-    }
+    for (int q = 0; q < 3; ++q) f[q] = f6[maxwell_slot<MODEL>(q)];
   }
 }
 

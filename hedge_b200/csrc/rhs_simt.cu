@@ -268,9 +268,10 @@ __global__ void __launch_bounds__(256) rhs_simt_kernel(SimtArgs<T, S> a) {
         for (int f = 0; f < F; ++f) acc[f] += l * fe[f * E * nfpt + p];
       }
       const int64_t node = (el0 + e) * np + i;
-      const T src = a.source ? T(a.source[node]) : T(0);
 #pragma unroll
       for (int f = 0; f < F; ++f) {
+        const int64_t si = model_src_index<MODEL>(f, node, Knp);
+        const T src = (a.source && si >= 0) ? T(a.source[si]) : T(0);
         const T r = model_finish<MODEL, DIM, T>(a.mp, f, vol[f], acc[f], src);
         const int64_t idx = f * Knp + node;
         if (a.mode == 0) {
@@ -380,6 +381,8 @@ static hb_status dispatch(Op* op, int mode, double ra, double rb, double dt,
   HB_CASE(HB_MODEL_VARWAVE, 2)
   HB_CASE(HB_MODEL_VARWAVE, 3)
   HB_CASE(HB_MODEL_MAXWELL, 3)
+  HB_CASE(HB_MODEL_MAXWELL_TM, 2)
+  HB_CASE(HB_MODEL_MAXWELL_TE, 2)
 #undef HB_CASE
   return fail(HB_ERR_UNSUPPORTED, "model/dimension combination not built");
 }

@@ -1232,10 +1232,11 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgsT<
       const float inv_m = MODEL == HB_MODEL_MAXWELL
                               ? 1.0f / (float)(fown < 3 ? a.mp.eps : a.mp.mu) : 1.0f;
       auto rhs_of = [&](int i, float vol, float lift) -> float {
+        const int64_t si = model_src_index<MODEL>(fown, (el0 + e_own) * NP + i, Knp);
+        const float src = (a.source && si >= 0) ? (float)a.source[si] : 0.f;
         if constexpr (MODEL == HB_MODEL_MAXWELL) {
-          return (vol + lift) * inv_m;
+          return (vol + lift) * inv_m + src;
         } else {
-          const float src = a.source ? (float)a.source[(el0 + e_own) * NP + i] : 0.f;
           return model_finish<MODEL, DIM, float>(a.mp, fown, vol, lift, src);
         }
       };
@@ -1961,7 +1962,8 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
           const float cnode = C ? scoef[e_own * NP + i] : 0.f;
           const float mine = volume_own<MODEL, DIM>(a.mp, g, base, fown, cnode);
           if (valid) {
-            const float src = a.source ? (float)a.source[(el0 + e_own) * NP + i] : 0.f;
+            const int64_t si = model_src_index<MODEL>(fown, (el0 + e_own) * NP + i, Knp);
+            const float src = (a.source && si >= 0) ? (float)a.source[si] : 0.f;
             sq[fown * FNP + e_own * NP + i] =
                 model_finish<MODEL, DIM, float>(a.mp, fown, mine, lv[c] * slift, src);
           }

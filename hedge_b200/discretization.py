@@ -23,7 +23,8 @@ from .facegroups import Boundary, build_compact_connectivity, build_interior_fac
 from .mesh import Mesh, TAG_ALL, TAG_NONE, check_bc_coverage
 from .lowering import as_descriptor
 from .optemplate import Expr
-from .models import (BC_GIVEN, BC_NONE, MODEL_MAXWELL, MODEL_VARWAVE, MODEL_WAVE,
+from .models import (BC_GIVEN, BC_NONE, MODEL_MAXWELL, MODEL_MAXWELL_TE, MODEL_MAXWELL_TM,
+                     MODEL_VARWAVE, MODEL_WAVE,
                      MODEL_ADVECTION, OpTemplate)
 from .refelem import make_element
 
@@ -396,11 +397,16 @@ class CompiledOperator:
         self._coeff = None
         self._source = None
         names = ot.fields or {}
+        self._msrc_spec = None
+        # Maxwell systems: number of carried E components (their source rows)
+        self._n_e = {MODEL_MAXWELL: 3, MODEL_MAXWELL_TM: 1, MODEL_MAXWELL_TE: 2}.get(ot.model, 0)
+        if self._n_e:
+            self._init_maxwell_source(names, model)
         if ot.model == MODEL_VARWAVE:
             c = model.c if model is not None else (None if names.get("coeff") else 1.0)
             if c is not None and not isinstance(c, Expr):
                 self.set_coefficient(c)
-        if names:
+        if names and not self._n_e:
             # lowered from a template: source = sign * (const + coef * field)
             self._src_spec = (-1.0 if ot.model == MODEL_VARWAVE else 1.0,
                               float(names.get("source_const", 0.0)), names.get("source"),
@@ -414,11 +420,59 @@ class CompiledOperator:
             src = self._source_from(val)
             if src is not None:
                 self._source = src
-        else:
+        elif not self._n_e:
             src = p.get("source", 0) if ot.model == MODEL_WAVE else (
                 getattr(model, "source", 0) if ot.model == MODEL_VARWAVE else 0)
             if not (np.isscalar(src) and src == 0):
                 self.set_source(src)
+
+    # -- Maxwell current ----------------------------------------------------------
+    def _init_maxwell_source(self, names, model):
+        """Maxwell's source rows: E_c's rhs gains s_c = -J_c / eps
+        (em.py:192-214).  From a lowered template: per E component
+        const + coef * field (``names["sources"]``); from a descriptor: the
+        model's current."""
+        if names:
+            self._msrc_spec = names.get("sources") or []
+        elif model is not None and hasattr(model, "current_template"):
+            eps = float(self.ot.params["eps"])
+            cur = model.current_template()
+            spec = []
+            if not (np.isscalar(cur) and cur == 0):
+                for o in range(self._n_e):
+                    x = cur[o]
+                    if isinstance(x, Expr):
+                        spec.append((o, 0.0, (x.name, x.index), -1.0 / eps))
+                    elif x != 0:
+                        spec.append((o, -float(x) / eps, None, 0.0))
+            self._msrc_spec = spec
+        else:
+            self._msrc_spec = []
+        if not self._msrc_spec:
+            return
+        value = model.current_value() if model is not None and \
+            hasattr(model, "current_value") else None
+        src = self._maxwell_source_from(value)
+        if src is not None:
+            self._source = src
+
+    def _maxwell_source_from(self, value):
+        """Device [n_E, K*Np] source rows for the current field's value
+        ([n_E, N] or numbers; None: not known yet and needed)."""
+        torch = _torch()
+        d = self.discr
+        out = torch.zeros((self._n_e, len(d)), dtype=torch.float64, device=d.device)
+        for o, const, fld, coef in self._msrc_spec:
+            row = torch.full((len(d),), float(const), dtype=torch.float64, device=d.device)
+            if fld is not None:
+                if value is None:
+                    return None
+                v = value[fld[1]] if fld[1] is not None else value
+                v = torch.full((len(d),), float(v), dtype=torch.float64, device=d.device) \
+                    if np.isscalar(v) else d.to_device(v, torch.float64).reshape(-1)
+                row = row + coef * v
+            out[o] = row
+        return out.contiguous()
 
     @property
     def state_dtype(self):
@@ -504,11 +558,12 @@ class CompiledOperator:
         tensors when given (FP64 [K*Np] on the device), else the operator's."""
         c = self._coeff if coeff is None else coeff
         s = self._source if source is None else source
-        for t in (coeff, source):
+        for t, rows in ((coeff, 1), (source, self._n_e or 1)):
             if t is not None:
                 if t.dtype != _torch().float64 or not t.is_contiguous() or \
-                        t.numel() != len(self.discr) or t.device != self.discr.device:
-                    raise ValueError("c / source: contiguous FP64 [K*Np] on the device")
+                        t.numel() != rows * len(self.discr) or t.device != self.discr.device:
+                    raise ValueError("c / source: contiguous FP64 [%d * K*Np] on the device"
+                                     % rows)
         return (c.data_ptr() if c is not None else None,
                 s.data_ptr() if s is not None else None)
 
@@ -592,6 +647,13 @@ class CompiledOperator:
         if names.get("coeff") in kwargs:
             coeff = self.discr.to_device(kwargs.pop(names["coeff"]), _torch().float64)
             coeff = coeff.reshape(-1).contiguous()
+        if self._msrc_spec:
+            fnames = {fld[0] for _, _, fld, _ in self._msrc_spec if fld is not None}
+            for nm in fnames:
+                if nm in kwargs:
+                    source = self._maxwell_source_from(kwargs.pop(nm))
+            if fnames and source is None and self._source is None:
+                raise ValueError("this template needs its current field %r" % sorted(fnames))
         src_name = names.get("source")
         if src_name is not None and src_name[0] in kwargs:
             val = kwargs.pop(src_name[0])
@@ -624,14 +686,18 @@ class BoundRHS:
         self.discr = compiled.discr
 
     def context(self, t):
+        """Given boundary data at time t that the model can evaluate itself
+        (advection inflow, wave Dirichlet values given as functions)."""
         if self.compiled.n_given:
             m = self.model
-            return {"bc_in": m.inflow_u.boundary_interpolant(t, self.discr,
-                                                             self.compiled.given_tag)}
+            if hasattr(m, "context"):
+                return m.context(self.discr, t)
         return {}
 
-    def __call__(self, t, w):
-        return self.compiled(w=w, t=t, **self.context(t))
+    def __call__(self, t, w, **extra_context):
+        kw = self.context(t)
+        kw.update(extra_context)
+        return self.compiled(w=w, t=t, **kw)
 
 
 __all__ = ["Discretization", "CompiledOperator", "BoundRHS", "PointEvaluator",

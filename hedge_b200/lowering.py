@@ -54,8 +54,9 @@ from . import flux as fl
 from . import optemplate as ot
 from .mesh import TAG_ALL, TAG_NONE
 from .models import (BC_ABSORB, BC_DIRICHLET, BC_GIVEN, BC_NEUMANN, BC_NONE, BC_PEC, BC_PMC,
-                     BC_RADIATION, MODEL_ADVECTION, MODEL_MAXWELL, MODEL_VARWAVE,
-                     MODEL_WAVE, MaxwellOperator, OpTemplate, StrongAdvectionOperator,
+                     BC_RADIATION, MODEL_ADVECTION, MODEL_MAXWELL, MODEL_MAXWELL_TE,
+                     MODEL_MAXWELL_TM, MODEL_VARWAVE, MODEL_WAVE, MaxwellOperator,
+                     TEMaxwellOperator, TMMaxwellOperator, OpTemplate, StrongAdvectionOperator,
                      StrongWaveOperator, VariableVelocityStrongWaveOperator)
 
 PROBES = 16
@@ -470,6 +471,7 @@ class _Roles:
 class _Family:
     model = None
     kinds = ()
+    source_outputs = ()      # outputs the kernel model can add a source to
 
     def applies(self, dims, F, ncoeff):
         return False
@@ -512,7 +514,8 @@ class _Advection(_Family):
 
 class _Wave(_Family):
     model = MODEL_WAVE
-    kinds = (BC_DIRICHLET, BC_NEUMANN, BC_RADIATION)
+    kinds = (BC_DIRICHLET, BC_NEUMANN, BC_RADIATION, BC_GIVEN)
+    source_outputs = (0,)
 
     def applies(self, dims, F, ncoeff):
         return F == dims + 1 and ncoeff == 0
@@ -527,20 +530,26 @@ class _Wave(_Family):
     def _tags(self, bc):
         t = {BC_DIRICHLET: TAG_NONE, BC_NEUMANN: TAG_NONE, BC_RADIATION: TAG_NONE}
         if bc is not None:
-            t[bc[1]] = bc[0]
+            # given data on a tag: inhomogeneous Dirichlet there
+            t[BC_DIRICHLET if bc[1] == BC_GIVEN else bc[1]] = bc[0]
         return dict(dirichlet_tag=t[BC_DIRICHLET], neumann_tag=t[BC_NEUMANN],
                     radiation_tag=t[BC_RADIATION])
 
     def build(self, roles, p, bc):
         dims = len(roles.state) - 1
+        given = bc is not None and bc[1] == BC_GIVEN
+        if given and roles.given is None:
+            return None
         m = StrongWaveOperator(p["c"], dims, source_f=0, flux_type=p["flux_type"],
-                               **self._tags(bc))
+                               dirichlet_bc_f=1 if given else 0, **self._tags(bc))
         m.source_f = roles.source
-        return m, _comps(m.op_template(w=roles.state))
+        return m, _comps(m.op_template(w=roles.state,
+                                       dir_bc_u=roles.given if given else None))
 
 
 class _VarWave(_Wave):
     model = MODEL_VARWAVE
+    kinds = (BC_DIRICHLET, BC_NEUMANN, BC_RADIATION)
 
     def applies(self, dims, F, ncoeff):
         return F == dims + 1 and ncoeff == 1
@@ -561,11 +570,14 @@ class _VarWave(_Wave):
 class _Maxwell(_Family):
     model = MODEL_MAXWELL
     kinds = (BC_PEC, BC_PMC, BC_ABSORB)
+    source_outputs = (0, 1, 2)
+    cls = MaxwellOperator
 
     def applies(self, dims, F, ncoeff):
         return dims == 3 and F == 6 and ncoeff == 0
 
     def volume_params(self, V):
+        # d/dy Hz -> Ex is 1/eps, d/dy Ez -> Hx is -1/mu
         a, b = V[0, 5, 1], V[3, 2, 1]
         if a <= 0 or b >= 0:
             return None
@@ -597,21 +609,61 @@ class _Maxwell(_Family):
         t = {BC_PEC: TAG_NONE, BC_PMC: TAG_NONE, BC_ABSORB: TAG_NONE}
         if bc is not None:
             t[bc[1]] = bc[0]
-        m = MaxwellOperator(p["eps"], p["mu"], p["flux_type"],
-                            bdry_flux_type=p.get("bdry_flux_type", p["flux_type"]),
-                            pec_tag=t[BC_PEC], pmc_tag=t[BC_PMC],
-                            absorb_tag=t[BC_ABSORB])
+        m = self.cls(p["eps"], p["mu"], p["flux_type"],
+                     bdry_flux_type=p.get("bdry_flux_type", p["flux_type"]),
+                     pec_tag=t[BC_PEC], pmc_tag=t[BC_PMC], absorb_tag=t[BC_ABSORB])
+        # E_c's rhs source s_c = -J_c / eps: the current is -eps s
+        ne = m.n_e
+        srcs = getattr(roles, "sources", None)
+        if srcs is not None and any(not ot.is_zero(x) for x in srcs[:ne]):
+            m.current = np.array([-p["eps"] * x if not ot.is_zero(x) else 0
+                                  for x in srcs[:ne]], dtype=object)
+        if srcs is not None and any(not ot.is_zero(x) for x in srcs[ne:]):
+            return None
         return m, _comps(m.op_template(w=roles.state))
 
 
-_FAMILIES = (_Advection(), _Wave(), _VarWave(), _Maxwell())
+class _MaxwellTM(_Maxwell):
+    model = MODEL_MAXWELL_TM
+    source_outputs = (0,)
+    cls = TMMaxwellOperator
+
+    def applies(self, dims, F, ncoeff):
+        return dims == 2 and F == 3 and ncoeff == 0
+
+    def volume_params(self, V):
+        # (Ez, Hx, Hy): d/dx Hy -> Ez is 1/eps, d/dy Ez -> Hx is -1/mu
+        a, b = V[0, 2, 0], V[1, 0, 1]
+        if a <= 0 or b >= 0:
+            return None
+        return {"eps": 1.0 / a, "mu": -1.0 / b}
+
+
+class _MaxwellTE(_Maxwell):
+    model = MODEL_MAXWELL_TE
+    source_outputs = (0, 1)
+    cls = TEMaxwellOperator
+
+    def applies(self, dims, F, ncoeff):
+        return dims == 2 and F == 3 and ncoeff == 0
+
+    def volume_params(self, V):
+        # (Ex, Ey, Hz): d/dy Hz -> Ex is 1/eps, d/dx Ey -> Hz is -1/mu
+        a, b = V[0, 2, 1], V[2, 1, 0]
+        if a <= 0 or b >= 0:
+            return None
+        return {"eps": 1.0 / a, "mu": -1.0 / b}
+
+
+_FAMILIES = (_Advection(), _Wave(), _VarWave(), _Maxwell(), _MaxwellTM(), _MaxwellTE())
 
 
 # --------------------------------------------------------------------------
 
 def _source(user, roles_keys, src_fields, dims):
-    """The template's source: output values with the state, derivatives and
-    fluxes at zero, as const + sum coef_k * field_k on output 0."""
+    """The template's sources: output values with the state, derivatives and
+    fluxes at zero, per output as const + sum coef_k * field_k.  Returns
+    (expressions, constants, terms) with one entry per output."""
     zero = {k: np.zeros(PROBES) for k in roles_keys}
 
     def at(fixed):
@@ -621,18 +673,19 @@ def _source(user, roles_keys, src_fields, dims):
 
     allzero = {k: np.zeros(PROBES) for k in src_fields}
     base = at(allzero)
-    const = base[0, 0]
-    expr = const if const != 0 else 0
-    terms = []
+    if np.any(base != base[:, :1]):
+        raise NotImplementedError("sources that vary with the state")
+    consts = base[:, 0]
+    exprs = [float(c) if c != 0 else 0 for c in consts]
+    terms = [[] for _ in consts]
     for k, f in src_fields.items():
         one = at({**allzero, k: np.ones(PROBES)})
-        coef = one[0, 0] - const
-        if coef != 0:
-            expr = expr + coef * f
-            terms.append((f.name, f.index, coef))
-    if np.any(base[1:] != 0) or np.any(base[0] != const):
-        raise NotImplementedError("source terms on fields other than the first")
-    return expr, const, terms
+        for o in range(len(consts)):
+            coef = one[o, 0] - consts[o]
+            if coef != 0:
+                exprs[o] = exprs[o] + coef * f
+                terms[o].append((f.name, f.index, coef))
+    return exprs, consts, terms
 
 
 def lower(template, dimensions, mesh=None):
@@ -670,12 +723,14 @@ def lower(template, dimensions, mesh=None):
     src_fields = {k: f for k, f in scan.outside_fields.items()
                   if k not in st_keys | co_keys and k not in diff}
     roles_keys = st_keys | co_keys | {f.key for f in given}
-    src_expr, src_const, src_terms = _source(outs, roles_keys, src_fields, dimensions)
-    if len(src_terms) > 1:
-        raise NotImplementedError("more than one source field")
+    src_exprs, src_consts, src_terms = _source(outs, roles_keys, src_fields, dimensions)
+    if any(len(t) > 1 for t in src_terms):
+        raise NotImplementedError("more than one source field on an output")
+    src_outputs = [o for o in range(F) if src_terms[o] or src_consts[o] != 0]
     state_arr = ot.join_fields(state)
     roles = _Roles(state_arr, coeff[0] if coeff else None, given[0] if given else None,
-                   src_expr)
+                   src_exprs[0])
+    roles.sources = src_exprs
 
     # volume coefficients V[f, g, x]: unit derivative probes less the
     # zero-derivative value (the constant source), coefficient fields = 1
@@ -716,6 +771,9 @@ def lower(template, dimensions, mesh=None):
             why[:] = [stage, msg]
     for fam in _FAMILIES:
         if not fam.applies(dimensions, F, len(coeff)):
+            continue
+        if any(o not in fam.source_outputs for o in src_outputs):
+            fail(1, "sources on outputs the %s kernel has none for" % type(fam).__name__[1:])
             continue
         params = fam.volume_params(V)
         if params is None:
@@ -774,12 +832,19 @@ def lower(template, dimensions, mesh=None):
             desc = model.descriptor()
             bcs = [(t, k) for t, k in bcs if not (k == BC_NONE and t is TAG_ALL)]
             names = roles.names()
-            if src_terms:
-                names["source"] = src_terms[0][:2]
-                names["source_coef"] = src_terms[0][2]
-            names["source_const"] = src_const
+            if desc.model in (MODEL_MAXWELL, MODEL_MAXWELL_TM, MODEL_MAXWELL_TE):
+                # per E component: the value added to its rhs, const + coef * field
+                names["sources"] = [(o, float(src_consts[o]),
+                                     src_terms[o][0][:2] if src_terms[o] else None,
+                                     src_terms[o][0][2] if src_terms[o] else 0.0)
+                                    for o in src_outputs]
+            else:
+                if src_terms[0]:
+                    names["source"] = src_terms[0][0][:2]
+                    names["source_coef"] = src_terms[0][0][2]
+                names["source_const"] = float(src_consts[0])
             return OpTemplate(desc.model, desc.dimensions, desc.n_fields, desc.flux_type,
-                              _lowered_params(desc, src_const), bcs, None, names)
+                              _lowered_params(desc, float(src_consts[0])), bcs, None, names)
     raise NotImplementedError("op template is not one the B200 kernels implement: " + why[1])
 
 

@@ -15,6 +15,8 @@ lowered form (:class:`OpTemplate`) directly:
   rhs = (ts c div v - source, ts c grad u) + M^-1 (fluxes of (c, u, v))
 * MaxwellOperator          hedge/models/em.py:38-387 (fixed material)
   rhs = ((curl H - J) , -curl E) + M^-1 (fluxes)) / (eps | mu)
+* TMMaxwellOperator, TEMaxwellOperator  hedge/models/em.py:485-515 (2D
+  subsets (Ez, Hx, Hy) and (Ex, Ey, Hz) of the same system)
 """
 
 from __future__ import annotations
@@ -34,6 +36,8 @@ MODEL_ADVECTION = 1
 MODEL_WAVE = 2
 MODEL_VARWAVE = 3
 MODEL_MAXWELL = 4
+MODEL_MAXWELL_TM = 5
+MODEL_MAXWELL_TE = 6
 
 # boundary-condition kinds shared with the C-ABI
 BC_NONE = 0        # face contributes no boundary flux
@@ -188,7 +192,7 @@ class StrongAdvectionOperator(HyperbolicOperator):
     def bc_tags(self):
         return [self.inflow_tag, self.outflow_tag]
 
-    def context(self, discr, t, fields):
+    def context(self, discr, t, fields=None):
         return {"bc_in": self.inflow_u.boundary_interpolant(t, discr, self.inflow_tag)}
 
 
@@ -217,11 +221,16 @@ class StrongWaveOperator(HyperbolicOperator):
     def __init__(self, c, dimensions, source_f=0, flux_type="upwind",
                  dirichlet_tag=TAG_ALL, dirichlet_bc_f=0,
                  neumann_tag=TAG_NONE, radiation_tag=TAG_NONE):
+        """``dirichlet_bc_f``: 0 (homogeneous Dirichlet walls), or the Dirichlet
+        value g of u on ``dirichlet_tag`` (ext state (2g - u, v), wave.py:133-142):
+        a TimeConstantGivenFunction / TimeDependentGivenFunction, which the
+        bound RHS and the steppers evaluate on the boundary, or any other true
+        value, in which case the caller passes the boundary vector as
+        ``rhs(t, w, dir_bc_u=...)`` (the reference's field name)."""
         assert isinstance(dimensions, int)
         if flux_type not in ("central", "upwind"):
             raise ValueError("invalid flux type '%s'" % flux_type)
-        if dirichlet_bc_f:
-            raise NotImplementedError("inhomogeneous Dirichlet data")
+        self.dirichlet_bc_f = dirichlet_bc_f
         self.c = float(c)
         self.dimensions = dimensions
         self.source_f = source_f
@@ -247,13 +256,17 @@ class StrongWaveOperator(HyperbolicOperator):
         flux_strong = ot.join_fields(np.dot(v.int, normal), u.int * normal) - flux_weak
         return -self.c * flux_strong
 
-    def op_template(self, w=None):
+    def op_template(self, w=None, dir_bc_u=None):
         """wave.py:110-180"""
         d = self.dimensions
         w = ot.make_sym_vector("w", d + 1) if w is None else w
         u, v = w[0], w[1:]
         B = ot.BoundarizeOperator
-        dir_bc = ot.join_fields(-(B(self.dirichlet_tag) * u), B(self.dirichlet_tag) * v)
+        if self.dirichlet_bc_f:
+            g = ot.Field("dir_bc_u") if dir_bc_u is None else dir_bc_u
+            dir_bc = ot.join_fields(2 * g - B(self.dirichlet_tag) * u, B(self.dirichlet_tag) * v)
+        else:
+            dir_bc = ot.join_fields(-(B(self.dirichlet_tag) * u), B(self.dirichlet_tag) * v)
         neu_bc = ot.join_fields(B(self.neumann_tag) * u, -(B(self.neumann_tag) * v))
         rn = ot.normal(self.radiation_tag, d)
         rad_u, rad_v = B(self.radiation_tag) * u, B(self.radiation_tag) * v
@@ -274,12 +287,20 @@ class StrongWaveOperator(HyperbolicOperator):
         return OpTemplate(MODEL_WAVE, self.dimensions, self.dimensions + 1,
                           1 if self.flux_type == "upwind" else 0,
                           {"c": self.c, "source": self.source_f},
-                          [(self.dirichlet_tag, BC_DIRICHLET),
+                          [(self.dirichlet_tag, BC_GIVEN if self.dirichlet_bc_f else BC_DIRICHLET),
                            (self.neumann_tag, BC_NEUMANN),
                            (self.radiation_tag, BC_RADIATION)], self)
 
     def bc_tags(self):
         return [self.dirichlet_tag, self.neumann_tag, self.radiation_tag]
+
+    def context(self, discr, t, fields=None):
+        """Boundary data of the bound RHS at time t (Dirichlet values given
+        as a function); empty when the caller supplies dir_bc_u."""
+        f = self.dirichlet_bc_f
+        if f and hasattr(f, "boundary_interpolant"):
+            return {"bc_in": f.boundary_interpolant(t, discr, self.dirichlet_tag)}
+        return {}
 
 
 class VariableVelocityStrongWaveOperator(HyperbolicOperator):
@@ -362,18 +383,28 @@ class VariableVelocityStrongWaveOperator(HyperbolicOperator):
 
 
 class MaxwellOperator(HyperbolicOperator):
-    """3D Maxwell, fixed isotropic material, field order [Ex Ey Ez Hx Hy Hz]."""
+    """Maxwell's equations, fixed isotropic material (em.py:38-387): the full
+    3D system, field order [Ex Ey Ez Hx Hy Hz]; the subclasses carry a subset
+    of the components (get_eh_subset) in 2D, the fields not carried and all
+    z derivatives (and normal z components) being zero."""
+
+    _default_dimensions = 3
+    model_id = MODEL_MAXWELL
 
     def __init__(self, epsilon, mu, flux_type, bdry_flux_type=None,
                  pec_tag=TAG_ALL, pmc_tag=TAG_NONE, absorb_tag=TAG_NONE,
                  incident_tag=TAG_NONE, current=0, dimensions=None):
-        self.dimensions = dimensions or 3
-        if self.dimensions != 3:
-            raise NotImplementedError("only the full 3D Maxwell system")
+        """``current``: the source current J of em.py:192-214 (the E equations
+        read eps dE/dt = curl H - J) over the carried E components: 0,
+        numbers, a volume field [n_E, K*Np] (array, tensor or vectors), or a
+        template vector."""
+        self.dimensions = dimensions or self._default_dimensions
+        if self.dimensions != self._default_dimensions:
+            raise NotImplementedError("%s is a %dD system" % (type(self).__name__,
+                                                             self._default_dimensions))
         if not (np.isscalar(epsilon) and np.isscalar(mu)):
             raise NotImplementedError("only fixed material")
-        if current != 0:
-            raise NotImplementedError("source currents are not on this path")
+        self.current = current
         if incident_tag is not TAG_NONE:
             raise NotImplementedError("incident boundary data is not on this path")
         self.epsilon, self.mu = float(epsilon), float(mu)
@@ -393,59 +424,123 @@ class MaxwellOperator(HyperbolicOperator):
         """em.py: which of (Ex, Ey, Ez, Hx, Hy, Hz) the operator carries."""
         return (True,) * 6
 
+    @property
+    def _slots(self):
+        return [i for i, on in enumerate(self.get_eh_subset()) if on]
+
+    @property
+    def n_e(self):
+        """Number of carried E components (they come first)."""
+        return sum(self.get_eh_subset()[:3])
+
+    @property
+    def n_fields(self):
+        return len(self._slots)
+
     def split_eh(self, w):
-        """(E, H) of a field vector [6, ...]."""
-        return w[0:3], w[3:6]
+        """(E, H) of a field vector [n_fields, ...] (carried components)."""
+        return w[0:self.n_e], w[self.n_e:self.n_fields]
 
     def assemble_eh(self, e, h):
         import torch
+        ne, nh = self.n_e, self.n_fields - self.n_e
         if isinstance(e, torch.Tensor):
-            return torch.cat([e.reshape(3, -1), h.reshape(3, -1)])
-        return np.concatenate([np.asarray(e).reshape(3, -1), np.asarray(h).reshape(3, -1)])
+            return torch.cat([e.reshape(ne, -1), h.reshape(nh, -1)])
+        return np.concatenate([np.asarray(e).reshape(ne, -1), np.asarray(h).reshape(nh, -1)])
+
+    def _embed(self, w):
+        """The 6 components (Ex .. Hz) of a carried-field vector, zeros elsewhere."""
+        full = np.array([0] * 6, dtype=object)
+        for k, slot in enumerate(self._slots):
+            full[slot] = w[k]
+        return full
+
+    def _pick(self, full):
+        return np.array([full[slot] for slot in self._slots], dtype=object)
+
+    @staticmethod
+    def _pad3(x):
+        return np.array(list(x) + [0] * (3 - len(x)), dtype=object)
 
     def max_eigenvalue(self, t=None, fields=None, discr=None):
         return 1 / sqrt(self.epsilon * self.mu)
 
     def flux(self, flux_type):
         """em.py:118-190, fixed material"""
-        normal = fl.make_normal(3)
-        w = fl.FluxVectorPlaceholder(6)
-        e, h = w[0:3], w[3:6]
+        normal = self._pad3(fl.make_normal(self.dimensions))
+        w = fl.FluxVectorPlaceholder(self.n_fields)
+        wi = self._embed([w[k].int for k in range(self.n_fields)])
+        we = self._embed([w[k].ext for k in range(self.n_fields)])
         epsilon = fl.FluxConstantPlaceholder(self.epsilon)
         mu = fl.FluxConstantPlaceholder(self.mu)
         Z_int = (mu.int / epsilon.int) ** 0.5
         Y_int = 1 / Z_int
         Z_ext = (mu.ext / epsilon.ext) ** 0.5
         Y_ext = 1 / Z_ext
-        de, dh = e.int - e.ext, h.int - h.ext
+        de, dh = wi[0:3] - we[0:3], wi[3:6] - we[3:6]
         if flux_type == "lf":
-            return ot.join_fields(0.5 * -ot.cross(normal, dh), 0.5 * ot.cross(normal, de))
-        return ot.join_fields(
-            -1 / (Z_int + Z_ext) * ot.cross(normal, Z_ext * dh - flux_type * ot.cross(normal, de)),
-            1 / (Y_int + Y_ext) * ot.cross(normal, Y_ext * de + flux_type * ot.cross(normal, dh)))
+            full = ot.join_fields(0.5 * -ot.cross(normal, dh), 0.5 * ot.cross(normal, de))
+        else:
+            full = ot.join_fields(
+                -1 / (Z_int + Z_ext) * ot.cross(normal, Z_ext * dh - flux_type * ot.cross(normal, de)),
+                1 / (Y_int + Y_ext) * ot.cross(normal, Y_ext * de + flux_type * ot.cross(normal, dh)))
+        return self._pick(full)
+
+    def current_template(self):
+        """The current over the carried E components as template terms: 0,
+        numbers, or the components of the volume field ``current``."""
+        ne = self.n_e
+        j = self.current
+        if isinstance(j, np.ndarray) and j.dtype == object:
+            return j
+        if np.isscalar(j):
+            return 0 if j == 0 else np.array([float(j)] * ne, dtype=object)
+        a = _to_numpy(j)
+        if isinstance(a, (list, tuple)) and len(a) == ne and all(np.isscalar(x) for x in a):
+            return np.array([float(x) if x != 0 else 0 for x in a], dtype=object)
+        return ot.make_sym_vector("current", ne)
+
+    def current_value(self):
+        """The current's volume values [n_E, K*Np] (or numbers) for binding."""
+        j = self.current
+        if isinstance(j, (list, tuple)) and not all(np.isscalar(x) for x in j):
+            return np.stack([np.asarray(_to_numpy(x), dtype=np.float64).reshape(-1) for x in j])
+        return _to_numpy(j)
 
     def local_derivatives(self, w):
-        """em.py:192-214: (current - curl H, curl E)"""
-        e, h = w[0:3], w[3:6]
-        nabla = ot.make_nabla(3)
-        return ot.join_fields(-ot.cross(nabla, h), ot.cross(nabla, e))
+        """em.py:192-214: (current - curl H, curl E), over the carried components"""
+        full = self._embed(w)
+        e, h = full[0:3], full[3:6]
+        nabla = self._pad3(ot.make_nabla(self.dimensions))
+        cur = self.current_template()
+        j = np.array([0] * 3, dtype=object)
+        if not (np.isscalar(cur) and cur == 0):
+            for k, slot in enumerate(self._slots[:self.n_e]):
+                j[slot] = cur[k]
+        return self._pick(ot.join_fields(j - ot.cross(nabla, h), ot.cross(nabla, e)))
 
     def op_template(self, w=None):
         """em.py:226-371, fixed material"""
-        w = ot.make_sym_vector("w", 6) if w is None else w
-        e, h = w[0:3], w[3:6]
+        F = self.n_fields
+        w = ot.make_sym_vector("w", F) if w is None else w
         B = ot.BoundarizeOperator
-        pec = ot.join_fields(-(B(self.pec_tag) * e), B(self.pec_tag) * h)
-        pmc = ot.join_fields(B(self.pmc_tag) * e, -(B(self.pmc_tag) * h))
-        an = ot.normal(self.absorb_tag, 3)
+
+        def bfull(tag):
+            return self._embed([B(tag) * w[k] for k in range(F)])
+        pe = bfull(self.pec_tag)
+        pec = self._pick(ot.join_fields(-pe[0:3], pe[3:6]))
+        pm = bfull(self.pmc_tag)
+        pmc = self._pick(ot.join_fields(pm[0:3], -pm[3:6]))
+        an = self._pad3(ot.normal(self.absorb_tag, self.dimensions))
         Z = (self.mu / self.epsilon) ** 0.5
-        ae, ah = B(self.absorb_tag) * e, B(self.absorb_tag) * h
-        absorb = ot.join_fields(
+        ab = bfull(self.absorb_tag)
+        ae, ah = ab[0:3], ab[3:6]
+        absorb = self._pick(ot.join_fields(
             ae + 0.5 * (ot.cross(an, ot.cross(an, ae)) - Z * ot.cross(an, ah)),
-            ah + 0.5 * (ot.cross(an, ot.cross(an, ah)) + (1 / Z) * ot.cross(an, ae)))
+            ah + 0.5 * (ot.cross(an, ot.cross(an, ah)) + (1 / Z) * ot.cross(an, ae))))
         flux_op = ot.get_flux_operator(self.flux(self.flux_type))
         bdry_flux_op = ot.get_flux_operator(self.flux(self.bdry_flux_type))
-        divisor = np.array([self.epsilon] * 3 + [self.mu] * 3)
+        divisor = np.array([self.epsilon] * self.n_e + [self.mu] * (F - self.n_e))
         bdry = sum(bdry_flux_op(ot.BoundaryPair(w, bc, tag)) for tag, bc in
                    [(self.pec_tag, pec), (self.pmc_tag, pmc), (self.absorb_tag, absorb)])
         return _remember(self, (-self.local_derivatives(w)
@@ -456,7 +551,7 @@ class MaxwellOperator(HyperbolicOperator):
             return (1, 0.0) if ft == "lf" else (0, float(ft))
         ft, alpha = code(self.flux_type)
         bft, balpha = code(self.bdry_flux_type)
-        return OpTemplate(MODEL_MAXWELL, 3, 6, ft,
+        return OpTemplate(self.model_id, self.dimensions, self.n_fields, ft,
                           {"eps": self.epsilon, "mu": self.mu, "alpha": alpha,
                            "bdry_flux_type": bft, "bdry_alpha": balpha},
                           [(self.pec_tag, BC_PEC), (self.pmc_tag, BC_PMC),
@@ -465,6 +560,26 @@ class MaxwellOperator(HyperbolicOperator):
 
     def bc_tags(self):
         return [self.pec_tag, self.absorb_tag, self.incident_tag]
+
+
+class TMMaxwellOperator(MaxwellOperator):
+    """2D TM Maxwell (em.py:485-498), field order [Ez Hx Hy]."""
+
+    _default_dimensions = 2
+    model_id = MODEL_MAXWELL_TM
+
+    def get_eh_subset(self):
+        return (False, False, True) + (True, True, False)
+
+
+class TEMaxwellOperator(MaxwellOperator):
+    """2D TE Maxwell (em.py:501-515), field order [Ex Ey Hz]."""
+
+    _default_dimensions = 2
+    model_id = MODEL_MAXWELL_TE
+
+    def get_eh_subset(self):
+        return (True, True, False) + (False, False, True)
 
 
 def _template_value(x, name):
@@ -488,7 +603,8 @@ def _to_numpy(x):
 
 
 __all__ = ["template_model", "StrongAdvectionOperator", "WeakAdvectionOperator", "StrongWaveOperator",
-           "VariableVelocityStrongWaveOperator", "MaxwellOperator",
+           "VariableVelocityStrongWaveOperator", "MaxwellOperator", "TMMaxwellOperator",
+           "TEMaxwellOperator",
            "OpTemplate", "make_tdep_constant", "TimeConstantGivenFunction",
            "TimeDependentGivenFunction",
            "check_bc_coverage"]

@@ -35,7 +35,9 @@ enum {
   HB_MODEL_ADVECTION = 1, /* hedge/models/advection.py:124-149 */
   HB_MODEL_WAVE = 2,      /* hedge/models/wave.py:37-197 */
   HB_MODEL_VARWAVE = 3,   /* hedge/models/wave.py:204-418 */
-  HB_MODEL_MAXWELL = 4    /* hedge/models/em.py:38-387 */
+  HB_MODEL_MAXWELL = 4,   /* hedge/models/em.py:38-387 */
+  HB_MODEL_MAXWELL_TM = 5, /* hedge/models/em.py:485-498, 2D, fields (Ez, Hx, Hy) */
+  HB_MODEL_MAXWELL_TE = 6  /* hedge/models/em.py:501-515, 2D, fields (Ex, Ey, Hz) */
 };
 
 enum {

@@ -39,7 +39,8 @@
 extern "C" {
 
 enum { OR_ADVECTION = 1, OR_WAVE = 2, OR_VARWAVE = 3, OR_MAXWELL = 4,
-       OR_NORMAL_DOT = 5 };  // test flux sum_k n_k (u_int,k - alpha u_ext,k)
+       OR_MAXWELL_TM = 5, OR_MAXWELL_TE = 6,  // 2D (Ez, Hx, Hy) and (Ex, Ey, Hz)
+       OR_NORMAL_DOT = 9 };  // test flux sum_k n_k (u_int,k - alpha u_ext,k)
 
 struct or_flux_params {
   int model;
@@ -181,6 +182,21 @@ static void model_flux(const or_flux_params& p, const double* ui,
       f[0] = s;
       break;
     }
+    case OR_MAXWELL_TM: case OR_MAXWELL_TE: {
+      // em.py:485-515: the 3D flux of the embedded fields (the others zero),
+      // normal with a zero z component
+      const int slot_tm[3] = {2, 3, 4}, slot_te[3] = {0, 1, 5};
+      const int* slot = p.model == OR_MAXWELL_TM ? slot_tm : slot_te;
+      double ui6[6] = {0, 0, 0, 0, 0, 0}, ue6[6] = {0, 0, 0, 0, 0, 0}, f6[6];
+      for (int k = 0; k < 3; ++k) { ui6[slot[k]] = ui[k]; ue6[slot[k]] = ue[k]; }
+      const double n3[3] = {n[0], n[1], 0.0};
+      or_flux_params p3 = p;
+      p3.model = OR_MAXWELL;
+      p3.dim = 3;
+      model_flux(p3, ui6, ue6, n3, f6);
+      for (int k = 0; k < 3; ++k) f[k] = f6[slot[k]];
+      break;
+    }
     case OR_MAXWELL: {
       const double* ei = ui; const double* hi = ui + 3;
       const double* ee = ue; const double* he = ue + 3;
@@ -220,6 +236,7 @@ static int n_flux_components(const or_flux_params& p) {
     case OR_WAVE: return p.dim + 1;
     case OR_VARWAVE: return p.dim + 1;
     case OR_MAXWELL: return 6;
+    case OR_MAXWELL_TM: case OR_MAXWELL_TE: return 3;
     case OR_NORMAL_DOT: return 1;
   }
   return 0;

@@ -31,7 +31,12 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 
-OR_ADVECTION, OR_WAVE, OR_VARWAVE, OR_MAXWELL, OR_NORMAL_DOT = 1, 2, 3, 4, 5
+OR_ADVECTION, OR_WAVE, OR_VARWAVE, OR_MAXWELL, OR_NORMAL_DOT = 1, 2, 3, 4, 9
+OR_MAXWELL_TM, OR_MAXWELL_TE = 5, 6        # 2D (Ez, Hx, Hy) and (Ex, Ey, Hz)
+_MAXWELLS = (OR_MAXWELL, OR_MAXWELL_TM, OR_MAXWELL_TE)
+# positions of a Maxwell system's fields in (Ex Ey Ez Hx Hy Hz), E count
+_SLOTS = {OR_MAXWELL: ([0, 1, 2, 3, 4, 5], 3), OR_MAXWELL_TM: ([2, 3, 4], 1),
+          OR_MAXWELL_TE: ([0, 1, 5], 2)}
 BC_NONE, BC_GIVEN, BC_DIRICHLET, BC_NEUMANN, BC_RADIATION, BC_PEC, BC_PMC, BC_ABSORB = range(8)
 
 
@@ -140,6 +145,12 @@ class OracleRHS:
             s = getattr(ot.operator, "source", 0)
             if not (np.isscalar(s) and s == 0):
                 self.source = s
+        if self.source is None and ot.model in _MAXWELLS and \
+                hasattr(ot.operator, "current_value"):
+            # Maxwell: the source is the current J (em.py:192-214)
+            j = ot.operator.current_value()
+            if not (np.isscalar(j) and j == 0):
+                self.source = j
         self.params = self._params(bdry=False)
         self.bparams = self._params(bdry=True)
         self.bdry = []
@@ -157,7 +168,7 @@ class OracleRHS:
             v[:len(p["v"])] = p["v"]
         ft = ot.flux_type
         alpha = p.get("alpha", 1.0)
-        if ot.model == OR_MAXWELL and bdry:
+        if ot.model in _MAXWELLS and bdry:
             ft, alpha = p["bdry_flux_type"], p["bdry_alpha"]
         return or_flux_params(ot.model, self.dim, ft, ot.n_flux_args,
                               (C.c_double * 3)(*v), p.get("c", 0.0), p.get("eps", 1.0),
@@ -192,6 +203,11 @@ class OracleRHS:
         """Ext-state vectors on a boundary (BoundarizeOperator + BC formula)."""
         ab = args[:, b.vol_indices]
         m = self.ot.model
+        if kind == BC_GIVEN and m == OR_WAVE:
+            # inhomogeneous Dirichlet data g (wave.py:133-142): (2 g - u, v)
+            out = ab.copy()
+            out[0] = 2.0 * np.asarray(bc_in, dtype=np.float64).reshape(-1) - ab[0]
+            return out
         if kind == BC_GIVEN:
             return np.asarray(bc_in, dtype=np.float64).reshape(1, -1)
         if m in (OR_WAVE, OR_VARWAVE):
@@ -209,19 +225,27 @@ class OracleRHS:
                 out[C0] = 0.5 * (u - sgn * nv)
                 out[C0 + 1:] = 0.5 * normals.T * (nv - sgn * u)
             return out
-        if m == OR_MAXWELL:
-            e, h = ab[:3], ab[3:]
+        if m in _MAXWELLS:
+            # em.py:226-287 on the six components (2D systems embedded, n_z = 0)
+            slots, _ = _SLOTS[m]
+            full = np.zeros((6, ab.shape[1]))
+            full[slots] = ab
+            e, h = full[:3], full[3:]
+            nrm = np.zeros((ab.shape[1], 3))
+            nrm[:, :normals.shape[1]] = normals
             if kind == BC_PEC:
-                return np.vstack([-e, h])
-            if kind == BC_PMC:
-                return np.vstack([e, -h])
-            if kind == BC_ABSORB:
+                out = np.vstack([-e, h])
+            elif kind == BC_PMC:
+                out = np.vstack([e, -h])
+            elif kind == BC_ABSORB:
                 p = self.ot.params
                 Z = np.sqrt(p["mu"] / p["eps"])
-                n = normals.T
-                ne, nh = np.cross(n.T, e.T).T, np.cross(n.T, h.T).T
-                nne, nnh = np.cross(n.T, ne.T).T, np.cross(n.T, nh.T).T
-                return np.vstack([e + 0.5 * (nne - Z * nh), h + 0.5 * (nnh + ne / Z)])
+                ne, nh = np.cross(nrm, e.T).T, np.cross(nrm, h.T).T
+                nne, nnh = np.cross(nrm, ne.T).T, np.cross(nrm, nh.T).T
+                out = np.vstack([e + 0.5 * (nne - Z * nh), h + 0.5 * (nnh + ne / Z)])
+            else:
+                raise ValueError("unsupported boundary kind %d" % kind)
+            return out[slots]
         raise ValueError("unsupported boundary kind %d" % kind)
 
     def flux_volume(self, fields, bc_in=None):
@@ -277,14 +301,24 @@ class OracleRHS:
                     else np.asarray(self.source)
                 out[0] += src if m == OR_WAVE else -src
             return out
-        if m == OR_MAXWELL:
-            g = np.stack([self.grad(fields[f]) for f in range(6)])   # [f, x, n]
+        if m in _MAXWELLS:
+            # the six components' gradients (2D systems: fields not carried
+            # and z derivatives zero)
+            slots, ne = _SLOTS[m]
+            g = np.zeros((6, 3, self.N))
+            for k, slot in enumerate(slots):
+                g[slot, :d] = self.grad(fields[k])
 
             def curl(a):
                 return np.stack([g[a + 2, 1] - g[a + 1, 2], g[a, 2] - g[a + 2, 0],
                                  g[a + 1, 0] - g[a, 1]])
-            vol = np.vstack([curl(3), -curl(0)])
-            div = np.array([p["eps"]] * 3 + [p["mu"]] * 3)[:, None]
+            vol = np.vstack([curl(3), -curl(0)])[slots]
+            if self.source is not None:
+                # eps dE/dt = curl H - J + lifted flux
+                j = np.asarray(self.source, dtype=np.float64)
+                vol[:ne] -= j.reshape(ne, -1) if j.size >= ne * self.N else \
+                    np.broadcast_to(j.reshape(-1, 1), (ne, self.N))
+            div = np.array([p["eps"]] * ne + [p["mu"]] * (len(slots) - ne))[:, None]
             return (vol + lifted) / div
         raise ValueError("unknown model")
 

@@ -108,6 +108,21 @@ def test_adjoint_maxwell(cuda_device, flux):
     _check_adjoint(d, op)
 
 
+@pytest.mark.parametrize("kind", ["tm", "te"])
+def test_adjoint_maxwell_2d(cuda_device, kind):
+    """2D TM / TE Maxwell (em.py:485-515) with PEC, PMC and absorbing walls."""
+    def tagger(fvi, el, fn, allv):
+        x = allv[list(fvi)].mean(0)
+        return ["abs"] if x[0] > 0.99 else (["pmc"] if x[0] < -0.99 else ["pec"])
+    m = hb.make_regular_rect_mesh((-1, -1), (1, 1), (4, 4), boundary_tagger=tagger,
+                                  jitter=0.05, seed=3)
+    d = hb.Discretization(m, order=3)
+    cls = hb.TMMaxwellOperator if kind == "tm" else hb.TEMaxwellOperator
+    op = cls(1.4, 0.6, flux_type=0.5, bdry_flux_type=1, pec_tag="pec", pmc_tag="pmc",
+             absorb_tag="abs")
+    _check_adjoint(d, op)
+
+
 def test_adjoint_c_gradient(cuda_device):
     import torch
     from oracle import OracleRHS

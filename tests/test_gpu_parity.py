@@ -107,6 +107,145 @@ def test_wave_3d(cuda_device, precision):
     _check(d, hb.StrongWaveOperator(1.0, 3, flux_type="upwind"), precision)
 
 
+def _lr_tagger(names):
+    def tagger(fvi, el, fn, allv):
+        x = allv[list(fvi)].mean(0)
+        if x[0] < -0.99:
+            return [names[0]]
+        if x[0] > 0.99:
+            return [names[1]]
+        return [names[2]]
+    return tagger
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32-simt", "fp16x3", "bf16x3"])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_wave_dirichlet_data(cuda_device, precision, dim):
+    """Inhomogeneous Dirichlet data g on a tag (ext state (2g - u, v),
+    wave.py:133-142), given as the boundary vector dir_bc_u."""
+    from oracle import OracleRHS
+    tagger = _lr_tagger(["neu", "dir", "dir"])
+    m = hb.make_regular_rect_mesh((-1, -1), (1, 1), (8, 8), boundary_tagger=tagger,
+                                  jitter=0.02, seed=5) if dim == 2 else \
+        hb.make_box_tet_mesh(n=(3, 3, 3), jitter=0.03, seed=5, boundary_tagger=tagger)
+    d = hb.Discretization(m, order=4)
+    op = hb.StrongWaveOperator(1.2, dim, dirichlet_tag="dir", dirichlet_bc_f=1,
+                               neumann_tag="neu")
+    g = np.cos(2 * d.get_boundary("dir").nodes[:, 1]) + 0.3
+    q = _fields(d, dim + 1, 7)
+    fp32 = precision in ("fp32", "fp32-simt")
+    qs = q.astype(np.float32).astype(np.float64) if fp32 else q
+    ref = OracleRHS(d, op.op_template())(qs, bc_in=g)
+    comp = d.compile(op.op_template(), precision=precision)
+    got = comp(w=qs, dir_bc_u=g).double().cpu().numpy()
+    comp.check()
+    tol = {"fp64": 1e-12, "fp32": 1e-5, "fp32-simt": 1e-5, "fp16x3": 1e-6, "bf16x3": 1e-5}
+    assert rel_l2(got, ref) <= tol[precision]
+
+
+def test_wave_dirichlet_data_time_dependent_steps(cuda_device):
+    """Time-dependent Dirichlet data given as a function: the bound RHS and
+    the fused LSRK4 stages evaluate it at every stage time; 20 steps against
+    the oracle's LSRK4 with the same data."""
+    from oracle import OracleRHS
+    m = hb.make_regular_rect_mesh((-1, -1), (1, 1), (9, 9), jitter=0.02, seed=6,
+                                  boundary_tagger=_lr_tagger(["dir", "rad", "dir"]))
+    d = hb.Discretization(m, order=4)
+    gf = hb.TimeDependentGivenFunction(lambda x, t: np.sin(3 * t) * np.cos(x[:, 1]))
+    op = hb.StrongWaveOperator(1.0, 2, dirichlet_tag="dir", dirichlet_bc_f=gf,
+                               radiation_tag="rad")
+    rhs = op.bind(d)
+    q = _fields(d, 3, 8)
+    dt = 0.5 * op.estimate_timestep(d)
+    orc = OracleRHS(d, op.op_template())
+    y = d.to_device(q).reshape(3, -1)
+    yo, res, t = q.copy(), np.zeros_like(q), 0.0
+    st = hb.LSRK4TimeStepper()
+    for _ in range(20):
+        y = st(y, t, dt, rhs)
+        yo, res = orc.lsrk4_step(yo, t, dt, res,
+                                 bc_fn=lambda tt: gf.boundary_interpolant(tt, d, "dir"))
+        t += dt
+    rhs.compiled.check()
+    assert rel_l2(y.cpu().numpy(), yo) <= 1e-11
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32-simt", "fp16x3", "bf16x3"])
+def test_maxwell_current(cuda_device, precision):
+    """Maxwell with a source current J [3, K*Np] (em.py:192-214), given with
+    the model and as the template's field ``current`` per call."""
+    from oracle import OracleRHS
+    d = hb.Discretization(box(3, 0.04, 9), order=4)
+    rng = np.random.default_rng(9)
+    J = np.sin(d.nodes.T) + 0.1 * rng.uniform(-1, 1, (3, len(d)))
+    op = hb.MaxwellOperator(1.5, 0.8, flux_type=1, current=J)
+    q = _fields(d, 6, 10)
+    fp32 = precision in ("fp32", "fp32-simt")
+    qs = q.astype(np.float32).astype(np.float64) if fp32 else q
+    ref = OracleRHS(d, op.op_template())(qs)
+    tol = {"fp64": 1e-12, "fp32": 1e-5, "fp32-simt": 1e-5, "fp16x3": 1e-6, "bf16x3": 1e-5}
+    rhs = op.bind(d.__class__(d.mesh, order=4, precision=precision))
+    got = rhs(0.0, qs).double().cpu().numpy()
+    rhs.compiled.check()
+    assert rel_l2(got, ref) <= tol[precision]
+    # the same template with the current passed per call
+    comp = d.__class__(d.mesh, order=4, precision=precision).compile(op.op_template())
+    J2 = 2 * J
+    ref2 = OracleRHS(d, hb.MaxwellOperator(1.5, 0.8, flux_type=1, current=J2).op_template())(qs)
+    got2 = comp(w=qs, current=J2).double().cpu().numpy()
+    comp.check()
+    assert rel_l2(got2, ref2) <= tol[precision]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32-simt"])
+@pytest.mark.parametrize("kind", ["tm", "te"])
+def test_maxwell_2d(cuda_device, kind, precision):
+    """2D TM (Ez, Hx, Hy) and TE (Ex, Ey, Hz) Maxwell (em.py:485-515): PEC, PMC
+    and absorbing walls, a numeric interior and an "lf" boundary flux, and a
+    source current, against the oracle."""
+    from oracle import OracleRHS
+    m = hb.make_regular_rect_mesh((-1, -1), (1, 1), (9, 9), jitter=0.03, seed=11,
+                                  boundary_tagger=_lr_tagger(["pmc", "abs", "pec"]))
+    d = hb.Discretization(m, order=5, precision=precision)
+    cls = hb.TMMaxwellOperator if kind == "tm" else hb.TEMaxwellOperator
+    ne = 1 if kind == "tm" else 2
+    J = np.cos(d.nodes.T[:ne] * 2.0)
+    op = cls(1.2, 0.9, flux_type=0.7, bdry_flux_type="lf", pec_tag="pec", pmc_tag="pmc",
+             absorb_tag="abs", current=J)
+    q = _fields(d, 3, 12)
+    fp32 = precision != "fp64"
+    qs = q.astype(np.float32).astype(np.float64) if fp32 else q
+    ref = OracleRHS(d, op.op_template())(qs)
+    rhs = op.bind(d)
+    got = rhs(0.0, qs).double().cpu().numpy()
+    rhs.compiled.check()
+    assert rel_l2(got, ref) <= (1e-12 if precision == "fp64" else 1e-5)
+
+
+@pytest.mark.parametrize("kind", ["tm", "te"])
+def test_maxwell_2d_lsrk_steps(cuda_device, kind):
+    """20 fused LSRK4 steps of a PEC cavity mode against the oracle's."""
+    from oracle import OracleRHS
+    d = hb.Discretization(rect(8, False, 0.02, 13), order=4)
+    cls = hb.TMMaxwellOperator if kind == "tm" else hb.TEMaxwellOperator
+    op = cls(1.0, 1.0, flux_type=1)
+    x, y = d.nodes.T
+    q = np.stack([np.sin(np.pi * (x + 1) / 2) * np.sin(np.pi * (y + 1) / 2),
+                  0 * x, 0 * x]) if kind == "tm" else _fields(d, 3, 14)
+    rhs = op.bind(d)
+    dt = 0.5 * op.estimate_timestep(d)
+    orc = OracleRHS(d, op.op_template())
+    yd = d.to_device(q).reshape(3, -1)
+    yo, res, t = q.copy(), np.zeros_like(q), 0.0
+    st = hb.LSRK4TimeStepper()
+    for _ in range(20):
+        yd = st(yd, t, dt, rhs)
+        yo, res = orc.lsrk4_step(yo, t, dt, res)
+        t += dt
+    rhs.compiled.check()
+    assert rel_l2(yd.cpu().numpy(), yo) <= 1e-11
+
+
 @pytest.mark.parametrize("dim", [2, 3])
 def test_varwave(cuda_device, dim):
     m = rect(8, False, 0.02, 4) if dim == 2 else box(2, 0.03, 4)

@@ -79,11 +79,16 @@ MODELS = [
     lambda: hb.StrongWaveOperator(1.0, 2, flux_type="central", dirichlet_tag="dir",
                                   neumann_tag="neu", radiation_tag="rad", source_f=0.25),
     lambda: hb.StrongWaveOperator(1.3, 3),
+    lambda: hb.StrongWaveOperator(0.9, 2, dirichlet_tag="dir", dirichlet_bc_f=1,
+                                  neumann_tag="neu"),
     lambda: hb.VariableVelocityStrongWaveOperator(np.ones(3), 2, time_sign=-1,
                                                   radiation_tag="rad", dirichlet_tag="dir"),
     lambda: hb.MaxwellOperator(1.0, 1.0, flux_type=1),
     lambda: hb.MaxwellOperator(2.0, 0.5, flux_type=0.5, bdry_flux_type="lf",
                                pec_tag="pec", pmc_tag="pmc", absorb_tag="abs"),
+    lambda: hb.TMMaxwellOperator(1.0, 1.0, flux_type=1),
+    lambda: hb.TEMaxwellOperator(1.5, 0.5, flux_type=0.25, bdry_flux_type="lf",
+                                 pec_tag="pec", absorb_tag="abs"),
 ]
 
 
@@ -102,8 +107,8 @@ def _executor_vs_oracle(d, template, desc, env, q, bc_in=None, c_field=None, sou
     return rel_l2(got, ref)
 
 
-CASES = ["adv_periodic", "adv_inflow", "wave_mixed", "wave3d", "varwave", "maxwell_pec",
-         "maxwell_mixed"]
+CASES = ["adv_periodic", "adv_inflow", "wave_mixed", "wave_dirichlet_data", "wave3d",
+         "varwave", "maxwell_pec", "maxwell_mixed"]
 
 
 @pytest.mark.parametrize("case", CASES)
@@ -122,6 +127,11 @@ def test_model_templates_match_oracle(case):
         d = hb.Discretization(rect(5, tagger=_tagger_lr(["neu", "rad", "dir"])), order=3)
         op = hb.StrongWaveOperator(-0.8, 2, dirichlet_tag="dir", neumann_tag="neu",
                                    radiation_tag="rad", source_f=0.3)
+    elif case == "wave_dirichlet_data":
+        d = hb.Discretization(rect(5, tagger=_tagger_lr(["neu", "dir", "dir"])), order=3)
+        op = hb.StrongWaveOperator(0.9, 2, dirichlet_tag="dir", dirichlet_bc_f=1,
+                                   neumann_tag="neu")
+        bc = np.cos(2 * d.get_boundary("dir").nodes[:, 1])
     elif case == "wave3d":
         d = hb.Discretization(box(2), order=2)
         op = hb.StrongWaveOperator(1.0, 3, flux_type="central")
@@ -148,6 +158,8 @@ def test_model_templates_match_oracle(case):
         env = {"u": q[0], "bc_in": bc if bc is not None else 0.0}
     else:
         env = {"w": q}
+        if bc is not None:
+            env["dir_bc_u"] = bc
     if c is not None:
         env["c"] = c
     if src is not None:
@@ -450,3 +462,65 @@ def test_over_integration_with_a_coefficient_field_is_refused():
                                    - flux(u))
     with pytest.raises(NotImplementedError):
         lower(tpl, 2)
+
+
+def test_wave_dirichlet_data_lowers_to_given_condition():
+    """Inhomogeneous Dirichlet data (wave.py:133-142) lowers onto the wave
+    kernel with a given-data condition on the Dirichlet tag, and the bound
+    RHS takes the data as dir_bc_u (the reference's field name)."""
+    op = hb.StrongWaveOperator(1.0, 2, dirichlet_tag="dir", dirichlet_bc_f=1,
+                               neumann_tag="neu")
+    desc = lower(op.op_template(), 2)
+    assert desc.model == MODEL_WAVE
+    assert ("dir", BC_GIVEN) in desc.bcs and ("neu", BC_NEUMANN) in desc.bcs
+    assert desc.fields["given"] == "dir_bc_u"
+    # homogeneous data: the plain Dirichlet condition
+    op0 = hb.StrongWaveOperator(1.0, 2, dirichlet_tag="dir", neumann_tag="neu")
+    assert ("dir", BC_DIRICHLET) in lower(op0.op_template(), 2).bcs
+
+
+@pytest.mark.parametrize("kind", ["field", "numbers"])
+def test_maxwell_current_lowers_and_matches_oracle(kind):
+    """Maxwell with a source current J (em.py:192-214: eps dE/dt = curl H - J
+    + flux): the template lowers onto the Maxwell kernel with per-E-component
+    sources -J/eps, and the executed template equals the oracle."""
+    from oracle import OracleRHS
+    from optemplate_exec import TemplateExecutor
+    d = hb.Discretization(box(2), order=2)
+    rng = np.random.default_rng(11)
+    J = rng.standard_normal((3, len(d))) if kind == "field" else [0.5, 0.0, -1.0]
+    op = hb.MaxwellOperator(2.0, 0.5, flux_type=1, current=J)
+    desc = lower(op.op_template(), 3)
+    assert desc.model == MODEL_MAXWELL
+    outs = sorted(o for o, *_ in desc.fields["sources"])
+    assert outs == ([0, 1, 2] if kind == "field" else [0, 2])
+    q = _fields(d, 6, 4)
+    env = {"w": q}
+    if kind == "field":
+        env["current"] = J
+    got = TemplateExecutor(d)(op.op_template(), **env)
+    ref = OracleRHS(d, op.op_template())(q)
+    assert rel_l2(got, ref) <= 1e-12
+
+
+@pytest.mark.parametrize("kind", ["tm", "te"])
+def test_maxwell_2d_templates_lower_and_match_oracle(kind):
+    """TM / TE Maxwell templates (em.py:485-515, subset cross products) lower
+    onto their kernel models, not onto each other, and the executed templates
+    equal the oracle with mixed walls and a source current."""
+    from hedge_b200.models import MODEL_MAXWELL_TE, MODEL_MAXWELL_TM
+    from oracle import OracleRHS
+    from optemplate_exec import TemplateExecutor
+    d = hb.Discretization(rect(5, tagger=_tagger_lr(["pmc", "abs", "pec"])), order=3)
+    cls = hb.TMMaxwellOperator if kind == "tm" else hb.TEMaxwellOperator
+    ne = 1 if kind == "tm" else 2
+    J = np.sin(d.nodes.T[:ne])
+    op = cls(0.8, 1.7, flux_type=0.6, bdry_flux_type=1, pec_tag="pec", pmc_tag="pmc",
+             absorb_tag="abs", current=J)
+    desc = lower(op.op_template(), 2)
+    assert desc.model == (MODEL_MAXWELL_TM if kind == "tm" else MODEL_MAXWELL_TE)
+    assert abs(desc.params["eps"] - 0.8) < 1e-12 and abs(desc.params["mu"] - 1.7) < 1e-12
+    q = _fields(d, 3, 5)
+    got = TemplateExecutor(d)(op.op_template(), w=q, current=J)
+    ref = OracleRHS(d, op.op_template())(q)
+    assert rel_l2(got, ref) <= 1e-12
