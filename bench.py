@@ -50,9 +50,11 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--precision", default="fp16x3",
                    choices=["fp64", "fp32", "fp32-simt", "bf16x3", "fp16x3"])
-    p.add_argument("--workload", default="maxwell", choices=["maxwell", "wave7"],
+    p.add_argument("--workload", default="maxwell", choices=["maxwell", "wave7", "varadv2d"],
                    help="maxwell: 3D Maxwell N=4 cavity (default); wave7: 3D acoustic "
-                        "wave N=7 Gaussian pulse (the high-order precision workload)")
+                        "wave N=7 Gaussian pulse (the high-order precision workload); "
+                        "varadv2d: 2D variable-coefficient advection N=5 with "
+                        "quadrature (the over-integration kernel; one GPU, FP64)")
     p.add_argument("--layout", default="partitioned", choices=["partitioned", "replicas"],
                    help="N > 1: partitioned = one mesh of N x the per-GPU size, "
                         "element-partitioned with a face-trace exchange every stage "
@@ -75,6 +77,10 @@ WORKLOADS = {
     "wave7": {"order": 7, "fields": 4,
               "metric": "DG RHS DOF-updates/s (3D acoustic wave N=7, LSRK4)",
               "label": "wave3d_pulse_K%d_N%d"},
+    "varadv2d": {"order": 5, "fields": 1, "n": 400,
+                 "metric": "DG RHS DOF-updates/s (2D variable-coefficient advection N=5, "
+                           "quadrature degree 15, LSRK4)",
+                 "label": "varadv2d_vortex_K%d_N%d"},
 }
 
 
@@ -571,11 +577,166 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def varadv_flops_per_element(discr, nq, nqf):
+    """FP64 operations of the quadrature kernel per element (2 per FMA):
+    u and v at the volume points, the chain rule and product with u, the
+    projection, both traces at the face points and the lift (the flux
+    arithmetic itself, ~10 per face point, is left out)."""
+    d, np_, nfp, nf = discr.dimensions, discr.Np, discr.Nfp, discr.Nfaces
+    nv = 1 + d
+    fma = (nv * np_ * nq + nq * d * (d + 1) + d * nq * np_
+           + nf * nqf * nfp * 2 * nv + nf * nqf * np_)
+    return 2 * fma
+
+
+def fp64_peak_tflops(dev):
+    """cuBLAS DGEMM 8192^3 (the FP64 pipes' throughput), best of 5."""
+    import torch
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    c = a @ b
+    best = None
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c = a @ b
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del a, b, c
+    return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def run_varadv(args):
+    """The quadrature kernel on the 2D variable-coefficient advection
+    workload (hedge_b200.workloads.varadv_problem), one GPU, FP64.  A step
+    is one LSRK4 step (5 fused RHS + stage launches).  The kernel is bound by
+    FP64 arithmetic (about 800 operations per DOF-update at N = 5), so the
+    roofline is against cuBLAS DGEMM measured in the same run; the HBM
+    fraction of the algorithmic bytes is reported beside it."""
+    import torch
+    import hedge_b200 as hb
+    from hedge_b200 import workloads
+    if args.gpus != 1:
+        raise SystemExit("varadv2d: one GPU")
+    dev = torch.device("cuda", torch.cuda.current_device())
+    n = args.n if args.n != 20 else WORKLOADS["varadv2d"]["n"]
+    d, op, u0 = workloads.varadv_problem(n, args.order, device=dev)
+    rhs = op.bind(d)
+    comp = rhs.compiled
+    dt = 0.5 * op.estimate_timestep(d, t=0.0)
+    stepper = hb.LSRK4TimeStepper()
+    y = d.to_device(u0).reshape(1, -1)
+    t = 0.0
+    for _ in range(args.warmup):
+        y = stepper(y, t, dt, rhs)
+        t += dt
+    comp.check()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clk:
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            y = stepper(y, t, dt, rhs)
+            t += dt
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = ev0.elapsed_time(ev1)
+    comp.check()
+    dofs = d.K * d.Np
+    value = dofs * 5 * args.steps / (ms * 1e-3)
+    launches = 5 * args.steps
+    launch_s = ms * 1e-3 / launches
+    vi, vp, fi, fl = d.quadrature_matrices("quad", 3 * d.order - 1)
+    nq, nqf = vi.shape[0], fi.shape[1]
+    flops = varadv_flops_per_element(d, nq, nqf) * d.K
+    g_el = 8 * (4 + 3 * 3) + 3 * 6
+    bpd = 4 * 8 + 2 * 8 + g_el / d.Np     # q in/out, res r/w, velocity; geometry
+    peak64 = fp64_peak_tflops(dev)
+    hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0)
+    achieved = flops / launch_s / 1e12
+    gbs = bpd * dofs / launch_s / 1e9
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                "frac": achieved / peak64,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                "flops_per_element": flops / d.K, "volume_points": nq, "face_points": nqf,
+                "hbm": {"achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                        "algorithmic_bytes_per_dof_update": bpd},
+                "traffic": load_traffic("rhs_quad_varadv2d_N%d" % d.order),
+                "kernel": "rhs_quad_kernel<2, double>"}
+    # end to end: the state copied in from pinned host memory and out again
+    # around every step (same stream, not overlapped)
+    host_in = torch.from_numpy(np.ascontiguousarray(u0.reshape(1, -1))).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    dev_in = torch.empty(host_in.shape, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        dev_in.copy_(host_in, non_blocking=True)
+        host_out.copy_(stepper(dev_in, 0.0, dt, rhs), non_blocking=True)
+    torch.cuda.synchronize(dev)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        dev_in.copy_(host_in, non_blocking=True)
+        host_out.copy_(stepper(dev_in, 0.0, dt, rhs), non_blocking=True)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    e_ms = ev0.elapsed_time(ev1)
+    nbytes = host_in.numel() * 8
+    e2e = {"value": dofs * 5 * args.steps / (e_ms * 1e-3), "unit": "DOF-updates/s",
+           "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes}
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = varadv_cpu_baseline(args.order)
+    line = {"metric": WORKLOADS["varadv2d"]["metric"], "value": value,
+            "unit": "DOF-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOADS["varadv2d"]["label"] % (d.K, d.order),
+                       "K": d.K, "order": d.order, "Np": d.Np, "quad_degree": 3 * d.order,
+                       "l2": "working set of a stage (q_in, q_out, res, v) 5 x %.1f MB > 126 "
+                             "MB L2, no flush" % (dofs * 8 / 1e6)},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clk.summary(),
+            "launch_config": comp.launch_info()}
+    print(json.dumps(line), flush=True)
+
+
+def varadv_cpu_baseline(order):
+    """The template executor (oracle/optemplate_exec.py: the reference's
+    quadrature integrals evaluated with numpy) on a bounded sample: one RHS
+    of the same operator on a 24 x 24 mesh, best of 2, one thread of numpy."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from optemplate_exec import TemplateExecutor
+    from hedge_b200 import workloads
+    from hedge_b200.mesh import TAG_ALL
+    d, op, u0 = workloads.varadv_problem(24, order)
+    ex = TemplateExecutor(d)
+    tpl = op.op_template()
+    env = {"u": u0, "v": op.advec_v.f(d.nodes),
+           "bc_u": op.bc_u_f.boundary_interpolant(0.0, d, TAG_ALL)}
+    ex(tpl, **env)
+    best = None
+    for _ in range(2):
+        t0 = time.perf_counter()
+        ex(tpl, **env)
+        el = time.perf_counter() - t0
+        best = el if best is None else min(best, el)
+    return {"value": d.K * d.Np / best, "unit": "DOF-updates/s", "cores": 1, "kind": "port",
+            "sample": "one RHS of the operator on a K=%d mesh (24 x 24 squares), template "
+                      "executor (numpy), best of 2" % d.K}
+
+
 def main():
     args = parse()
     if args.order is None:
         args.order = WORKLOADS[args.workload]["order"]
-    if args.impl == "reference":
+    if args.workload == "varadv2d":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "value": varadv_cpu_baseline(args.order)}))
+            return
+        run_varadv(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

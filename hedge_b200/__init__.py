@@ -11,7 +11,7 @@ from .refelem import TriangleElement, TetrahedronElement, make_element
 from .models import (StrongAdvectionOperator, WeakAdvectionOperator, StrongWaveOperator,
                      VariableVelocityStrongWaveOperator, MaxwellOperator,
                      TMMaxwellOperator, TEMaxwellOperator,
-                     make_tdep_constant, TimeConstantGivenFunction,
+                     VariableCoefficientAdvectionOperator, make_tdep_constant, TimeConstantGivenFunction,
                      TimeDependentGivenFunction)
 from .discretization import Discretization, CompiledOperator, BoundRHS
 from .timestep import GraphedLSRK4, LSRK4TimeStepper, RK4TimeStepper
@@ -23,7 +23,7 @@ __all__ = [
     "check_bc_coverage", "TriangleElement", "TetrahedronElement", "make_element",
     "StrongAdvectionOperator", "WeakAdvectionOperator", "StrongWaveOperator",
     "VariableVelocityStrongWaveOperator", "MaxwellOperator", "TMMaxwellOperator",
-    "TEMaxwellOperator", "make_tdep_constant",
+    "TEMaxwellOperator", "VariableCoefficientAdvectionOperator", "make_tdep_constant",
     "TimeConstantGivenFunction", "TimeDependentGivenFunction", "Discretization", "CompiledOperator", "BoundRHS",
     "LSRK4TimeStepper", "RK4TimeStepper", "GraphedLSRK4", "GradientOperator", "DivergenceOperator",
     "VtkVisualizer", "LegacyVtkVisualizer",

@@ -42,6 +42,12 @@ class hb_batch_member(C.Structure):
                 ("res", C.c_void_p), ("dt", C.c_double), ("tile_elems", C.c_int32)]
 
 
+class hb_quad_desc(C.Structure):
+    _fields_ = [("nq", C.c_int32), ("nqf", C.c_int32),
+                ("vol_interp", C.c_void_p), ("vol_project", C.c_void_p),
+                ("face_interp", C.c_void_p), ("face_lift", C.c_void_p)]
+
+
 class hb_op_desc(C.Structure):
     _fields_ = [("model", C.c_int32), ("num_fields", C.c_int32),
                 ("precision", C.c_int32), ("flux_type", C.c_int32),
@@ -50,7 +56,8 @@ class hb_op_desc(C.Structure):
                 ("mu", C.c_double), ("alpha", C.c_double), ("bdry_alpha", C.c_double),
                 ("time_sign", C.c_double),
                 ("conn", C.c_void_p), ("num_given_bdry_nodes", C.c_int64),
-                ("num_halo_faces", C.c_int64)]
+                ("num_halo_faces", C.c_int64),
+                ("quadrature", C.POINTER(hb_quad_desc))]
 
 
 EXPORTED = [

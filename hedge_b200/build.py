@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhedge_b200.so")
 SOURCES = ["api.cu", "rhs_simt.cu", "rhs_split.cu", "norm.cu", "adjoint.cu", "ensemble.cu",
-           "waitcheck.cu"]
+           "waitcheck.cu", "rhs_quad.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

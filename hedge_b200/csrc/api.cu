@@ -88,6 +88,46 @@ hb_status launch_split(Op* op, int mode, double ra, double rb, double dt,
 void free_split(Op* op);
 hb_status launch_wait_selftest(int* err, uint64_t limit_ns, cudaStream_t s);
 
+// The quadrature matrices in the kernel's layouts (each transposed so that
+// consecutive threads read consecutive entries): It [np][nq],
+// Bt [dim][nq][np], Ft [nf][nfp][nqf], Lt [nf*nqf][np], back to back; FP32
+// copies for FP32 operators; the element-maximum buffer for the LF flux.
+static hb_status upload_quadrature(Op* op, const hb_quad_desc* qd) {
+  const Discr* d = op->d;
+  const int np = d->np, nfp = d->nfp, nf = d->nfaces, dim = d->dim;
+  const int nq = qd->nq, nqf = qd->nqf;
+  const size_t nI = (size_t)np * nq, nB = (size_t)dim * nq * np, nF = (size_t)nf * nfp * nqf;
+  const size_t nL = (size_t)nf * nqf * np;
+  std::vector<double> h(nI + nB + nF + nL);
+  for (int q = 0; q < nq; ++q)
+    for (int j = 0; j < np; ++j) h[(size_t)j * nq + q] = qd->vol_interp[(size_t)q * np + j];
+  for (int r = 0; r < dim; ++r)
+    for (int i = 0; i < np; ++i)
+      for (int q = 0; q < nq; ++q)
+        h[nI + ((size_t)r * nq + q) * np + i] = qd->vol_project[((size_t)r * np + i) * nq + q];
+  for (int f = 0; f < nf; ++f)
+    for (int q = 0; q < nqf; ++q)
+      for (int k = 0; k < nfp; ++k)
+        h[nI + nB + ((size_t)f * nfp + k) * nqf + q] =
+            qd->face_interp[((size_t)f * nqf + q) * nfp + k];
+  for (int i = 0; i < np; ++i)
+    for (int p = 0; p < nf * nqf; ++p)
+      h[nI + nB + nF + (size_t)p * np + i] = qd->face_lift[(size_t)i * nf * nqf + p];
+  for (double x : h)
+    if (!std::isfinite(x)) return fail(HB_ERR_INVALID_ARGUMENT, "non-finite quadrature matrix");
+  op->nq = nq;
+  op->nqf = nqf;
+  hb_status st;
+  if ((st = upload(&op->quad64, h.data(), h.size()))) return st;
+  if (op->precision == HB_PREC_FP32) {
+    std::vector<float> h32(h.begin(), h.end());
+    if ((st = upload(&op->quad32, h32.data(), h32.size()))) return st;
+  }
+  if (cudaMalloc(&op->elmax, sizeof(double) * d->K) != cudaSuccess)
+    return fail(HB_ERR_CUDA, "cannot allocate the element maxima");
+  return HB_OK;
+}
+
 }  // namespace hb
 
 using namespace hb;
@@ -181,7 +221,25 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
     case HB_MODEL_MAXWELL_TM: case HB_MODEL_MAXWELL_TE:
       if (d->dim != 2) return fail(HB_ERR_UNSUPPORTED, "TM / TE Maxwell needs a 2D mesh");
       F = 3; break;
+    case HB_MODEL_VARADV: F = 1; break;
     default: return fail(HB_ERR_INVALID_ARGUMENT, "unknown model id");
+  }
+  const hb_quad_desc* qd = desc->quadrature;
+  if (model == HB_MODEL_VARADV) {
+    if (!qd) return fail(HB_ERR_INVALID_ARGUMENT, "variable-coefficient advection needs the "
+                                                  "quadrature grid (hb_op_desc.quadrature)");
+    if (qd->nq < 1 || qd->nqf < 1 || qd->nq > 4096 || qd->nqf > 1024 || !qd->vol_interp ||
+        !qd->vol_project || !qd->face_interp || !qd->face_lift)
+      return fail(HB_ERR_INVALID_ARGUMENT, "bad quadrature descriptor");
+    if (desc->flux_type < 0 || desc->flux_type > 2)
+      return fail(HB_ERR_INVALID_ARGUMENT, "flux type: 0 central, 1 upwind, 2 LF");
+    if (desc->num_halo_faces != 0)
+      return fail(HB_ERR_UNSUPPORTED, "quadrature operator: no halo faces");
+    if (desc->precision != HB_PREC_FP64 && desc->precision != HB_PREC_FP32 &&
+        desc->precision != HB_PREC_FP32_SIMT)
+      return fail(HB_ERR_UNSUPPORTED, "quadrature operator: FP64 or FP32 only");
+  } else if (qd) {
+    return fail(HB_ERR_INVALID_ARGUMENT, "quadrature grid given for a model without one");
   }
   if (desc->num_fields != F)
     return fail(HB_ERR_INVALID_ARGUMENT, "num_fields does not match the model");
@@ -232,6 +290,7 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
   hb_status st;
   auto bail = [&](hb_status s) {
     cudaFree(op->conn); cudaFree(op->err_flag);
+    cudaFree(op->quad64); cudaFree(op->quad32); cudaFree(op->elmax);
     free_split(op);
     delete op;
     return s;
@@ -242,7 +301,10 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
       cudaMemset(op->err_flag, 0, sizeof(int)) != cudaSuccess)
     return bail(fail(HB_ERR_CUDA, "cannot allocate the device error flag"));
   if (op->precision == HB_PREC_FP32 && (st = ensure_fp32(d))) return bail(st);
-  if (op->precision == HB_PREC_BF16X3 || op->precision == HB_PREC_FP16X3) {
+  if (model == HB_MODEL_VARADV) {
+    st = upload_quadrature(op, qd);
+    if (!st) st = prepare_quad(op);
+  } else if (op->precision == HB_PREC_BF16X3 || op->precision == HB_PREC_FP16X3) {
     st = prepare_split(op);
     op->split = 1;
   } else if (op->precision == HB_PREC_FP32 && desc->precision != HB_PREC_FP32_SIMT) {
@@ -268,6 +330,7 @@ hb_status hb_op_destroy(hb_op* handle) {
   DeviceGuard g(op->d->device);
   cudaFree(op->conn);
   cudaFree(op->err_flag);
+  cudaFree(op->quad64); cudaFree(op->quad32); cudaFree(op->elmax);
   free_split(op);
   delete op;
   return HB_OK;
@@ -281,6 +344,8 @@ static hb_status check_inputs(Op* op, const void* q_in, const void* q_out,
     return fail(HB_ERR_INVALID_ARGUMENT, "halo faces but no halo buffer (hb_op_set_halo)");
   if (op->model == HB_MODEL_VARWAVE && !coeff)
     return fail(HB_ERR_INVALID_ARGUMENT, "variable-velocity wave needs the c field");
+  if (op->model == HB_MODEL_VARADV && !coeff)
+    return fail(HB_ERR_INVALID_ARGUMENT, "variable-coefficient advection needs the velocity");
   return HB_OK;
 }
 
@@ -290,6 +355,8 @@ static hb_status run(Op* op, int mode, double a, double b, double dt, const void
   DeviceGuard g(op->d->device);
   if (!g.ok) return fail(HB_ERR_CUDA, "cannot select the CUDA device");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (op->model == HB_MODEL_VARADV)
+    return launch_quad(op, mode, a, b, dt, q_in, q_out, res, coeff, bdry, s);
   if (op->split)
     return launch_split(op, mode, a, b, dt, q_in, q_out, res, coeff, bdry, source, s);
   return launch_simt(op, mode, a, b, dt, q_in, q_out, res, coeff, bdry, source, s);

@@ -97,6 +97,13 @@ struct Op {
   int blocks_per_sm = 0;
   // split-precision operator planes (BF16X3)
   void* split_ops = nullptr;
+  // quadrature operator (variable-coefficient advection): point counts, the
+  // four matrices (FP64 and, for FP32 operators, FP32 copies) and the
+  // element maxima of |v|^2 the LF flux reads
+  int nq = 0, nqf = 0;
+  double* quad64 = nullptr;
+  float* quad32 = nullptr;
+  double* elmax = nullptr;
 };
 
 hb_status check_device_flag(Op* op, cudaStream_t s);
@@ -123,5 +130,11 @@ hb_status launch_simt(Op* op, int mode, double a, double b, double dt,
                       const double* coeff, const double* bdry,
                       const double* source, cudaStream_t s);
 hb_status prepare_simt(Op* op);
+
+// quadrature kernel (rhs_quad.cu); vel = the velocity field [dim][K*Np]
+hb_status prepare_quad(Op* op);
+hb_status launch_quad(Op* op, int mode, double ra, double rb, double dt, const void* q_in,
+                      void* q_out, void* res, const double* vel, const double* bdry,
+                      cudaStream_t s);
 
 }  // namespace hb

@@ -24,8 +24,9 @@ from .mesh import Mesh, TAG_ALL, TAG_NONE, check_bc_coverage
 from .lowering import as_descriptor
 from .optemplate import Expr
 from .models import (BC_GIVEN, BC_NONE, MODEL_MAXWELL, MODEL_MAXWELL_TE, MODEL_MAXWELL_TM,
-                     MODEL_VARWAVE, MODEL_WAVE,
+                     MODEL_VARADV, MODEL_VARWAVE, MODEL_WAVE,
                      MODEL_ADVECTION, OpTemplate)
+from .quadrature import ElementQuadrature
 from .refelem import make_element
 
 PRECISIONS = {"plain": None, "fp64": _native.PREC_FP64, "fp32": _native.PREC_FP32,
@@ -60,8 +61,7 @@ class Discretization:
             raise TypeError("mesh must be of type hedge_b200.mesh.Mesh")
         if (order is None) == (local_discretization is None):
             raise ValueError("must supply exactly one of local_discretization and order")
-        if quad_min_degrees:
-            raise NotImplementedError("quadrature (over-integration) is not on this path")
+        self.quad_min_degrees = dict(quad_min_degrees or {})
         self.mesh = mesh
         self.ldis = local_discretization or make_element(mesh.dimensions, order)
         self.dimensions = mesh.dimensions
@@ -196,6 +196,52 @@ class Discretization:
         if err >= 1e-13:
             raise AssertionError("face node mismatch %g" % err)
         return err
+
+    # -- quadrature grids (discretization/__init__.py:779-889) -------------------
+    def get_quadrature_info(self, quad_tag, volume_rule="reference"):
+        """The element quadrature of ``quad_tag``'s minimum degree
+        (:class:`hedge_b200.quadrature.ElementQuadrature`); RuntimeError when
+        the discretization has no degree for the tag, as the reference."""
+        try:
+            degree = self.quad_min_degrees[quad_tag]
+        except KeyError:
+            raise RuntimeError("minimum degree for quadrature tag '%s' is undefined"
+                               % quad_tag)
+        cache = self.__dict__.setdefault("_quad_cache", {})
+        key = (quad_tag, volume_rule)
+        if key not in cache:
+            cache[key] = ElementQuadrature(self.ldis, degree, volume_rule)
+        return cache[key]
+
+    def quadrature_matrices(self, quad_tag, integrand_degree):
+        """(vol_interp, vol_project, face_interp, face_lift) of the
+        quadrature kernel for an integrand of ``integrand_degree`` in the
+        volume: the reference's rules, except that the volume rule is the
+        collapsed Gauss-Jacobi one when both are exact for the integrand and
+        it has fewer points.  Without a degree for the tag, the nodal
+        operators (the reference's fallback to nodal evaluation,
+        mappers/__init__.py:937-958): identity interpolation,
+        M^-1 D_r^T M, the face nodes and LIFT."""
+        ld = self.ldis
+        if self.quad_min_degrees.get(quad_tag) is None:
+            import warnings
+            warnings.warn("No minimum degree for quadrature tag '%s' specified--"
+                          "falling back to nodal evaluation" % quad_tag)
+            np_, nfp, nf = self.Np, self.Nfp, self.Nfaces
+            M, Minv = ld.mass_matrix, ld.inverse_mass_matrix
+            proj = np.stack([Minv @ D.T @ M for D in ld.differentiation_matrices])
+            fint = np.broadcast_to(np.eye(nfp), (nf, nfp, nfp))
+            return (np.eye(np_), proj, np.ascontiguousarray(fint),
+                    np.ascontiguousarray(ld.lifting_matrix))
+        q = vol = self.get_quadrature_info(quad_tag)
+        if q.exact_to_degree >= integrand_degree:
+            cache = self.__dict__.setdefault("_quad_cache", {})
+            key = ("exact-volume", integrand_degree)
+            if key not in cache:
+                cache[key] = ElementQuadrature(self.ldis, integrand_degree, "exact")
+            if cache[key].nq < q.nq:
+                vol = cache[key]
+        return vol.vol_interp, vol.vol_project, q.face_interp, q.face_lift
 
     # -- time step factors (local.py:531-540, 1052-1056, 1378-1386) -----------
     def dt_non_geometric_factor(self):
@@ -355,8 +401,9 @@ def build_face_table(discr, ot):
     return conn, n_given, given_tag
 
 
-def op_descriptor(ot, prec, conn, n_given, num_halo_faces=0):
-    """hb_op_desc of a model operator over a face table."""
+def op_descriptor(ot, prec, conn, n_given, num_halo_faces=0, quadrature=None):
+    """hb_op_desc of a model operator over a face table (``quadrature``: an
+    hb_quad_desc for the quadrature models)."""
     p = ot.params
     v = np.zeros(3)
     if "v" in p:
@@ -365,7 +412,19 @@ def op_descriptor(ot, prec, conn, n_given, num_halo_faces=0):
         ot.model, ot.n_fields, prec, ot.flux_type, p.get("bdry_flux_type", ot.flux_type),
         (C.c_double * 3)(*v), p.get("c", 0.0), p.get("eps", 1.0), p.get("mu", 1.0),
         p.get("alpha", 1.0), p.get("bdry_alpha", p.get("alpha", 1.0)),
-        p.get("time_sign", 1.0), conn.ctypes.data, n_given, int(num_halo_faces))
+        p.get("time_sign", 1.0), conn.ctypes.data, n_given, int(num_halo_faces),
+        C.pointer(quadrature) if quadrature is not None else None)
+
+
+def quadrature_descriptor(discr, ot):
+    """(hb_quad_desc, host arrays it points to) of a quadrature operator:
+    the integrand of the variable-coefficient advection volume term,
+    v u d(phi)/dx, has degree 3N - 1."""
+    mats = discr.quadrature_matrices(ot.params.get("quad_tag", "quad"), 3 * discr.order - 1)
+    keep = [np.ascontiguousarray(m, dtype=np.float64) for m in mats]
+    q = _native.hb_quad_desc(keep[0].shape[0], keep[2].shape[1], keep[0].ctypes.data,
+                             keep[1].ctypes.data, keep[2].ctypes.data, keep[3].ctypes.data)
+    return q, keep
 
 
 class CompiledOperator:
@@ -388,7 +447,12 @@ class CompiledOperator:
         self.prec_code = prec
         model = ot.operator
         p = ot.params
-        desc = op_descriptor(ot, prec, self.conn, self.n_given)
+        quad = None
+        if ot.model == MODEL_VARADV:
+            if precision not in ("fp64", "fp32", "fp32-simt"):
+                raise NotImplementedError("the quadrature operator runs in fp64 or fp32")
+            quad, self._quad_keep = quadrature_descriptor(discr, ot)
+        desc = op_descriptor(ot, prec, self.conn, self.n_given, quadrature=quad)
         lib = _native.load()
         h = C.c_void_p()
         _native.check(lib.hb_op_create(discr._native_handle(), C.byref(desc), C.byref(h)))
@@ -481,9 +545,18 @@ class CompiledOperator:
             else torch.float64
 
     def set_coefficient(self, c):
-        """Variable-velocity wave speed: a number or a volume vector."""
+        """Variable-velocity wave speed: a number or a volume vector; for the
+        quadrature advection the velocity [d, K*Np], kept for calls (and
+        recorded stages) that pass none."""
         torch = _torch()
         d = self.discr
+        if self.ot.model == MODEL_VARADV:
+            t = d.to_device(np.asarray(c) if not isinstance(c, torch.Tensor) else c,
+                            torch.float64).reshape(-1).contiguous()
+            if t.numel() != d.dimensions * len(d):
+                raise ValueError("the velocity must be [%d, %d]" % (d.dimensions, len(d)))
+            self._coeff = t
+            return
         if np.isscalar(c):
             t = torch.full((len(d),), float(c), dtype=torch.float64, device=d.device)
         else:
@@ -554,11 +627,13 @@ class CompiledOperator:
 
     # -- evaluation -------------------------------------------------------------
     def _field_ptrs(self, coeff, source):
-        """Device pointers of the c field and the source: the per-call
-        tensors when given (FP64 [K*Np] on the device), else the operator's."""
+        """Device pointers of the c field (the velocity [d * K*Np] of the
+        quadrature advection) and the source: the per-call tensors when given
+        (FP64 on the device), else the operator's."""
         c = self._coeff if coeff is None else coeff
         s = self._source if source is None else source
-        for t, rows in ((coeff, 1), (source, self._n_e or 1)):
+        crows = self.discr.dimensions if self.ot.model == MODEL_VARADV else 1
+        for t, rows in ((coeff, crows), (source, self._n_e or 1)):
             if t is not None:
                 if t.dtype != _torch().float64 or not t.is_contiguous() or \
                         t.numel() != rows * len(self.discr) or t.device != self.discr.device:
@@ -631,12 +706,14 @@ class CompiledOperator:
                                               ee.data_ptr(), self._stream()))
         return ii, ee
 
-    def __call__(self, w=None, t=0.0, bc_in=None, u=None, **kwargs):
+    def __call__(self, w=None, t=0.0, bc_in=None, u=None, coeff=None, **kwargs):
         """Evaluate the RHS.  A compiled template takes its fields by the
         names it uses (state, given boundary data, coefficient, source),
-        like the reference's compiled templates (``op(w=..., c=...)``)."""
+        like the reference's compiled templates (``op(w=..., c=...)``);
+        ``coeff`` gives the coefficient as the device tensor the kernels
+        read (FP64, contiguous)."""
         names = self.ot.fields or {}
-        coeff = source = None
+        source = None
         if names.get("state") in kwargs:
             w = kwargs.pop(names["state"])
         elif names.get("state_keys") and names["state_keys"][0][0] in kwargs:
@@ -645,7 +722,12 @@ class CompiledOperator:
         if names.get("given") in kwargs:
             bc_in = kwargs.pop(names["given"])
         if names.get("coeff") in kwargs:
-            coeff = self.discr.to_device(kwargs.pop(names["coeff"]), _torch().float64)
+            cval = kwargs.pop(names["coeff"])
+            if isinstance(cval, (list, tuple)) or (isinstance(cval, np.ndarray)
+                                                   and cval.dtype == object):
+                cval = _torch().stack([self.discr.to_device(x, _torch().float64)
+                                       for x in cval])
+            coeff = self.discr.to_device(cval, _torch().float64)
             coeff = coeff.reshape(-1).contiguous()
         if self._msrc_spec:
             fnames = {fld[0] for _, _, fld, _ in self._msrc_spec if fld is not None}
@@ -665,12 +747,16 @@ class CompiledOperator:
         if self.ot.model == MODEL_VARWAVE and coeff is None and self._coeff is None:
             raise ValueError("this template needs its coefficient field %r"
                              % names.get("coeff", "c"))
+        if self.ot.model == MODEL_VARADV and coeff is None and self._coeff is None:
+            raise ValueError("this template needs its velocity field %r"
+                             % names.get("coeff", "v"))
         if src_name is not None and source is None and self._source is None:
             raise ValueError("this template needs its source field %r" % src_name[0])
         q = self.as_state(w)
         out = self.discr.volume_empty((self.F,), self.state_dtype)
         self.rhs_into(q, out, bc_in=bc_in, coeff=coeff, source=source)
-        return out[0] if self.F == 1 and self.ot.model == MODEL_ADVECTION else out
+        return out[0] if self.F == 1 and self.ot.model in (MODEL_ADVECTION, MODEL_VARADV) \
+            else out
 
     def bind_model(self, model):
         return BoundRHS(self, model)
@@ -688,7 +774,7 @@ class BoundRHS:
     def context(self, t):
         """Given boundary data at time t that the model can evaluate itself
         (advection inflow, wave Dirichlet values given as functions)."""
-        if self.compiled.n_given:
+        if self.compiled.n_given or self.compiled.ot.model == MODEL_VARADV:
             m = self.model
             if hasattr(m, "context"):
                 return m.context(self.discr, t)

@@ -39,6 +39,17 @@ dropped when every integrand they feed is a polynomial of degree <= 2N
 face), which the nodal operators integrate exactly; a template with a
 coefficient field under a quadrature operator is refused.
 
+Templates that integrate a product of fields by quadrature (a coefficient
+field under an up-sampler or a quadrature stiffness operator, or an element
+maximum) go to the quadrature kernel instead: they must equal the
+variable-coefficient advection template (advection.py:282-368) built from
+the same fields, for one of its flux types and with or without given inflow
+data.  The comparison evaluates both templates on the same probes, with the
+up-samplers as identities (their operands' values at a point are the same
+polynomial's), each weak derivative S_x^T a random factor per axis times its
+integrand, and the element maximum a fixed non-linear function of its
+operand.
+
 A template that no kernel model reproduces raises ``NotImplementedError``
 naming the part that differs.
 """
@@ -55,9 +66,10 @@ from . import optemplate as ot
 from .mesh import TAG_ALL, TAG_NONE
 from .models import (BC_ABSORB, BC_DIRICHLET, BC_GIVEN, BC_NEUMANN, BC_NONE, BC_PEC, BC_PMC,
                      BC_RADIATION, MODEL_ADVECTION, MODEL_MAXWELL, MODEL_MAXWELL_TE,
-                     MODEL_MAXWELL_TM, MODEL_VARWAVE, MODEL_WAVE, MaxwellOperator,
-                     TEMaxwellOperator, TMMaxwellOperator, OpTemplate, StrongAdvectionOperator,
-                     StrongWaveOperator, VariableVelocityStrongWaveOperator)
+                     MODEL_MAXWELL_TM, MODEL_VARADV, MODEL_VARWAVE, MODEL_WAVE,
+                     MaxwellOperator, TEMaxwellOperator, TMMaxwellOperator, OpTemplate,
+                     StrongAdvectionOperator, StrongWaveOperator,
+                     VariableCoefficientAdvectionOperator, VariableVelocityStrongWaveOperator)
 
 PROBES = 16
 TOL = 1e-10
@@ -348,6 +360,10 @@ class _Ctx:
             return self.deriv(key, axis)
         return _rand(("d", key, axis, self.salt), -1, 1, self.P)
 
+    def weak(self, axis):
+        """Stand-in for the test-function derivative of S_axis^T."""
+        return _rand(("w", axis, self.salt), -1, 1, self.P)
+
 
 def _ev(x, ctx, interior=True):
     if _is_num(x):
@@ -374,10 +390,15 @@ def _ev(x, ctx, interior=True):
         op = x.op
         if isinstance(op, ot.DifferentiationOperator):
             return ctx.der(x.field.key, op.xyz_axis)
-        if isinstance(op, (ot.InverseMassOperator, ot.BoundarizeOperator)):
+        if isinstance(op, (ot.InverseMassOperator, ot.BoundarizeOperator) + _QUAD_SAMPLERS):
             return _ev(x.field, ctx, interior)
         if isinstance(op, ot.FluxOperator):
             return _ev_binding(op, x.field, ctx)
+        if isinstance(op, (ot.StiffnessTOperator, ot.QuadratureStiffnessTOperator)):
+            return ctx.weak(op.xyz_axis) * _ev(x.field, ctx, interior)
+        if isinstance(op, ot.ElementwiseMaxOperator):
+            y = _ev(x.field, ctx, interior)
+            return 1.7 * y + np.sin(y)
     raise NotImplementedError("cannot evaluate %r" % (x,))
 
 
@@ -694,6 +715,8 @@ def lower(template, dimensions, mesh=None):
     kernel model reproduces it.  With ``mesh``, boundary faces that carry
     none of the template's specific tags are known to exist or not (else a
     TAG_ALL-only boundary condition must match too)."""
+    if _needs_quadrature_kernel(_comps(template)):
+        return _lower_quadrature(_comps(template), dimensions)
     rw = _Rewrites()
     outs = rw.run(_comps(template))
     F = len(outs)
@@ -846,6 +869,97 @@ def lower(template, dimensions, mesh=None):
             return OpTemplate(desc.model, desc.dimensions, desc.n_fields, desc.flux_type,
                               _lowered_params(desc, float(src_consts[0])), bcs, None, names)
     raise NotImplementedError("op template is not one the B200 kernels implement: " + why[1])
+
+
+def _needs_quadrature_kernel(outs):
+    """Whether the template integrates a product of fields by quadrature
+    (or takes an element maximum): the work of the quadrature kernel."""
+    for x in outs:
+        for n in ot.walk(x):
+            if not isinstance(n, ot.OperatorBinding):
+                continue
+            if isinstance(n.op, ot.ElementwiseMaxOperator):
+                return True
+            if isinstance(n.op, _QUAD_SAMPLERS + (ot.QuadratureStiffnessTOperator,)) and \
+                    not _linear_in_fields(n.field):
+                return True
+            if isinstance(n.op, ot.StiffnessTOperator) and any(
+                    isinstance(m, ot.OperatorBinding) and isinstance(m.op, _QUAD_SAMPLERS)
+                    for m in ot.walk(n.field)) and not _linear_in_fields(n.field):
+                return True
+    return False
+
+
+def _strip_samplers(x):
+    return _rebuild(x, lambda n: n.field if isinstance(n, ot.OperatorBinding)
+                    and isinstance(n.op, _QUAD_SAMPLERS) else n)
+
+
+def _lower_quadrature(outs, dims):
+    """The variable-coefficient advection operator a quadrature template
+    equals (see the module docstring)."""
+    if len(outs) != 1:
+        raise NotImplementedError("quadrature templates: one output (the advected field)")
+    tags = {n.op.quadrature_tag for x in outs for n in ot.walk(x)
+            if isinstance(n, ot.OperatorBinding)
+            and isinstance(n.op, _QUAD_SAMPLERS + (ot.QuadratureStiffnessTOperator,))}
+    if len(tags) > 1:
+        raise NotImplementedError("more than one quadrature tag")
+    qtag = tags.pop() if tags else "quad"
+    interior, pairs = [], []
+    for n in ot.walk(outs[0]):
+        if isinstance(n, ot.OperatorBinding) and isinstance(n.op, ot.FluxOperator):
+            (pairs if isinstance(n.field, ot.BoundaryPair) else interior).append(n.field)
+    if not interior:
+        raise NotImplementedError("quadrature template without an interior flux")
+    arg = [_strip_samplers(c) for c in _comps(interior[0])]
+    if len(arg) != dims + 2 or not all(isinstance(c, ot.Field) for c in arg[:dims + 1]):
+        raise NotImplementedError(
+            "quadrature template: the flux argument must be (u, v_0 .. v_%d, c) with "
+            "u and v fields" % (dims - 1))
+    u, v = arg[0], arg[1:dims + 1]
+    if not all(f.name == v[0].name and f.index == i for i, f in enumerate(v)):
+        raise NotImplementedError("the velocity components must be one vector field "
+                                  "(make_sym_vector)")
+    given = None
+    for p in pairs:
+        b0 = _strip_samplers(_comps(p.bfield)[0])
+        if isinstance(b0, ot.Field):
+            given = b0
+    v_arr = ot.join_fields(v)
+    why = "no flux type of the variable-coefficient advection kernel matches"
+    for has_bc in ((True, False) if given is not None else (False,)):
+        for ft in VariableCoefficientAdvectionOperator.flux_types:
+            m = VariableCoefficientAdvectionOperator(dims, None, bc_u_f=1 if has_bc else "None",
+                                                     flux_type=ft)
+            canon = _comps(m.op_template(u=u, v=v_arr, bc_u=given if has_bc else None))
+            canon = [_rebuild(c, lambda n: _retag(n, qtag)) for c in canon]
+            ok = True
+            for face in (None, "interior", TAG_ALL):
+                ctx = _Ctx(dims, face=face)
+                if not _close(evaluate(outs, ctx), evaluate(canon, ctx)):
+                    if face is None:
+                        why = "volume terms differ from the variable-coefficient advection kernel's"
+                    ok = False
+                    break
+            if ok:
+                names = {"state": u.name, "coeff": v[0].name,
+                         "given": given.name if has_bc else None}
+                return OpTemplate(MODEL_VARADV, dims, 1,
+                                  VariableCoefficientAdvectionOperator.flux_types.index(ft),
+                                  {"quad_tag": qtag},
+                                  [(TAG_ALL, BC_GIVEN if has_bc else BC_DIRICHLET)], None, names)
+    raise NotImplementedError("op template is not one the B200 kernels implement: " + why)
+
+
+def _retag(n, tag):
+    """The model template's up-samplers with the user template's tag."""
+    if isinstance(n, ot.OperatorBinding):
+        if isinstance(n.op, ot.QuadratureGridUpsampler):
+            return ot.OperatorBinding(ot.QuadratureGridUpsampler(tag), n.field)
+        if isinstance(n.op, ot.QuadratureInteriorFacesGridUpsampler):
+            return ot.OperatorBinding(ot.QuadratureInteriorFacesGridUpsampler(tag), n.field)
+    return n
 
 
 def _uncovered(mesh, tags):

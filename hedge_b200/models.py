@@ -17,6 +17,9 @@ lowered form (:class:`OpTemplate`) directly:
   rhs = ((curl H - J) , -curl E) + M^-1 (fluxes)) / (eps | mu)
 * TMMaxwellOperator, TEMaxwellOperator  hedge/models/em.py:485-515 (2D
   subsets (Ez, Hx, Hy) and (Ex, Ey, Hz) of the same system)
+* VariableCoefficientAdvectionOperator  hedge/models/advection.py:190-391
+  rhs = M^-1 (S^T_quad (v u) - fluxes of (u, v, elmax |v|^2) on the face
+  quadrature grid), the velocity a volume field given per call
 """
 
 from __future__ import annotations
@@ -38,6 +41,7 @@ MODEL_VARWAVE = 3
 MODEL_MAXWELL = 4
 MODEL_MAXWELL_TM = 5
 MODEL_MAXWELL_TE = 6
+MODEL_VARADV = 7
 
 # boundary-condition kinds shared with the C-ABI
 BC_NONE = 0        # face contributes no boundary flux
@@ -117,6 +121,9 @@ class TimeConstantGivenFunction:
     def boundary_interpolant(self, t, discr, tag):
         return discr.interpolate_boundary_function(self.f, tag)
 
+    def volume_interpolant(self, t, discr):
+        return discr.interpolate_volume_function(self.f, kind="numpy")
+
 
 class TimeDependentGivenFunction:
     """Boundary/volume data given as f(x, t) with x an [N, d] array
@@ -129,7 +136,7 @@ class TimeDependentGivenFunction:
         return discr.interpolate_boundary_function(lambda x: self.f(x, t), tag)
 
     def volume_interpolant(self, t, discr):
-        return discr.interpolate_volume_function(lambda x: self.f(x, t))
+        return discr.interpolate_volume_function(lambda x: self.f(x, t), kind="numpy")
 
 
 def make_tdep_constant(value):
@@ -582,6 +589,115 @@ class TEMaxwellOperator(MaxwellOperator):
         return (True, True, False) + (False, False, True)
 
 
+class VariableCoefficientAdvectionOperator(HyperbolicOperator):
+    """Space- and time-dependent advection in weak form with over-integration
+    (advection.py:190-391): the velocity ``advec_v`` is a given function
+    (``volume_interpolant(t, discr)`` -> [d, K*Np]), ``bc_u_f`` the inflow
+    data on every boundary face (``"None"``: zero).  The volume and face
+    integrals are taken on the quadrature grid "quad" of the
+    discretization's ``quad_min_degrees`` (nodal evaluation when it has no
+    degree for "quad", as the reference falls back to).  Diffusion
+    (second-order terms) is not on this path."""
+
+    flux_types = ["central", "upwind", "lf"]
+
+    def __init__(self, dimensions, advec_v, bc_u_f="None", flux_type="central",
+                 diffusion_coeff=None, diffusion_scheme=None):
+        if flux_type not in self.flux_types:
+            raise ValueError("invalid flux type")
+        if diffusion_coeff is not None and diffusion_coeff != 0:
+            raise NotImplementedError("diffusion (second-order terms) is not on this path")
+        self.dimensions = int(dimensions)
+        self.advec_v = advec_v
+        self.bc_u_f = bc_u_f
+        self.flux_type = flux_type
+        self.diffusion_coeff = diffusion_coeff
+
+    def _has_bc(self):
+        return not (isinstance(self.bc_u_f, str) and self.bc_u_f == "None")
+
+    def flux(self):
+        """advection.py:224-266, w = (u, v, c)."""
+        d = self.dimensions
+        w = fl.FluxVectorPlaceholder(1 + d + 1)
+        u, v, c = w[0], w[1:d + 1], w[1 + d]
+        normal = fl.make_normal(d)
+        if self.flux_type == "central":
+            return (u.int * np.dot(v.int, normal) + u.ext * np.dot(v.ext, normal)) * 0.5
+        if self.flux_type == "lf":
+            n_vint = np.dot(normal, v.int)
+            n_vext = np.dot(normal, v.ext)
+            return 0.5 * (n_vint * u.int + n_vext * u.ext) \
+                - 0.5 * (u.ext - u.int) * fl.flux_max(c.int, c.ext)
+        return fl.IfPositive(np.dot(normal, v.avg),
+                             np.dot(normal, v.int) * u.int,
+                             np.dot(normal, v.ext) * u.ext)
+
+    def op_template(self, u=None, v=None, bc_u=None, with_sensor=False):
+        """advection.py:282-368 without the diffusion part."""
+        if with_sensor:
+            raise NotImplementedError("diffusion (second-order terms) is not on this path")
+        d = self.dimensions
+        u = ot.Field("u") if u is None else u
+        v = ot.make_sym_vector("v", d) if v is None else v
+        c = ot.ElementwiseMaxOperator()(ot.ptwise_dot(1, 1, v, v))
+        to_quad = ot.QuadratureGridUpsampler("quad")
+        to_if_quad = ot.QuadratureInteriorFacesGridUpsampler("quad")
+        quad_u = to_quad(u)
+        quad_v = to_quad(v)
+        w = ot.join_fields(u, v, c)
+        quad_face_w = to_if_quad(w)
+        bc_c = to_quad(ot.BoundarizeOperator(TAG_ALL)(c))
+        bc_v = to_quad(ot.BoundarizeOperator(TAG_ALL)(v))
+        if self._has_bc():
+            bc_w = ot.join_fields(to_quad(ot.Field("bc_u") if bc_u is None else bc_u),
+                                  bc_v, bc_c)
+        else:
+            bc_w = ot.join_fields(0, bc_v, bc_c)
+        minv_st = ot.make_stiffness_t(d)
+        m_inv = ot.InverseMassOperator()
+        flux_op = ot.get_flux_operator(self.flux())
+        return _remember(self, m_inv(
+            np.dot(minv_st, quad_v * quad_u)
+            - (flux_op(quad_face_w) + flux_op(ot.BoundaryPair(quad_face_w, bc_w, TAG_ALL)))))
+
+    def descriptor(self):
+        return OpTemplate(MODEL_VARADV, self.dimensions, 1,
+                          self.flux_types.index(self.flux_type), {"quad_tag": "quad"},
+                          [(TAG_ALL, BC_GIVEN if self._has_bc() else BC_DIRICHLET)], self,
+                          {"state": "u", "coeff": "v", "given": "bc_u" if self._has_bc()
+                           else None})
+
+    def bc_tags(self):
+        return [TAG_ALL]
+
+    def context(self, discr, t, fields=None):
+        """The velocity at time t as the device coefficient [d * K*Np] (FP64;
+        computed once for a time-constant velocity) and the inflow data."""
+        if isinstance(self.advec_v, TimeConstantGivenFunction):
+            cache = self.__dict__.setdefault("_v_dev", {})
+            if id(discr) not in cache:
+                cache.clear()
+                cache[id(discr)] = self._velocity(discr, t)
+            v = cache[id(discr)]
+        else:
+            v = self._velocity(discr, t)
+        ctx = {"coeff": v}
+        if self._has_bc():
+            ctx["bc_in"] = self.bc_u_f.boundary_interpolant(t, discr, TAG_ALL)
+        return ctx
+
+    def _velocity(self, discr, t):
+        import torch
+        v = self.advec_v.volume_interpolant(t, discr)
+        return discr.to_device(v, torch.float64).reshape(-1).contiguous()
+
+    def max_eigenvalue(self, t=None, fields=None, discr=None):
+        """advection.py:381-391: the largest nodal |v|."""
+        v = np.asarray(_to_numpy(self.advec_v.volume_interpolant(t, discr)), dtype=np.float64)
+        return float(np.sqrt(np.max(np.sum(v.reshape(self.dimensions, -1) ** 2, axis=0))))
+
+
 def _template_value(x, name):
     """A model datum as a template term: expressions and numbers as they
     are, volume vectors as the field ``name`` (bound when the model binds)."""
@@ -604,7 +720,7 @@ def _to_numpy(x):
 
 __all__ = ["template_model", "StrongAdvectionOperator", "WeakAdvectionOperator", "StrongWaveOperator",
            "VariableVelocityStrongWaveOperator", "MaxwellOperator", "TMMaxwellOperator",
-           "TEMaxwellOperator",
+           "TEMaxwellOperator", "VariableCoefficientAdvectionOperator",
            "OpTemplate", "make_tdep_constant", "TimeConstantGivenFunction",
            "TimeDependentGivenFunction",
            "check_bc_coverage"]

@@ -405,6 +405,14 @@ class InverseMassOperator(Operator):
         return "MInv"
 
 
+class ElementwiseMaxOperator(Operator):
+    """Each element's nodes set to the largest of its nodal values
+    (operators.py:256-257; volume_operators.hpp:356-369)."""
+
+    def __str__(self):
+        return "ElMax"
+
+
 class BoundarizeOperator(Operator):
     """Restriction of a volume vector to the nodes of boundary ``tag``."""
 
@@ -494,6 +502,17 @@ def cse(expr, prefix=None):
     return expr
 
 
+def ptwise_dot(logdims1, logdims2, a1, a2):
+    """Pointwise dot product of two object vectors (optemplate/tools.py:228-248
+    for vectors: sum_k a1[k] * a2[k])."""
+    if logdims1 != 1 or logdims2 != 1:
+        raise NotImplementedError("ptwise_dot of vectors only")
+    r = 0
+    for x, y in zip(a1, a2):
+        r = add(r, mul(x, y))
+    return r
+
+
 def cross(a, b):
     """3-vector cross product of object arrays (hedge.tools cross products
     with full subsets)."""
@@ -536,6 +555,6 @@ __all__ = ["Field", "make_field", "make_sym_vector", "make_vector_field",
            "StiffnessOperator", "StiffnessTOperator", "QuadratureGridUpsampler",
            "QuadratureInteriorFacesGridUpsampler", "QuadratureBoundaryGridUpsampler",
            "QuadratureStiffnessTOperator", "make_stiffness", "make_stiffness_t",
-           "InverseMassOperator", "BoundarizeOperator", "FluxOperator",
+           "InverseMassOperator", "ElementwiseMaxOperator", "BoundarizeOperator", "FluxOperator",
            "VectorFluxOperator", "get_flux_operator", "make_nabla", "join_fields",
-           "make_obj_array", "cse", "cross", "is_zero", "pretty", "walk"]
+           "make_obj_array", "cse", "cross", "ptwise_dot", "is_zero", "pretty", "walk"]

@@ -8,6 +8,11 @@ full-size parity tests so that both see the same meshes and fields.
 * 3D acoustic wave pulse: the same mesh at order 7, c = 1, upwind flux,
   reflecting (Dirichlet) walls; a Gaussian pressure pulse of width 0.15 at
   rest.
+* 2D variable-coefficient advection (the reference's var-velocity example,
+  examples/advection/var-velocity.py): [-1,1]^2 in n x n squares of two
+  triangles, order 5, quadrature degree 3N = 15, rotating velocity (-y, x),
+  inflow u = 1 where x > 0, upwind flux; a Gaussian pulse of width 1/8 at
+  (0.3, 0.5).
 """
 
 from __future__ import annotations
@@ -61,3 +66,20 @@ def pulse_ic(discr):
 
 def initial_state(discr, workload="maxwell"):
     return pulse_ic(discr) if workload == "wave7" else cavity_ic(discr)
+
+
+def varadv_problem(n=400, order=5, device=None, precision="fp64"):
+    """(discretization, operator, initial u) of the 2D variable-coefficient
+    advection workload."""
+    from . import models
+    from .discretization import Discretization
+    from .mesh import make_regular_rect_mesh
+    mesh = make_regular_rect_mesh((-1, -1), (1, 1), (n, n))
+    d = Discretization(mesh, order=order, precision=precision, device=device,
+                       quad_min_degrees={"quad": 3 * order})
+    vf = models.TimeConstantGivenFunction(lambda x: np.stack([-x[:, 1], x[:, 0]]))
+    bf = models.TimeConstantGivenFunction(lambda x: (x[:, 0] > 0).astype(np.float64))
+    op = models.VariableCoefficientAdvectionOperator(2, vf, bc_u_f=bf, flux_type="upwind")
+    x = d.nodes
+    u0 = np.exp(-64 * np.sum((x - np.array([0.3, 0.5])) ** 2, axis=1))
+    return d, op, u0

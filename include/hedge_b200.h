@@ -37,7 +37,15 @@ enum {
   HB_MODEL_VARWAVE = 3,   /* hedge/models/wave.py:204-418 */
   HB_MODEL_MAXWELL = 4,   /* hedge/models/em.py:38-387 */
   HB_MODEL_MAXWELL_TM = 5, /* hedge/models/em.py:485-498, 2D, fields (Ez, Hx, Hy) */
-  HB_MODEL_MAXWELL_TE = 6  /* hedge/models/em.py:501-515, 2D, fields (Ex, Ey, Hz) */
+  HB_MODEL_MAXWELL_TE = 6, /* hedge/models/em.py:501-515, 2D, fields (Ex, Ey, Hz) */
+  HB_MODEL_VARADV = 7      /* hedge/models/advection.py:190-368: variable-coefficient
+                              advection, weak form, integrals by quadrature (one
+                              field u; the velocity field is the coeff argument,
+                              [dim][K*Np] FP64; hb_op_desc.quadrature required).
+                              Boundary kinds: HB_BC_GIVEN (u outside = the given
+                              values, bc_u_f), HB_BC_DIRICHLET (u outside = 0,
+                              bc_u_f "None"), HB_BC_NONE (no flux); v outside =
+                              v inside.  FP64 and FP32 precisions. */
 };
 
 enum {
@@ -90,6 +98,20 @@ hb_status hb_discr_destroy(hb_discr* discr);
  * interior face: (neighbour element, nbr_face | perm_id << 2);
  * boundary face: (-1 - b, bc kind), b = the face's number in the
  * BC_GIVEN boundary vector (nodes b*nfp .. b*nfp+nfp-1). */
+/* Quadrature matrices of one reference element for one degree
+ * (hedge/discretization/local.py:545-690, QuadratureInfo), host FP64,
+ * row-major.  Weights are the reference element's: d r / d x and
+ * Fscale = face Jacobian / |J| are applied per element. */
+typedef struct {
+  int32_t nq;                /* volume quadrature points */
+  int32_t nqf;               /* quadrature points per face */
+  const double* vol_interp;  /* [nq][np]: nodal values -> volume points */
+  const double* vol_project; /* [dim][np][nq]: M^-1 (d phi_i / d r_r at q)^T w_q */
+  const double* face_interp; /* [nfaces][nqf][nfp]: face f's nodes (fmask order)
+                                -> its quadrature points */
+  const double* face_lift;   /* [np][nfaces*nqf]: M^-1 phi_i(face point) w_face */
+} hb_quad_desc;
+
 typedef struct {
   int32_t model, num_fields, precision;
   int32_t flux_type, bdry_flux_type;
@@ -103,6 +125,10 @@ typedef struct {
   int64_t num_halo_faces;  /* faces whose neighbour lives on another partition
                               (conn neighbour K + h, h < num_halo_faces); their
                               ext values come from hb_op_set_halo; 0 = none */
+  const hb_quad_desc* quadrature; /* HB_MODEL_VARADV: the quadrature grid (copied
+                              at create); NULL for every other model.  Replaces
+                              Discretization.get_quadrature_info
+                              (hedge/discretization/__init__.py:779-889). */
 } hb_op_desc;
 
 /* Replaces Discretization.compile -> jit Executor construction
@@ -116,7 +142,8 @@ hb_status hb_op_destroy(hb_op* op);
  * flux gather interior + boundary (jit/flux.py:239-480), lift
  * (jit/lift.py:110-141) and inverse mass (jit/__init__.py:501-519).
  * q, rhs: [F][K*Np] in the operator's state dtype.  coeff: var-c wave
- * speed [K*Np] FP64 (else NULL); bdry: BC_GIVEN values [n] FP64 (else NULL);
+ * speed [K*Np] FP64, or the variable-coefficient advection velocity
+ * [dim][K*Np] FP64 (else NULL); bdry: BC_GIVEN values [n] FP64 (else NULL);
  * source: var-c / constant-c wave source on u, [K*Np] FP64 (else NULL). */
 hb_status hb_rhs(hb_op* op, const void* q, void* rhs, const double* coeff,
                  const double* bdry, const double* source, void* stream);

@@ -23,13 +23,20 @@ lowering.
   (operators.py:141-143 with the reference element's matrices);
 * over-integration (operators.py:149-168, 262-314, 593-631): where a
   stiffness-transpose or a flux operator acts on up-sampled fields, the
-  integrals are taken with collapsed Gauss-Jacobi rules (Duffy transform,
-  Gauss-Legendre x Gauss-Jacobi(1,0) [x Gauss-Jacobi(2,0)] points, exact to
-  degree 2(N+2)-1 per direction) on the elements and on every face, with the
-  interior / exterior traces evaluated from each element's own polynomial at
-  the physical quadrature points and boundary data interpolated from the
-  face nodes.  This is an independent evaluation of the integrals the
-  nodal operators compute in closed form.
+  integrals are taken by quadrature on the elements and on every face, with
+  the interior / exterior traces evaluated from each element's own
+  polynomial at the physical quadrature points and boundary data
+  interpolated from the face nodes.  The rule: when the discretization has a
+  minimum degree for the up-samplers' tag (``quad_min_degrees``), the
+  reference's own (hedge/quadrature.py:379-400: Gauss-Legendre with s + 1
+  points on 1D faces, Grundmann-Moeller of index s otherwise,
+  s = ceil((degree - 1) / 2)), restated here in ``reference_cubature``;
+  else collapsed Gauss-Jacobi rules (Duffy transform, Gauss-Legendre x
+  Gauss-Jacobi(1,0) [x Gauss-Jacobi(2,0)] points, exact to degree
+  2(N+2)-1 per direction), an independent evaluation of the integrals the
+  nodal operators compute in closed form;
+* ElementwiseMaxOperator: each element's nodes set to its largest nodal
+  value (volume_operators.hpp:356-369).
 """
 
 from __future__ import annotations
@@ -76,8 +83,48 @@ def simplex_rule(dim, n):
     return np.stack([r.ravel(), s_.ravel(), Cc.ravel()], 1), w
 
 
+def reference_cubature(exact_to_degree, dim):
+    """The reference's simplex rule for ``exact_to_degree``
+    (hedge/quadrature.py:241-327, 379-400): points on the biunit simplex
+    and weights.  1D: the s+1-point Gauss-Legendre rule; dim >= 2: the
+    Grundmann-Moeller rule of index s (Grundmann, Moeller, SIAM J. Numer.
+    Anal. 15 (1978) 282-290): weight (-1)^i 2^(-2s) (d+n-2i)^d / (i! (d+n-i)!)
+    at the barycentric points ((2 b_k + 1) / (d+n-2i))_k for every
+    composition b of s - i into n + 1 parts, i = 0..s, d = 2s + 1; equal
+    points merged; times 2^n for the biunit simplex."""
+    from fractions import Fraction
+    from itertools import product
+    from math import ceil, factorial
+    s = int(ceil((exact_to_degree - 1) / 2))
+    if dim == 1:
+        x, w = np.polynomial.legendre.leggauss(s + 1)
+        return x[:, None], w
+    n, d = dim, 2 * s + 1
+    acc = {}
+    for i in range(s + 1):
+        den = d + n - 2 * i
+        wt = Fraction((-1) ** i * den ** d, 4 ** s * factorial(i) * factorial(d + n - i))
+        for b in product(range(s - i + 1), repeat=n):
+            if sum(b) > s - i:
+                continue
+            bb = (s - i - sum(b),) + b
+            key = tuple(Fraction(2 * k + 1, den) for k in bb)
+            acc[key] = acc.get(key, Fraction(0)) + wt
+    pts = np.array([[2 * float(lam[k]) - 1 for k in range(1, n + 1)] for lam in acc])
+    wts = np.array([float(w * 2 ** n) for w in acc.values()])
+    return pts, wts
+
+
 def _num(x):
     return isinstance(x, numbers.Number) and not isinstance(x, bool)
+
+
+def _quad_tag(x):
+    for n in ot.walk(x):
+        if isinstance(n, ot.OperatorBinding) and isinstance(
+                n.op, _QUAD + (ot.QuadratureStiffnessTOperator,)):
+            return n.op.quadrature_tag
+    return None
 
 
 class TemplateExecutor:
@@ -92,7 +139,7 @@ class TemplateExecutor:
         self.imd = discr.mesh.inv_map_a                             # [K, r, x]
         self.absj = np.abs(discr.mesh.jacobians)
         self._groups = {}
-        self._quad = None
+        self._quad = {}
 
     # -- nodal basis at arbitrary points ----------------------------------------------
     def _phi(self, r):
@@ -110,16 +157,22 @@ class TemplateExecutor:
         m = self.d.mesh
         return (x - m.map_b[k]) @ m.inv_map_a[k].T
 
-    def _setup_quadrature(self):
-        """Volume and face quadrature of degree 2 (N + 2) - 1 per direction."""
-        if self._quad is not None:
-            return self._quad
+    def _setup_quadrature(self, tag=None):
+        """Volume and face quadrature of ``tag``: the reference's rule of the
+        discretization's minimum degree for the tag, else collapsed rules of
+        degree 2 (N + 2) - 1 per direction."""
+        if tag in self._quad:
+            return self._quad[tag]
         d, N, m = self.dim, self.d.order, self.d.mesh
-        n = N + 2
-        rq, wq = simplex_rule(d, n)
+        degree = getattr(self.d, "quad_min_degrees", {}).get(tag)
+        if degree is not None:
+            rq, wq = reference_cubature(degree, d)
+            fr, fw = reference_cubature(degree, d - 1)
+        else:
+            rq, wq = simplex_rule(d, N + 2)
+            fr, fw = simplex_rule(d - 1, N + 2)
         phi_q, dphi_q = self._phi(rq)
         # faces: physical points, weights, normals, int / ext basis values
-        fr, fw = simplex_rule(d - 1, n)
         nf = d + 1
         ftab = face_vertex_table(d)
         K = self.K
@@ -144,8 +197,8 @@ class TemplateExecutor:
                 phi_e = self._phi(self._to_ref(e, x))[0] if e is not None else None
                 faces.append(dict(k=k, f=f, x=x, dA=dA, n=m.face_normals[k, f],
                                   phi_i=phi_i, ext=e, phi_e=phi_e, P=P))
-        self._quad = dict(wq=wq, phi_q=phi_q, dphi_q=dphi_q, faces=faces)
-        return self._quad
+        self._quad[tag] = dict(wq=wq, phi_q=phi_q, dphi_q=dphi_q, faces=faces)
+        return self._quad[tag]
 
     # -- element-local operators ---------------------------------------------------
     def grad(self, u, axis):
@@ -163,27 +216,28 @@ class TemplateExecutor:
             out += (self.imd[:, r, axis] * self.absj)[:, None] * (fe @ S)
         return out.reshape(-1)
 
-    def _qvol(self, x, env):
+    def _qvol(self, x, env, tag=None):
         """An up-sampled expression at the volume quadrature points [K, Q]."""
-        q = self._setup_quadrature()
+        q = self._setup_quadrature(tag)
         if _num(x):
             return np.full((self.K, len(q["wq"])), float(x))
         if isinstance(x, ot.Field):
             return self.vol(x, env).reshape(self.K, self.Np) @ q["phi_q"].T
         if isinstance(x, ot.Sum):
-            return sum(self._qvol(c, env) for c in x.children)
+            return sum(self._qvol(c, env, tag) for c in x.children)
         if isinstance(x, ot.Product):
             r = 1.0
             for c in x.children:
-                r = r * self._qvol(c, env)
+                r = r * self._qvol(c, env, tag)
             return r
         if isinstance(x, ot.OperatorBinding) and isinstance(x.op, ot.QuadratureGridUpsampler):
-            return self._qvol(x.field, env)
+            return self._qvol(x.field, env, tag)
         raise NotImplementedError("quadrature-grid node %r" % (x,))
 
-    def quad_stiffness_t(self, x, axis, env):
-        q = self._setup_quadrature()
-        fq = self._qvol(x, env)                                     # [K, Q]
+    def quad_stiffness_t(self, x, axis, env, tag=None):
+        tag = _quad_tag(x) if tag is None else tag
+        q = self._setup_quadrature(tag)
+        fq = self._qvol(x, env, tag)                                # [K, Q]
         dphi = np.einsum("kr,rqi->kqi", self.imd[:, :, axis], q["dphi_q"])
         return (np.einsum("q,kq,kqi->ki", q["wq"], fq, dphi) * self.absj[:, None]).reshape(-1)
 
@@ -260,7 +314,8 @@ class TemplateExecutor:
         """Face integrals of the flux against the test functions, by face
         quadrature, on interior faces (arg a volume vector) or on a
         boundary pair's faces."""
-        q = self._setup_quadrature()
+        q = self._setup_quadrature(_quad_tag(arg.field if isinstance(arg, ot.BoundaryPair)
+                                             else arg))
         out = np.zeros((self.K, self.Np))
         pair = arg if isinstance(arg, ot.BoundaryPair) else None
         field = self._strip(pair.field if pair is not None else arg)
@@ -390,7 +445,10 @@ class TemplateExecutor:
             if isinstance(op, ot.InverseMassOperator):
                 return self.inverse_mass(self.vol(x.field, env))
             if isinstance(op, ot.QuadratureStiffnessTOperator):
-                return self.quad_stiffness_t(x.field, op.xyz_axis, env)
+                return self.quad_stiffness_t(x.field, op.xyz_axis, env, op.quadrature_tag)
+            if isinstance(op, ot.ElementwiseMaxOperator):
+                v = np.asarray(self.vol(x.field, env)).reshape(self.K, self.Np)
+                return np.repeat(v.max(axis=1), self.Np)
             if isinstance(op, ot.StiffnessTOperator):
                 if _has_quad(x.field):
                     return self.quad_stiffness_t(x.field, op.xyz_axis, env)

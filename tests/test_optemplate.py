@@ -450,10 +450,11 @@ def test_weak_form_needs_every_boundary_face_tagged():
         lower(tpl, 2)
 
 
-def test_over_integration_with_a_coefficient_field_is_refused():
-    """Variable-velocity advection (the velocity a field under the
-    quadrature stiffness, advection.py:300-368) is not integrated exactly by
-    the nodal operators."""
+def test_other_quadrature_templates_are_refused():
+    """A coefficient field under the quadrature stiffness goes to the
+    quadrature kernel, which implements the variable-coefficient advection
+    operator (advection.py:282-368) only: this template (no velocity in the
+    flux, no boundary pair) is refused."""
     u, vx = ot.Field("u"), ot.Field("vx")
     to_quad = ot.QuadratureGridUpsampler("quad")
     U = fl.FluxScalarPlaceholder(0)
