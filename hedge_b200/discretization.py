@@ -20,7 +20,7 @@ import numpy as np
 
 from . import _native
 from .facegroups import Boundary, build_compact_connectivity, build_interior_face_group
-from .mesh import Mesh, TAG_ALL, TAG_NONE, check_bc_coverage
+from .mesh import Mesh, TAG_ALL, TAG_NONE
 from .lowering import as_descriptor
 from .optemplate import Expr
 from .models import (BC_GIVEN, BC_NONE, MODEL_MAXWELL, MODEL_MAXWELL_TE, MODEL_MAXWELL_TM,
@@ -376,9 +376,8 @@ def build_face_table(discr, ot):
     and the given tag."""
     ot = as_descriptor(ot, discr.dimensions, discr.mesh)
     mesh = discr.mesh
-    model = ot.operator
-    if model is not None and hasattr(model, "bc_tags"):
-        check_bc_coverage(mesh, model.bc_tags())
+    # BC coverage is checked where the reference checks it: in the models'
+    # bind (em.py:373-377, wave.py:182-186, advection.py:86-90), not here
     nbr = discr.nbr.astype(np.int64).copy()
     code = discr.nbr_code.astype(np.int64).copy()
     bdry_faces = nbr < 0
