@@ -118,11 +118,8 @@ static hb_status upload_quadrature(Op* op, const hb_quad_desc* qd) {
   op->nq = nq;
   op->nqf = nqf;
   hb_status st;
+  // FP64 matrices for both precisions (the FP32 path computes in FP64)
   if ((st = upload(&op->quad64, h.data(), h.size()))) return st;
-  if (op->precision == HB_PREC_FP32) {
-    std::vector<float> h32(h.begin(), h.end());
-    if ((st = upload(&op->quad32, h32.data(), h32.size()))) return st;
-  }
   if (cudaMalloc(&op->elmax, sizeof(double) * d->K) != cudaSuccess)
     return fail(HB_ERR_CUDA, "cannot allocate the element maxima");
   return HB_OK;
@@ -290,7 +287,7 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
   hb_status st;
   auto bail = [&](hb_status s) {
     cudaFree(op->conn); cudaFree(op->err_flag);
-    cudaFree(op->quad64); cudaFree(op->quad32); cudaFree(op->elmax);
+    cudaFree(op->quad64); cudaFree(op->elmax);
     free_split(op);
     delete op;
     return s;
@@ -330,7 +327,7 @@ hb_status hb_op_destroy(hb_op* handle) {
   DeviceGuard g(op->d->device);
   cudaFree(op->conn);
   cudaFree(op->err_flag);
-  cudaFree(op->quad64); cudaFree(op->quad32); cudaFree(op->elmax);
+  cudaFree(op->quad64); cudaFree(op->elmax);
   free_split(op);
   delete op;
   return HB_OK;

@@ -102,7 +102,6 @@ struct Op {
   // element maxima of |v|^2 the LF flux reads
   int nq = 0, nqf = 0;
   double* quad64 = nullptr;
-  float* quad32 = nullptr;
   double* elmax = nullptr;
 };
 

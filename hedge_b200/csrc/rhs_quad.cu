@@ -27,16 +27,20 @@
 //   D. node i: sum_r sum_q B_r[i, q] g_r(q) - sum_p L[i, p] flux_p, written
 //      as the RHS or as the LSRK stage update
 //      (hedge/timestep/runge_kutta.py:123-128).
-// The element work is FP64 (or FP32) FMA on the CUDA cores; the matrices sit
-// in shared memory when they leave room for a batch, else they are read
-// through L1.
+// The element work is FP64 FMA on the CUDA cores, also for FP32 state
+// vectors; the matrices sit in shared memory when they leave room for a
+// batch, else they are read through L1.
 #include "common.cuh"
 
 #include <algorithm>
 
 namespace hb {
 
-template <typename T>
+// T: the type the kernel computes and stages in; IO: the type of the state,
+// residual and output vectors (the FP32 path: FP64 arithmetic on FP32
+// vectors, since the weak form's volume and face integrals nearly cancel for
+// smooth fields and FP32 sums of them miss the FP32 path's 1e-5 bound)
+template <typename T, typename IO = T>
 struct QuadArgs {
   int64_t K, nbatch, n_given;
   int np, nfp, nf, nperm, G, E, nq, nqf;
@@ -48,10 +52,10 @@ struct QuadArgs {
   const int2* conn;
   const int* fmask;
   const int* shuffle;
-  const T* q_in;
-  T* q_out;
-  T* res;
-  T* rhs_out;
+  const IO* q_in;
+  IO* q_out;
+  IO* res;
+  IO* rhs_out;
   const double* vel;     // [dim][K*np]
   const double* bdry;    // given boundary values (BC_GIVEN faces)
   const double* elmax;   // [K] element maxima of |v|^2 (LF flux), else null
@@ -113,8 +117,8 @@ __global__ void elmax_kernel(int64_t K, int np, int dim, const double* __restric
   }
 }
 
-template <int DIM, typename T>
-__global__ void __launch_bounds__(256) rhs_quad_kernel(QuadArgs<T> a) {
+template <int DIM, typename T, typename IO>
+__global__ void __launch_bounds__(256) rhs_quad_kernel(QuadArgs<T, IO> a) {
   constexpr int NV = 1 + DIM;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int np = a.np, nfp = a.nfp, nf = a.nf, E = a.E, G = a.G;
@@ -158,7 +162,7 @@ __global__ void __launch_bounds__(256) rhs_quad_kernel(QuadArgs<T> a) {
     __syncthreads();  // previous batch done with the shared buffers
     // ---- A: stage u, v, geometry, face table ----
     for (int x = tid; x < ne * np; x += nthr) {
-      sw[x] = a.q_in[el0 * np + x];
+      sw[x] = (T)a.q_in[el0 * np + x];
 #pragma unroll
       for (int c = 0; c < DIM; ++c)
         sw[((1 + c) * E) * np + x] = T(a.vel[c * Knp + el0 * np + x]);
@@ -184,7 +188,7 @@ __global__ void __launch_bounds__(256) rhs_quad_kernel(QuadArgs<T> a) {
           qflag(a.err, cn.x >= a.K ? DEV_BAD_NEIGHBOUR : DEV_BAD_CODE);
         } else {
           const int64_t gi = (int64_t)cn.x * np + sfm[nface * nfp + ssh[perm * nfp + k]];
-          w[0] = a.q_in[gi];
+          w[0] = (T)a.q_in[gi];
 #pragma unroll
           for (int c = 0; c < DIM; ++c) w[1 + c] = T(__ldg(a.vel + c * Knp + gi));
         }
@@ -307,11 +311,11 @@ __global__ void __launch_bounds__(256) rhs_quad_kernel(QuadArgs<T> a) {
       for (int p = 0; p < nfq; ++p) acc -= sL[p * np + i] * fe[p];
       const int64_t node = (el0 + e) * np + i;
       if (a.mode == 0) {
-        a.rhs_out[node] = acc;
+        a.rhs_out[node] = (IO)acc;
       } else {
-        const T rv = T(a.ra) * a.res[node] + T(a.dt) * acc;
-        a.res[node] = rv;
-        a.q_out[node] = sw[e * np + i] + T(a.rb) * rv;
+        const T rv = T(a.ra) * (T)a.res[node] + T(a.dt) * acc;
+        a.res[node] = (IO)rv;
+        a.q_out[node] = (IO)(sw[e * np + i] + T(a.rb) * rv);
       }
     }
   }
@@ -325,11 +329,11 @@ static size_t quad_smem(const Op* op, int E, int ops) {
                      op->nq, op->nqf, ops).total;
 }
 
-template <int DIM, typename T>
+template <int DIM, typename T, typename IO>
 static hb_status quad_launch(Op* op, int mode, double ra, double rb, double dt,
                              const void* q_in, void* q_out, void* res, const double* vel,
                              const double* bdry, cudaStream_t s, bool configure) {
-  auto kern = rhs_quad_kernel<DIM, T>;
+  auto kern = rhs_quad_kernel<DIM, T, IO>;
   Discr* d = op->d;
   if (configure) {
     int dev;
@@ -366,28 +370,27 @@ static hb_status quad_launch(Op* op, int mode, double ra, double rb, double dt,
     elmax_kernel<<<grid, 256, 0, s>>>(d->K, d->np, d->dim, vel, op->elmax);
     HB_CUDA(cudaGetLastError());
   }
-  QuadArgs<T> a;
+  QuadArgs<T, IO> a;
   a.K = d->K;
   a.E = op->elems_per_block;
   a.nbatch = (d->K + a.E - 1) / a.E;
   a.n_given = op->n_given;
   a.np = d->np; a.nfp = d->nfp; a.nf = d->nfaces; a.nperm = d->nperm; a.G = d->G;
   a.nq = op->nq; a.nqf = op->nqf;
-  const T* ops = static_cast<const T*>(sizeof(T) == 8 ? (const void*)op->quad64
-                                                      : (const void*)op->quad32);
+  static_assert(sizeof(T) == 8, "the quadrature kernel computes in FP64");
+  const T* ops = op->quad64;
   const size_t nI = (size_t)d->np * op->nq, nB = (size_t)d->dim * op->nq * d->np;
   const size_t nF = (size_t)d->nfaces * d->nfp * op->nqf;
   a.It = ops;
   a.Bt = ops + nI;
   a.Ft = ops + nI + nB;
   a.Lt = ops + nI + nB + nF;
-  if constexpr (sizeof(T) == 8) a.geo = reinterpret_cast<const T*>(d->geo);
-  else a.geo = reinterpret_cast<const T*>(d->geo32);
+  a.geo = d->geo;
   a.conn = op->conn; a.fmask = d->fmask; a.shuffle = d->shuffle;
-  a.q_in = static_cast<const T*>(q_in);
-  a.q_out = static_cast<T*>(q_out);
-  a.res = static_cast<T*>(res);
-  a.rhs_out = static_cast<T*>(q_out);
+  a.q_in = static_cast<const IO*>(q_in);
+  a.q_out = static_cast<IO*>(q_out);
+  a.res = static_cast<IO*>(res);
+  a.rhs_out = static_cast<IO*>(q_out);
   a.vel = vel; a.bdry = bdry;
   a.elmax = op->mp.flux_type == 2 ? op->elmax : nullptr;
   a.ra = ra; a.rb = rb; a.dt = dt; a.mode = mode;
@@ -399,29 +402,33 @@ static hb_status quad_launch(Op* op, int mode, double ra, double rb, double dt,
   return HB_OK;
 }
 
-template <typename T>
+template <typename T, typename IO>
 static hb_status quad_dispatch(Op* op, int mode, double ra, double rb, double dt,
                                const void* q_in, void* q_out, void* res, const double* vel,
                                const double* bdry, cudaStream_t s, bool configure) {
   if (op->d->dim == 2)
-    return quad_launch<2, T>(op, mode, ra, rb, dt, q_in, q_out, res, vel, bdry, s, configure);
-  return quad_launch<3, T>(op, mode, ra, rb, dt, q_in, q_out, res, vel, bdry, s, configure);
+    return quad_launch<2, T, IO>(op, mode, ra, rb, dt, q_in, q_out, res, vel, bdry, s,
+                                 configure);
+  return quad_launch<3, T, IO>(op, mode, ra, rb, dt, q_in, q_out, res, vel, bdry, s,
+                               configure);
 }
 
 hb_status prepare_quad(Op* op) {
   if (op->precision == HB_PREC_FP32)
-    return quad_dispatch<float>(op, 0, 0, 0, 0, nullptr, nullptr, nullptr, nullptr, nullptr, 0,
-                                true);
-  return quad_dispatch<double>(op, 0, 0, 0, 0, nullptr, nullptr, nullptr, nullptr, nullptr, 0,
-                               true);
+    return quad_dispatch<double, float>(op, 0, 0, 0, 0, nullptr, nullptr, nullptr, nullptr,
+                                        nullptr, 0, true);
+  return quad_dispatch<double, double>(op, 0, 0, 0, 0, nullptr, nullptr, nullptr, nullptr,
+                                       nullptr, 0, true);
 }
 
 hb_status launch_quad(Op* op, int mode, double ra, double rb, double dt, const void* q_in,
                       void* q_out, void* res, const double* vel, const double* bdry,
                       cudaStream_t s) {
   if (op->precision == HB_PREC_FP32)
-    return quad_dispatch<float>(op, mode, ra, rb, dt, q_in, q_out, res, vel, bdry, s, false);
-  return quad_dispatch<double>(op, mode, ra, rb, dt, q_in, q_out, res, vel, bdry, s, false);
+    return quad_dispatch<double, float>(op, mode, ra, rb, dt, q_in, q_out, res, vel, bdry, s,
+                                        false);
+  return quad_dispatch<double, double>(op, mode, ra, rb, dt, q_in, q_out, res, vel, bdry, s,
+                                       false);
 }
 
 }  // namespace hb

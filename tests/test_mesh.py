@@ -45,3 +45,20 @@ def test_single_element_geometry(dim, flip):
     vol /= 2.0 if dim == 2 else 6.0
     ref_vol = 2.0 if dim == 2 else 4.0 / 3.0     # the reference simplex
     assert np.isclose(abs(m.jacobians[0]) * ref_vol, vol, rtol=1e-13)
+
+
+def test_bind_checks_coverage_compile_does_not():
+    """The models' bind checks boundary coverage (Maxwell: the PEC,
+    absorbing and incident tags only, em.py:373-377; hedge/mesh/__init__.py
+    check_bc_coverage); Discretization.compile does not, so a PMC-walled
+    mesh compiles directly (its face table is built without a check)."""
+    from hedge_b200.discretization import build_face_table
+    def tagger(fvi, el, fn, allv):
+        return ["pmc"] if allv[list(fvi)].mean(0)[0] < -0.99 else ["pec"]
+    m = hb.make_regular_rect_mesh((-1, -1), (1, 1), (4, 4), boundary_tagger=tagger)
+    d = hb.Discretization(m, order=2)
+    op = hb.TMMaxwellOperator(1.0, 1.0, flux_type=1, pec_tag="pec", pmc_tag="pmc")
+    with pytest.raises(MeshError):
+        op.bind(d)
+    conn = build_face_table(d, op.op_template())[0]
+    assert conn.shape == (d.K, d.dimensions + 1, 2)
