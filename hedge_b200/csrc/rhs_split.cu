@@ -72,6 +72,10 @@ hb_status ensure_fp32(Discr* d);
 #define HB_SPLIT_NCW 20
 #endif
 constexpr int NCW = HB_SPLIT_NCW;
+// coalesced update: 16-byte accesses where the alignment allows
+#ifndef HB_SPLIT_VUPD
+#define HB_SPLIT_VUPD 1
+#endif
 // face-flux phase: elements a consumer warp takes per round (0: the default
 // per dimension)
 #ifndef HB_SPLIT_ER
@@ -930,7 +934,61 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgsT<
               const ST ra = (ST)a.ra, rb = (ST)a.rb, dtt = (ST)a.dt;
               ST* res0 = a.res + g0;
               ST* qo0 = a.q_out + g0;
-              if constexpr (S::RES) {
+              // 16-byte accesses where every field's vectors share the
+              // alignment of position 0 (K Np a multiple of the vector
+              // width) and the output vectors are 16-byte aligned
+              constexpr int V = 16 / (int)sizeof(ST);
+              const bool vec = HB_SPLIT_VUPD && S::RES && Knp % V == 0 &&
+                               ((reinterpret_cast<uintptr_t>(a.res) |
+                                 reinterpret_cast<uintptr_t>(a.q_out)) & 15u) == 0;
+              if (vec) {
+                // positions [0, h) and [h + V nv, cnt) one at a time, the
+                // V-groups between as 16-byte loads and stores (the stage
+                // and residual buffers share the global offsets' alignment:
+                // their field strides and batch offsets are multiples of V)
+                using VT = typename std::conditional<sizeof(ST) == 8, double2, float4>::type;
+                const ST* rs = rbuf + e_first * NP;
+                const int h = (int)((V - (g0 & (V - 1))) & (V - 1));
+                const int nv = (cnt - h) / V;
+                const int nsc = h + (cnt - h - nv * V);      // scalar positions
+                auto one = [&](int x) {
+                  const int ro = x + (x / NP) * (F * NPR - NP);
+#pragma unroll
+                  for (int f = 0; f < F; ++f) {
+                    const ST nr = ra * rs[f * FNP + x] + dtt * (ST)rq[ro + f * NPR];
+                    res0[(int64_t)f * Knp + x] = nr;
+                    qo0[(int64_t)f * Knp + x] = qs[f * FNP + x] + rb * nr;
+                  }
+                };
+#pragma unroll 1
+                for (int m = t; m < nv; m += QT) {
+                  const int x = h + m * V;
+                  int ro[V];
+#pragma unroll
+                  for (int j = 0; j < V; ++j) ro[j] = x + j + ((x + j) / NP) * (F * NPR - NP);
+#pragma unroll
+                  for (int f = 0; f < F; ++f) {
+                    const VT qv = *reinterpret_cast<const VT*>(qs + f * FNP + x);
+                    const VT rv = *reinterpret_cast<const VT*>(rs + f * FNP + x);
+                    const ST* qa = reinterpret_cast<const ST*>(&qv);
+                    const ST* ra0 = reinterpret_cast<const ST*>(&rv);
+                    VT nrv, qov;
+                    ST* nr = reinterpret_cast<ST*>(&nrv);
+                    ST* qo = reinterpret_cast<ST*>(&qov);
+#pragma unroll
+                    for (int j = 0; j < V; ++j) {
+                      nr[j] = ra * ra0[j] + dtt * (ST)rq[ro[j] + f * NPR];
+                      qo[j] = qa[j] + rb * nr[j];
+                    }
+                    *reinterpret_cast<VT*>(res0 + (int64_t)f * Knp + x) = nrv;
+                    *reinterpret_cast<VT*>(qo0 + (int64_t)f * Knp + x) = qov;
+                  }
+                }
+                if (t >= QT - nsc) {
+                  const int j = t - (QT - nsc);
+                  one(j < h ? j : h + nv * V + (j - h));
+                }
+              } else if constexpr (S::RES) {
                 // residual from the residual buffer (short latency): one
                 // value at a time, few registers live
                 const ST* rs = rbuf + e_first * NP;
