@@ -84,6 +84,11 @@ constexpr int NCW = HB_SPLIT_NCW;
 static_assert(NCW % 4 == 0, "consumer warps must cover the TMEM quadrants evenly");
 constexpr int CONSUMERS = NCW * 32;
 constexpr int SPLIT_THREADS = CONSUMERS + 64;
+// programmatic dependent launch (the next kernel's set-up overlaps the end
+// of this one)
+#ifndef HB_SPLIT_PDL
+#define HB_SPLIT_PDL 1
+#endif
 // bounded waits (tensor core, producer/consumer hand-offs): 2 s, far above any
 // batch's time
 constexpr uint64_t MBAR_MAX_NS = 2000000000ull;
@@ -224,6 +229,9 @@ struct Shape {
 template <typename ST>
 struct SplitArgsT {
   int64_t K, nbatch, n_given;
+  // batch b starts at element bunit (b bq + min(b, brem)); the last one ends at K
+  int64_t bq, brem;
+  int bunit;
   int nperm;
   const uint8_t* ops;   // [D_hi | D_lo | L_hi | L_lo] canonical images
   const float* geo32;
@@ -246,6 +254,17 @@ struct SplitArgsT {
   int* err;
 };
 using SplitArgs = SplitArgsT<double>;
+
+// the elements of batch b: [batch_first(b), batch_first(b + 1)), the last
+// batch ending at K
+template <typename A>
+__device__ __forceinline__ int64_t batch_first(const A& a, int64_t b) {
+  return (int64_t)a.bunit * (b * a.bq + (b < a.brem ? b : a.brem));
+}
+template <typename A>
+__device__ __forceinline__ int batch_size(const A& a, int64_t b) {
+  return (int)((b + 1 >= a.nbatch ? a.K : batch_first(a, b + 1)) - batch_first(a, b));
+}
 
 // byte offset of element (row, k) in a K-major no-swizzle operand image with
 // K padded to kp: 8x8 core matrices (8 rows x 16 bytes), K chunks 128 B
@@ -453,6 +472,15 @@ __device__ __forceinline__ void bulk_wait_read() {
 __device__ __forceinline__ void bulk_wait_all() {
   asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
+// Programmatic dependent launch: wait until the preceding kernel of the
+// stream has completed and its memory is visible (a no-op without the launch
+// attribute); then allow the next kernel to be scheduled.
+__device__ __forceinline__ void grid_dep_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void grid_dep_launch() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 __device__ __forceinline__ bool aligned16(const void* p, uint32_t bytes) {
   return ((reinterpret_cast<uintptr_t>(p) | bytes) & 15u) == 0;
 }
@@ -605,6 +633,12 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgsT<
     }
     if (warp == 0) tc::tmem_alloc(tmem_slot, S::TMEM_COLS);
     tc::fence_proxy_async();
+    // launched as a programmatic dependent of the previous kernel in the
+    // stream: everything above (constant operators and tables) overlapped
+    // its last CTAs; the state, residual and data it wrote are read only
+    // after this wait; the next launch may then start its own set-up
+    grid_dep_wait();
+    grid_dep_launch();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
@@ -691,12 +725,12 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgsT<
     __syncwarp();
   } else if (warp == NCW) {
     // ====== I/O warp: stage buffers in (bulk copies), L2 prefetches ======
-    auto batch_el0 = [&](int64_t i) { return ((int64_t)blockIdx.x + i * gridDim.x) * EB; };
-    auto batch_ne = [&](int64_t el0) { return (int)((a.K - el0) < EB ? (a.K - el0) : EB); };
+    auto batch_el0 = [&](int64_t i) { return batch_first(a, (int64_t)blockIdx.x + i * gridDim.x); };
+    auto batch_ne = [&](int64_t i) { return batch_size(a, (int64_t)blockIdx.x + i * gridDim.x); };
     auto load_stage = [&](int64_t i) {
       const int b = NSTG == 2 ? (int)(i & 1) : 0;
       const int64_t el0 = batch_el0(i);
-      const int ne = batch_ne(el0);
+      const int ne = batch_ne(i);
       uint8_t* stg = smem + S::ostg + b * S::bStage;
       uint64_t* mb = &mbar[MB_FULL + b];
       if (lane == 0) {
@@ -719,7 +753,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgsT<
     };
     auto load_res = [&](int64_t i) {
       const int64_t el0 = batch_el0(i);
-      const int ne = batch_ne(el0);
+      const int ne = batch_ne(i);
       uint64_t* mb = &mbar[MB_RES_FULL];
       if (lane == 0) {
         uint32_t want = 0;
@@ -735,7 +769,7 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgsT<
     auto prefetch = [&](int64_t j, bool state, bool res) {
       if (lane != 0 || j >= nb_cta) return;
       const int64_t e0 = batch_el0(j);
-      const uint32_t bytes = (uint32_t)batch_ne(e0) * NP * (uint32_t)sizeof(ST);
+      const uint32_t bytes = (uint32_t)batch_ne(j) * NP * (uint32_t)sizeof(ST);
       for (int f = 0; f < F; ++f) {
         const ST* q = a.q_in + f * Knp + e0 * NP;
         if (state && aligned16(q, bytes)) prefetch_l2(q, bytes);
@@ -794,8 +828,8 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgsT<
     auto split = [&](uint32_t its, float (&lin_out)[DIM]) -> bool {
       const int b = NSTG == 2 ? (int)(its & 1u) : 0;
       const uint32_t par = its & 1u;
-      const int64_t el0 = ((int64_t)blockIdx.x + (int64_t)its * gridDim.x) * EB;
-      const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
+      const int64_t el0 = batch_first(a, (int64_t)blockIdx.x + (int64_t)its * gridDim.x);
+      const int ne = batch_size(a, (int64_t)blockIdx.x + (int64_t)its * gridDim.x);
       ST* st = reinterpret_cast<ST*>(smem + S::ostg + b * S::bStage);
       const bool valid = lane_used && e_lane < ne;
       const int e_own = valid ? e_lane : 0;
@@ -893,8 +927,8 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgsT<
     // (and the residual buffer) go back to the I/O warp.
     auto update = [&](uint32_t its) {
       const int b = NSTG == 2 ? (int)(its & 1u) : 0;
-      const int64_t el0 = ((int64_t)blockIdx.x + (int64_t)its * gridDim.x) * EB;
-      const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
+      const int64_t el0 = batch_first(a, (int64_t)blockIdx.x + (int64_t)its * gridDim.x);
+      const int ne = batch_size(a, (int64_t)blockIdx.x + (int64_t)its * gridDim.x);
       ST* st = reinterpret_cast<ST*>(smem + S::ostg + b * S::bStage);
       if (!bad && stage_res && !warp_wait(&mbar[MB_RES_FULL], its & 1u)) {
         if (lane == 0) atomicCAS(a.err, 0, DEV_MMA_TIMEOUT);
@@ -938,14 +972,18 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgsT<
               // alignment of position 0 (K Np a multiple of the vector
               // width) and the output vectors are 16-byte aligned
               constexpr int V = 16 / (int)sizeof(ST);
+              // (the stage and residual buffers hold the batch from their
+              // first byte: their alignment equals the global one only when
+              // the batch's first value el0 Np is a multiple of V)
               const bool vec = HB_SPLIT_VUPD && S::RES && Knp % V == 0 &&
+                               ((el0 * NP) & (V - 1)) == 0 &&
                                ((reinterpret_cast<uintptr_t>(a.res) |
                                  reinterpret_cast<uintptr_t>(a.q_out)) & 15u) == 0;
               if (vec) {
                 // positions [0, h) and [h + V nv, cnt) one at a time, the
                 // V-groups between as 16-byte loads and stores (the stage
                 // and residual buffers share the global offsets' alignment:
-                // their field strides and batch offsets are multiples of V)
+                // their field strides and el0 Np are multiples of V)
                 using VT = typename std::conditional<sizeof(ST) == 8, double2, float4>::type;
                 const ST* rs = rbuf + e_first * NP;
                 const int h = (int)((V - (g0 & (V - 1))) & (V - 1));
@@ -1052,8 +1090,8 @@ __global__ void __launch_bounds__(SPLIT_THREADS, 1) rhs_split_kernel(SplitArgsT<
     for (int64_t batch = blockIdx.x; !leave && batch < a.nbatch; batch += gridDim.x, ++it) {
       const int b = NSTG == 2 ? (int)(it & 1u) : 0;
       const uint32_t par = it & 1u;
-      const int64_t el0 = batch * EB;
-      const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
+      const int64_t el0 = batch_first(a, batch);
+      const int ne = batch_size(a, batch);
       ST* st = reinterpret_cast<ST*>(smem + S::ostg + b * S::bStage);  // [F][EB][NP]
       const uint8_t* stg = smem + S::ostg + b * S::bStage;
       const float* sgeo = reinterpret_cast<const float*>(stg + S::sGeo);
@@ -1611,6 +1649,9 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
     }
     if (warp == 0) tc::tmem_alloc(tmem_slot, S::TMEM_COLS);
     tc::fence_proxy_async();
+    // programmatic dependent launch, as in the resident kernel
+    grid_dep_wait();
+    grid_dep_launch();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
@@ -1664,8 +1705,8 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
 
   uint32_t it = 0;
   for (int64_t batch = blockIdx.x; batch < a.nbatch; batch += gridDim.x, ++it) {
-    const int64_t el0 = batch * EB;
-    const int ne = (int)((a.K - el0) < EB ? (a.K - el0) : EB);
+    const int64_t el0 = batch_first(a, batch);
+    const int ne = batch_size(a, batch);
     const bool valid = lane_used && e_lane < ne;
     const int e_own = valid ? e_lane : 0;
     uint32_t* rmx = rsq;
@@ -1780,8 +1821,8 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
         // batch's residual (the stage update), overlapping this batch's work
         const int64_t nxt = batch + gridDim.x;
         if (nxt < a.nbatch) {
-          const int64_t n0 = nxt * EB;
-          const int nn = (int)((a.K - n0) < EB ? (a.K - n0) : EB);
+          const int64_t n0 = batch_first(a, nxt);
+          const int nn = batch_size(a, nxt);
           for (int f = 0; f < F; ++f) {
             const double* src = a.q_in + f * Knp + n0 * NP;
             if (aligned16(src, (uint32_t)(nn * NP * 8))) prefetch_l2(src, (uint32_t)(nn * NP * 8));
@@ -2178,6 +2219,40 @@ static double plane_scale(const std::vector<double>& m, int pt) {
   return std::ldexp(1.0, e - 14);
 }
 
+// Batches of a persistent grid of `grid` CTAs.  ceil(K / EB) batches of EB
+// elements leave the last round partly empty (2400 batches on 148 CTAs: 16
+// rounds and 32 batches of 20 elements, so 32 CTAs run one batch more than
+// the rest).  Rounding the count up to whole rounds and spreading the
+// elements evenly over them, in units of `unit` elements (at most EB per
+// batch; the last batch also takes the K % unit elements left over), makes
+// the batches of every CTA add up to about the same work.  `unit` keeps every
+// batch's state, geometry and face-table slices 16-byte aligned (bulk copies,
+// 16-byte update accesses).  Fills nbatch, bq, brem, bunit.
+template <typename A>
+static void balance_batches(A& a, int64_t K, int EB, int unit, int grid) {
+  const int64_t nb0 = (K + EB - 1) / EB;
+  a.nbatch = nb0; a.bq = 1; a.brem = 0; a.bunit = EB;   // plain batches of EB
+  if (grid <= 0 || nb0 <= grid || unit < 1 || EB % unit != 0) return;
+  const int64_t nb = (nb0 + grid - 1) / grid * grid;
+  const int64_t units = K / unit, left = K % unit;
+  const int64_t bq = units / nb, brem = units % nb;
+  const int64_t largest = std::max<int64_t>(unit * (bq + (brem > 0 ? 1 : 0)), unit * bq + left);
+  if (bq < 1 || largest > EB) return;
+  a.nbatch = nb; a.bq = bq; a.brem = brem; a.bunit = unit;
+}
+// smallest element count whose slices of `bytes_per_element` bytes end on a
+// 16-byte boundary
+static constexpr int align_unit(int bytes_per_element) {
+  int u = 1;
+  while ((u * bytes_per_element) % 16 != 0) ++u;
+  return u;
+}
+static constexpr int lcm_small(int x, int y) {
+  int m = x;
+  while (m % y != 0) m += x;
+  return m;
+}
+
 template <int MODEL, int DIM, int ORDER, int PT, typename ST = double>
 static hb_status configure_split(Op* op) {
   using S = Shape<MODEL, DIM, ORDER, (int)sizeof(ST)>;
@@ -2307,7 +2382,12 @@ static hb_status launch_split_t(Op* op, int mode, double ra, double rb, double d
     SplitOps* so = static_cast<SplitOps*>(op->split_ops);
     SplitArgsT<ST> a;
     a.K = d->K;
-    a.nbatch = (d->K + S::EB - 1) / S::EB;
+    {
+      constexpr int unit = lcm_small(
+          lcm_small(align_unit(S::NP * (int)sizeof(ST)), align_unit(S::G * 4)),
+          lcm_small(align_unit(S::NF * 8), S::C ? align_unit(S::NP * 8) : 1));
+      balance_batches(a, d->K, S::EB, unit, op->grid);
+    }
     a.n_given = op->n_given;
     a.nperm = d->nperm;
     a.ops = so->dev;
@@ -2325,8 +2405,17 @@ static hb_status launch_split_t(Op* op, int mode, double ra, double rb, double d
     a.op_scale_l = so->scale_l;
     a.mp = op->mp;
     a.err = op->err_flag;
-    rhs_split_kernel<MODEL, DIM, ORDER, PT, ST><<<op->grid, op->threads, op->smem, s>>>(a);
-    HB_CUDA(cudaGetLastError());
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)op->grid);
+    cfg.blockDim = dim3((unsigned)op->threads);
+    cfg.dynamicSmemBytes = op->smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = HB_SPLIT_PDL ? 1 : 0;
+    HB_CUDA(cudaLaunchKernelEx(&cfg, rhs_split_kernel<MODEL, DIM, ORDER, PT, ST>, a));
     return HB_OK;
   }
 }
@@ -2457,7 +2546,11 @@ static hb_status launch_stream_t(Op* op, int mode, double ra, double rb, double 
     SplitOps* so = static_cast<SplitOps*>(op->split_ops);
     SplitArgs a;
     a.K = d->K;
-    a.nbatch = (d->K + S::EB - 1) / S::EB;
+    {
+      constexpr int unit = lcm_small(lcm_small(align_unit(S::NP * 8), align_unit(S::G * 4)),
+                                     align_unit(S::NF * 8));
+      balance_batches(a, d->K, S::EB, unit, op->grid);
+    }
     a.n_given = op->n_given;
     a.nperm = d->nperm;
     a.ops = so->dev;
@@ -2472,8 +2565,17 @@ static hb_status launch_stream_t(Op* op, int mode, double ra, double rb, double 
     a.op_scale_l = so->scale_l;
     a.mp = op->mp;
     a.err = op->err_flag;
-    rhs_split_stream_kernel<MODEL, DIM, ORDER, PT><<<op->grid, op->threads, op->smem, s>>>(a);
-    HB_CUDA(cudaGetLastError());
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)op->grid);
+    cfg.blockDim = dim3((unsigned)op->threads);
+    cfg.dynamicSmemBytes = op->smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = HB_SPLIT_PDL ? 1 : 0;
+    HB_CUDA(cudaLaunchKernelEx(&cfg, rhs_split_stream_kernel<MODEL, DIM, ORDER, PT>, a));
     return HB_OK;
   }
 }
