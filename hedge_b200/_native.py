@@ -62,7 +62,8 @@ class hb_op_desc(C.Structure):
 
 EXPORTED = [
     "hb_discr_create", "hb_discr_destroy", "hb_op_create", "hb_op_destroy",
-    "hb_rhs", "hb_lsrk_stage", "hb_lincomb", "hb_gather_map", "hb_op_check",
+    "hb_rhs", "hb_lsrk_stage", "hb_rhs_elements", "hb_lsrk_stage_elements", "hb_lincomb",
+    "hb_gather_map", "hb_op_check",
     "hb_op_launch_info", "hb_norm", "hb_norm_noalloc", "hb_rhs_adjoint_work_size",
     "hb_rhs_adjoint", "hb_batch_create", "hb_batch_destroy", "hb_batch_stage",
     "hb_batch_info", "hb_batch_check", "hb_op_set_halo", "hb_pack",
@@ -92,6 +93,8 @@ def load(path=LIB_PATH):
             "hb_op_destroy": [vp],
             "hb_rhs": [vp, vp, vp, vp, vp, vp, vp],
             "hb_lsrk_stage": [vp, d, d, d, vp, vp, vp, vp, vp, vp, vp],
+            "hb_rhs_elements": [vp, i64, i64, vp, vp, vp, vp, vp, vp],
+            "hb_lsrk_stage_elements": [vp, i64, i64, d, d, d, vp, vp, vp, vp, vp, vp, vp],
             "hb_lincomb": [i64, i32, d, vp, d, vp, vp, vp],
             "hb_gather_map": [vp, vp, vp, vp],
             "hb_op_check": [vp, vp],

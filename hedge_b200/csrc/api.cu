@@ -84,7 +84,8 @@ hb_status launch_lincomb(int64_t n, int dtype, double a, const void* x, double b
 hb_status prepare_split(Op* op);
 hb_status launch_split(Op* op, int mode, double ra, double rb, double dt,
                        const void* q_in, void* q_out, void* res, const double* coeff,
-                       const double* bdry, const double* source, cudaStream_t s);
+                       const double* bdry, const double* source, int64_t e0, int64_t e1,
+                       cudaStream_t s);
 void free_split(Op* op);
 hb_status launch_wait_selftest(int* err, uint64_t limit_ns, cudaStream_t s);
 
@@ -348,15 +349,26 @@ static hb_status check_inputs(Op* op, const void* q_in, const void* q_out,
 
 static hb_status run(Op* op, int mode, double a, double b, double dt, const void* q_in,
                      void* q_out, void* res, const double* coeff, const double* bdry,
-                     const double* source, void* stream) {
+                     const double* source, void* stream, int64_t e0 = 0, int64_t e1 = -1) {
   DeviceGuard g(op->d->device);
   if (!g.ok) return fail(HB_ERR_CUDA, "cannot select the CUDA device");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  if (op->model == HB_MODEL_VARADV)
+  const bool whole = e0 == 0 && (e1 < 0 || e1 == op->d->K);
+  if (e1 < 0) e1 = op->d->K;
+  if (e0 == e1) return HB_OK;
+  if (op->model == HB_MODEL_VARADV) {
+    if (!whole) return fail(HB_ERR_UNSUPPORTED, "element ranges: not on the quadrature kernel");
     return launch_quad(op, mode, a, b, dt, q_in, q_out, res, coeff, bdry, s);
+  }
   if (op->split)
-    return launch_split(op, mode, a, b, dt, q_in, q_out, res, coeff, bdry, source, s);
-  return launch_simt(op, mode, a, b, dt, q_in, q_out, res, coeff, bdry, source, s);
+    return launch_split(op, mode, a, b, dt, q_in, q_out, res, coeff, bdry, source, e0, e1, s);
+  return launch_simt(op, mode, a, b, dt, q_in, q_out, res, coeff, bdry, source, e0, e1, s);
+}
+
+static hb_status check_range(Op* op, int64_t e0, int64_t e1) {
+  if (e0 < 0 || e1 < e0 || e1 > op->d->K)
+    return fail(HB_ERR_INVALID_ARGUMENT, "element range outside [0, K]");
+  return HB_OK;
 }
 
 hb_status hb_rhs(hb_op* handle, const void* q, void* rhs, const double* coeff,
@@ -377,6 +389,30 @@ hb_status hb_lsrk_stage(hb_op* handle, double a, double b, double dt, const void
   if (st) return st;
   if (!res) return fail(HB_ERR_INVALID_ARGUMENT, "null residual pointer");
   return run(op, 1, a, b, dt, q_in, q_out, res, coeff, bdry, source, stream);
+}
+
+hb_status hb_rhs_elements(hb_op* handle, int64_t el_begin, int64_t el_end, const void* q,
+                          void* rhs, const double* coeff, const double* bdry,
+                          const double* source, void* stream) {
+  if (!handle) return fail(HB_ERR_INVALID_ARGUMENT, "null operator");
+  Op* op = reinterpret_cast<Op*>(handle);
+  hb_status st = check_inputs(op, q, rhs, coeff);
+  if (st) return st;
+  if ((st = check_range(op, el_begin, el_end))) return st;
+  return run(op, 0, 0, 0, 0, q, rhs, nullptr, coeff, bdry, source, stream, el_begin, el_end);
+}
+
+hb_status hb_lsrk_stage_elements(hb_op* handle, int64_t el_begin, int64_t el_end, double a,
+                                 double b, double dt, const void* q_in, void* q_out,
+                                 void* res, const double* coeff, const double* bdry,
+                                 const double* source, void* stream) {
+  if (!handle) return fail(HB_ERR_INVALID_ARGUMENT, "null operator");
+  Op* op = reinterpret_cast<Op*>(handle);
+  hb_status st = check_inputs(op, q_in, q_out, coeff);
+  if (st) return st;
+  if (!res) return fail(HB_ERR_INVALID_ARGUMENT, "null residual pointer");
+  if ((st = check_range(op, el_begin, el_end))) return st;
+  return run(op, 1, a, b, dt, q_in, q_out, res, coeff, bdry, source, stream, el_begin, el_end);
 }
 
 hb_status hb_lincomb(int64_t n, int32_t dtype, double a, const void* x, double b,

@@ -124,10 +124,11 @@ hb_status launch_pack(int64_t n, int dtype, int nfields, int64_t field_stride,
                       const int64_t* idx, const void* src, void* dst, cudaStream_t s);
 
 // kernel launchers (rhs_simt.cu)
+// e0, e1: the elements [e0, e1) the launch updates
 hb_status launch_simt(Op* op, int mode, double a, double b, double dt,
                       const void* q_in, void* q_out, void* res,
                       const double* coeff, const double* bdry,
-                      const double* source, cudaStream_t s);
+                      const double* source, int64_t e0, int64_t e1, cudaStream_t s);
 hb_status prepare_simt(Op* op);
 
 // quadrature kernel (rhs_quad.cu); vel = the velocity field [dim][K*Np]

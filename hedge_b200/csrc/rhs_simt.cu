@@ -29,6 +29,7 @@ namespace hb {
 template <typename T, typename S>
 struct SimtArgs {
   int64_t K, nbatch, n_given;
+  int64_t e_begin, e_end;   // the elements this launch updates (of K)
   int np, nfp, nf, nperm, G, E;
   const T* dmats_t;
   const T* lift_t;
@@ -137,8 +138,8 @@ __global__ void __launch_bounds__(256) rhs_simt_kernel(SimtArgs<T, S> a) {
   const int64_t Knp = a.K * np;
 
   for (int64_t batch = blockIdx.x; batch < a.nbatch; batch += gridDim.x) {
-    const int64_t el0 = batch * E;
-    const int ne = (int)((a.K - el0) < E ? (a.K - el0) : E);
+    const int64_t el0 = a.e_begin + batch * E;
+    const int ne = (int)((a.e_end - el0) < E ? (a.e_end - el0) : E);
     __syncthreads();  // previous batch done with shared buffers
     for (int f = 0; f < F; ++f) {
       const S* src = a.q_in + f * Knp + el0 * np;
@@ -299,7 +300,8 @@ template <int MODEL, int DIM, typename T, typename S>
 static hb_status launch_one(Op* op, int mode, double ra, double rb, double dt,
                             const void* q_in, void* q_out, void* res,
                             const double* coeff, const double* bdry,
-                            const double* source, cudaStream_t s, bool configure) {
+                            const double* source, int64_t e0, int64_t e1, cudaStream_t s,
+                            bool configure) {
   auto kern = rhs_simt_kernel<MODEL, DIM, T, S>;
   Discr* d = op->d;
   if (configure) {
@@ -337,8 +339,10 @@ static hb_status launch_one(Op* op, int mode, double ra, double rb, double dt,
   }
   SimtArgs<T, S> a;
   a.K = d->K;
+  a.e_begin = e0;
+  a.e_end = e1;
   a.E = op->elems_per_block;
-  a.nbatch = (d->K + a.E - 1) / a.E;
+  a.nbatch = (e1 - e0 + a.E - 1) / a.E;
   a.n_given = op->n_given;
   a.np = d->np; a.nfp = d->nfp; a.nf = d->nfaces; a.nperm = d->nperm; a.G = d->G;
   if constexpr (sizeof(T) == 8) {
@@ -359,7 +363,7 @@ static hb_status launch_one(Op* op, int mode, double ra, double rb, double dt,
   a.ops_in_smem = op->ops_in_smem;
   a.mp = op->mp;
   a.err = op->err_flag;
-  kern<<<op->grid, op->threads, op->smem, s>>>(a);
+  kern<<<(unsigned)std::min<int64_t>(op->grid, a.nbatch), op->threads, op->smem, s>>>(a);
   HB_CUDA(cudaGetLastError());
   return HB_OK;
 }
@@ -368,12 +372,13 @@ template <typename T, typename S>
 static hb_status dispatch(Op* op, int mode, double ra, double rb, double dt,
                           const void* q_in, void* q_out, void* res,
                           const double* coeff, const double* bdry,
-                          const double* source, cudaStream_t s, bool configure) {
+                          const double* source, int64_t e0, int64_t e1, cudaStream_t s,
+                          bool configure) {
   const int dim = op->d->dim;
 #define HB_CASE(M, D)                                                          \
   if (op->model == M && dim == D)                                              \
     return launch_one<M, D, T, S>(op, mode, ra, rb, dt, q_in, q_out, res,      \
-                                  coeff, bdry, source, s, configure);
+                                  coeff, bdry, source, e0, e1, s, configure);
   HB_CASE(HB_MODEL_ADVECTION, 2)
   HB_CASE(HB_MODEL_ADVECTION, 3)
   HB_CASE(HB_MODEL_WAVE, 2)
@@ -390,20 +395,20 @@ static hb_status dispatch(Op* op, int mode, double ra, double rb, double dt,
 hb_status prepare_simt(Op* op) {
   if (op->precision == HB_PREC_FP32)
     return dispatch<float, float>(op, 0, 0, 0, 0, nullptr, nullptr, nullptr,
-                                  nullptr, nullptr, nullptr, 0, true);
+                                  nullptr, nullptr, nullptr, 0, op->d->K, 0, true);
   return dispatch<double, double>(op, 0, 0, 0, 0, nullptr, nullptr, nullptr,
-                                  nullptr, nullptr, nullptr, 0, true);
+                                  nullptr, nullptr, nullptr, 0, op->d->K, 0, true);
 }
 
 hb_status launch_simt(Op* op, int mode, double ra, double rb, double dt,
                       const void* q_in, void* q_out, void* res,
                       const double* coeff, const double* bdry,
-                      const double* source, cudaStream_t s) {
+                      const double* source, int64_t e0, int64_t e1, cudaStream_t s) {
   if (op->precision == HB_PREC_FP32)
     return dispatch<float, float>(op, mode, ra, rb, dt, q_in, q_out, res, coeff,
-                                  bdry, source, s, false);
+                                  bdry, source, e0, e1, s, false);
   return dispatch<double, double>(op, mode, ra, rb, dt, q_in, q_out, res, coeff,
-                                  bdry, source, s, false);
+                                  bdry, source, e0, e1, s, false);
 }
 
 // ---------------------------------------------------------------------------

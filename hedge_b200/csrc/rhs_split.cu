@@ -229,7 +229,10 @@ struct Shape {
 template <typename ST>
 struct SplitArgsT {
   int64_t K, nbatch, n_given;
-  // batch b starts at element bunit (b bq + min(b, brem)); the last one ends at K
+  // the elements [e_begin, e_end) this launch updates (of K); batch b starts
+  // at element e_begin + bunit (b bq + min(b, brem)), the last one ends at
+  // e_end
+  int64_t e_begin, e_end;
   int64_t bq, brem;
   int bunit;
   int nperm;
@@ -259,11 +262,11 @@ using SplitArgs = SplitArgsT<double>;
 // batch ending at K
 template <typename A>
 __device__ __forceinline__ int64_t batch_first(const A& a, int64_t b) {
-  return (int64_t)a.bunit * (b * a.bq + (b < a.brem ? b : a.brem));
+  return a.e_begin + (int64_t)a.bunit * (b * a.bq + (b < a.brem ? b : a.brem));
 }
 template <typename A>
 __device__ __forceinline__ int batch_size(const A& a, int64_t b) {
-  return (int)((b + 1 >= a.nbatch ? a.K : batch_first(a, b + 1)) - batch_first(a, b));
+  return (int)((b + 1 >= a.nbatch ? a.e_end : batch_first(a, b + 1)) - batch_first(a, b));
 }
 
 // byte offset of element (row, k) in a K-major no-swizzle operand image with
@@ -1870,7 +1873,31 @@ __global__ void __launch_bounds__(256, 1) rhs_split_stream_kernel(SplitArgs a) {
       const int nb = cn.x;
       const int64_t gm = (el0 + e) * NP + lnode;
       bool have = true, bdry = false;
-      if (nb >= 0) {
+      if (nb >= a.K) {
+        // neighbour on another partition: ext values from the halo buffer
+        if (nb - a.K >= a.n_halo || a.halo == nullptr) {
+          atomicCAS(a.err, 0, DEV_BAD_NEIGHBOUR);
+          return false;
+        }
+        const int64_t hk = ((int64_t)nb - a.K) * NFP + k;
+        if constexpr (JumpLinear<MODEL>::value) {
+#pragma unroll
+          for (int f = 0; f < F; ++f) {
+            uM[f] = (float)(__ldg(a.q_in + f * Knp + gm) - a.halo[hk * F + f]);
+            uP[f] = 0.f;
+          }
+        } else {
+          if constexpr (C != 0) {
+            uM[0] = scoef[e * NP + lnode];
+            uP[0] = (float)a.halo_c[hk];
+          }
+#pragma unroll
+          for (int f = 0; f < F; ++f) {
+            uM[C + f] = (float)__ldg(a.q_in + f * Knp + gm);
+            uP[C + f] = (float)a.halo[hk * F + f];
+          }
+        }
+      } else if (nb >= 0) {
         const int nface = cn.y & 3, perm = cn.y >> 2;
         if (!(nface < NF && perm < a.nperm && nb < a.K)) {
           atomicCAS(a.err, 0, DEV_BAD_CODE);
@@ -2373,7 +2400,8 @@ template <int MODEL, int DIM, int ORDER, int PT, typename ST = double>
 static hb_status launch_split_t(Op* op, int mode, double ra, double rb, double dt,
                                 const void* q_in, void* q_out, void* res,
                                 const double* coeff, const double* bdry,
-                                const double* source, cudaStream_t s) {
+                                const double* source, int64_t e0, int64_t e1,
+                                cudaStream_t s) {
   using S = Shape<MODEL, DIM, ORDER, (int)sizeof(ST)>;
   if constexpr (!S::FITS) {
     return fail(HB_ERR_UNSUPPORTED, "BF16x3 kernel: element beyond one MMA");
@@ -2382,11 +2410,13 @@ static hb_status launch_split_t(Op* op, int mode, double ra, double rb, double d
     SplitOps* so = static_cast<SplitOps*>(op->split_ops);
     SplitArgsT<ST> a;
     a.K = d->K;
+    a.e_begin = e0;
+    a.e_end = e1;
     {
       constexpr int unit = lcm_small(
           lcm_small(align_unit(S::NP * (int)sizeof(ST)), align_unit(S::G * 4)),
           lcm_small(align_unit(S::NF * 8), S::C ? align_unit(S::NP * 8) : 1));
-      balance_batches(a, d->K, S::EB, unit, op->grid);
+      balance_batches(a, e1 - e0, S::EB, unit, op->grid);
     }
     a.n_given = op->n_given;
     a.nperm = d->nperm;
@@ -2406,7 +2436,7 @@ static hb_status launch_split_t(Op* op, int mode, double ra, double rb, double d
     a.mp = op->mp;
     a.err = op->err_flag;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)op->grid);
+    cfg.gridDim = dim3((unsigned)std::min<int64_t>(op->grid, a.nbatch));
     cfg.blockDim = dim3((unsigned)op->threads);
     cfg.dynamicSmemBytes = op->smem;
     cfg.stream = s;
@@ -2455,8 +2485,6 @@ static hb_status configure_stream(Op* op) {
   } else {
     if (d->np != S::NP || d->nfp != S::NFP)
       return fail(HB_ERR_INVALID_ARGUMENT, "element sizes do not match the order");
-    if (op->n_halo > 0)
-      return fail(HB_ERR_UNSUPPORTED, "halo faces: not on the streamed high-order split kernel");
     auto kern = rhs_split_stream_kernel<MODEL, DIM, ORDER, PT>;
     int dev, max_optin = 0, sms = 0;
     HB_CUDA(cudaGetDevice(&dev));
@@ -2537,7 +2565,8 @@ template <int MODEL, int DIM, int ORDER, int PT>
 static hb_status launch_stream_t(Op* op, int mode, double ra, double rb, double dt,
                                  const void* q_in, void* q_out, void* res,
                                  const double* coeff, const double* bdry,
-                                 const double* source, cudaStream_t s) {
+                                 const double* source, int64_t e0, int64_t e1,
+                                 cudaStream_t s) {
   using S = ShapeS<MODEL, DIM, ORDER>;
   if constexpr (!S::FITS) {
     return fail(HB_ERR_UNSUPPORTED, "split kernel: element too large for the streamed variant");
@@ -2546,10 +2575,12 @@ static hb_status launch_stream_t(Op* op, int mode, double ra, double rb, double 
     SplitOps* so = static_cast<SplitOps*>(op->split_ops);
     SplitArgs a;
     a.K = d->K;
+    a.e_begin = e0;
+    a.e_end = e1;
     {
       constexpr int unit = lcm_small(lcm_small(align_unit(S::NP * 8), align_unit(S::G * 4)),
                                      align_unit(S::NF * 8));
-      balance_batches(a, d->K, S::EB, unit, op->grid);
+      balance_batches(a, e1 - e0, S::EB, unit, op->grid);
     }
     a.n_given = op->n_given;
     a.nperm = d->nperm;
@@ -2560,13 +2591,16 @@ static hb_status launch_stream_t(Op* op, int mode, double ra, double rb, double 
     a.q_out = static_cast<double*>(q_out);
     a.res = static_cast<double*>(res);
     a.coeff = coeff; a.bdry = bdry; a.source = source;
+    a.halo = static_cast<const double*>(op->halo);
+    a.halo_c = op->halo_c;
+    a.n_halo = op->n_halo;
     a.ra = ra; a.rb = rb; a.dt = dt; a.mode = mode;
     a.op_scale_d = so->scale_d;
     a.op_scale_l = so->scale_l;
     a.mp = op->mp;
     a.err = op->err_flag;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)op->grid);
+    cfg.gridDim = dim3((unsigned)std::min<int64_t>(op->grid, a.nbatch));
     cfg.blockDim = dim3((unsigned)op->threads);
     cfg.dynamicSmemBytes = op->smem;
     cfg.stream = s;
@@ -2596,10 +2630,10 @@ static hb_status launch_stream_t(Op* op, int mode, double ra, double rb, double 
   X(HB_MODEL_VARWAVE, 2, 6) X(HB_MODEL_VARWAVE, 3, 3) X(HB_MODEL_VARWAVE, 3, 4)        \
   X(HB_MODEL_MAXWELL, 3, 3) X(HB_MODEL_MAXWELL, 3, 4) X(HB_MODEL_MAXWELL, 3, 5)
 
-// Operators without halo faces take the streamed-operator kernel where it is
-// built: at 3D N = 5 the resident kernel's operator planes leave room for one
-// state stage and no residual buffer, and the streamed kernel is 13-14 %
-// faster there.  Halo faces need the resident kernel.
+// The streamed-operator kernel serves the instances it is built for (with or
+// without halo faces): at 3D N = 5 the resident kernel's operator planes
+// leave room for one state stage and no residual buffer, and the streamed
+// kernel is 13-14 % faster there; at N >= 6 it is the only one.
 hb_status prepare_split(Op* op) {
   Discr* d = op->d;
   hb_status st = ensure_fp32(d);
@@ -2617,7 +2651,7 @@ hb_status prepare_split(Op* op) {
     return fail(HB_ERR_UNSUPPORTED, "no FP32-state tensor-core kernel for this instance");
   }
   const int pt = op->precision == HB_PREC_FP16X3 ? PT_FP16 : PT_BF16;
-  if (op->n_halo == 0) {
+  {
     // a streamed variant that this device refuses (e.g. its shared memory)
     // falls back to the resident kernel where one is built
     bool tried = false;
@@ -2645,13 +2679,6 @@ hb_status prepare_split(Op* op) {
                          : configure_split<M, D, O, PT_BF16>(op);
   HB_SPLIT_INSTANCES(HB_CASE)
 #undef HB_CASE
-  // (with halo faces: reports that the streamed kernel takes none)
-#define HB_CASE(M, D, O)                                                       \
-  if (op->model == M && dim == D && order == O)                                \
-    return pt == PT_FP16 ? configure_stream<M, D, O, PT_FP16>(op)              \
-                         : configure_stream<M, D, O, PT_BF16>(op);
-  HB_SPLIT_STREAM_INSTANCES(HB_CASE)
-#undef HB_CASE
   return fail(HB_ERR_UNSUPPORTED,
               "split path: this (model, dimension, order) is not built (see "
               "HB_SPLIT_INSTANCES, HB_SPLIT_STREAM_INSTANCES)");
@@ -2659,7 +2686,8 @@ hb_status prepare_split(Op* op) {
 
 hb_status launch_split(Op* op, int mode, double ra, double rb, double dt,
                        const void* q_in, void* q_out, void* res, const double* coeff,
-                       const double* bdry, const double* source, cudaStream_t s) {
+                       const double* bdry, const double* source, int64_t e0, int64_t e1,
+                       cudaStream_t s) {
   const int dim = op->d->dim, order = op->d->order;
   const int pt = op->precision == HB_PREC_FP16X3 ? PT_FP16 : PT_BF16;
   const SplitOps* so = static_cast<const SplitOps*>(op->split_ops);
@@ -2668,7 +2696,7 @@ hb_status launch_split(Op* op, int mode, double ra, double rb, double dt,
 #define HB_CASE(M, D, O)                                                              \
   if (op->model == M && dim == D && order == O)                                       \
     return launch_split_t<M, D, O, PT_FP16, float>(op, mode, ra, rb, dt, q_in, q_out,  \
-                                                   res, coeff, bdry, source, s);
+                                                   res, coeff, bdry, source, e0, e1, s);
     HB_SPLIT_INSTANCES(HB_CASE)
 #undef HB_CASE
     return fail(HB_ERR_UNSUPPORTED, "model/dimension/order combination not built");
@@ -2678,9 +2706,9 @@ hb_status launch_split(Op* op, int mode, double ra, double rb, double dt,
   if (op->model == M && dim == D && order == O)                                       \
     return pt == PT_FP16                                                              \
                ? launch_stream_t<M, D, O, PT_FP16>(op, mode, ra, rb, dt, q_in, q_out, \
-                                                   res, coeff, bdry, source, s)       \
+                                                   res, coeff, bdry, source, e0, e1, s) \
                : launch_stream_t<M, D, O, PT_BF16>(op, mode, ra, rb, dt, q_in, q_out, \
-                                                   res, coeff, bdry, source, s);
+                                                   res, coeff, bdry, source, e0, e1, s);
     HB_SPLIT_STREAM_INSTANCES(HB_CASE)
 #undef HB_CASE
   } else {
@@ -2688,9 +2716,9 @@ hb_status launch_split(Op* op, int mode, double ra, double rb, double dt,
   if (op->model == M && dim == D && order == O)                                       \
     return pt == PT_FP16                                                              \
                ? launch_split_t<M, D, O, PT_FP16>(op, mode, ra, rb, dt, q_in, q_out,  \
-                                                  res, coeff, bdry, source, s)        \
+                                                  res, coeff, bdry, source, e0, e1, s) \
                : launch_split_t<M, D, O, PT_BF16>(op, mode, ra, rb, dt, q_in, q_out,  \
-                                                  res, coeff, bdry, source, s);
+                                                  res, coeff, bdry, source, e0, e1, s);
     HB_SPLIT_INSTANCES(HB_CASE)
 #undef HB_CASE
   }

@@ -18,8 +18,14 @@ side, sends each rank's traces on the cut faces to the neighbouring rank
   the values to send, an exchange object moves them into the halo buffer
   (``DistExchange``: torch.distributed point-to-point, NCCL between GPUs or
   gloo on CPU tensors; ``LocalExchange``: all parts in one process), and the
-  CUDA-core right-hand side / LSRK stage kernels read the halo faces from it
-  (hb_op_set_halo).
+  right-hand side / LSRK stage kernels read the halo faces from it
+  (hb_op_set_halo).  A part numbers its elements without halo faces first:
+  with a ``DistExchange`` a stage packs the traces, posts the exchange,
+  launches the kernel on those elements while the traces are in flight,
+  makes the stream wait for the exchange and launches it on the elements
+  with halo faces (hb_lsrk_stage_elements) -- the reference's futures
+  (hedge/backends/mpi/__init__.py:184-216, hedge/compiler.py:414-467) on
+  CUDA streams.
 """
 
 from __future__ import annotations
@@ -63,13 +69,15 @@ def partition_elements(discr, nparts):
 
 
 class PartPlan:
-    """One part's view: owned elements (global ids, ascending), local face
-    table, halo receive counts per source part and send lists per
-    destination part (local volume node indices)."""
+    """One part's view: owned elements (global ids; those without halo faces
+    first, each group ascending), local face table, halo receive counts per
+    source part and send lists per destination part (local volume node
+    indices)."""
 
     def __init__(self, rank):
         self.rank = rank
-        self.elements = None
+        self.elements = None      # owned elements: without halo faces, then with
+        self.n_interior = 0       # how many have no halo face
         self.conn = None
         self.n_halo_faces = 0
         self.recv_nodes = {}      # source part -> halo nodes received from it
@@ -91,8 +99,15 @@ class PartitionPlan:
         shuffle = np.asarray(ld.face_shuffle_table)
         local_index = np.empty(K, dtype=np.int64)
         self.parts = [PartPlan(r) for r in range(nparts)]
+        nbr_all = conn[..., 0].astype(np.int64)
+        cut = (nbr_all >= 0) & (self.owner[np.maximum(nbr_all, 0)] != self.owner[:, None])
+        cut_el = cut.any(1)                       # elements with a halo face
         for r, p in enumerate(self.parts):
-            p.elements = np.nonzero(self.owner == r)[0]
+            own = np.nonzero(self.owner == r)[0]
+            # elements without halo faces first (launched while the traces
+            # are exchanged), then those with halo faces
+            p.elements = np.concatenate([own[~cut_el[own]], own[cut_el[own]]])
+            p.n_interior = int((~cut_el[own]).sum())
             local_index[p.elements] = np.arange(len(p.elements))
         for r, p in enumerate(self.parts):
             E = p.elements
@@ -139,7 +154,10 @@ class DistExchange:
     def __init__(self, plan, rank, group=None):
         self.plan, self.rank, self.group = plan, rank, group
 
-    def __call__(self, send, halo):
+    def start(self, send, halo):
+        """Posts the sends and receives; returns their requests.  With NCCL
+        the transfers run on NCCL's stream once the current stream's work
+        (the pack) is done, so kernels launched meanwhile overlap them."""
         import torch.distributed as dist
         p = self.plan.parts[self.rank]
         ops = []
@@ -153,9 +171,17 @@ class DistExchange:
             n = p.recv_nodes[s]
             ops.append(dist.P2POp(dist.irecv, halo[off:off + n], s, group=self.group))
             off += n
-        if ops:
-            for req in dist.batch_isend_irecv(ops):
-                req.wait()
+        return dist.batch_isend_irecv(ops) if ops else []
+
+    @staticmethod
+    def finish(reqs):
+        """Waits for the requests (NCCL: the current stream waits; the host
+        does not)."""
+        for req in reqs:
+            req.wait()
+
+    def __call__(self, send, halo):
+        self.finish(self.start(send, halo))
 
 
 def sum_over_ranks(value, group=None, device=None):
@@ -204,7 +230,7 @@ class LocalExchange:
 
 class PartitionedOperator:
     """One part of an element-partitioned model operator on one device
-    (any precision path; the split ones below order 6 in 3D)."""
+    (any precision path)."""
 
     def __init__(self, discr, model, plan, rank, precision="fp64", device=None, exchange=None):
         torch = _torch()
@@ -214,6 +240,7 @@ class PartitionedOperator:
         self.F = ot.n_fields
         self.Np = discr.Np
         self.K = len(p.elements)
+        self.n_interior = p.n_interior
         self.device = torch.device(device) if device is not None else discr.device
         prec = {"fp64": _native.PREC_FP64, "fp32": _native.PREC_FP32,
                 "fp32-simt": _native.PREC_FP32_SIMT,
@@ -308,26 +335,48 @@ class PartitionedOperator:
         if self.exchange is not None:
             self.exchange(self.send[:self.n_send], self.halo)
 
-    def rhs(self, q, exchanged=False):
-        """RHS of this part's elements; the halo is refreshed first unless
-        ``exchanged`` (a LocalExchange already filled it)."""
-        torch = _torch()
+    def _run(self, launch, q, exchanged, by_ranges):
+        """``launch(e0, e1)`` over this part's elements, the halo refreshed
+        from ``q`` first unless ``exchanged`` (a LocalExchange already filled
+        it).  A DistExchange overlaps the transfer with the launch on the
+        elements without halo faces; ``by_ranges`` launches the two element
+        ranges separately after an exchange that is already done."""
+        if not exchanged and self.exchange is not None and hasattr(self.exchange, "start"):
+            self.pack(q)
+            reqs = self.exchange.start(self.send[:self.n_send], self.halo)
+            launch(0, self.n_interior)
+            self.exchange.finish(reqs)
+            launch(self.n_interior, self.K)
+            return
         if not exchanged:
             self._exchange(q)
+        if by_ranges:
+            launch(0, self.n_interior)
+            launch(self.n_interior, self.K)
+        else:
+            launch(0, self.K)
+
+    def rhs(self, q, exchanged=False, by_ranges=False):
+        """RHS of this part's elements."""
+        torch = _torch()
         out = torch.empty_like(q)
-        _native.check(self.lib.hb_rhs(
-            self._h, q.data_ptr(), out.data_ptr(),
-            self.coeff.data_ptr() if self.coeff is not None else None, None, None,
-            self._stream()))
+        coeff = self.coeff.data_ptr() if self.coeff is not None else None
+
+        def launch(e0, e1):
+            _native.check(self.lib.hb_rhs_elements(
+                self._h, e0, e1, q.data_ptr(), out.data_ptr(), coeff, None, None,
+                self._stream()))
+        self._run(launch, q, exchanged, by_ranges)
         return out
 
-    def lsrk_stage(self, a, b, dt, q_in, q_out, res, exchanged=False):
-        if not exchanged:
-            self._exchange(q_in)
-        _native.check(self.lib.hb_lsrk_stage(
-            self._h, float(a), float(b), float(dt), q_in.data_ptr(), q_out.data_ptr(),
-            res.data_ptr(), self.coeff.data_ptr() if self.coeff is not None else None, None,
-            None, self._stream()))
+    def lsrk_stage(self, a, b, dt, q_in, q_out, res, exchanged=False, by_ranges=False):
+        coeff = self.coeff.data_ptr() if self.coeff is not None else None
+
+        def launch(e0, e1):
+            _native.check(self.lib.hb_lsrk_stage_elements(
+                self._h, e0, e1, float(a), float(b), float(dt), q_in.data_ptr(),
+                q_out.data_ptr(), res.data_ptr(), coeff, None, None, self._stream()))
+        self._run(launch, q_in, exchanged, by_ranges)
 
     def check(self):
         _native.check(self.lib.hb_op_check(self._h, self._stream()))

@@ -156,6 +156,24 @@ hb_status hb_lsrk_stage(hb_op* op, double a, double b, double dt,
                         const double* coeff, const double* bdry,
                         const double* source, void* stream);
 
+/* hb_rhs / hb_lsrk_stage for the elements [el_begin, el_end) of the
+ * operator's K only (the other elements' outputs are left as they are; the
+ * inputs are the whole [F][K*Np] vectors).  They split one stage of an
+ * element partition into the elements without halo faces, launched while
+ * the face traces of the cut faces are exchanged, and the elements with
+ * halo faces, launched once the halo buffer is filled: the reference posts
+ * its trace exchange as futures and evaluates the local terms in between
+ * (hedge/backends/mpi/__init__.py:184-216, hedge/compiler.py:414-467).
+ * HB_ERR_INVALID_ARGUMENT for a range outside [0, K]; HB_ERR_UNSUPPORTED
+ * for a partial range of the quadrature operator. */
+hb_status hb_rhs_elements(hb_op* op, int64_t el_begin, int64_t el_end, const void* q,
+                          void* rhs, const double* coeff, const double* bdry,
+                          const double* source, void* stream);
+hb_status hb_lsrk_stage_elements(hb_op* op, int64_t el_begin, int64_t el_end, double a,
+                                 double b, double dt, const void* q_in, void* q_out,
+                                 void* res, const double* coeff, const double* bdry,
+                                 const double* source, void* stream);
+
 /* out = a*x + b*y, n elements of dtype (0 = FP64, 1 = FP32).  Replaces
  * NumpyLinearCombiner (hedge/vector_primitives.py:58-77). */
 hb_status hb_lincomb(int64_t n, int32_t dtype, double a, const void* x,
@@ -257,8 +275,8 @@ hb_status hb_batch_check(hb_batch* batch, void* stream);
  * this face's node order) and, for the variable-velocity wave, halo_coeff
  * [num_halo_faces * nfp].  Both are device buffers of the caller, refreshed
  * between stages (typically by hb_pack on the owner + a point-to-point
- * exchange).  All paths except the streamed high-order split kernel (3D,
- * N >= 6).  Replaces the reference's MPI face-trace
+ * exchange).  Every kernel path reads it (CUDA cores, the resident and the
+ * streamed split kernels).  Replaces the reference's MPI face-trace
  * exchange (hedge/backends/mpi/__init__.py:184-216, 284-340). */
 hb_status hb_op_set_halo(hb_op* op, const void* halo, const double* halo_coeff);
 

@@ -26,9 +26,10 @@ def _setup(kind, nparts, precision):
     return d, model, plan, parts, LocalExchange(plan, parts)
 
 
+@pytest.mark.parametrize("by_ranges", [False, True])
 @pytest.mark.parametrize("kind", ["maxwell", "varwave"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32-simt", "fp16x3", "bf16x3"])
-def test_partitioned_rhs_equals_global(cuda_device, kind, precision):
+def test_partitioned_rhs_equals_global(cuda_device, kind, precision, by_ranges):
     import torch
     d, model, plan, parts, ex = _setup(kind, 3, precision)
     F = model.descriptor().n_fields
@@ -42,7 +43,7 @@ def test_partitioned_rhs_equals_global(cuda_device, kind, precision):
         p.pack(x)
     ex.exchange_all()
     for p, x in zip(parts, ql):
-        got = p.rhs(x, exchanged=True)
+        got = p.rhs(x, exchanged=True, by_ranges=by_ranges)
         p.check()
         want = ref[:, p.local_nodes()]
         g = got.double().cpu().numpy()
@@ -53,7 +54,11 @@ def test_partitioned_rhs_equals_global(cuda_device, kind, precision):
             assert rel_l2(g, want) <= 1e-13, rel_l2(g, want)
 
 
-def test_partitioned_lsrk_step(cuda_device):
+@pytest.mark.parametrize("by_ranges", [False, True])
+def test_partitioned_lsrk_step(cuda_device, by_ranges):
+    """Five fused stages per part, as one launch or as the two element
+    ranges of the overlapped stage (hb_lsrk_stage_elements), bitwise equal
+    to the unpartitioned LSRK4 step."""
     import torch
     from hedge_b200.timestep import RK4A, RK4B
     d, model, plan, parts, ex = _setup("maxwell", 4, "fp64")
@@ -70,7 +75,7 @@ def test_partitioned_lsrk_step(cuda_device):
         nxt = []
         for p, x, r in zip(parts, cur, res):
             o = torch.empty_like(x)
-            p.lsrk_stage(RK4A[s], RK4B[s], dt, x, o, r, exchanged=True)
+            p.lsrk_stage(RK4A[s], RK4B[s], dt, x, o, r, exchanged=True, by_ranges=by_ranges)
             nxt.append(o)
         cur = nxt
     for p, x in zip(parts, cur):
@@ -119,29 +124,74 @@ def test_partitioned_norm_equals_global(cuda_device):
     assert abs(parts[0].norm(x) - parts[0].norm_sq(x) ** 0.5) <= 1e-15 * parts[0].norm(x)
 
 
+@pytest.mark.parametrize("kind,order", [("maxwell", 5), ("wave", 7)])
 @pytest.mark.parametrize("precision", ["fp64", "fp16x3", "bf16x3"])
-def test_partitioned_maxwell_n5(cuda_device, precision):
-    """3D N = 5: an operator without halo faces takes the streamed-operator
-    split kernel, the parts (with halo faces) the resident one; each part's
-    RHS against the oracle on its elements."""
+def test_partitioned_high_order(cuda_device, precision, kind, order):
+    """3D N = 5 Maxwell and N = 7 wave: the parts, with halo faces, run on the
+    streamed-operator split kernel (256 threads per CTA) on the split
+    precisions; each part's RHS against the oracle on its elements."""
+    import ctypes as C
     from oracle import OracleRHS
     from hedge_b200.partition import LocalExchange, PartitionPlan, PartitionedOperator
     from test_gpu_parity import _fields
-    d = hb.Discretization(hb.make_box_tet_mesh(n=(2, 2, 2), jitter=0.03, seed=5), order=5)
-    model = hb.MaxwellOperator(1.0, 1.0, flux_type=1)
+    d = hb.Discretization(hb.make_box_tet_mesh(n=(2, 2, 2), jitter=0.03, seed=5), order=order)
+    model = hb.MaxwellOperator(1.0, 1.0, flux_type=1) if kind == "maxwell" else \
+        hb.StrongWaveOperator(1.0, 3, flux_type="upwind")
+    F = 6 if kind == "maxwell" else 4
     plan = PartitionPlan(d, model.op_template(), 3)
     parts = [PartitionedOperator(d, model, plan, r, precision=precision) for r in range(3)]
     ex = LocalExchange(plan, parts)
-    q = _fields(d, 6, 12)
-    ref = OracleRHS(d, model.op_template())(q).reshape(6, -1)
+    q = _fields(d, F, 12)
+    ref = OracleRHS(d, model.op_template())(q).reshape(F, -1)
     tol = {"fp64": 1e-12, "fp16x3": 1e-6, "bf16x3": 1e-5}[precision]
     ql = [p.scatter(q) for p in parts]
     for p, x in zip(parts, ql):
         p.pack(x)
     ex.exchange_all()
     for p, x in zip(parts, ql):
-        got = p.rhs(x, exchanged=True)
-        p.check()
-        err = rel_l2(got.double().cpu().numpy(), ref[:, p.local_nodes()])
-        print("%s maxwell N=5 part rel-L2 %.3e" % (precision, err))
-        assert err <= tol
+        assert p.part.n_halo_faces > 0
+        if precision != "fp64":
+            info = (C.c_int64 * 6)()
+            p.lib.hb_op_launch_info(p._h, info, 6)
+            assert info[1] == 256, list(info)
+        for by_ranges in (False, True):
+            got = p.rhs(x, exchanged=True, by_ranges=by_ranges)
+            p.check()
+            err = rel_l2(got.double().cpu().numpy(), ref[:, p.local_nodes()])
+            print("%s %s N=%d part rel-L2 %.3e" % (precision, kind, order, err))
+            assert err <= tol
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp16x3", "bf16x3"])
+def test_stage_over_element_ranges(cuda_device, precision):
+    """hb_lsrk_stage_elements over [0, k) then [k, K), k not a multiple of
+    any batch size, equals one hb_lsrk_stage (bitwise); ranges outside
+    [0, K] are refused."""
+    import torch
+    from hedge_b200 import _native
+    d = hb.Discretization(hb.make_box_tet_mesh(n=(4, 4, 4), jitter=0.03, seed=7), order=4,
+                          precision=precision)
+    model = hb.MaxwellOperator(1.0, 1.0, flux_type=1)
+    comp = model.bind(d).compiled
+    lib, h = comp._lib, comp._handle
+    dt = torch.float32 if precision == "fp32" else torch.float64
+    rng = np.random.default_rng(3)
+    q = torch.as_tensor(rng.standard_normal((6, len(d))), dtype=dt, device=d.device)
+    r0 = torch.as_tensor(rng.standard_normal((6, len(d))), dtype=dt, device=d.device)
+    a, b, step = -0.41, 0.37, 1e-3
+    st = comp._stream()
+    want_q, want_r = torch.empty_like(q), r0.clone()
+    _native.check(lib.hb_lsrk_stage(h, a, b, step, q.data_ptr(), want_q.data_ptr(),
+                                    want_r.data_ptr(), None, None, None, st))
+    got_q, got_r = torch.empty_like(q), r0.clone()
+    k = 137
+    for e0, e1 in ((0, k), (k, d.K)):
+        _native.check(lib.hb_lsrk_stage_elements(h, e0, e1, a, b, step, q.data_ptr(),
+                                                 got_q.data_ptr(), got_r.data_ptr(), None,
+                                                 None, None, st))
+    comp.check()
+    assert torch.equal(got_q, want_q) and torch.equal(got_r, want_r)
+    for e0, e1 in ((-1, 5), (5, 4), (0, d.K + 1)):
+        assert lib.hb_lsrk_stage_elements(h, e0, e1, a, b, step, q.data_ptr(),
+                                          got_q.data_ptr(), got_r.data_ptr(), None, None,
+                                          None, st) == _native.HB_ERR_INVALID_ARGUMENT

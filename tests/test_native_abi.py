@@ -32,6 +32,10 @@ def test_null_arguments_are_rejected_without_touching_the_gpu():
     assert lib.hb_discr_create(None, C.byref(h)) == _native.HB_ERR_INVALID_ARGUMENT
     assert b"null" in lib.hb_last_error_string()
     assert lib.hb_rhs(None, None, None, None, None, None, None) == _native.HB_ERR_INVALID_ARGUMENT
+    assert lib.hb_rhs_elements(None, 0, 1, None, None, None, None, None, None) == \
+        _native.HB_ERR_INVALID_ARGUMENT
+    assert lib.hb_lsrk_stage_elements(None, 0, 1, 0.0, 0.0, 0.0, None, None, None, None, None,
+                                      None, None) == _native.HB_ERR_INVALID_ARGUMENT
     assert lib.hb_lincomb(-1, 0, 1.0, None, 1.0, None, None, None) == \
         _native.HB_ERR_INVALID_ARGUMENT
     assert lib.hb_op_destroy(None) == _native.HB_OK

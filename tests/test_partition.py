@@ -1,7 +1,8 @@
 """Element partitions and the face-trace exchange (host side, no GPU).
 
 * every element has one owner and the parts are contiguous along the Morton
-  order; local face tables reproduce the global neighbours;
+  order; local face tables reproduce the global neighbours; a part's
+  elements without halo faces come first;
 * the halo a part receives (the owners' packed values, concatenated by
   source part) equals the ext values the global face-pair map gives for its
   cut faces, node by node in the receiver's face-node order;
@@ -85,6 +86,23 @@ def test_halo_matches_global_gather():
                     c = d.nbr_code[e, f]
                     want = gnb * d.Np + fmask[c & 3][sh[c >> 2]]
                     np.testing.assert_array_equal(p.halo_global[h * d.Nfp:(h + 1) * d.Nfp], want)
+
+
+@pytest.mark.parametrize("dim,nparts", [(2, 3), (3, 4)])
+def test_interior_elements_first(dim, nparts):
+    """A part lists its elements without halo faces first (the range the
+    overlapped stage launches while the traces are exchanged): none of the
+    first n_interior elements has a halo face, every later one has."""
+    d, op = _discr(dim)
+    plan = PartitionPlan(d, op.op_template(), nparts)
+    for p in plan.parts:
+        Kr = len(p.elements)
+        halo_el = (p.conn[..., 0] >= Kr).any(1)
+        assert not halo_el[:p.n_interior].any()
+        assert halo_el[p.n_interior:].all()
+        assert 0 < p.n_interior < Kr
+        for grp in (p.elements[:p.n_interior], p.elements[p.n_interior:]):
+            assert np.all(np.diff(grp) > 0)
 
 
 def test_partition_is_balanced():
