@@ -155,3 +155,38 @@ def test_exchange_gloo(tmp_path, world):
                        start_method="spawn")
     for r in range(world):
         assert open("%s.%d" % (res, r)).read() == "ok"
+
+
+def test_overlapped_stage_order():
+    """With an exchange that can be started and finished separately, a part's
+    stage packs, posts the exchange, launches the elements without halo
+    faces, waits for the exchange, then launches the rest; without one (or
+    after a LocalExchange) it launches all elements at once."""
+    import types
+    from hedge_b200.partition import PartitionedOperator
+    log = []
+
+    class Ex:
+        def start(self, send, halo):
+            log.append("start")
+            return ["req"]
+
+        def finish(self, reqs):
+            log.append("finish")
+
+    stub = types.SimpleNamespace(
+        pack=lambda q: log.append("pack"), exchange=Ex(), send=np.zeros((4, 1)), n_send=3,
+        halo=None, n_interior=7, K=10, _exchange=lambda q: log.append("exchange"))
+    launch = lambda e0, e1: log.append((e0, e1))  # noqa: E731
+    PartitionedOperator._run(stub, launch, None, exchanged=False, by_ranges=False)
+    assert log == ["pack", "start", (0, 7), "finish", (7, 10)]
+    log.clear()
+    PartitionedOperator._run(stub, launch, None, exchanged=True, by_ranges=False)
+    assert log == [(0, 10)]
+    log.clear()
+    PartitionedOperator._run(stub, launch, None, exchanged=True, by_ranges=True)
+    assert log == [(0, 7), (7, 10)]
+    log.clear()
+    stub.exchange = lambda send, halo: log.append("blocking")
+    PartitionedOperator._run(stub, launch, None, exchanged=False, by_ranges=False)
+    assert log == ["exchange", (0, 10)]
