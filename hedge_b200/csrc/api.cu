@@ -344,6 +344,11 @@ static hb_status check_inputs(Op* op, const void* q_in, const void* q_out,
     return fail(HB_ERR_INVALID_ARGUMENT, "variable-velocity wave needs the c field");
   if (op->model == HB_MODEL_VARADV && !coeff)
     return fail(HB_ERR_INVALID_ARGUMENT, "variable-coefficient advection needs the velocity");
+  const bool maxwell = op->model == HB_MODEL_MAXWELL || op->model == HB_MODEL_MAXWELL_TM ||
+                       op->model == HB_MODEL_MAXWELL_TE;
+  if (maxwell && coeff && op->split)
+    return fail(HB_ERR_UNSUPPORTED, "Maxwell with variable material: CUDA-core kernels only "
+                                    "(HB_PREC_FP64, HB_PREC_FP32_SIMT)");
   return HB_OK;
 }
 
@@ -467,6 +472,9 @@ hb_status hb_rhs_adjoint(hb_op* handle, const double* q, const double* lam, doub
     return fail(HB_ERR_INVALID_ARGUMENT, "variable-velocity wave needs the c field");
   if (c_bar && op->model != HB_MODEL_VARWAVE)
     return fail(HB_ERR_INVALID_ARGUMENT, "c_bar: only the variable-velocity wave has a c field");
+  if (coeff && (op->model == HB_MODEL_MAXWELL || op->model == HB_MODEL_MAXWELL_TM ||
+                op->model == HB_MODEL_MAXWELL_TE))
+    return fail(HB_ERR_UNSUPPORTED, "adjoint: Maxwell with variable material is not built");
   if (c_bar && !q) return fail(HB_ERR_INVALID_ARGUMENT, "c_bar needs the state q");
   DeviceGuard g(op->d->device);
   if (!g.ok) return fail(HB_ERR_CUDA, "cannot select the CUDA device");

@@ -255,6 +255,65 @@ __device__ __forceinline__ void maxwell_flux3(const ModelParams& mp, bool bdry, 
   }
 }
 
+// The same flux for variable material (em.py:118-190 with epsilon, mu volume
+// fields): the impedances Z = sqrt(mu / eps) of the interior and exterior
+// sides enter the numeric flux type; "lf" does not depend on the material.
+template <typename T>
+__device__ __forceinline__ void maxwell_flux3_var(const ModelParams& mp, bool bdry, const T* de,
+                                                  const T* dh, const T* n, T Zi, T Ze, T* f) {
+  const int ft = bdry ? mp.bdry_flux_type : mp.flux_type;
+  const T alpha = T(bdry ? mp.bdry_alpha : mp.alpha);
+  T t[3];
+  if (ft == 1) {
+    cross3(n, dh, t);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) f[k] = T(0.5) * (-t[k]);
+    cross3(n, de, t);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) f[3 + k] = T(0.5) * t[k];
+  } else {
+    const T Yi = T(1) / Zi, Ye = T(1) / Ze;
+    T nde[3], ndh[3], a[3];
+    cross3(n, de, nde);
+    cross3(n, dh, ndh);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) a[k] = Ze * dh[k] - alpha * nde[k];
+    cross3(n, a, t);
+    const T fe = T(-1) / (Zi + Ze), fh = T(1) / (Yi + Ye);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) f[k] = fe * t[k];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) a[k] = Ye * de[k] + alpha * ndh[k];
+    cross3(n, a, t);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) f[3 + k] = fh * t[k];
+  }
+}
+
+// Maxwell systems (3D, TM, TE) with variable material: the flux of the jumps
+// with the interior and exterior impedances Zi, Ze.
+template <int MODEL, int DIM, typename T>
+__device__ __forceinline__ void maxwell_flux_var(const ModelParams& mp, bool bdry,
+                                                 const T (&uM)[Args<MODEL, DIM>::N],
+                                                 const T (&uP)[Args<MODEL, DIM>::N],
+                                                 const T (&n)[DIM], T Zi, T Ze,
+                                                 T (&f)[Traits<MODEL, DIM>::F]) {
+  if constexpr (MODEL == HB_MODEL_MAXWELL) {
+    T de[3], dh[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { de[k] = uM[k] - uP[k]; dh[k] = uM[3 + k] - uP[3 + k]; }
+    maxwell_flux3_var<T>(mp, bdry, de, dh, &n[0], Zi, Ze, f);
+  } else if constexpr (IsMaxwell<MODEL>::value) {
+    T d6[6] = {T(0), T(0), T(0), T(0), T(0), T(0)}, f6[6];
+    const T n3[3] = {n[0], n[1], T(0)};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) d6[maxwell_slot<MODEL>(q)] = uM[q] - uP[q];
+    maxwell_flux3_var<T>(mp, bdry, d6, d6 + 3, n3, Zi, Ze, f6);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) f[q] = f6[maxwell_slot<MODEL>(q)];
+  }
+}
+
 // ---- numerical fluxes (strong form, before the face-Jacobian scale) --------
 template <int MODEL, int DIM, typename T>
 __device__ __forceinline__ void model_flux(const ModelParams& mp, bool bdry,

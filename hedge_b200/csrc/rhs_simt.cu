@@ -136,6 +136,11 @@ __global__ void __launch_bounds__(256) rhs_simt_kernel(SimtArgs<T, S> a) {
   const int e = tid / np;
   const int i = tid - e * np;
   const int64_t Knp = a.K * np;
+  // Maxwell with variable material: coeff = [eps | mu], [2][K*Np] FP64
+  // (em.py:38-100, 309-371): per-node divisors, both sides' impedances in
+  // the flux, the local impedance in the absorbing condition
+  constexpr bool MAXW = IsMaxwell<MODEL>::value;
+  const bool varmat = MAXW && a.coeff != nullptr;
 
   for (int64_t batch = blockIdx.x; batch < a.nbatch; batch += gridDim.x) {
     const int64_t el0 = a.e_begin + batch * E;
@@ -188,6 +193,7 @@ __global__ void __launch_bounds__(256) rhs_simt_kernel(SimtArgs<T, S> a) {
         }
       const T cnode = C ? sc[e * np + i] : T(0);
       model_volume<MODEL, DIM, T>(a.mp, g, cnode, vol);
+      const int64_t el_base = (el0 + e) * np;
 
       // ---- surface: flux at this thread's face points ----
       for (int p = i; p < nfpt; p += np) {
@@ -205,7 +211,21 @@ __global__ void __launch_bounds__(256) rhs_simt_kernel(SimtArgs<T, S> a) {
         const int2 cn = sconn[e * nf + face];
         bool have = true;
         bool bdry = false;
+        // variable material: interior and exterior impedances (the exterior
+        // side's at the matched neighbour node; the interior one on
+        // boundary faces)
+        T Zi = T(1), Ze = T(1);
+        if (varmat) {
+          const int64_t gm = el_base + lnode;
+          Zi = sqrt(T(a.coeff[Knp + gm]) / T(a.coeff[gm]));
+          Ze = Zi;
+        }
         if (cn.x >= a.K) {
+          if (varmat) {
+            // the halo carries no material values
+            flag(a.err, DEV_MISSING_INPUT);
+            have = false;
+          }
           // neighbour on another partition: ext values from the halo buffer
           const int64_t h = (int64_t)cn.x - a.K;
           if (h >= a.n_halo || a.halo == nullptr) {
@@ -228,6 +248,7 @@ __global__ void __launch_bounds__(256) rhs_simt_kernel(SimtArgs<T, S> a) {
             if constexpr (C != 0) uP[0] = T(__ldg(a.coeff + gi));
 #pragma unroll
             for (int f = 0; f < F; ++f) uP[C + f] = ldg_as<T>(a.q_in + f * Knp + gi);
+            if (varmat) Ze = sqrt(T(__ldg(a.coeff + Knp + gi)) / T(__ldg(a.coeff + gi)));
           }
         } else {
           bdry = true;
@@ -241,11 +262,22 @@ __global__ void __launch_bounds__(256) rhs_simt_kernel(SimtArgs<T, S> a) {
               given = T(__ldg(a.bdry + bi));
             }
           }
-          if (have) have = model_bc<MODEL, DIM, T>(a.mp, cn.y, uM, n, given, uP);
+          if (have) {
+            ModelParams mpl = a.mp;
+            if (varmat) {
+              mpl.Z = (double)Zi;
+              mpl.Y = 1.0 / (double)Zi;
+            }
+            have = model_bc<MODEL, DIM, T>(mpl, cn.y, uM, n, given, uP);
+          }
         }
         T* dst = sfl + e * nfpt + p;
         if (have) {
-          model_flux<MODEL, DIM, T>(a.mp, bdry, uM, uP, n, fl);
+          if (varmat) {
+            if constexpr (MAXW) maxwell_flux_var<MODEL, DIM, T>(a.mp, bdry, uM, uP, n, Zi, Ze, fl);
+          } else {
+            model_flux<MODEL, DIM, T>(a.mp, bdry, uM, uP, n, fl);
+          }
 #pragma unroll
           for (int f = 0; f < F; ++f) dst[f * E * nfpt] = fscale * fl[f];
         } else {
@@ -269,11 +301,17 @@ __global__ void __launch_bounds__(256) rhs_simt_kernel(SimtArgs<T, S> a) {
         for (int f = 0; f < F; ++f) acc[f] += l * fe[f * E * nfpt + p];
       }
       const int64_t node = (el0 + e) * np + i;
+      ModelParams mpn = a.mp;
+      if (varmat) {
+        // the material divisor at this node
+        mpn.eps = a.coeff[node];
+        mpn.mu = a.coeff[Knp + node];
+      }
 #pragma unroll
       for (int f = 0; f < F; ++f) {
         const int64_t si = model_src_index<MODEL>(f, node, Knp);
         const T src = (a.source && si >= 0) ? T(a.source[si]) : T(0);
-        const T r = model_finish<MODEL, DIM, T>(a.mp, f, vol[f], acc[f], src);
+        const T r = model_finish<MODEL, DIM, T>(mpn, f, vol[f], acc[f], src);
         const int64_t idx = f * Knp + node;
         if (a.mode == 0) {
           a.rhs_out[idx] = S(r);

@@ -443,6 +443,14 @@ class CompiledOperator:
         prec = PRECISIONS[precision] if precision != "plain" else (
             _native.PREC_FP64 if discr.default_scalar_type == np.float64
             else _native.PREC_FP32)
+        # Maxwell with variable material: the CUDA-core kernels
+        self.var_material = bool(ot.params.get("variable_material"))
+        if self.var_material:
+            if prec in (_native.PREC_BF16X3, _native.PREC_FP16X3):
+                raise NotImplementedError("Maxwell with variable material: fp64 or fp32 "
+                                          "(CUDA-core kernels)")
+            if prec == _native.PREC_FP32:
+                prec = _native.PREC_FP32_SIMT
         self.prec_code = prec
         model = ot.operator
         p = ot.params
@@ -469,6 +477,10 @@ class CompiledOperator:
             c = model.c if model is not None else (None if names.get("coeff") else 1.0)
             if c is not None and not isinstance(c, Expr):
                 self.set_coefficient(c)
+        if self.var_material and model is not None and hasattr(model, "material_values"):
+            e, m = model.material_values(discr)
+            if e is not None and m is not None:
+                self.set_coefficient((e, m))
         if names and not self._n_e:
             # lowered from a template: source = sign * (const + coef * field)
             self._src_spec = (-1.0 if ot.model == MODEL_VARWAVE else 1.0,
@@ -545,10 +557,21 @@ class CompiledOperator:
 
     def set_coefficient(self, c):
         """Variable-velocity wave speed: a number or a volume vector; for the
-        quadrature advection the velocity [d, K*Np], kept for calls (and
-        recorded stages) that pass none."""
+        quadrature advection the velocity [d, K*Np]; for Maxwell with
+        variable material the pair (epsilon, mu) of numbers or volume
+        vectors.  Kept for calls (and recorded stages) that pass none."""
         torch = _torch()
         d = self.discr
+        if self.var_material:
+            eps, mu = c
+            t = torch.cat([d.to_device(np.full(len(d), float(x)) if np.isscalar(x) else x,
+                                       torch.float64).reshape(-1) for x in (eps, mu)])
+            if t.numel() != 2 * len(d):
+                raise ValueError("epsilon and mu must be volume vectors of length %d" % len(d))
+            if bool((t <= 0).any()):
+                raise ValueError("epsilon and mu must be positive")
+            self._coeff = t.contiguous()
+            return
         if self.ot.model == MODEL_VARADV:
             t = d.to_device(np.asarray(c) if not isinstance(c, torch.Tensor) else c,
                             torch.float64).reshape(-1).contiguous()
@@ -631,7 +654,8 @@ class CompiledOperator:
         (FP64 on the device), else the operator's."""
         c = self._coeff if coeff is None else coeff
         s = self._source if source is None else source
-        crows = self.discr.dimensions if self.ot.model == MODEL_VARADV else 1
+        crows = self.discr.dimensions if self.ot.model == MODEL_VARADV else (
+            2 if self.var_material else 1)
         for t, rows in ((coeff, crows), (source, self._n_e or 1)):
             if t is not None:
                 if t.dtype != _torch().float64 or not t.is_contiguous() or \
@@ -720,7 +744,13 @@ class CompiledOperator:
             w = [kwargs[n] if i is None else kwargs[n][i] for n, i in names["state_keys"]]
         if names.get("given") in kwargs:
             bc_in = kwargs.pop(names["given"])
-        if names.get("coeff") in kwargs:
+        if names.get("coeffs") and all(n in kwargs for n, _ in names["coeffs"]):
+            # variable material: epsilon, mu by their template names
+            vals = [kwargs.pop(n) if i is None else kwargs.pop(n)[i] for n, i in names["coeffs"]]
+            cval = _torch().cat([self.discr.to_device(x, _torch().float64).reshape(-1)
+                                 for x in vals])
+            coeff = cval.contiguous()
+        elif names.get("coeff") in kwargs:
             cval = kwargs.pop(names["coeff"])
             if isinstance(cval, (list, tuple)) or (isinstance(cval, np.ndarray)
                                                    and cval.dtype == object):
@@ -749,6 +779,10 @@ class CompiledOperator:
         if self.ot.model == MODEL_VARADV and coeff is None and self._coeff is None:
             raise ValueError("this template needs its velocity field %r"
                              % names.get("coeff", "v"))
+        if self.var_material and coeff is None and self._coeff is None:
+            raise ValueError("this template needs its material fields %r"
+                             % [n for n, _ in names.get("coeffs", [("epsilon", None),
+                                                                   ("mu", None)])])
         if src_name is not None and source is None and self._source is None:
             raise ValueError("this template needs its source field %r" % src_name[0])
         q = self.as_state(w)

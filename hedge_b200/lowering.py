@@ -471,9 +471,10 @@ def _close(a, b):
 # kernel models
 
 class _Roles:
-    def __init__(self, state, coeff, given, source):
+    def __init__(self, state, coeff, given, source, coeffs=()):
         self.state = state          # object array of the state Fields
-        self.coeff = coeff          # Field or None
+        self.coeff = coeff          # Field or None (one coefficient field)
+        self.coeffs = list(coeffs)  # every coefficient field (Maxwell material: eps, mu)
         self.given = given          # Field or None
         self.source = source        # expression of the user's source (or 0)
 
@@ -484,6 +485,8 @@ class _Roles:
              "state_keys": [f.key for f in st]}
         if self.coeff is not None:
             d["coeff"] = self.coeff.name
+        elif len(self.coeffs) > 1:
+            d["coeffs"] = [(f.name, f.index) for f in self.coeffs]
         if self.given is not None:
             d["given"] = self.given.name
         return d
@@ -616,14 +619,14 @@ class _Maxwell(_Family):
         return float(np.sum((y - ys[0]) * dy) / den) if den > 0 else 0.0
 
     def flux_choices(self, user, roles, params, dims):
-        ctx = _Ctx(dims, face="interior")
+        ctx = _Ctx(dims, face="interior", coeff_keys=[f.key for f in roles.coeffs])
         alpha = self._fit(user, roles, dict(params, bdry_flux_type=0.0), ctx, "flux_type",
                           None)
         return [dict(params, flux_type="lf", bdry_flux_type="lf"),
                 dict(params, flux_type=alpha, bdry_flux_type=alpha)]
 
     def bdry_choices(self, user, roles, params, dims, tag, kind):
-        ctx = _Ctx(dims, face=tag)
+        ctx = _Ctx(dims, face=tag, coeff_keys=[f.key for f in roles.coeffs])
         return ["lf", self._fit(user, roles, params, ctx, "bdry_flux_type", (tag, kind))]
 
     def build(self, roles, p, bc):
@@ -642,6 +645,54 @@ class _Maxwell(_Family):
         if srcs is not None and any(not ot.is_zero(x) for x in srcs[ne:]):
             return None
         return m, _comps(m.op_template(w=roles.state))
+
+
+class _MaxwellVar(_Maxwell):
+    """Maxwell with variable material: the flux argument's first two fields
+    are epsilon and mu (em.py:309-371)."""
+    source_outputs = ()
+
+    def applies(self, dims, F, ncoeff):
+        return dims == 3 and F == 6 and ncoeff == 2
+
+    def volume_params(self, V):
+        # with the material probed at 1: d/dy Hz -> Ex is 1/eps = 1, d/dy Ez
+        # -> Hx is -1/mu = -1
+        return {} if _close(np.array([V[0, 5, 1], V[3, 2, 1]]), np.array([1.0, -1.0])) \
+            else None
+
+    def build(self, roles, p, bc):
+        t = {BC_PEC: TAG_NONE, BC_PMC: TAG_NONE, BC_ABSORB: TAG_NONE}
+        if bc is not None:
+            t[bc[1]] = bc[0]
+        m = self.cls(roles.coeffs[0], roles.coeffs[1], p["flux_type"],
+                     bdry_flux_type=p.get("bdry_flux_type", p["flux_type"]),
+                     pec_tag=t[BC_PEC], pmc_tag=t[BC_PMC], absorb_tag=t[BC_ABSORB])
+        return m, _comps(m.op_template(w=roles.state))
+
+
+class _MaxwellTMVar(_MaxwellVar):
+    model = MODEL_MAXWELL_TM
+    cls = TMMaxwellOperator
+
+    def applies(self, dims, F, ncoeff):
+        return dims == 2 and F == 3 and ncoeff == 2
+
+    def volume_params(self, V):
+        return {} if _close(np.array([V[0, 2, 0], V[1, 0, 1]]), np.array([1.0, -1.0])) \
+            else None
+
+
+class _MaxwellTEVar(_MaxwellVar):
+    model = MODEL_MAXWELL_TE
+    cls = TEMaxwellOperator
+
+    def applies(self, dims, F, ncoeff):
+        return dims == 2 and F == 3 and ncoeff == 2
+
+    def volume_params(self, V):
+        return {} if _close(np.array([V[0, 2, 1], V[2, 1, 0]]), np.array([1.0, -1.0])) \
+            else None
 
 
 class _MaxwellTM(_Maxwell):
@@ -676,16 +727,19 @@ class _MaxwellTE(_Maxwell):
         return {"eps": 1.0 / a, "mu": -1.0 / b}
 
 
-_FAMILIES = (_Advection(), _Wave(), _VarWave(), _Maxwell(), _MaxwellTM(), _MaxwellTE())
+_FAMILIES = (_Advection(), _Wave(), _VarWave(), _Maxwell(), _MaxwellTM(), _MaxwellTE(),
+             _MaxwellVar(), _MaxwellTMVar(), _MaxwellTEVar())
 
 
 # --------------------------------------------------------------------------
 
-def _source(user, roles_keys, src_fields, dims):
+def _source(user, roles_keys, src_fields, dims, coeff_keys=()):
     """The template's sources: output values with the state, derivatives and
-    fluxes at zero, per output as const + sum coef_k * field_k.  Returns
-    (expressions, constants, terms) with one entry per output."""
+    fluxes at zero (coefficient fields at one), per output as
+    const + sum coef_k * field_k.  Returns (expressions, constants, terms)
+    with one entry per output."""
     zero = {k: np.zeros(PROBES) for k in roles_keys}
+    zero.update({k: np.ones(PROBES) for k in coeff_keys})
 
     def at(fixed):
         ctx = _Ctx(dims, face=None, fixed={**zero, **fixed},
@@ -733,8 +787,8 @@ def lower(template, dimensions, mesh=None):
     diff = set(scan.diff_keys)
     state = [x for x in arg if x.key in diff]
     coeff = [x for x in arg if x.key not in diff]
-    if len(coeff) > 1 or (coeff and arg[0] is not coeff[0]):
-        raise NotImplementedError("at most one coefficient field, first in the flux argument")
+    if len(coeff) > 2 or any(arg[k] is not coeff[k] for k in range(len(coeff))):
+        raise NotImplementedError("at most two coefficient fields, first in the flux argument")
     if len(state) != F:
         raise NotImplementedError("%d outputs but %d differentiated state fields in the "
                                   "flux argument" % (F, len(state)))
@@ -746,13 +800,14 @@ def lower(template, dimensions, mesh=None):
     src_fields = {k: f for k, f in scan.outside_fields.items()
                   if k not in st_keys | co_keys and k not in diff}
     roles_keys = st_keys | co_keys | {f.key for f in given}
-    src_exprs, src_consts, src_terms = _source(outs, roles_keys, src_fields, dimensions)
+    src_exprs, src_consts, src_terms = _source(outs, roles_keys, src_fields, dimensions,
+                                               co_keys)
     if any(len(t) > 1 for t in src_terms):
         raise NotImplementedError("more than one source field on an output")
     src_outputs = [o for o in range(F) if src_terms[o] or src_consts[o] != 0]
     state_arr = ot.join_fields(state)
-    roles = _Roles(state_arr, coeff[0] if coeff else None, given[0] if given else None,
-                   src_exprs[0])
+    roles = _Roles(state_arr, coeff[0] if len(coeff) == 1 else None,
+                   given[0] if given else None, src_exprs[0], coeffs=coeff)
     roles.sources = src_exprs
 
     # volume coefficients V[f, g, x]: unit derivative probes less the

@@ -390,10 +390,17 @@ class VariableVelocityStrongWaveOperator(HyperbolicOperator):
 
 
 class MaxwellOperator(HyperbolicOperator):
-    """Maxwell's equations, fixed isotropic material (em.py:38-387): the full
-    3D system, field order [Ex Ey Ez Hx Hy Hz]; the subclasses carry a subset
-    of the components (get_eh_subset) in 2D, the fields not carried and all
-    z derivatives (and normal z components) being zero."""
+    """Maxwell's equations, isotropic non-dispersive material (em.py:38-387):
+    the full 3D system, field order [Ex Ey Ez Hx Hy Hz]; the subclasses carry
+    a subset of the components (get_eh_subset) in 2D, the fields not carried
+    and all z derivatives (and normal z components) being zero.
+
+    ``epsilon`` and ``mu`` are numbers (fixed material) or, for spatially
+    variable material, volume fields: given functions
+    (TimeConstantGivenFunction, ``volume_interpolant(t, discr)``), callables
+    f(x) of the node coordinates, volume vectors [K*Np], or template fields.
+    Variable material runs on the CUDA-core kernels (fp64, fp32) without a
+    source current."""
 
     _default_dimensions = 3
     model_id = MODEL_MAXWELL
@@ -409,12 +416,16 @@ class MaxwellOperator(HyperbolicOperator):
         if self.dimensions != self._default_dimensions:
             raise NotImplementedError("%s is a %dD system" % (type(self).__name__,
                                                              self._default_dimensions))
-        if not (np.isscalar(epsilon) and np.isscalar(mu)):
-            raise NotImplementedError("only fixed material")
+        self.fixed_material = bool(np.isscalar(epsilon) and np.isscalar(mu))
         self.current = current
         if incident_tag is not TAG_NONE:
             raise NotImplementedError("incident boundary data is not on this path")
-        self.epsilon, self.mu = float(epsilon), float(mu)
+        if self.fixed_material:
+            self.epsilon, self.mu = float(epsilon), float(mu)
+        else:
+            if not (np.isscalar(current) and current == 0):
+                raise NotImplementedError("variable material with a source current")
+            self.epsilon, self.mu = epsilon, mu
         self.flux_type = flux_type
         self.bdry_flux_type = flux_type if bdry_flux_type is None else bdry_flux_type
         for ft in (self.flux_type, self.bdry_flux_type):
@@ -425,7 +436,36 @@ class MaxwellOperator(HyperbolicOperator):
 
     @property
     def c(self):
+        if not self.fixed_material:
+            raise RuntimeError("Cannot compute speed of light for non-constant material")
         return 1 / sqrt(self.mu * self.epsilon)
+
+    def material_templates(self):
+        """(epsilon, mu) as they enter the template: numbers (fixed
+        material) or template fields ("epsilon", "mu" unless given as
+        fields)."""
+        if self.fixed_material:
+            return self.epsilon, self.mu
+        e = self.epsilon if isinstance(self.epsilon, ot.Expr) else ot.Field("epsilon")
+        m = self.mu if isinstance(self.mu, ot.Expr) else ot.Field("mu")
+        return e, m
+
+    def material_values(self, discr):
+        """(epsilon, mu) at the nodes of ``discr``, two numpy vectors [K*Np]
+        (None for a material given as a template field)."""
+        def vals(x):
+            if isinstance(x, ot.Expr):
+                return None
+            if np.isscalar(x):
+                return np.full(len(discr), float(x))
+            if hasattr(x, "volume_interpolant"):
+                return np.asarray(_to_numpy(x.volume_interpolant(0.0, discr)),
+                                  dtype=np.float64).reshape(-1)
+            if callable(x):
+                return np.asarray(discr.interpolate_volume_function(x, kind="numpy"),
+                                  dtype=np.float64).reshape(-1)
+            return np.asarray(_to_numpy(x), dtype=np.float64).reshape(-1)
+        return vals(self.epsilon), vals(self.mu)
 
     def get_eh_subset(self):
         """em.py: which of (Ex, Ey, Ez, Hx, Hy, Hz) the operator carries."""
@@ -470,16 +510,38 @@ class MaxwellOperator(HyperbolicOperator):
         return np.array(list(x) + [0] * (3 - len(x)), dtype=object)
 
     def max_eigenvalue(self, t=None, fields=None, discr=None):
-        return 1 / sqrt(self.epsilon * self.mu)
+        """1/sqrt(eps mu) (em.py:466-482).  Variable material: the reference
+        raises here (use max_eigenvalue_expr); with ``discr`` this evaluates
+        that expression, the nodal maximum of 1/sqrt(eps mu), instead."""
+        if self.fixed_material:
+            return 1 / sqrt(self.epsilon * self.mu)
+        if discr is None:
+            raise ValueError("max_eigenvalue of variable material needs the discretization")
+        e, m = self.material_values(discr)
+        if e is None or m is None:
+            raise ValueError("material given as template fields: no values to evaluate")
+        return float(np.max(1.0 / np.sqrt(e * m)))
+
+    def estimate_timestep(self, discr, stepper=None, stepper_class=None,
+                          stepper_args=None, t=None, fields=None):
+        return (1 / self.max_eigenvalue(t, fields, discr)
+                * discr.dt_non_geometric_factor() * discr.dt_geometric_factor())
 
     def flux(self, flux_type):
-        """em.py:118-190, fixed material"""
+        """em.py:118-190: fixed material (constants), or variable material
+        (the flux argument carries epsilon and mu first)."""
         normal = self._pad3(fl.make_normal(self.dimensions))
-        w = fl.FluxVectorPlaceholder(self.n_fields)
-        wi = self._embed([w[k].int for k in range(self.n_fields)])
-        we = self._embed([w[k].ext for k in range(self.n_fields)])
-        epsilon = fl.FluxConstantPlaceholder(self.epsilon)
-        mu = fl.FluxConstantPlaceholder(self.mu)
+        if self.fixed_material:
+            w = fl.FluxVectorPlaceholder(self.n_fields)
+            epsilon = fl.FluxConstantPlaceholder(self.epsilon)
+            mu = fl.FluxConstantPlaceholder(self.mu)
+            fw = [w[k] for k in range(self.n_fields)]
+        else:
+            w = fl.FluxVectorPlaceholder(2 + self.n_fields)
+            epsilon, mu = w[0], w[1]
+            fw = [w[2 + k] for k in range(self.n_fields)]
+        wi = self._embed([x.int for x in fw])
+        we = self._embed([x.ext for x in fw])
         Z_int = (mu.int / epsilon.int) ** 0.5
         Y_int = 1 / Z_int
         Z_ext = (mu.ext / epsilon.ext) ** 0.5
@@ -527,10 +589,13 @@ class MaxwellOperator(HyperbolicOperator):
         return self._pick(ot.join_fields(j - ot.cross(nabla, h), ot.cross(nabla, e)))
 
     def op_template(self, w=None):
-        """em.py:226-371, fixed material"""
+        """em.py:226-371: (-local derivatives + M^-1 (fluxes)) / material
+        divisor; with variable material the flux argument is
+        (epsilon, mu, w) and every boundary vector (B(eps), B(mu), bc)."""
         F = self.n_fields
         w = ot.make_sym_vector("w", F) if w is None else w
         B = ot.BoundarizeOperator
+        eps, mu = self.material_templates()
 
         def bfull(tag):
             return self._embed([B(tag) * w[k] for k in range(F)])
@@ -539,7 +604,10 @@ class MaxwellOperator(HyperbolicOperator):
         pm = bfull(self.pmc_tag)
         pmc = self._pick(ot.join_fields(pm[0:3], -pm[3:6]))
         an = self._pad3(ot.normal(self.absorb_tag, self.dimensions))
-        Z = (self.mu / self.epsilon) ** 0.5
+        if self.fixed_material:
+            Z = (self.mu / self.epsilon) ** 0.5
+        else:
+            Z = (B(self.absorb_tag) * mu / (B(self.absorb_tag) * eps)) ** 0.5
         ab = bfull(self.absorb_tag)
         ae, ah = ab[0:3], ab[3:6]
         absorb = self._pick(ot.join_fields(
@@ -547,20 +615,33 @@ class MaxwellOperator(HyperbolicOperator):
             ah + 0.5 * (ot.cross(an, ot.cross(an, ah)) + (1 / Z) * ot.cross(an, ae))))
         flux_op = ot.get_flux_operator(self.flux(self.flux_type))
         bdry_flux_op = ot.get_flux_operator(self.flux(self.bdry_flux_type))
-        divisor = np.array([self.epsilon] * self.n_e + [self.mu] * (F - self.n_e))
-        bdry = sum(bdry_flux_op(ot.BoundaryPair(w, bc, tag)) for tag, bc in
+        divisor = np.array([eps] * self.n_e + [mu] * (F - self.n_e), dtype=object)
+        if self.fixed_material:
+            flux_w = w
+
+            def bvec(tag, bc):
+                return bc
+        else:
+            flux_w = ot.join_fields(eps, mu, w)
+
+            def bvec(tag, bc):
+                return ot.join_fields(B(tag) * eps, B(tag) * mu, bc)
+        bdry = sum(bdry_flux_op(ot.BoundaryPair(flux_w, bvec(tag, bc), tag)) for tag, bc in
                    [(self.pec_tag, pec), (self.pmc_tag, pmc), (self.absorb_tag, absorb)])
         return _remember(self, (-self.local_derivatives(w)
-                                + ot.InverseMassOperator()(flux_op(w) + bdry)) / divisor)
+                                + ot.InverseMassOperator()(flux_op(flux_w) + bdry)) / divisor)
 
     def descriptor(self):
         def code(ft):
             return (1, 0.0) if ft == "lf" else (0, float(ft))
         ft, alpha = code(self.flux_type)
         bft, balpha = code(self.bdry_flux_type)
-        return OpTemplate(self.model_id, self.dimensions, self.n_fields, ft,
-                          {"eps": self.epsilon, "mu": self.mu, "alpha": alpha,
-                           "bdry_flux_type": bft, "bdry_alpha": balpha},
+        eps, mu = (self.epsilon, self.mu) if self.fixed_material else (1.0, 1.0)
+        params = {"eps": eps, "mu": mu, "alpha": alpha,
+                  "bdry_flux_type": bft, "bdry_alpha": balpha}
+        if not self.fixed_material:
+            params["variable_material"] = True
+        return OpTemplate(self.model_id, self.dimensions, self.n_fields, ft, params,
                           [(self.pec_tag, BC_PEC), (self.pmc_tag, BC_PMC),
                            (self.absorb_tag, BC_ABSORB),
                            (self.incident_tag, BC_NONE)], self)

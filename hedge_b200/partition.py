@@ -235,6 +235,9 @@ class PartitionedOperator:
     def __init__(self, discr, model, plan, rank, precision="fp64", device=None, exchange=None):
         torch = _torch()
         ot = as_descriptor(model.op_template(), discr.dimensions, discr.mesh)
+        if ot.params.get("variable_material"):
+            raise NotImplementedError("partitions of Maxwell with variable material "
+                                      "(the halo carries no material values)")
         self.ot, self.plan, self.rank = ot, plan, rank
         self.part = p = plan.parts[rank]
         self.F = ot.n_fields

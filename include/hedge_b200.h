@@ -143,7 +143,10 @@ hb_status hb_op_destroy(hb_op* op);
  * (jit/lift.py:110-141) and inverse mass (jit/__init__.py:501-519).
  * q, rhs: [F][K*Np] in the operator's state dtype.  coeff: var-c wave
  * speed [K*Np] FP64, or the variable-coefficient advection velocity
- * [dim][K*Np] FP64 (else NULL); bdry: BC_GIVEN values [n] FP64 (else NULL);
+ * [dim][K*Np] FP64, or for the Maxwell models the material [eps | mu]
+ * [2][K*Np] FP64 (variable material, em.py:38-100, 309-371; NULL: the
+ * descriptor's eps, mu; CUDA-core precisions only, no halo faces) (else
+ * NULL); bdry: BC_GIVEN values [n] FP64 (else NULL);
  * source: var-c / constant-c wave source on u, [K*Np] FP64 (else NULL). */
 hb_status hb_rhs(hb_op* op, const void* q, void* rhs, const double* coeff,
                  const double* bdry, const double* source, void* stream);

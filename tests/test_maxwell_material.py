@@ -1,0 +1,93 @@
+"""Maxwell with spatially variable material (em.py:38-100, 118-190, 309-371),
+host side: the template with epsilon and mu as volume fields, evaluated by
+the CPU template executor, equals the fixed-material template wherever the
+fields are constant (3D, TM and TE; every flux type; PEC, PMC and absorbing
+walls), the lowering recognises it as the Maxwell kernel with variable
+material, and the constructor refuses what the path does not carry."""
+import numpy as np
+import pytest
+
+import hedge_b200 as hb
+from hedge_b200.lowering import lower
+from hedge_b200.models import BC_ABSORB, BC_PEC, BC_PMC
+
+from conftest import rel_l2
+from test_optemplate import box, rect
+
+
+def _tagger(fvi, el, fn, allv):
+    c = allv[list(fvi)].mean(0)
+    return ["abs"] if c[0] > 0.99 else (["pmc"] if c[0] < -0.99 else ["pec"])
+
+
+def _discr(kind):
+    if kind == "3d":
+        m = hb.make_box_tet_mesh(n=(2, 2, 2), jitter=0.03, seed=3, boundary_tagger=_tagger)
+        return hb.Discretization(m, order=3), hb.MaxwellOperator, 6
+    m = hb.make_regular_rect_mesh((-1, -1), (1, 1), (5, 5), jitter=0.03, seed=4,
+                                  boundary_tagger=_tagger)
+    cls = hb.TMMaxwellOperator if kind == "tm" else hb.TEMaxwellOperator
+    return hb.Discretization(m, order=3), cls, 3
+
+
+FLUXES = [(1, 1), (0.5, "lf"), ("lf", 0.3), (0.0, 0.0)]
+
+
+@pytest.mark.parametrize("ft,bft", FLUXES)
+@pytest.mark.parametrize("kind", ["3d", "tm", "te"])
+def test_constant_fields_equal_fixed_material(kind, ft, bft):
+    from optemplate_exec import TemplateExecutor
+    d, cls, F = _discr(kind)
+    kw = dict(flux_type=ft, bdry_flux_type=bft, pec_tag="pec", pmc_tag="pmc", absorb_tag="abs")
+    fixed = cls(1.3, 0.7, **kw)
+    var = cls(np.full(len(d), 1.3), np.full(len(d), 0.7), **kw)
+    w = np.random.default_rng(1).standard_normal((F, len(d)))
+    ex = TemplateExecutor(d)
+    rf = np.asarray(ex(fixed.op_template(), w=w), dtype=np.float64)
+    rv = np.asarray(ex(var.op_template(), w=w, epsilon=np.full(len(d), 1.3),
+                       mu=np.full(len(d), 0.7)), dtype=np.float64)
+    assert rel_l2(rv, rf) <= 1e-13
+
+
+@pytest.mark.parametrize("ft,bft", FLUXES)
+@pytest.mark.parametrize("kind", ["3d", "tm", "te"])
+def test_lowering_recognises_variable_material(kind, ft, bft):
+    d, cls, F = _discr(kind)
+    op = cls(np.linspace(1.0, 2.0, len(d)), 0.8, flux_type=ft, bdry_flux_type=bft,
+             pec_tag="pec", pmc_tag="pmc", absorb_tag="abs")
+    desc = lower(op.op_template(), d.dimensions, d.mesh)
+    want = op.descriptor()
+    assert desc.model == want.model
+    assert desc.params.get("variable_material") is True
+    assert desc.flux_type == want.flux_type
+    assert abs(desc.params["alpha"] - want.params["alpha"]) <= 1e-9
+    if bft == 0.0:
+        # on a boundary both sides have the same impedance, so the numeric
+        # flux with alpha = 0 is the "lf" flux: either lowering is exact
+        assert desc.params["bdry_flux_type"] == 1 or abs(desc.params["bdry_alpha"]) <= 1e-9
+    else:
+        for k in ("bdry_flux_type", "bdry_alpha"):
+            assert abs(desc.params[k] - want.params[k]) <= 1e-9, k
+    assert dict(desc.bcs) == {"pec": BC_PEC, "pmc": BC_PMC, "abs": BC_ABSORB}
+    assert desc.fields["coeffs"] == [("epsilon", None), ("mu", None)]
+
+
+def test_material_arguments():
+    d, cls, F = _discr("3d")
+    x = d.nodes
+    eps = hb.TimeConstantGivenFunction(lambda p: 1.0 + 0.5 * p[..., 0] ** 2)
+    op = hb.MaxwellOperator(eps, lambda p: 2.0 + 0.0 * p[..., 0], flux_type=1)
+    e, m = op.material_values(d)
+    assert np.allclose(e, 1.0 + 0.5 * x[:, 0] ** 2) and np.allclose(m, 2.0)
+    assert not op.fixed_material
+    lam = op.max_eigenvalue(discr=d)
+    assert abs(lam - np.max(1 / np.sqrt(e * m))) <= 1e-15
+    assert op.estimate_timestep(d) > 0
+    with pytest.raises(ValueError):
+        op.max_eigenvalue()
+    with pytest.raises(RuntimeError):
+        op.c
+    with pytest.raises(NotImplementedError):
+        hb.MaxwellOperator(np.ones(len(d)), 1.0, flux_type=1, current=1.0)
+    fixed = hb.MaxwellOperator(2.0, 0.5, flux_type=1)
+    assert fixed.fixed_material and abs(fixed.c - 1.0) <= 1e-15
