@@ -258,8 +258,11 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
       if (nbr >= nb_end || (code & 3) >= d->nfaces || (code >> 2) >= d->nperm || code < 0)
         return fail(HB_ERR_INVALID_ARGUMENT, "connectivity entry out of range");
     } else {
-      if (code < HB_BC_NONE || code > HB_BC_ABSORB)
+      if (code < HB_BC_NONE || code > HB_BC_INCIDENT)
         return fail(HB_ERR_INVALID_ARGUMENT, "unknown boundary-condition kind");
+      if (code == HB_BC_INCIDENT && model != HB_MODEL_MAXWELL &&
+          model != HB_MODEL_MAXWELL_TM && model != HB_MODEL_MAXWELL_TE)
+        return fail(HB_ERR_INVALID_ARGUMENT, "incident boundary on a model other than Maxwell");
       if (code == HB_BC_GIVEN)
         max_given = std::max<int64_t>(max_given, ((int64_t)(-1 - nbr) + 1) * d->nfp);
     }

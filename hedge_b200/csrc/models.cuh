@@ -127,8 +127,9 @@ __device__ __forceinline__ int64_t model_src_index(int f, int64_t node, int64_t 
   else return f == 0 ? node : -1;
 }
 
-// Maxwell boundary states of (E, H) = u[0..3), u[3..6) (em.py:226-287):
-// PEC (-E, H), PMC (E, -H), first-order absorbing.  False: no boundary flux.
+// Maxwell boundary states of (E, H) = u[0..3), u[3..6) (em.py:226-307):
+// PEC (-E, H), PMC (E, -H), first-order absorbing, incident (zero data).
+// False: no boundary flux.
 template <typename T>
 __device__ __forceinline__ bool maxwell_bc3(const ModelParams& mp, int kind, const T* u,
                                             const T* n, T* uP) {
@@ -152,6 +153,10 @@ __device__ __forceinline__ bool maxwell_bc3(const ModelParams& mp, int kind, con
       uP[k] = e[k] + T(0.5) * (nne[k] - Z * nh[k]);
       uP[3 + k] = h[k] + T(0.5) * (nnh[k] + Y * ne[k]);
     }
+  } else if (kind == HB_BC_INCIDENT) {
+    // the reference's default incident data is zero (em.py:289-307)
+#pragma unroll
+    for (int k = 0; k < 6; ++k) uP[k] = T(0);
   } else {
     return false;
   }

@@ -64,8 +64,8 @@ import numpy as np
 from . import flux as fl
 from . import optemplate as ot
 from .mesh import TAG_ALL, TAG_NONE
-from .models import (BC_ABSORB, BC_DIRICHLET, BC_GIVEN, BC_NEUMANN, BC_NONE, BC_PEC, BC_PMC,
-                     BC_RADIATION, MODEL_ADVECTION, MODEL_MAXWELL, MODEL_MAXWELL_TE,
+from .models import (BC_ABSORB, BC_DIRICHLET, BC_GIVEN, BC_INCIDENT, BC_NEUMANN, BC_NONE,
+                     BC_PEC, BC_PMC, BC_RADIATION, MODEL_ADVECTION, MODEL_MAXWELL, MODEL_MAXWELL_TE,
                      MODEL_MAXWELL_TM, MODEL_VARADV, MODEL_VARWAVE, MODEL_WAVE,
                      MaxwellOperator, TEMaxwellOperator, TMMaxwellOperator, OpTemplate,
                      StrongAdvectionOperator, StrongWaveOperator,
@@ -593,7 +593,7 @@ class _VarWave(_Wave):
 
 class _Maxwell(_Family):
     model = MODEL_MAXWELL
-    kinds = (BC_PEC, BC_PMC, BC_ABSORB)
+    kinds = (BC_PEC, BC_PMC, BC_ABSORB, BC_INCIDENT)
     source_outputs = (0, 1, 2)
     cls = MaxwellOperator
 
@@ -630,12 +630,13 @@ class _Maxwell(_Family):
         return ["lf", self._fit(user, roles, params, ctx, "bdry_flux_type", (tag, kind))]
 
     def build(self, roles, p, bc):
-        t = {BC_PEC: TAG_NONE, BC_PMC: TAG_NONE, BC_ABSORB: TAG_NONE}
+        t = {BC_PEC: TAG_NONE, BC_PMC: TAG_NONE, BC_ABSORB: TAG_NONE, BC_INCIDENT: TAG_NONE}
         if bc is not None:
             t[bc[1]] = bc[0]
         m = self.cls(p["eps"], p["mu"], p["flux_type"],
                      bdry_flux_type=p.get("bdry_flux_type", p["flux_type"]),
-                     pec_tag=t[BC_PEC], pmc_tag=t[BC_PMC], absorb_tag=t[BC_ABSORB])
+                     pec_tag=t[BC_PEC], pmc_tag=t[BC_PMC], absorb_tag=t[BC_ABSORB],
+                     incident_tag=t[BC_INCIDENT])
         # E_c's rhs source s_c = -J_c / eps: the current is -eps s
         ne = m.n_e
         srcs = getattr(roles, "sources", None)
@@ -662,12 +663,13 @@ class _MaxwellVar(_Maxwell):
             else None
 
     def build(self, roles, p, bc):
-        t = {BC_PEC: TAG_NONE, BC_PMC: TAG_NONE, BC_ABSORB: TAG_NONE}
+        t = {BC_PEC: TAG_NONE, BC_PMC: TAG_NONE, BC_ABSORB: TAG_NONE, BC_INCIDENT: TAG_NONE}
         if bc is not None:
             t[bc[1]] = bc[0]
         m = self.cls(roles.coeffs[0], roles.coeffs[1], p["flux_type"],
                      bdry_flux_type=p.get("bdry_flux_type", p["flux_type"]),
-                     pec_tag=t[BC_PEC], pmc_tag=t[BC_PMC], absorb_tag=t[BC_ABSORB])
+                     pec_tag=t[BC_PEC], pmc_tag=t[BC_PMC], absorb_tag=t[BC_ABSORB],
+                     incident_tag=t[BC_INCIDENT])
         return m, _comps(m.op_template(w=roles.state))
 
 

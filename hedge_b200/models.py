@@ -52,6 +52,7 @@ BC_RADIATION = 4   # wave: characteristic
 BC_PEC = 5         # Maxwell: (-E, H)
 BC_PMC = 6         # Maxwell: (E, -H)
 BC_ABSORB = 7      # Maxwell: first-order absorbing
+BC_INCIDENT = 8    # Maxwell: incident field, zero data (0, 0)
 
 
 @dataclass
@@ -407,19 +408,33 @@ class MaxwellOperator(HyperbolicOperator):
 
     def __init__(self, epsilon, mu, flux_type, bdry_flux_type=None,
                  pec_tag=TAG_ALL, pmc_tag=TAG_NONE, absorb_tag=TAG_NONE,
-                 incident_tag=TAG_NONE, current=0, dimensions=None):
+                 incident_tag=TAG_NONE, incident_bc=lambda maxwell_op, e, h: 0,
+                 current=0, dimensions=None):
         """``current``: the source current J of em.py:192-214 (the E equations
         read eps dE/dt = curl H - J) over the carried E components: 0,
         numbers, a volume field [n_E, K*Np] (array, tensor or vectors), or a
-        template vector."""
+        template vector.
+
+        ``incident_tag`` / ``incident_bc``: the incident-field boundary of
+        em.py:289-307, whose exterior state is -incident_bc(op, e, h).  The
+        reference's default incident_bc (zero) is carried: the exterior
+        state is zero on those faces (all kernels).  Other incident data is
+        refused."""
         self.dimensions = dimensions or self._default_dimensions
         if self.dimensions != self._default_dimensions:
             raise NotImplementedError("%s is a %dD system" % (type(self).__name__,
                                                              self._default_dimensions))
         self.fixed_material = bool(np.isscalar(epsilon) and np.isscalar(mu))
         self.current = current
+        self.incident_bc_data = incident_bc
         if incident_tag is not TAG_NONE:
-            raise NotImplementedError("incident boundary data is not on this path")
+            e, h = self.split_eh(ot.make_sym_vector("w", self.n_fields))
+            data = incident_bc(self, e, h)
+            if not ot.is_zero(data) and not (
+                    isinstance(data, (np.ndarray, list, tuple))
+                    and all(ot.is_zero(x) for x in np.asarray(data, dtype=object).reshape(-1))):
+                raise NotImplementedError("incident boundary data other than zero is "
+                                          "not on this path")
         if self.fixed_material:
             self.epsilon, self.mu = float(epsilon), float(mu)
         else:
@@ -626,8 +641,12 @@ class MaxwellOperator(HyperbolicOperator):
 
             def bvec(tag, bc):
                 return ot.join_fields(B(tag) * eps, B(tag) * mu, bc)
+        # incident boundary: the exterior state is -(incident data) = 0
+        # (em.py:289-307)
+        incident = np.array([0] * F, dtype=object)
         bdry = sum(bdry_flux_op(ot.BoundaryPair(flux_w, bvec(tag, bc), tag)) for tag, bc in
-                   [(self.pec_tag, pec), (self.pmc_tag, pmc), (self.absorb_tag, absorb)])
+                   [(self.pec_tag, pec), (self.pmc_tag, pmc), (self.absorb_tag, absorb),
+                    (self.incident_tag, incident)])
         return _remember(self, (-self.local_derivatives(w)
                                 + ot.InverseMassOperator()(flux_op(flux_w) + bdry)) / divisor)
 
@@ -644,7 +663,7 @@ class MaxwellOperator(HyperbolicOperator):
         return OpTemplate(self.model_id, self.dimensions, self.n_fields, ft, params,
                           [(self.pec_tag, BC_PEC), (self.pmc_tag, BC_PMC),
                            (self.absorb_tag, BC_ABSORB),
-                           (self.incident_tag, BC_NONE)], self)
+                           (self.incident_tag, BC_INCIDENT)], self)
 
     def bc_tags(self):
         return [self.pec_tag, self.absorb_tag, self.incident_tag]

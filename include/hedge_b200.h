@@ -64,7 +64,10 @@ enum {
 
 enum {
   HB_BC_NONE = 0, HB_BC_GIVEN = 1, HB_BC_DIRICHLET = 2, HB_BC_NEUMANN = 3,
-  HB_BC_RADIATION = 4, HB_BC_PEC = 5, HB_BC_PMC = 6, HB_BC_ABSORB = 7
+  HB_BC_RADIATION = 4, HB_BC_PEC = 5, HB_BC_PMC = 6, HB_BC_ABSORB = 7,
+  HB_BC_INCIDENT = 8  /* Maxwell models only: incident-field boundary with the
+                         reference's default incident data (em.py:289-307,
+                         incident_bc returning 0): the exterior state is zero */
 };
 
 typedef struct hb_discr hb_discr;

@@ -37,7 +37,8 @@ _MAXWELLS = (OR_MAXWELL, OR_MAXWELL_TM, OR_MAXWELL_TE)
 # positions of a Maxwell system's fields in (Ex Ey Ez Hx Hy Hz), E count
 _SLOTS = {OR_MAXWELL: ([0, 1, 2, 3, 4, 5], 3), OR_MAXWELL_TM: ([2, 3, 4], 1),
           OR_MAXWELL_TE: ([0, 1, 5], 2)}
-BC_NONE, BC_GIVEN, BC_DIRICHLET, BC_NEUMANN, BC_RADIATION, BC_PEC, BC_PMC, BC_ABSORB = range(8)
+(BC_NONE, BC_GIVEN, BC_DIRICHLET, BC_NEUMANN, BC_RADIATION, BC_PEC, BC_PMC, BC_ABSORB,
+ BC_INCIDENT) = range(9)
 
 
 class or_flux_params(C.Structure):
@@ -226,7 +227,7 @@ class OracleRHS:
                 out[C0 + 1:] = 0.5 * normals.T * (nv - sgn * u)
             return out
         if m in _MAXWELLS:
-            # em.py:226-287 on the six components (2D systems embedded, n_z = 0)
+            # em.py:226-307 on the six components (2D systems embedded, n_z = 0)
             slots, _ = _SLOTS[m]
             full = np.zeros((6, ab.shape[1]))
             full[slots] = ab
@@ -243,6 +244,9 @@ class OracleRHS:
                 ne, nh = np.cross(nrm, e.T).T, np.cross(nrm, h.T).T
                 nne, nnh = np.cross(nrm, ne.T).T, np.cross(nrm, nh.T).T
                 out = np.vstack([e + 0.5 * (nne - Z * nh), h + 0.5 * (nnh + ne / Z)])
+            elif kind == BC_INCIDENT:
+                # -incident_bc_data with the default (zero) data (em.py:289-307)
+                out = np.zeros_like(full)
             else:
                 raise ValueError("unsupported boundary kind %d" % kind)
             return out[slots]
