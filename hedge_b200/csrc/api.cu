@@ -263,7 +263,7 @@ hb_status hb_op_create(hb_discr* discr, const hb_op_desc* desc, hb_op** out) {
       if (code == HB_BC_INCIDENT && model != HB_MODEL_MAXWELL &&
           model != HB_MODEL_MAXWELL_TM && model != HB_MODEL_MAXWELL_TE)
         return fail(HB_ERR_INVALID_ARGUMENT, "incident boundary on a model other than Maxwell");
-      if (code == HB_BC_GIVEN)
+      if (code == HB_BC_GIVEN || (code == HB_BC_INCIDENT && desc->num_given_bdry_nodes > 0))
         max_given = std::max<int64_t>(max_given, ((int64_t)(-1 - nbr) + 1) * d->nfp);
     }
   }
@@ -338,7 +338,7 @@ hb_status hb_op_destroy(hb_op* handle) {
 }
 
 static hb_status check_inputs(Op* op, const void* q_in, const void* q_out,
-                              const double* coeff) {
+                              const double* coeff, const double* bdry) {
   if (!q_in || !q_out) return fail(HB_ERR_INVALID_ARGUMENT, "null state pointer");
   if (q_in == q_out) return fail(HB_ERR_INVALID_ARGUMENT, "output aliases the input state");
   if (op->n_halo > 0 && !op->halo)
@@ -351,6 +351,9 @@ static hb_status check_inputs(Op* op, const void* q_in, const void* q_out,
                        op->model == HB_MODEL_MAXWELL_TE;
   if (maxwell && coeff && op->split)
     return fail(HB_ERR_UNSUPPORTED, "Maxwell with variable material: CUDA-core kernels only "
+                                    "(HB_PREC_FP64, HB_PREC_FP32_SIMT)");
+  if (maxwell && bdry && op->split)
+    return fail(HB_ERR_UNSUPPORTED, "Maxwell incident data: CUDA-core kernels only "
                                     "(HB_PREC_FP64, HB_PREC_FP32_SIMT)");
   return HB_OK;
 }
@@ -383,7 +386,7 @@ hb_status hb_rhs(hb_op* handle, const void* q, void* rhs, const double* coeff,
                  const double* bdry, const double* source, void* stream) {
   if (!handle) return fail(HB_ERR_INVALID_ARGUMENT, "null operator");
   Op* op = reinterpret_cast<Op*>(handle);
-  hb_status st = check_inputs(op, q, rhs, coeff);
+  hb_status st = check_inputs(op, q, rhs, coeff, bdry);
   if (st) return st;
   return run(op, 0, 0, 0, 0, q, rhs, nullptr, coeff, bdry, source, stream);
 }
@@ -393,7 +396,7 @@ hb_status hb_lsrk_stage(hb_op* handle, double a, double b, double dt, const void
                         const double* source, void* stream) {
   if (!handle) return fail(HB_ERR_INVALID_ARGUMENT, "null operator");
   Op* op = reinterpret_cast<Op*>(handle);
-  hb_status st = check_inputs(op, q_in, q_out, coeff);
+  hb_status st = check_inputs(op, q_in, q_out, coeff, bdry);
   if (st) return st;
   if (!res) return fail(HB_ERR_INVALID_ARGUMENT, "null residual pointer");
   return run(op, 1, a, b, dt, q_in, q_out, res, coeff, bdry, source, stream);
@@ -404,7 +407,7 @@ hb_status hb_rhs_elements(hb_op* handle, int64_t el_begin, int64_t el_end, const
                           const double* source, void* stream) {
   if (!handle) return fail(HB_ERR_INVALID_ARGUMENT, "null operator");
   Op* op = reinterpret_cast<Op*>(handle);
-  hb_status st = check_inputs(op, q, rhs, coeff);
+  hb_status st = check_inputs(op, q, rhs, coeff, bdry);
   if (st) return st;
   if ((st = check_range(op, el_begin, el_end))) return st;
   return run(op, 0, 0, 0, 0, q, rhs, nullptr, coeff, bdry, source, stream, el_begin, el_end);
@@ -416,7 +419,7 @@ hb_status hb_lsrk_stage_elements(hb_op* handle, int64_t el_begin, int64_t el_end
                                  const double* source, void* stream) {
   if (!handle) return fail(HB_ERR_INVALID_ARGUMENT, "null operator");
   Op* op = reinterpret_cast<Op*>(handle);
-  hb_status st = check_inputs(op, q_in, q_out, coeff);
+  hb_status st = check_inputs(op, q_in, q_out, coeff, bdry);
   if (st) return st;
   if (!res) return fail(HB_ERR_INVALID_ARGUMENT, "null residual pointer");
   if ((st = check_range(op, el_begin, el_end))) return st;

@@ -270,6 +270,20 @@ __global__ void __launch_bounds__(256) rhs_simt_kernel(SimtArgs<T, S> a) {
             }
             have = model_bc<MODEL, DIM, T>(mpl, cn.y, uM, n, given, uP);
           }
+          if constexpr (MAXW) {
+            // incident data d (em.py:289-307): exterior state -d, field f's
+            // values at bdry[f * n_given + node]; no data: zero exterior
+            if (have && cn.y == HB_BC_INCIDENT && a.bdry != nullptr) {
+              const int64_t bi = (int64_t)(-1 - cn.x) * nfp + k;
+              if (bi >= a.n_given) {
+                flag(a.err, DEV_BAD_BDRY_INDEX);
+                have = false;
+              } else {
+#pragma unroll
+                for (int f = 0; f < F; ++f) uP[f] = -T(__ldg(a.bdry + f * a.n_given + bi));
+              }
+            }
+          }
         }
         T* dst = sfl + e * nfpt + p;
         if (have) {

@@ -23,8 +23,8 @@ from .facegroups import Boundary, build_compact_connectivity, build_interior_fac
 from .mesh import Mesh, TAG_ALL, TAG_NONE
 from .lowering import as_descriptor
 from .optemplate import Expr
-from .models import (BC_GIVEN, BC_NONE, MODEL_MAXWELL, MODEL_MAXWELL_TE, MODEL_MAXWELL_TM,
-                     MODEL_VARADV, MODEL_VARWAVE, MODEL_WAVE,
+from .models import (BC_GIVEN, BC_INCIDENT, BC_NONE, MODEL_MAXWELL, MODEL_MAXWELL_TE,
+                     MODEL_MAXWELL_TM, MODEL_VARADV, MODEL_VARWAVE, MODEL_WAVE,
                      MODEL_ADVECTION, OpTemplate)
 from .quadrature import ElementQuadrature
 from .refelem import make_element
@@ -372,8 +372,9 @@ class PointEvaluator:
 def build_face_table(discr, ot):
     """Host face table of an operator: [K][Nf][2] int32, interior faces
     (neighbour, nbr_face | perm << 2), boundary faces (-1 - b, BC kind) with
-    b numbering the BC_GIVEN faces; and the number of given boundary nodes
-    and the given tag."""
+    b numbering the BC_GIVEN faces (or the Maxwell incident faces with
+    incident data); and the number of given boundary nodes and the given
+    tag."""
     ot = as_descriptor(ot, discr.dimensions, discr.mesh)
     mesh = discr.mesh
     # BC coverage is checked where the reference checks it: in the models'
@@ -392,7 +393,7 @@ def build_face_table(discr, ot):
         if len(ef) == 0:
             continue
         code[ef[:, 0], ef[:, 1]] = kind
-        if kind == BC_GIVEN:
+        if kind == BC_GIVEN or (kind == BC_INCIDENT and ot.params.get("incident_data")):
             nbr[ef[:, 0], ef[:, 1]] = -1 - np.arange(len(ef))
             given_tag = tag
             n_given = len(ef) * discr.Nfp
@@ -443,12 +444,15 @@ class CompiledOperator:
         prec = PRECISIONS[precision] if precision != "plain" else (
             _native.PREC_FP64 if discr.default_scalar_type == np.float64
             else _native.PREC_FP32)
-        # Maxwell with variable material: the CUDA-core kernels
+        # Maxwell with variable material or incident data: the CUDA-core kernels
         self.var_material = bool(ot.params.get("variable_material"))
-        if self.var_material:
+        self.incident_data = bool(ot.params.get("incident_data"))
+        self.given_rows = ot.n_fields if self.incident_data else 1
+        if self.var_material or self.incident_data:
             if prec in (_native.PREC_BF16X3, _native.PREC_FP16X3):
-                raise NotImplementedError("Maxwell with variable material: fp64 or fp32 "
-                                          "(CUDA-core kernels)")
+                raise NotImplementedError(
+                    "Maxwell with %s: fp64 or fp32 (CUDA-core kernels)"
+                    % ("variable material" if self.var_material else "incident data"))
             if prec == _native.PREC_FP32:
                 prec = _native.PREC_FP32_SIMT
         self.prec_code = prec
@@ -638,9 +642,14 @@ class CompiledOperator:
         torch = _torch()
         if bc_in is None:
             raise ValueError("this operator needs boundary values (bc_in)")
-        t = self.discr.to_device(bc_in, torch.float64)
-        if t.numel() != self.n_given:
-            raise ValueError("bc_in must have %d entries" % self.n_given)
+        if isinstance(bc_in, (list, tuple)) or (isinstance(bc_in, np.ndarray)
+                                                 and bc_in.dtype == object):
+            bc_in = torch.stack([self.discr.to_device(x, torch.float64).reshape(-1)
+                                 for x in bc_in])
+        t = self.discr.to_device(bc_in, torch.float64).contiguous()
+        if t.numel() != self.given_rows * self.n_given:
+            raise ValueError("bc_in must have %s%d entries" % (
+                "%d x " % self.given_rows if self.given_rows > 1 else "", self.n_given))
         return t, t.data_ptr()
 
     def _stream(self):
@@ -744,6 +753,11 @@ class CompiledOperator:
             w = [kwargs[n] if i is None else kwargs[n][i] for n, i in names["state_keys"]]
         if names.get("given") in kwargs:
             bc_in = kwargs.pop(names["given"])
+        elif names.get("given_keys") and all(n in kwargs for n, _ in names["given_keys"]):
+            # incident data components named one by one
+            bc_in = [kwargs[n] if i is None else kwargs[n][i] for n, i in names["given_keys"]]
+            for n, _ in names["given_keys"]:
+                kwargs.pop(n, None)
         if names.get("coeffs") and all(n in kwargs for n, _ in names["coeffs"]):
             # variable material: epsilon, mu by their template names
             vals = [kwargs.pop(n) if i is None else kwargs.pop(n)[i] for n, i in names["coeffs"]]

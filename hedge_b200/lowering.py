@@ -471,11 +471,12 @@ def _close(a, b):
 # kernel models
 
 class _Roles:
-    def __init__(self, state, coeff, given, source, coeffs=()):
+    def __init__(self, state, coeff, given, source, coeffs=(), givens=()):
         self.state = state          # object array of the state Fields
         self.coeff = coeff          # Field or None (one coefficient field)
         self.coeffs = list(coeffs)  # every coefficient field (Maxwell material: eps, mu)
-        self.given = given          # Field or None
+        self.given = given          # Field or None (one given boundary field)
+        self.givens = list(givens)  # every given boundary field (Maxwell incident data)
         self.source = source        # expression of the user's source (or 0)
 
     def names(self):
@@ -489,6 +490,11 @@ class _Roles:
             d["coeffs"] = [(f.name, f.index) for f in self.coeffs]
         if self.given is not None:
             d["given"] = self.given.name
+        elif len(self.givens) > 1:
+            g = self.givens
+            if all(f.name == g[0].name for f in g):
+                d["given"] = g[0].name
+            d["given_keys"] = [f.key for f in g]
         return d
 
 
@@ -629,6 +635,15 @@ class _Maxwell(_Family):
         ctx = _Ctx(dims, face=tag, coeff_keys=[f.key for f in roles.coeffs])
         return ["lf", self._fit(user, roles, params, ctx, "bdry_flux_type", (tag, kind))]
 
+    @staticmethod
+    def _incident(roles, bc):
+        """incident_bc of the kernel model: the given boundary fields (one per
+        component, the data whose negative is the exterior state), or zero."""
+        if bc is not None and bc[1] == BC_INCIDENT and len(roles.givens) > 1:
+            data = np.array(roles.givens, dtype=object)
+            return lambda op, e, h: data
+        return lambda op, e, h: 0
+
     def build(self, roles, p, bc):
         t = {BC_PEC: TAG_NONE, BC_PMC: TAG_NONE, BC_ABSORB: TAG_NONE, BC_INCIDENT: TAG_NONE}
         if bc is not None:
@@ -636,7 +651,7 @@ class _Maxwell(_Family):
         m = self.cls(p["eps"], p["mu"], p["flux_type"],
                      bdry_flux_type=p.get("bdry_flux_type", p["flux_type"]),
                      pec_tag=t[BC_PEC], pmc_tag=t[BC_PMC], absorb_tag=t[BC_ABSORB],
-                     incident_tag=t[BC_INCIDENT])
+                     incident_tag=t[BC_INCIDENT], incident_bc=self._incident(roles, bc))
         # E_c's rhs source s_c = -J_c / eps: the current is -eps s
         ne = m.n_e
         srcs = getattr(roles, "sources", None)
@@ -669,7 +684,7 @@ class _MaxwellVar(_Maxwell):
         m = self.cls(roles.coeffs[0], roles.coeffs[1], p["flux_type"],
                      bdry_flux_type=p.get("bdry_flux_type", p["flux_type"]),
                      pec_tag=t[BC_PEC], pmc_tag=t[BC_PMC], absorb_tag=t[BC_ABSORB],
-                     incident_tag=t[BC_INCIDENT])
+                     incident_tag=t[BC_INCIDENT], incident_bc=self._incident(roles, bc))
         return m, _comps(m.op_template(w=roles.state))
 
 
@@ -797,8 +812,15 @@ def lower(template, dimensions, mesh=None):
     st_keys = {x.key for x in state}
     co_keys = {x.key for x in coeff}
     given = [f for k, f in scan.given_fields.items() if k not in st_keys | co_keys]
-    if len(given) > 1:
-        raise NotImplementedError("more than one given boundary field")
+    if len(given) > 1 and len(given) != F:
+        raise NotImplementedError("%d given boundary fields: one, or one per output "
+                                  "(Maxwell incident data)" % len(given))
+    # several given fields: a Maxwell system's incident data, one per
+    # component, in the order the boundary data names them (a vector's
+    # components in index order)
+    if len(given) > 1 and all(f.name == given[0].name and f.index is not None
+                              for f in given):
+        given.sort(key=lambda f: f.index)
     src_fields = {k: f for k, f in scan.outside_fields.items()
                   if k not in st_keys | co_keys and k not in diff}
     roles_keys = st_keys | co_keys | {f.key for f in given}
@@ -809,7 +831,8 @@ def lower(template, dimensions, mesh=None):
     src_outputs = [o for o in range(F) if src_terms[o] or src_consts[o] != 0]
     state_arr = ot.join_fields(state)
     roles = _Roles(state_arr, coeff[0] if len(coeff) == 1 else None,
-                   given[0] if given else None, src_exprs[0], coeffs=coeff)
+                   given[0] if len(given) == 1 else None, src_exprs[0], coeffs=coeff,
+                   givens=given)
     roles.sources = src_exprs
 
     # volume coefficients V[f, g, x]: unit derivative probes less the
@@ -912,6 +935,12 @@ def lower(template, dimensions, mesh=None):
             desc = model.descriptor()
             bcs = [(t, k) for t, k in bcs if not (k == BC_NONE and t is TAG_ALL)]
             names = roles.names()
+            if len(roles.givens) > 1:
+                inc = [t for t, k in bcs if k == BC_INCIDENT]
+                if len(inc) != 1:
+                    fail(3, "given boundary fields outside one incident boundary")
+                    continue
+                desc.params["incident_data"] = True
             if desc.model in (MODEL_MAXWELL, MODEL_MAXWELL_TM, MODEL_MAXWELL_TE):
                 # per E component: the value added to its rhs, const + coef * field
                 names["sources"] = [(o, float(src_consts[o]),

@@ -417,9 +417,11 @@ class MaxwellOperator(HyperbolicOperator):
 
         ``incident_tag`` / ``incident_bc``: the incident-field boundary of
         em.py:289-307, whose exterior state is -incident_bc(op, e, h).  The
-        reference's default incident_bc (zero) is carried: the exterior
-        state is zero on those faces (all kernels).  Other incident data is
-        refused."""
+        reference's default incident_bc (zero) gives a zero exterior state
+        (every kernel); incident data given per call as boundary vectors
+        (template fields outside any BoundarizeOperator, one per carried
+        component, e.g. ``make_sym_vector("inc", n_fields)``) runs on the
+        CUDA-core kernels."""
         self.dimensions = dimensions or self._default_dimensions
         if self.dimensions != self._default_dimensions:
             raise NotImplementedError("%s is a %dD system" % (type(self).__name__,
@@ -427,14 +429,17 @@ class MaxwellOperator(HyperbolicOperator):
         self.fixed_material = bool(np.isscalar(epsilon) and np.isscalar(mu))
         self.current = current
         self.incident_bc_data = incident_bc
+        self.incident_data = None     # [n_fields] template terms, or None (zero)
         if incident_tag is not TAG_NONE:
             e, h = self.split_eh(ot.make_sym_vector("w", self.n_fields))
             data = incident_bc(self, e, h)
-            if not ot.is_zero(data) and not (
-                    isinstance(data, (np.ndarray, list, tuple))
-                    and all(ot.is_zero(x) for x in np.asarray(data, dtype=object).reshape(-1))):
-                raise NotImplementedError("incident boundary data other than zero is "
-                                          "not on this path")
+            if not ot.is_zero(data):
+                arr = np.asarray(data, dtype=object).reshape(-1)
+                if len(arr) != self.n_fields:
+                    raise ValueError("incident data: %d components, one per carried field"
+                                     % self.n_fields)
+                if not all(ot.is_zero(x) for x in arr):
+                    self.incident_data = arr
         if self.fixed_material:
             self.epsilon, self.mu = float(epsilon), float(mu)
         else:
@@ -641,9 +646,10 @@ class MaxwellOperator(HyperbolicOperator):
 
             def bvec(tag, bc):
                 return ot.join_fields(B(tag) * eps, B(tag) * mu, bc)
-        # incident boundary: the exterior state is -(incident data) = 0
+        # incident boundary: the exterior state is -(incident data)
         # (em.py:289-307)
-        incident = np.array([0] * F, dtype=object)
+        incident = np.array([0] * F, dtype=object) if self.incident_data is None else \
+            np.array([-x for x in self.incident_data], dtype=object)
         bdry = sum(bdry_flux_op(ot.BoundaryPair(flux_w, bvec(tag, bc), tag)) for tag, bc in
                    [(self.pec_tag, pec), (self.pmc_tag, pmc), (self.absorb_tag, absorb),
                     (self.incident_tag, incident)])
@@ -660,6 +666,8 @@ class MaxwellOperator(HyperbolicOperator):
                   "bdry_flux_type": bft, "bdry_alpha": balpha}
         if not self.fixed_material:
             params["variable_material"] = True
+        if self.incident_data is not None and self.incident_tag is not TAG_NONE:
+            params["incident_data"] = True
         return OpTemplate(self.model_id, self.dimensions, self.n_fields, ft, params,
                           [(self.pec_tag, BC_PEC), (self.pmc_tag, BC_PMC),
                            (self.absorb_tag, BC_ABSORB),

@@ -65,9 +65,10 @@ enum {
 enum {
   HB_BC_NONE = 0, HB_BC_GIVEN = 1, HB_BC_DIRICHLET = 2, HB_BC_NEUMANN = 3,
   HB_BC_RADIATION = 4, HB_BC_PEC = 5, HB_BC_PMC = 6, HB_BC_ABSORB = 7,
-  HB_BC_INCIDENT = 8  /* Maxwell models only: incident-field boundary with the
-                         reference's default incident data (em.py:289-307,
-                         incident_bc returning 0): the exterior state is zero */
+  HB_BC_INCIDENT = 8  /* Maxwell models only: incident-field boundary
+                         (em.py:289-307), exterior state -(incident data):
+                         the bdry argument's [F][n] values, or zero (the
+                         reference's default incident_bc) when it is NULL */
 };
 
 typedef struct hb_discr hb_discr;
@@ -100,7 +101,8 @@ hb_status hb_discr_destroy(hb_discr* discr);
 /* One compiled model operator.  conn: host [K][nfaces][2] int32,
  * interior face: (neighbour element, nbr_face | perm_id << 2);
  * boundary face: (-1 - b, bc kind), b = the face's number in the
- * BC_GIVEN boundary vector (nodes b*nfp .. b*nfp+nfp-1). */
+ * BC_GIVEN (or Maxwell HB_BC_INCIDENT) boundary vector (nodes
+ * b*nfp .. b*nfp+nfp-1); num_given_bdry_nodes = that vector's length. */
 /* Quadrature matrices of one reference element for one degree
  * (hedge/discretization/local.py:545-690, QuadratureInfo), host FP64,
  * row-major.  Weights are the reference element's: d r / d x and
@@ -149,7 +151,10 @@ hb_status hb_op_destroy(hb_op* op);
  * [dim][K*Np] FP64, or for the Maxwell models the material [eps | mu]
  * [2][K*Np] FP64 (variable material, em.py:38-100, 309-371; NULL: the
  * descriptor's eps, mu; CUDA-core precisions only, no halo faces) (else
- * NULL); bdry: BC_GIVEN values [n] FP64 (else NULL);
+ * NULL); bdry: BC_GIVEN values [n] FP64, or for the Maxwell models the
+ * incident data [F][n] FP64 (exterior state -data on HB_BC_INCIDENT faces;
+ * NULL: zero data; CUDA-core precisions only), n = num_given_bdry_nodes
+ * (else NULL);
  * source: var-c / constant-c wave source on u, [K*Np] FP64 (else NULL). */
 hb_status hb_rhs(hb_op* op, const void* q, void* rhs, const double* coeff,
                  const double* bdry, const double* source, void* stream);

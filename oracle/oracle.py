@@ -245,7 +245,10 @@ class OracleRHS:
                 nne, nnh = np.cross(nrm, ne.T).T, np.cross(nrm, nh.T).T
                 out = np.vstack([e + 0.5 * (nne - Z * nh), h + 0.5 * (nnh + ne / Z)])
             elif kind == BC_INCIDENT:
-                # -incident_bc_data with the default (zero) data (em.py:289-307)
+                # -(incident data) (em.py:289-307): the given [F][n] values,
+                # or the default zero data
+                if bc_in is not None:
+                    return -np.asarray(bc_in, dtype=np.float64).reshape(len(slots), -1)
                 out = np.zeros_like(full)
             else:
                 raise ValueError("unsupported boundary kind %d" % kind)

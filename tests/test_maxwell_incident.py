@@ -1,9 +1,10 @@
-"""Maxwell's incident-field boundary (em.py:289-307) with the reference's
-default incident data (zero), host side: the template's exterior state is
-zero on the incident faces; the jit-loop oracle and the template executor
-agree on it (3D, TM, TE; fixed and variable material; every flux type); the
-lowering names the incident kind; bind checks that the tag is covered; and
-incident data other than zero is refused."""
+"""Maxwell's incident-field boundary (em.py:289-307), host side: with the
+reference's default incident data (zero) the exterior state is zero on the
+incident faces, with incident data given per call as boundary vectors it
+is minus the data; the jit-loop oracle and the template executor agree on
+both (3D, TM, TE; fixed and variable material; every flux type); the
+lowering names the incident kind and the data; bind checks that the tag is
+covered; and data of the wrong shape is refused."""
 import numpy as np
 import pytest
 
@@ -105,9 +106,69 @@ def test_bind_checks_incident_coverage_and_refuses_data():
     conn = build_face_table(d, op.op_template())[0]
     n_inc = np.count_nonzero((conn[..., 0] < 0) & (conn[..., 1] == BC_INCIDENT))
     assert n_inc == len(d.mesh.boundary_faces("inc")) > 0
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(ValueError):
         hb.MaxwellOperator(1.0, 1.0, flux_type=1, incident_tag="inc",
-                           incident_bc=lambda o, e, h: ot.make_sym_vector("inc", 6))
+                           incident_bc=lambda o, e, h: ot.make_sym_vector("inc", 5))
     # zero data written out as a vector is the default
     hb.MaxwellOperator(1.0, 1.0, flux_type=1, incident_tag="inc",
                        incident_bc=lambda o, e, h: np.zeros(6, dtype=object))
+
+
+def _inc_op(cls, F, ft=0.5, bft="lf", eps=1.3, mu=0.7):
+    from hedge_b200 import optemplate as ot
+    return cls(eps, mu, flux_type=ft, bdry_flux_type=bft, pec_tag="pec", pmc_tag="pmc",
+               incident_tag="abs", incident_bc=lambda o, e, h: ot.make_sym_vector("inc", F))
+
+
+def _inc_data(d, F, seed=5):
+    x = d.get_boundary("abs").nodes
+    rng = np.random.default_rng(seed)
+    return np.stack([np.sin((f + 1) * x[:, 1] + 0.4 * f) + 0.1 * rng.standard_normal(len(x))
+                     for f in range(F)])
+
+
+@pytest.mark.parametrize("ft,bft", [(1, 1), (0.5, "lf"), ("lf", 0.3)])
+@pytest.mark.parametrize("kind", ["3d", "tm", "te"])
+def test_incident_data_oracle_equals_executor(kind, ft, bft):
+    from oracle import OracleRHS
+    from optemplate_exec import TemplateExecutor
+    d, cls, F = _discr(kind)
+    op = _inc_op(cls, F, ft, bft)
+    w = np.random.default_rng(6).standard_normal((F, len(d)))
+    g = _inc_data(d, F)
+    ref = np.asarray(TemplateExecutor(d)(op.op_template(), w=w, inc=g), dtype=np.float64)
+    got = OracleRHS(d, op.descriptor())(w, bc_in=g)
+    assert rel_l2(got, ref) <= 1e-12
+    # zero data is the default incident boundary
+    zero = np.asarray(TemplateExecutor(d)(op.op_template(), w=w, inc=0 * g), dtype=np.float64)
+    base = np.asarray(TemplateExecutor(d)(_op(cls, ft, bft).op_template(), w=w),
+                      dtype=np.float64)
+    assert rel_l2(zero, base) <= 1e-13
+
+
+@pytest.mark.parametrize("kind", ["3d", "tm", "te"])
+def test_lowering_names_incident_data(kind):
+    from hedge_b200.discretization import build_face_table
+    d, cls, F = _discr(kind)
+    for eps in (1.3, np.linspace(1.0, 2.0, len(d))):
+        op = _inc_op(cls, F, 1, 1, eps=eps)
+        desc = lower(op.op_template(), d.dimensions, d.mesh)
+        assert dict(desc.bcs) == {"pec": BC_PEC, "pmc": BC_PMC, "abs": BC_INCIDENT}
+        assert desc.params.get("incident_data") is True
+        assert desc.fields["given"] == "inc"
+        assert op.descriptor().params.get("incident_data") is True
+        conn, n_given, tag = build_face_table(d, op.op_template())
+        assert tag == "abs" and n_given == len(d.mesh.boundary_faces("abs")) * d.Nfp
+        b = -1 - conn[..., 0][conn[..., 1] == BC_INCIDENT]
+        assert sorted(b.tolist()) == list(range(len(d.mesh.boundary_faces("abs"))))
+
+
+def test_incident_data_components_named_one_by_one():
+    from hedge_b200 import optemplate as ot
+    d, cls, F = _discr("tm")
+    data = np.array([ot.Field("ez_inc"), ot.Field("b_hx"), ot.Field("a_hy")], dtype=object)
+    op = cls(1.0, 1.0, flux_type=0.5, pec_tag="pec", pmc_tag="pmc", incident_tag="abs",
+             incident_bc=lambda o, e, h: data)
+    desc = lower(op.op_template(), d.dimensions, d.mesh)
+    assert desc.params.get("incident_data") is True
+    assert [n for n, _ in desc.fields["given_keys"]] == ["ez_inc", "b_hx", "a_hy"]
