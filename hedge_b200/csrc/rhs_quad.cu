@@ -29,7 +29,11 @@
 //      (hedge/timestep/runge_kutta.py:123-128).
 // The element work is FP64 FMA on the CUDA cores, also for FP32 state
 // vectors; the matrices sit in shared memory when they leave room for a
-// batch, else they are read through L1.
+// batch, else they are read through L1.  The kernel is bound by its
+// shared-memory loads, so each thread computes two volume points in C and
+// one node of two elements in D (every matrix entry loaded once serves two
+// products), and the rows of g_r have an odd stride so that the two
+// elements a warp reads in D sit in different banks.
 #include "common.cuh"
 
 #include <algorithm>
@@ -83,7 +87,7 @@ __host__ __device__ inline QuadLayout quad_layout(int ts, int dim, int np, int n
   L.oF = o;    o = qalign16(o + (size_t)ts * nf * nfp * nqf * ops);
   L.oL = o;    o = qalign16(o + (size_t)ts * nf * nqf * np * ops);
   L.ow = o;    o = qalign16(o + (size_t)ts * nv * E * np);
-  L.og = o;    o = qalign16(o + (size_t)ts * dim * E * nq);
+  L.og = o;    o = qalign16(o + (size_t)ts * dim * E * (nq | 1));
   L.ox = o;    o = qalign16(o + (size_t)ts * E * nf * nv * nfp);
   L.ofl = o;   o = qalign16(o + (size_t)ts * E * nf * nqf);
   L.ogeo = o;  o = qalign16(o + (size_t)ts * E * G);
@@ -123,6 +127,9 @@ __global__ void __launch_bounds__(256) rhs_quad_kernel(QuadArgs<T, IO> a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int np = a.np, nfp = a.nfp, nf = a.nf, E = a.E, G = a.G;
   const int nq = a.nq, nqf = a.nqf, nfq = nf * nqf;
+  // an odd row stride of the volume-point integrands: the rows of two
+  // elements that one warp reads in the projection start in different banks
+  const int nqs = nq | 1;
   const QuadLayout L = quad_layout((int)sizeof(T), DIM, np, nfp, nf, a.nperm, G, E, nq, nqf,
                                    a.ops_in_smem);
   const T* sI = a.ops_in_smem ? reinterpret_cast<const T*>(smem_raw + L.oI) : a.It;
@@ -130,7 +137,7 @@ __global__ void __launch_bounds__(256) rhs_quad_kernel(QuadArgs<T, IO> a) {
   const T* sF = a.ops_in_smem ? reinterpret_cast<const T*>(smem_raw + L.oF) : a.Ft;
   const T* sL = a.ops_in_smem ? reinterpret_cast<const T*>(smem_raw + L.oL) : a.Lt;
   T* sw = reinterpret_cast<T*>(smem_raw + L.ow);      // [NV][E][np]: u, v_0 ..
-  T* sg = reinterpret_cast<T*>(smem_raw + L.og);      // [DIM][E][nq]
+  T* sg = reinterpret_cast<T*>(smem_raw + L.og);      // [DIM][E][nqs]
   T* sx = reinterpret_cast<T*>(smem_raw + L.ox);      // [E][nf][NV][nfp] other side
   T* sfl = reinterpret_cast<T*>(smem_raw + L.ofl);    // [E][nf*nqf]
   T* sgeo = reinterpret_cast<T*>(smem_raw + L.ogeo);  // [E][G]
@@ -224,25 +231,40 @@ __global__ void __launch_bounds__(256) rhs_quad_kernel(QuadArgs<T, IO> a) {
     __syncthreads();
 
     // ---- C: volume points ----
-    for (int it = tid; it < ne * nq; it += nthr) {
-      const int e = it / nq;
-      const int q = it - e * nq;
-      T acc[NV];
+    // two volume points per thread (q and q + nqh): each staged nodal value
+    // serves both
+    const int nqh = (nq + 1) >> 1;
+    for (int it = tid; it < ne * nqh; it += nthr) {
+      const int e = it / nqh;
+      const int q = it - e * nqh;
+      const int q2 = q + nqh;
+      const bool two = q2 < nq;
+      const int q2c = two ? q2 : q;
+      T acc[NV], acc2[NV];
 #pragma unroll
-      for (int c = 0; c < NV; ++c) acc[c] = T(0);
+      for (int c = 0; c < NV; ++c) acc[c] = acc2[c] = T(0);
 #pragma unroll 4
       for (int j = 0; j < np; ++j) {
         const T I = sI[j * nq + q];
+        const T I2 = sI[j * nq + q2c];
 #pragma unroll
-        for (int c = 0; c < NV; ++c) acc[c] += I * sw[(c * E + e) * np + j];
+        for (int c = 0; c < NV; ++c) {
+          const T w = sw[(c * E + e) * np + j];
+          acc[c] += I * w;
+          acc2[c] += I2 * w;
+        }
       }
       const T* ge = sgeo + e * G;
 #pragma unroll
       for (int r = 0; r < DIM; ++r) {
-        T g = T(0);
+        T g = T(0), g2 = T(0);
 #pragma unroll
-        for (int x = 0; x < DIM; ++x) g += ge[r * DIM + x] * acc[1 + x];
-        sg[(r * E + e) * nq + q] = acc[0] * g;
+        for (int x = 0; x < DIM; ++x) {
+          g += ge[r * DIM + x] * acc[1 + x];
+          g2 += ge[r * DIM + x] * acc2[1 + x];
+        }
+        sg[(r * E + e) * nqs + q] = acc[0] * g;
+        if (two) sg[(r * E + e) * nqs + q2] = acc2[0] * g2;
       }
     }
     // ---- C: face points ----
@@ -295,27 +317,48 @@ __global__ void __launch_bounds__(256) rhs_quad_kernel(QuadArgs<T, IO> a) {
     __syncthreads();
 
     // ---- D: projection, lift, output ----
-    for (int it = tid; it < ne * np; it += nthr) {
+    // two elements per thread (e and e + eh): each operator entry serves both
+    const int eh = (ne + 1) >> 1;
+    for (int it = tid; it < eh * np; it += nthr) {
       const int e = it / np;
       const int i = it - e * np;
-      T acc = T(0);
+      const int e2 = e + eh;
+      const bool two = e2 < ne;
+      const int e2c = two ? e2 : e;
+      T acc = T(0), acc2 = T(0);
 #pragma unroll
       for (int r = 0; r < DIM; ++r) {
-        const T* gr = sg + (r * E + e) * nq;
+        const T* gr = sg + (r * E + e) * nqs;
+        const T* gr2 = sg + (r * E + e2c) * nqs;
         const T* br = sB + (size_t)r * nq * np + i;
 #pragma unroll 4
-        for (int q = 0; q < nq; ++q) acc += br[q * np] * gr[q];
+        for (int q = 0; q < nq; ++q) {
+          const T b = br[q * np];
+          acc += b * gr[q];
+          acc2 += b * gr2[q];
+        }
       }
       const T* fe = sfl + e * nfq;
+      const T* fe2 = sfl + e2c * nfq;
 #pragma unroll 4
-      for (int p = 0; p < nfq; ++p) acc -= sL[p * np + i] * fe[p];
-      const int64_t node = (el0 + e) * np + i;
-      if (a.mode == 0) {
-        a.rhs_out[node] = (IO)acc;
-      } else {
-        const T rv = T(a.ra) * (T)a.res[node] + T(a.dt) * acc;
-        a.res[node] = (IO)rv;
-        a.q_out[node] = (IO)(sw[e * np + i] + T(a.rb) * rv);
+      for (int p = 0; p < nfq; ++p) {
+        const T l = sL[p * np + i];
+        acc -= l * fe[p];
+        acc2 -= l * fe2[p];
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (h == 1 && !two) break;
+        const int ee = h ? e2 : e;
+        const T v = h ? acc2 : acc;
+        const int64_t node = (el0 + ee) * np + i;
+        if (a.mode == 0) {
+          a.rhs_out[node] = (IO)v;
+        } else {
+          const T rv = T(a.ra) * (T)a.res[node] + T(a.dt) * v;
+          a.res[node] = (IO)rv;
+          a.q_out[node] = (IO)(sw[ee * np + i] + T(a.rb) * rv);
+        }
       }
     }
   }
@@ -341,9 +384,10 @@ static hb_status quad_launch(Op* op, int mode, double ra, double rb, double dt,
     int max_optin = 0, sms = 0;
     HB_CUDA(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     HB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    // a batch of about 256 / np elements (one node per thread in the
-    // output phase); the matrices in shared memory when a batch of at least
-    // a quarter of that still fits beside them
+    // a batch of about 256 / np elements (two elements' node per thread in
+    // the output phase; twice that batch costs the third CTA per SM and ran
+    // slower); the matrices in shared memory when a batch of at least a
+    // quarter of that still fits beside them
     int E = std::max(1, 256 / d->np);
     int ops = 1;
     const int Emin = std::max(1, E / 4);

@@ -3,8 +3,10 @@
 Two calls in a row (a larger mesh, then a smaller one, so the second call
 reads a scratch array the first one left full), each within 1e-13 of hb_norm
 and, since both run the same kernels in the same reduction order, equal to it
-bit for bit; plus the size limit and operands that are not memory of the
-current device, both rejected before any launch."""
+bit for bit; a call captured into a CUDA graph (which an allocation or a
+synchronisation would break) and replayed; plus the size limit and operands
+that are not memory of the current device, both rejected before any
+launch."""
 import numpy as np
 import pytest
 
@@ -49,6 +51,31 @@ def test_noalloc_norm_matches_hb_norm_twice(cuda_device):
     got = _noalloc(d, u, mass, absjac)
     assert abs(got - d.norm(u)) <= TOL * d.norm(u)
     assert got == d.norm(u)
+
+
+def test_noalloc_norm_captures_in_a_cuda_graph(cuda_device):
+    """After its first call on the device, a call captures into a CUDA
+    graph (stream capture fails on an allocation or a synchronisation) and
+    the replay gives hb_norm's value bit for bit, also after the field
+    changed in place."""
+    import torch
+    d, u, mass, absjac = _case(4, 4, 6, 8)
+    _noalloc(d, u, mass, absjac)          # first call: the scratch address lookup
+    lib = _native.load()
+    out = torch.full((1,), -1.0, dtype=torch.float64, device=d.device)
+    graph = torch.cuda.CUDAGraph()
+    status = []
+    with torch.cuda.graph(graph):
+        status.append(lib.hb_norm_noalloc(
+            d.K, d.Np, u.shape[0], 0, mass.data_ptr(), absjac.data_ptr(), u.data_ptr(),
+            out.data_ptr(), torch.cuda.current_stream(d.device).cuda_stream))
+    assert status == [_native.HB_OK]
+    for scale in (1.0, 0.5):
+        u.mul_(scale)
+        out.fill_(-1.0)
+        graph.replay()
+        torch.cuda.synchronize(d.device)
+        assert float(out.item()) == d.norm(u)
 
 
 def test_noalloc_norm_rejects_oversized_mesh(cuda_device):
