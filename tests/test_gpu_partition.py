@@ -16,6 +16,12 @@ def _setup(kind, nparts, precision):
     if kind == "maxwell":
         d = hb.Discretization(hb.make_box_tet_mesh(n=(3, 3, 3), jitter=0.03, seed=5), order=3)
         model = hb.MaxwellOperator(1.0, 1.0, flux_type=1)
+    elif kind == "maxwell_incident":
+        def tagger(fvi, el, fn, allv):
+            return ["inc"] if allv[list(fvi)].mean(0)[0] > 0.99 else ["pec"]
+        m = hb.make_box_tet_mesh(n=(3, 3, 3), jitter=0.03, seed=5, boundary_tagger=tagger)
+        d = hb.Discretization(m, order=3)
+        model = hb.MaxwellOperator(1.0, 1.0, flux_type=0.5, pec_tag="pec", incident_tag="inc")
     else:
         m = hb.make_regular_rect_mesh((-1, -1), (1, 1), (9, 9), jitter=0.02, seed=4)
         d = hb.Discretization(m, order=4)
@@ -27,7 +33,7 @@ def _setup(kind, nparts, precision):
 
 
 @pytest.mark.parametrize("by_ranges", [False, True])
-@pytest.mark.parametrize("kind", ["maxwell", "varwave"])
+@pytest.mark.parametrize("kind", ["maxwell", "maxwell_incident", "varwave"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32-simt", "fp16x3", "bf16x3"])
 def test_partitioned_rhs_equals_global(cuda_device, kind, precision, by_ranges):
     import torch

@@ -190,3 +190,25 @@ def test_overlapped_stage_order():
     stub.exchange = lambda send, halo: log.append("blocking")
     PartitionedOperator._run(stub, launch, None, exchanged=False, by_ranges=False)
     assert log == ["exchange", (0, 10)]
+
+
+def test_incident_walls_partition():
+    """A Maxwell operator with incident walls partitions with its incident
+    faces kept as boundary faces of that kind; incident data given per call
+    (a given boundary vector) is refused, like every given boundary data."""
+    from hedge_b200 import optemplate as ot
+    from hedge_b200.models import BC_INCIDENT
+
+    def tagger(fvi, el, fn, allv):
+        return ["inc"] if allv[list(fvi)].mean(0)[0] > 0.99 else ["pec"]
+    d = hb.Discretization(hb.make_box_tet_mesh(n=(2, 2, 2), jitter=0.03, seed=2,
+                                               boundary_tagger=tagger), order=2)
+    op = hb.MaxwellOperator(1.0, 1.0, flux_type=0.5, pec_tag="pec", incident_tag="inc")
+    plan = PartitionPlan(d, op.op_template(), 3)
+    n_inc = sum(int(np.count_nonzero((p.conn[..., 0] < 0) & (p.conn[..., 1] == BC_INCIDENT)))
+                for p in plan.parts)
+    assert n_inc == len(d.mesh.boundary_faces("inc")) > 0
+    data = hb.MaxwellOperator(1.0, 1.0, flux_type=0.5, pec_tag="pec", incident_tag="inc",
+                              incident_bc=lambda o, e, h: ot.make_sym_vector("inc", 6))
+    with pytest.raises(NotImplementedError):
+        PartitionPlan(d, data.op_template(), 3)
