@@ -671,6 +671,13 @@ class CompiledOperator:
                         t.numel() != rows * len(self.discr) or t.device != self.discr.device:
                     raise ValueError("c / source: contiguous FP64 [%d * K*Np] on the device"
                                      % rows)
+        if self.var_material and s is not None and c is not None:
+            # the source rows hold -J (the template's source with the
+            # material at 1); the kernel adds them after dividing by
+            # epsilon, so they go in as -J / epsilon (em.py:192-214, 339-371)
+            n = len(self.discr)
+            s = (s.reshape(self._n_e, n) / c[:n]).contiguous()
+            self._src_over_eps = s       # alive until the launch is queued
         return (c.data_ptr() if c is not None else None,
                 s.data_ptr() if s is not None else None)
 

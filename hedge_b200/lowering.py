@@ -665,8 +665,10 @@ class _Maxwell(_Family):
 
 class _MaxwellVar(_Maxwell):
     """Maxwell with variable material: the flux argument's first two fields
-    are epsilon and mu (em.py:309-371)."""
-    source_outputs = ()
+    are epsilon and mu (em.py:309-371).  A source current J enters the E
+    rows as (curl H - J) / eps; with the material probed at 1 the source
+    probe reads -J."""
+    source_outputs = (0, 1, 2)
 
     def applies(self, dims, F, ncoeff):
         return dims == 3 and F == 6 and ncoeff == 2
@@ -685,12 +687,20 @@ class _MaxwellVar(_Maxwell):
                      bdry_flux_type=p.get("bdry_flux_type", p["flux_type"]),
                      pec_tag=t[BC_PEC], pmc_tag=t[BC_PMC], absorb_tag=t[BC_ABSORB],
                      incident_tag=t[BC_INCIDENT], incident_bc=self._incident(roles, bc))
+        ne = m.n_e
+        srcs = getattr(roles, "sources", None)
+        if srcs is not None and any(not ot.is_zero(x) for x in srcs[:ne]):
+            m.current = np.array([-1 * x if not ot.is_zero(x) else 0 for x in srcs[:ne]],
+                                 dtype=object)
+        if srcs is not None and any(not ot.is_zero(x) for x in srcs[ne:]):
+            return None
         return m, _comps(m.op_template(w=roles.state))
 
 
 class _MaxwellTMVar(_MaxwellVar):
     model = MODEL_MAXWELL_TM
     cls = TMMaxwellOperator
+    source_outputs = (0,)
 
     def applies(self, dims, F, ncoeff):
         return dims == 2 and F == 3 and ncoeff == 2
@@ -703,6 +713,7 @@ class _MaxwellTMVar(_MaxwellVar):
 class _MaxwellTEVar(_MaxwellVar):
     model = MODEL_MAXWELL_TE
     cls = TEMaxwellOperator
+    source_outputs = (0, 1)
 
     def applies(self, dims, F, ncoeff):
         return dims == 2 and F == 3 and ncoeff == 2

@@ -400,8 +400,7 @@ class MaxwellOperator(HyperbolicOperator):
     variable material, volume fields: given functions
     (TimeConstantGivenFunction, ``volume_interpolant(t, discr)``), callables
     f(x) of the node coordinates, volume vectors [K*Np], or template fields.
-    Variable material runs on the CUDA-core kernels (fp64, fp32) without a
-    source current."""
+    Variable material runs on the CUDA-core kernels (fp64, fp32)."""
 
     _default_dimensions = 3
     model_id = MODEL_MAXWELL
@@ -443,8 +442,6 @@ class MaxwellOperator(HyperbolicOperator):
         if self.fixed_material:
             self.epsilon, self.mu = float(epsilon), float(mu)
         else:
-            if not (np.isscalar(current) and current == 0):
-                raise NotImplementedError("variable material with a source current")
             self.epsilon, self.mu = epsilon, mu
         self.flux_type = flux_type
         self.bdry_flux_type = flux_type if bdry_flux_type is None else bdry_flux_type

@@ -2,7 +2,8 @@
 kernels): the bound model's RHS against the CPU template executor on the
 model's own template (FP64 <= 1e-12, FP32 <= 1e-5 on FP32-rounded inputs),
 for smooth eps(x), mu(x) in 3D, TM and TE with PEC, PMC and absorbing walls
-and every flux type; constant fields against the fixed-material kernel; 20
+and every flux type; with a source current (given with the model and by
+name per call); constant fields against the fixed-material kernel; 20
 fused LSRK4 steps against the executor's; the material passed by name to a
 compiled template; the split precisions and the adjoint refused."""
 import numpy as np
@@ -114,3 +115,36 @@ def test_material_by_name_and_refusals(cuda_device):
     lam = torch.ones((6, len(d)), dtype=torch.float64, device=d.device)
     with pytest.raises(Exception):
         c2.adjoint(lam)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("kind", ["3d", "tm", "te"])
+def test_variable_material_current(cuda_device, kind, precision):
+    """(curl H - J + lift) / eps(x) on the E rows: the current given with
+    the model (bound RHS) and by name per call (compiled template), against
+    the template executor."""
+    from optemplate_exec import TemplateExecutor
+    d, cls, F = _discr(kind)
+    eps, mu = _material(d)
+    ne = {"3d": 3, "tm": 1, "te": 2}[kind]
+    x = d.nodes
+    J = np.stack([np.cos((k + 1) * x[:, 0] - 0.3 * x[:, 1]) for k in range(ne)])
+    op = cls(eps, mu, flux_type=0.5, bdry_flux_type="lf", pec_tag="pec", pmc_tag="pmc",
+             absorb_tag="abs", current=J)
+    q = _fields(d, F, 11)
+    if precision == "fp32":
+        q = q.astype(np.float32).astype(np.float64)
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    ex = TemplateExecutor(d)
+    tpl = op.op_template()
+    ref = np.asarray(ex(tpl, w=q, epsilon=eps, mu=mu, current=J), dtype=np.float64)
+    dp = hb.Discretization(d.mesh, order=d.order, precision=precision)
+    rhs = dp.compile(tpl).bind_model(op)
+    got = rhs(0.0, q).double().cpu().numpy()
+    rhs.compiled.check()
+    assert rel_l2(got, ref) <= tol
+    ref2 = np.asarray(ex(tpl, w=q, epsilon=eps, mu=mu, current=-2 * J), dtype=np.float64)
+    comp = dp.compile(tpl)
+    got2 = comp(w=q, epsilon=eps, mu=mu, current=-2 * J).double().cpu().numpy()
+    comp.check()
+    assert rel_l2(got2, ref2) <= tol

@@ -87,7 +87,34 @@ def test_material_arguments():
         op.max_eigenvalue()
     with pytest.raises(RuntimeError):
         op.c
-    with pytest.raises(NotImplementedError):
-        hb.MaxwellOperator(np.ones(len(d)), 1.0, flux_type=1, current=1.0)
+    # a source current with variable material (em.py:192-214, 339-371)
+    hb.MaxwellOperator(np.ones(len(d)), 1.0, flux_type=1, current=1.0)
     fixed = hb.MaxwellOperator(2.0, 0.5, flux_type=1)
     assert fixed.fixed_material and abs(fixed.c - 1.0) <= 1e-15
+
+
+@pytest.mark.parametrize("kind", ["3d", "tm", "te"])
+def test_variable_material_with_current(kind):
+    """A source current with variable material: the template's E rows read
+    (curl H - J + lift) / eps; with constant fields it equals the fixed
+    material's template with the same current, and the lowering names the
+    current as the E rows' source field."""
+    from optemplate_exec import TemplateExecutor
+    d, cls, F = _discr(kind)
+    ne = {"3d": 3, "tm": 1, "te": 2}[kind]
+    rng = np.random.default_rng(7)
+    J = rng.standard_normal((ne, len(d)))
+    kw = dict(flux_type=0.5, pec_tag="pec", pmc_tag="pmc", absorb_tag="abs", current=J)
+    w = rng.standard_normal((F, len(d)))
+    ex = TemplateExecutor(d)
+    fixed = np.asarray(ex(cls(1.3, 0.7, **kw).op_template(), w=w, current=J), dtype=np.float64)
+    var = cls(np.full(len(d), 1.3), np.full(len(d), 0.7), **kw)
+    got = np.asarray(ex(var.op_template(), w=w, current=J, epsilon=np.full(len(d), 1.3),
+                        mu=np.full(len(d), 0.7)), dtype=np.float64)
+    assert rel_l2(got, fixed) <= 1e-13
+    desc = lower(var.op_template(), d.dimensions, d.mesh)
+    assert desc.params.get("variable_material") is True
+    src = desc.fields["sources"]
+    assert [o for o, _, _, _ in src] == list(range(ne))
+    assert all(f == ("current", o) and abs(c + 1.0) <= 1e-9 and k == 0.0
+               for o, k, f, c in src)
