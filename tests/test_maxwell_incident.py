@@ -172,3 +172,15 @@ def test_incident_data_components_named_one_by_one():
     desc = lower(op.op_template(), d.dimensions, d.mesh)
     assert desc.params.get("incident_data") is True
     assert [n for n, _ in desc.fields["given_keys"]] == ["ez_inc", "b_hx", "a_hy"]
+
+
+def test_incident_data_of_the_state_is_refused():
+    """Incident data that is an expression of the state (not a given
+    boundary field) matches no kernel boundary condition."""
+    from hedge_b200 import optemplate as ot
+    d, cls, F = _discr("3d")
+    op = cls(1.0, 1.0, flux_type=0.5, pec_tag="pec", pmc_tag="pmc", incident_tag="abs",
+             incident_bc=lambda o, e, h: np.array(
+                 [ot.BoundarizeOperator("abs")(x) for x in list(e) + list(h)], dtype=object))
+    with pytest.raises(NotImplementedError):
+        lower(op.op_template(), d.dimensions, d.mesh)
