@@ -73,6 +73,10 @@ class OpTemplate:
 
     @property
     def n_flux_args(self):
+        """Fields of the flux argument: the state, plus c (variable-velocity
+        wave) or epsilon and mu (Maxwell with variable material)."""
+        if self.params.get("variable_material"):
+            return self.n_fields + 2
         return self.n_fields + (1 if self.model == MODEL_VARWAVE else 0)
 
 

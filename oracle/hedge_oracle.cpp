@@ -184,22 +184,32 @@ static void model_flux(const or_flux_params& p, const double* ui,
     }
     case OR_MAXWELL_TM: case OR_MAXWELL_TE: {
       // em.py:485-515: the 3D flux of the embedded fields (the others zero),
-      // normal with a zero z component
+      // normal with a zero z component; variable material (5 arguments):
+      // epsilon and mu lead the argument vector
       const int slot_tm[3] = {2, 3, 4}, slot_te[3] = {0, 1, 5};
       const int* slot = p.model == OR_MAXWELL_TM ? slot_tm : slot_te;
-      double ui6[6] = {0, 0, 0, 0, 0, 0}, ue6[6] = {0, 0, 0, 0, 0, 0}, f6[6];
-      for (int k = 0; k < 3; ++k) { ui6[slot[k]] = ui[k]; ue6[slot[k]] = ue[k]; }
+      const int off = p.n_args == 5 ? 2 : 0;
+      double ui8[8] = {0, 0, 0, 0, 0, 0, 0, 0}, ue8[8] = {0, 0, 0, 0, 0, 0, 0, 0}, f6[6];
+      for (int k = 0; k < off; ++k) { ui8[k] = ui[k]; ue8[k] = ue[k]; }
+      for (int k = 0; k < 3; ++k) {
+        ui8[off + slot[k]] = ui[off + k];
+        ue8[off + slot[k]] = ue[off + k];
+      }
       const double n3[3] = {n[0], n[1], 0.0};
       or_flux_params p3 = p;
       p3.model = OR_MAXWELL;
       p3.dim = 3;
-      model_flux(p3, ui6, ue6, n3, f6);
+      p3.n_args = 6 + off;
+      model_flux(p3, ui8, ue8, n3, f6);
       for (int k = 0; k < 3; ++k) f[k] = f6[slot[k]];
       break;
     }
     case OR_MAXWELL: {
-      const double* ei = ui; const double* hi = ui + 3;
-      const double* ee = ue; const double* he = ue + 3;
+      // variable material (em.py:118-190 with flux_w = (epsilon, mu, w)):
+      // 8 arguments, the impedances from each side's epsilon and mu
+      const int off = p.n_args == 8 ? 2 : 0;
+      const double* ei = ui + off; const double* hi = ui + off + 3;
+      const double* ee = ue + off; const double* he = ue + off + 3;
       double de[3], dh[3];
       for (int k = 0; k < 3; ++k) { de[k] = ei[k] - ee[k]; dh[k] = hi[k] - he[k]; }
       auto cross = [](const double* a, const double* b, double* r) {
@@ -214,16 +224,18 @@ static void model_flux(const or_flux_params& p, const double* ui,
         cross(n, de, t);
         for (int k = 0; k < 3; ++k) f[3 + k] = 0.5 * t[k];
       } else {
-        const double Z = std::sqrt(p.mu / p.eps), Y = 1.0 / Z;
+        const double Zi = off ? std::sqrt(ui[1] / ui[0]) : std::sqrt(p.mu / p.eps);
+        const double Ze = off ? std::sqrt(ue[1] / ue[0]) : Zi;
+        const double Yi = 1.0 / Zi, Ye = 1.0 / Ze;
         double nde[3], ndh[3], a[3], t[3];
         cross(n, de, nde);
         cross(n, dh, ndh);
-        for (int k = 0; k < 3; ++k) a[k] = Z * dh[k] - p.alpha * nde[k];
+        for (int k = 0; k < 3; ++k) a[k] = Ze * dh[k] - p.alpha * nde[k];
         cross(n, a, t);
-        for (int k = 0; k < 3; ++k) f[k] = -1.0 / (Z + Z) * t[k];
-        for (int k = 0; k < 3; ++k) a[k] = Y * de[k] + p.alpha * ndh[k];
+        for (int k = 0; k < 3; ++k) f[k] = -1.0 / (Zi + Ze) * t[k];
+        for (int k = 0; k < 3; ++k) a[k] = Ye * de[k] + p.alpha * ndh[k];
         cross(n, a, t);
-        for (int k = 0; k < 3; ++k) f[3 + k] = 1.0 / (Y + Y) * t[k];
+        for (int k = 0; k < 3; ++k) f[3 + k] = 1.0 / (Yi + Ye) * t[k];
       }
       break;
     }

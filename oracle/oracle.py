@@ -117,7 +117,9 @@ class OracleRHS:
     discr: a hedge_b200 Discretization (only its host-side set-up arrays are
     read: reference matrices, geometry, face groups, boundaries)."""
 
-    def __init__(self, discr, optemplate, c_field=None, source=None):
+    def __init__(self, discr, optemplate, c_field=None, source=None, material=None):
+        """material: (epsilon, mu) volume vectors of a Maxwell operator with
+        variable material (default: the model's own values)."""
         from hedge_b200.lowering import as_descriptor
         self.discr = discr
         self.ot = ot = as_descriptor(optemplate, discr.dimensions, discr.mesh)
@@ -152,6 +154,14 @@ class OracleRHS:
             j = ot.operator.current_value()
             if not (np.isscalar(j) and j == 0):
                 self.source = j
+        self.material = None
+        if ot.model in _MAXWELLS and p.get("variable_material"):
+            if material is None and hasattr(ot.operator, "material_values"):
+                material = ot.operator.material_values(discr)
+            if material is None or any(x is None for x in material):
+                raise ValueError("variable material: pass material=(epsilon, mu)")
+            self.material = np.ascontiguousarray(
+                np.stack([np.asarray(x, dtype=np.float64).reshape(-1) for x in material]))
         self.params = self._params(bdry=False)
         self.bparams = self._params(bdry=True)
         self.bdry = []
@@ -198,6 +208,9 @@ class OracleRHS:
     def flux_args(self, fields):
         if self.ot.model == OR_VARWAVE:
             return np.ascontiguousarray(np.vstack([self.c_field[None], fields]))
+        if self.material is not None:
+            # em.py:309-371: flux_w = (epsilon, mu, w)
+            return np.ascontiguousarray(np.vstack([self.material, fields]))
         return np.ascontiguousarray(fields)
 
     def bc_values(self, kind, args, b, normals, bc_in):
@@ -227,8 +240,13 @@ class OracleRHS:
                 out[C0 + 1:] = 0.5 * normals.T * (nv - sgn * u)
             return out
         if m in _MAXWELLS:
-            # em.py:226-307 on the six components (2D systems embedded, n_z = 0)
+            # em.py:226-307 on the six components (2D systems embedded, n_z =
+            # 0); variable material: the boundary vector is (B(eps), B(mu),
+            # bc) and the absorbing impedance is the local one
             slots, _ = _SLOTS[m]
+            mat = ab[:2] if self.material is not None else None
+            if mat is not None:
+                ab = ab[2:]
             full = np.zeros((6, ab.shape[1]))
             full[slots] = ab
             e, h = full[:3], full[3:]
@@ -240,7 +258,7 @@ class OracleRHS:
                 out = np.vstack([e, -h])
             elif kind == BC_ABSORB:
                 p = self.ot.params
-                Z = np.sqrt(p["mu"] / p["eps"])
+                Z = np.sqrt(p["mu"] / p["eps"]) if mat is None else np.sqrt(mat[1] / mat[0])
                 ne, nh = np.cross(nrm, e.T).T, np.cross(nrm, h.T).T
                 nne, nnh = np.cross(nrm, ne.T).T, np.cross(nrm, nh.T).T
                 out = np.vstack([e + 0.5 * (nne - Z * nh), h + 0.5 * (nnh + ne / Z)])
@@ -248,11 +266,13 @@ class OracleRHS:
                 # -(incident data) (em.py:289-307): the given [F][n] values,
                 # or the default zero data
                 if bc_in is not None:
-                    return -np.asarray(bc_in, dtype=np.float64).reshape(len(slots), -1)
-                out = np.zeros_like(full)
+                    out = np.zeros_like(full)
+                    out[slots] = -np.asarray(bc_in, dtype=np.float64).reshape(len(slots), -1)
+                else:
+                    out = np.zeros_like(full)
             else:
                 raise ValueError("unsupported boundary kind %d" % kind)
-            return out[slots]
+            return out[slots] if mat is None else np.vstack([mat, out[slots]])
         raise ValueError("unsupported boundary kind %d" % kind)
 
     def flux_volume(self, fields, bc_in=None):
@@ -325,7 +345,10 @@ class OracleRHS:
                 j = np.asarray(self.source, dtype=np.float64)
                 vol[:ne] -= j.reshape(ne, -1) if j.size >= ne * self.N else \
                     np.broadcast_to(j.reshape(-1, 1), (ne, self.N))
-            div = np.array([p["eps"]] * ne + [p["mu"]] * (len(slots) - ne))[:, None]
+            if self.material is not None:
+                div = np.vstack([self.material[0]] * ne + [self.material[1]] * (len(slots) - ne))
+            else:
+                div = np.array([p["eps"]] * ne + [p["mu"]] * (len(slots) - ne))[:, None]
             return (vol + lifted) / div
         raise ValueError("unknown model")
 

@@ -118,3 +118,31 @@ def test_variable_material_with_current(kind):
     assert [o for o, _, _, _ in src] == list(range(ne))
     assert all(f == ("current", o) and abs(c + 1.0) <= 1e-9 and k == 0.0
                for o, k, f, c in src)
+
+
+@pytest.mark.parametrize("ft,bft", FLUXES)
+@pytest.mark.parametrize("kind", ["3d", "tm", "te"])
+def test_oracle_variable_material_equals_executor(kind, ft, bft):
+    """The jit-loop oracle with variable material (flux argument
+    (epsilon, mu, w), impedances from each side, the local absorbing
+    impedance, the per-node divisor) against the template executor, with
+    PEC, PMC and absorbing walls, and with incident walls and a current."""
+    from oracle import OracleRHS
+    from optemplate_exec import TemplateExecutor
+    d, cls, F = _discr(kind)
+    x = d.nodes
+    eps = 1.0 + 0.4 * np.sin(1.7 * x[:, 0] + 0.3) * np.cos(0.9 * x[:, 1])
+    mu = 1.2 + 0.3 * np.cos(1.1 * x[:, 1] - 0.2 * x[:, 0])
+    w = np.random.default_rng(8).standard_normal((F, len(d)))
+    ex = TemplateExecutor(d)
+    op = cls(eps, mu, flux_type=ft, bdry_flux_type=bft, pec_tag="pec", pmc_tag="pmc",
+             absorb_tag="abs")
+    ref = np.asarray(ex(op.op_template(), w=w, epsilon=eps, mu=mu), dtype=np.float64)
+    assert rel_l2(OracleRHS(d, op.op_template())(w), ref) <= 1e-12
+    ne = {"3d": 3, "tm": 1, "te": 2}[kind]
+    J = np.cos(x[:, :1].T * np.arange(1, ne + 1)[:, None])
+    op2 = cls(eps, mu, flux_type=ft, bdry_flux_type=bft, pec_tag="pec", pmc_tag="pmc",
+              incident_tag="abs", current=J)
+    ref2 = np.asarray(ex(op2.op_template(), w=w, epsilon=eps, mu=mu, current=J),
+                      dtype=np.float64)
+    assert rel_l2(OracleRHS(d, op2.op_template())(w), ref2) <= 1e-12
