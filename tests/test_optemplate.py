@@ -525,3 +525,29 @@ def test_maxwell_2d_templates_lower_and_match_oracle(kind):
     got = TemplateExecutor(d)(op.op_template(), w=q, current=J)
     ref = OracleRHS(d, op.op_template())(q)
     assert rel_l2(got, ref) <= 1e-12
+
+
+def test_maxwell_two_tags_of_one_kind():
+    """A hand-written Maxwell template with PEC walls on two tags and an
+    absorbing one on a third (a combination no model constructor makes)
+    lowers with each tag's kind, and the oracle on the lowered descriptor
+    agrees with the executor on the tree."""
+    from oracle import OracleRHS
+    from optemplate_exec import TemplateExecutor
+
+    def tagger(fvi, el, fn, allv):
+        c = allv[list(fvi)].mean(0)
+        return ["a"] if c[0] > 0.99 else (["b"] if c[0] < -0.99 else ["c"])
+    d = hb.Discretization(box(2, tagger=tagger), order=2)
+    w = ot.make_sym_vector("w", 6)
+    B = ot.BoundarizeOperator
+    op = hb.MaxwellOperator(1.0, 1.0, flux_type=0.5, pec_tag="a", absorb_tag="b")
+    pec_c = ot.join_fields(*[-1 * (B("c") * w[k]) for k in range(3)],
+                           *[B("c") * w[k] for k in range(3, 6)])
+    tpl = op.op_template(w) + ot.InverseMassOperator()(
+        ot.get_flux_operator(op.flux(0.5))(ot.BoundaryPair(w, pec_c, "c")))
+    desc = lower(tpl, 3, d.mesh)
+    assert dict(desc.bcs) == {"a": BC_PEC, "b": BC_ABSORB, "c": BC_PEC}
+    q = np.random.default_rng(1).standard_normal((6, len(d)))
+    ref = np.asarray(TemplateExecutor(d)(tpl, w=q), dtype=np.float64)
+    assert rel_l2(OracleRHS(d, desc)(q), ref) <= 1e-12
