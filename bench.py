@@ -694,10 +694,7 @@ def run_varadv(args):
             "unit": "DOF-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOADS["varadv2d"]["label"] % (d.K, d.order),
-                       "K": d.K, "order": d.order, "Np": d.Np, "quad_degree": 3 * d.order,
-                       "l2": "working set of a stage (q_in, q_out, res, v) 5 x %.1f MB > 126 "
-                             "MB L2, no flush" % (dofs * 8 / 1e6)},
+            "config": varadv_config(d.K, d.order, d.Np),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches, "clocks": clk.summary(),
             "launch_config": comp.launch_info()}
@@ -729,13 +726,62 @@ def varadv_cpu_baseline(order):
                       "executor (numpy), best of 2" % d.K}
 
 
+def varadv_config(K, order, Np):
+    """The quadrature workload's config as both arms report it."""
+    return {"workload": WORKLOADS["varadv2d"]["label"] % (K, order), "K": K, "order": order,
+            "Np": Np, "quad_degree": 3 * order,
+            "l2": "working set of a stage (q_in, q_out, res, v) 5 x %.1f MB > 126 "
+                  "MB L2, no flush" % (K * Np * 8 / 1e6)}
+
+
+def run_varadv_reference(args):
+    """The reference arm of the quadrature workload: the template executor
+    (oracle/optemplate_exec.py, the reference's quadrature integrals with
+    numpy; no other CPU implementation of this operator exists here) on a
+    bounded sample, one RHS of the same operator on a 24 x 24 mesh per step,
+    on rank 0 only."""
+    if int(os.environ.get("RANK", 0)) != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from optemplate_exec import TemplateExecutor
+    from hedge_b200 import workloads
+    from hedge_b200.mesh import TAG_ALL, make_regular_rect_mesh
+    n = args.n if args.n != 20 else WORKLOADS["varadv2d"]["n"]
+    K_full = len(make_regular_rect_mesh((-1, -1), (1, 1), (n, n)).elements)
+    d, op, u0 = workloads.varadv_problem(24, args.order)
+    ex = TemplateExecutor(d)
+    tpl = op.op_template()
+    env = {"u": u0, "v": op.advec_v.f(d.nodes),
+           "bc_u": op.bc_u_f.boundary_interpolant(0.0, d, TAG_ALL)}
+    for _ in range(args.warmup):
+        ex(tpl, **env)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ex(tpl, **env)
+    el = time.perf_counter() - t0
+    v = d.K * d.Np * args.steps / el
+    sample = ("one RHS of the operator on a K=%d mesh (24 x 24 squares) per step, template "
+              "executor (numpy, the reference's quadrature integrals), one thread" % d.K)
+    line = {"impl": "reference", "metric": WORKLOADS["varadv2d"]["metric"], "value": v,
+            "unit": "DOF-updates/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / max(args.steps, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": varadv_config(K_full, args.order, d.Np),
+            "cpu_baseline": {"value": v, "unit": "DOF-updates/s", "cores": 1,
+                             "cpu_model": cpu_model(), "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.order is None:
         args.order = WORKLOADS[args.workload]["order"]
     if args.workload == "varadv2d":
         if args.impl == "reference":
-            print(json.dumps({"impl": "reference", "value": varadv_cpu_baseline(args.order)}))
+            run_varadv_reference(args)
             return
         run_varadv(args)
     elif args.impl == "reference":
